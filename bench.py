@@ -1,0 +1,323 @@
+"""Benchmark: cell-updates/s of the structured SSP-RK2 step on B200.
+
+Workload (per GPU): the 4096 x 4096 wet/dry configuration - dx = dy = 5 m, a
+bed of 32 seeded Gaussians (amplitudes U[-4, 12] m, widths U[50, 500] m), a
+0.5 m / 200 m hump at the centre, Manning n = 0.025, walls - advanced in
+FP64 through librakali.so.  One "step" is one full SSP-RK2 step of the grid.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 runs N independent replicas (one per rank, launched by torchrun): the
+step does not exchange data between instances, so scaling is weak and no
+collective sits on the data path; the ranks only meet for the barrier and
+the max-over-ranks of the timed region.
+
+Timing: W untimed steps, then K steps bracketed by CUDA events recorded on
+the simulation's own stream (rkb_time_steps), max over ranks.  Each field is
+16.8 M cells x 8 B = 134 MB, so every step streams more than L2 holds.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_CELLS_SIDE = 4096
+METRIC = "cell-updates/s on 1 B200: FP64 plain vs FP32, batched, fwd+adjoint, at stated err"
+# algorithmic bytes per cell-update of the two fused stage kernels (FP64):
+# stage 1 reads h, hu, hv, b and writes h*, hu*, hv* (7 words); stage 2 reads
+# h*, hu*, hv*, b, h^n, hu^n, hv^n and writes h^{n+1}, hu^{n+1}, hv^{n+1} (10).
+BYTES_STAGE1 = 7 * 8
+BYTES_STAGE2 = 10 * 8
+BYTES_PER_CELL_UPDATE = BYTES_STAGE1 + BYTES_STAGE2
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.is_file():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.gpu)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() in ("active", "1", "yes"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def visible_gpu_index(local_rank: int) -> int:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        if local_rank < len(ids) and ids[local_rank].isdigit():
+            return int(ids[local_rank])
+    return local_rank
+
+
+def traffic_per_launch(n_cells: int):
+    """DRAM bytes per stage-2 launch from the committed ncu summary, scaled by cells."""
+    p = ROOT / "profiles" / "stage2_fp64_ncu.json"
+    if not p.is_file():
+        return None
+    d = json.loads(p.read_text())
+    return d["dram_bytes_per_launch"] * n_cells / d["cells"]
+
+
+def cpu_baseline(threads: int, side: int = 1024, steps: int = 2, seed: int = 2024):
+    """Oracle (OpenMP) on a side x side window of the workload family."""
+    from oracle import oracle as orc
+    from rakali_b200 import workloads as wl
+    used = orc.set_threads(threads)
+    b, h = wl.config2(n=side, seed=seed)
+    cfg = dict(nx=side, ny=side, **wl.CONFIG2_KW)
+    o = orc.OracleSim.from_config(cfg, bathymetry=b, initial_h=h)
+    o.step(1)  # warm-up
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    return {"value": side * side * steps / dt, "unit": "cell-updates/s", "cores": used,
+            "kind": "port",
+            "sample": f"{steps} SSP-RK2 steps of a {side}x{side} window of the 4096^2 "
+                      f"configuration (same bed family, dx = 5 m, n = 0.025), FP64, "
+                      f"{used} OpenMP threads"}
+
+
+def run_reference(args, rank, world):
+    """CPU implementation of the path (the oracle port), all host threads."""
+    if rank != 0:
+        return 0
+    from oracle import oracle as orc
+    from rakali_b200 import workloads as wl
+    threads = os.cpu_count() or 1
+    used = orc.set_threads(threads)
+    side = 1024
+    b, h = wl.config2(n=side, seed=2024)
+    cfg = dict(nx=side, ny=side, **wl.CONFIG2_KW)
+    o = orc.OracleSim.from_config(cfg, bathymetry=b, initial_h=h)
+    o.step(args.warmup)
+    t0 = time.perf_counter()
+    o.step(args.steps)
+    elapsed = time.perf_counter() - t0
+    value = side * side * args.steps / elapsed
+    sample = (f"each step: one SSP-RK2 step of a {side}x{side} window of the 4096^2 "
+              f"configuration (same bed family), FP64, {used} OpenMP threads")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-updates/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"structured SSP-RK2 wet/dry step, {side}x{side} window of "
+                               "the 4096x4096 configuration (CPU oracle port)",
+                   "cells": side * side, "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": used,
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(args, rank, world, local_rank, dist):
+    import ctypes
+
+    import torch
+
+    from rakali_b200 import Rakali
+    from rakali_b200 import workloads as wl
+
+    torch.cuda.set_device(local_rank)
+    n = N_CELLS_SIDE
+    b, h = wl.config2(n=n, seed=2024 + rank)
+    sim = Rakali(defer_init=True, nx=n, ny=n, **wl.CONFIG2_KW)
+    sim.set_bathymetry(b)
+    sim.set_initial_h(h)
+    sim.finalize()
+    lib = sim._lib
+    cells = n * n
+
+    def device_steps(k):
+        ms = ctypes.c_double()
+        rc = lib.rkb_time_steps(sim._handle, int(k), ctypes.byref(ms))
+        if rc != 0:
+            raise RuntimeError(f"rkb_time_steps failed rc={rc}")
+        return ms.value
+
+    device_steps(max(args.warmup, 3))
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(visible_gpu_index(local_rank)) as clk:
+        ms = device_steps(args.steps)
+    torch.cuda.synchronize()
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = world * cells * args.steps / (ms * 1e-3)
+
+    # per-kernel device times (events between launches, same stream)
+    prof = (ctypes.c_double * 5)()
+    rc = lib.rkb_profile_steps(sim._handle, 5, prof)
+    if rc != 0:
+        raise RuntimeError("rkb_profile_steps failed")
+    t_bc1, t_s1, t_bc2, t_s2, launches = prof[0], prof[1], prof[2], prof[3], int(prof[4])
+
+    # end to end through the public API with host buffers: upload the state,
+    # K steps, read the fields back (D2H) - wall clock around all of it.
+    state = [np.asfortranarray(a) for a in (sim.h_phys.copy(), sim.hu_phys.copy(),
+                                            sim.hv_phys.copy())]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sim.set_h(state[0])
+    sim.set_hu(state[1])
+    sim.set_hv(state[2])
+    sim.step(args.steps)
+    h_back = sim.h_phys
+    _ = float(h_back[0, 0])
+    e2e_s = time.perf_counter() - t0
+    nxt = n + 2 * sim.nghost
+    h2d = 3 * 8 * cells  # interior h, hu, hv
+    d2h = 7 * 8 * nxt * nxt  # h, hu, hv, b, h0, hu0, hv0 with ghosts
+    e2e = {"value": world * cells * args.steps / e2e_s, "unit": "cell-updates/s",
+           "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps}
+    if dist is not None:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e["value"] = world * cells * args.steps / float(t.item())
+
+    if rank != 0:
+        sim.close()
+        return 0
+    hbm, peak_kind = peaks()
+    achieved = BYTES_STAGE2 * cells / (t_s2 * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": traffic_per_launch(cells),
+                "kernel": "k_stage<stage 2> (fused flux + update + RK2 average)",
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                if peak_kind == "measured" else "fallback 6650 GB/s",
+                "stage_ms": {"bc_stage1": t_bc1, "stage1": t_s1, "bc_stage2": t_bc2,
+                             "stage2": t_s2},
+                "step_frac_of_hbm": BYTES_PER_CELL_UPDATE * value / world / 1e9 / hbm}
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "structured SSP-RK2 wet/dry step, 4096x4096 per GPU, dx=5 m, "
+                               "32-Gaussian bed, 0.5 m hump, Manning 0.025, walls, FP64 "
+                               "(parity build)",
+                   "cells_per_gpu": cells, "tile": "32x8", "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (3 x 134 MB per buffer)"},
+        "e2e": e2e,
+        "gpu_launches": launches * args.steps,
+        "roofline": roofline,
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
+    print(json.dumps(line), flush=True)
+    sim.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1 and args.impl == "b200":
+        import datetime
+
+        import torch
+        import torch.distributed as td
+        torch.cuda.set_device(local_rank)
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = td
+    try:
+        if args.impl == "reference":
+            return run_reference(args, rank, world)
+        return run_b200(args, rank, world, local_rank, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

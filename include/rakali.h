@@ -1,0 +1,172 @@
+/*
+ * librakali.so (B200 build): C ABI of the structured 2D shallow-water step.
+ *
+ * Part 1 is the drop-in boundary: every symbol the reference's Python
+ * wrapper binds at import (python/rakali/_core.py:88-283), with the
+ * reference's signatures and return codes (src/api/rki_api.F90:157-1507).
+ * The unmodified `rakali` package loads this library through RAKALI_LIB.
+ *
+ * Return codes (src/api/rki_api.F90:22-27):
+ *     0  success
+ *    -1  not initialised / not finalised / device failure
+ *    -2  grid mismatch / already finalised / invalid namelist value
+ *    -3  mode not active (multilayer, restart, unsupported solver mode)
+ *  -100  invalid handle (null, destroyed or foreign pointer)
+ * Invalid configurations return an error code (the reference stops the
+ * process); rki_last_error() gives the message.
+ *
+ * Field pointers are host memory owned by the library, Fortran order
+ * (nx_total, ny_total) with ghost cells, valid until rki_destroy.
+ *
+ * Part 2 adds entry points with no counterpart in the reference: kernel-level
+ * calls on caller-owned device arrays (mirroring the structured kernels of
+ * src/core/coastal/kernels/structured/barotropic), device-resident views for
+ * zero-copy torch interop, and diagnostics.
+ */
+#ifndef RAKALI_B200_H
+#define RAKALI_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- Part 1: reference C ABI ------------------------------------------ */
+
+/* rki_api.F90:157-167 */
+int rki_working_precision(void);
+
+/* rki_api.F90:169-217; a missing file keeps the defaults, as the reference. */
+int rki_create(const char *filename, int len, void **handle);
+/* rki_api.F90:219-259 */
+int rki_finalize(void *handle);
+/* rki_api.F90:261-272 */
+int rki_create_from_namelist(const char *filename, int len, void **handle);
+/* rki_api.F90:274-313 */
+int rki_create_from_string(const char *text, int len, void **handle);
+/* rki_api.F90:315-326 */
+int rki_create_from_namelist_string(const char *text, int len, void **handle);
+/* rki_api.F90:328-356 (nulls *handle; idempotent) */
+void rki_destroy(void **handle);
+
+/* rki_api.F90:358-383: n steps, each capped at t_end - t */
+int rki_step(void *handle, int n_steps);
+/* rki_api.F90:385-410: steps while t < target - 1e-10, last one capped */
+int rki_advance(void *handle, double target_time);
+
+/* rki_api.F90:412-498 */
+double rki_get_time(void *handle);
+double rki_get_dt(void *handle);
+void rki_get_grid_info(void *handle, int *nx, int *ny, int *nghost, double *dx, double *dy);
+int rki_get_step_count(void *handle);
+int rki_get_nz_ml(void *handle);
+
+/* rki_api.F90:502-698: zero-copy host views, (nx_total, ny_total) F-order */
+int rki_get_h_ptr(void *handle, void **ptr, int *nx_total, int *ny_total);
+int rki_get_hu_ptr(void *handle, void **ptr, int *nx_total, int *ny_total);
+int rki_get_hv_ptr(void *handle, void **ptr, int *nx_total, int *ny_total);
+int rki_get_b_ptr(void *handle, void **ptr, int *nx_total, int *ny_total);
+int rki_get_h0_ptr(void *handle, void **ptr, int *nx_total, int *ny_total);
+int rki_get_hu0_ptr(void *handle, void **ptr, int *nx_total, int *ny_total);
+int rki_get_hv0_ptr(void *handle, void **ptr, int *nx_total, int *ny_total);
+
+/* rki_api.F90:702-834: multilayer fields (return -1: multilayer not active) */
+int rki_get_h_layer_ptr(void *handle, void **ptr, int *nx_total, int *ny_total, int *nz);
+int rki_get_hu_layer_ptr(void *handle, void **ptr, int *nx_total, int *ny_total, int *nz);
+int rki_get_hv_layer_ptr(void *handle, void **ptr, int *nx_total, int *ny_total, int *nz);
+int rki_get_salinity_ptr(void *handle, void **ptr, int *nx_total, int *ny_total, int *nz);
+int rki_get_temperature_ptr(void *handle, void **ptr, int *nx_total, int *ny_total, int *nz);
+
+/* rki_api.F90:836-890 (pre-finalize fields, interior (nx, ny) F-order) */
+int rki_set_bathymetry(void *handle, const double *b, int nx, int ny);
+int rki_set_initial_h(void *handle, const double *h, int nx, int ny);
+
+/* rki_api.F90:896-1036 (forcing; wind/pressure/precipitation activate it) */
+int rki_set_wind(void *handle, const double *wx, const double *wy, int nx, int ny);
+int rki_set_atm_pressure(void *handle, const double *p, int nx, int ny);
+int rki_set_precipitation(void *handle, const double *p, int nx, int ny);
+int rki_set_heat_flux(void *handle, const double *q, int nx, int ny);
+int rki_set_evap_minus_precip(void *handle, const double *ep, int nx, int ny);
+
+/* rki_api.F90:1040-1123 (mid-run state injection) */
+int rki_set_h(void *handle, const double *h, int nx, int ny);
+int rki_set_hu(void *handle, const double *hu, int nx, int ny);
+int rki_set_hv(void *handle, const double *hv, int nx, int ny);
+/* rki_api.F90:1125-1199 (multilayer tracers: -3 when not multilayer) */
+int rki_set_salinity(void *handle, const double *s, int nx, int ny, int nz);
+int rki_set_temperature(void *handle, const double *t, int nx, int ny, int nz);
+
+/* rki_api.F90:1205-1303 (boundary scalars) */
+int rki_set_inflow_velocity(void *handle, double v);
+int rki_set_inflow_salinity(void *handle, double s);
+int rki_set_inflow_temperature(void *handle, double t);
+int rki_set_discharge_flux(void *handle, double q);
+int rki_set_clamped_elevation(void *handle, double eta);
+double rki_get_clamped_elevation(void *handle);
+double rki_get_manning_n(void *handle);
+double rki_get_coriolis_f(void *handle);
+/* rki_api.F90:1335-1366 */
+int rki_set_tidal_constituents(void *handle, const double *amp, const double *phase,
+                               const double *omega, int n);
+
+/* rki_api.F90:1372-1403 */
+void rki_sync_host(void *handle);
+void rki_sync_from_device(void *handle);
+
+/* rki_api.F90:1409-1471: restart files (see DESIGN; returns -3) */
+int rki_save_restart(void *handle, const char *filename, int len);
+int rki_load_restart(void *handle, const char *filename, int len);
+
+/* rki_api.F90:1473-1507 */
+int rki_set_use_ppm_tracer(void *handle, int flag);
+int rki_set_use_hllc(void *handle, int flag);
+
+/* ---- Part 2: additions (no counterpart in the reference) ---------------- */
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *rki_last_error(void);
+
+/* Parse + validate a namelist without a GPU: 0, -2 or -3 as rki_create. */
+int rkb_validate_namelist(const char *text, int len, char *err, int err_len);
+
+/* Boundary volume budget: out[0] = mass_out, out[1] = mass_src
+ * (rki_solver.F90:507-657).  Returns 0 or an error code. */
+int rkb_get_mass_budget(void *handle, double *out);
+
+/* Device views of the current state for zero-copy torch interop: ptrs[0..3]
+ * = h, hu, hv, b (device, pitched), *pitch in elements.  Valid until the
+ * next step (the state ping-pongs between two buffers). */
+int rkb_get_device_fields(void *handle, void **ptrs, int *pitch);
+
+/* Tile shape of the fused stage kernel (0: 32x8, 1: 32x16, 2: 64x4, 3: 16x16). */
+int rkb_set_tile(void *handle, int tile);
+int rkb_get_tile(void *handle);
+
+/* Run n steps bracketed by CUDA events on the simulation's own stream;
+ * *ms = device time of the n steps (state already resident). */
+int rkb_time_steps(void *handle, int n, double *ms);
+/* Run n steps one launch at a time; out5[0..3] = mean ms per step of the
+ * stage-1 boundary fill, stage 1, stage-2 boundary fill, stage 2;
+ * out5[4] = kernel launches per step. */
+int rkb_profile_steps(void *handle, int n, double *out5);
+
+/*
+ * Kernel-level entry points on caller-owned DEVICE arrays, Fortran order
+ * with leading dimension `ld` (>= nx_total).  All run on the current
+ * device's legacy default stream and synchronise before returning.
+ */
+/* compute_flux_hll / compute_flux_hllc (rki_kernel_flux.F90:17-102):
+ * flux divergence and per-face HLL mass fluxes of every interior cell. */
+int rkb_compute_flux(int use_hllc, const double *h, const double *hu, const double *hv,
+                     const double *b, double *flux_h, double *flux_hu, double *flux_hv,
+                     double *mass_flux_x, double *mass_flux_y, int nx_total, int ny_total,
+                     int nghost, int ld, double dx, double dy);
+
+/* compute_timestep (rki_kernel_timestep.F90:16-74): *dt_out on the host. */
+int rkb_compute_timestep(const double *h, const double *hu, const double *hv, int nx_total,
+                         int ny_total, int nghost, int ld, double dx, double dy, double cfl,
+                         double *dt_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,519 @@
+"""``Rakali``: the structured-grid front end over the B200 ``librakali.so``.
+
+Same calls, argument meaning and error behaviour as the reference wrapper
+(python/rakali/_core.py:449-1860): keyword or namelist creation, one-shot or
+two-phase (``defer_init``) setup, ``step`` / ``advance`` (with callbacks),
+zero-copy Fortran-order field views (``h``, ``h_phys`` ...) that keep the
+simulation alive, state and forcing setters, and ``close`` / context-manager
+teardown.  Bad input raises a Python exception; the library never stops the
+process.
+
+Additions: ``device_fields()`` returns zero-copy torch CUDA views of the
+device-resident state, and ``mass_budget()`` the boundary/source volume
+accounting of the solver.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from pathlib import Path
+
+import numpy as np
+
+from . import _lib
+
+TIME_EPS = 1.0e-10  # the stop tolerance of rki_advance (rki_api.F90:401)
+
+# kwarg -> namelist group (python/rakali/_core.py:329-447).  The namelist key is
+# the kwarg itself.
+_GROUPS = {
+    "grid_nml": ("nx", "ny", "dx", "dy", "nghost"),
+    "time_nml": ("t_end", "cfl", "dt_max", "dt_fixed", "cfl_interval", "time_scheme"),
+    "physics_nml": ("manning_n", "dry_threshold", "wind_stress_x", "wind_stress_y",
+                    "coriolis_f", "use_hllc"),
+    "output_nml": ("output_to_file", "output_dir", "output_interval", "output_format",
+                   "restart_interval", "async_output", "async_buffer_slots", "bathymetry_file",
+                   "restart_file", "forcing_file", "forcing_x_origin", "forcing_y_origin",
+                   "gauge_file", "gauge_output_interval", "compress_output", "compress_level",
+                   "out_h_layer", "out_velocity", "out_salinity", "out_temperature",
+                   "out_density", "out_w"),
+    "boundary_nml": ("bc_west", "bc_east", "bc_south", "bc_north", "tidal_amplitude",
+                     "tidal_period", "n_tidal_constituents", "tidal_amp", "tidal_phase",
+                     "tidal_omega", "inflow_velocity", "inflow_salinity", "inflow_temperature",
+                     "discharge_flux", "clamped_elevation", "sponge_width", "sponge_strength",
+                     "sponge_h_ref", "nesting_file", "nesting_x_origin", "nesting_y_origin"),
+    "nonhydrostatic_nml": ("use_nonhydrostatic", "use_multilayer", "nz_layers", "nh_tolerance",
+                           "nh_max_iterations", "nh_preconditioner", "nh_solve_interval",
+                           "bpg_method", "ml_min_depth", "rho_0", "vmix_nu_max", "vmix_nu_bg",
+                           "vmix_ri_alpha", "hdiff_kappa", "smagorinsky_cs", "split_ratio",
+                           "split_averaging"),
+    "tracer_nml": ("initial_salinity", "S_ref", "beta_S", "S_min", "S_max", "kappa_S_bg",
+                   "initial_temperature", "T_ref", "alpha_T", "T_min", "T_max", "kappa_T_bg",
+                   "use_ppm_tracer"),
+    "initial_condition_nml": ("init_condition", "eta_initial", "h0", "hump_amplitude",
+                              "hump_sigma", "hump_x_offset", "hump_y_offset", "init_u_shear"),
+    "vcoord_nml": ("vcoord_type", "remap_method", "vcoord_depth_transition",
+                   "vcoord_blend_width", "zstar_h_surf_target", "zstar_stretching",
+                   "zstar_h_min", "zstar_n_surf"),
+    "logging_nml": ("log_level", "status_interval"),
+    "metadata_nml": ("reference_time", "institution"),
+}
+PARAM_GROUP = {k: g for g, keys in _GROUPS.items() for k in keys}
+
+# Read only by the Fortran driver executable, never by the library API: a
+# kwarg here would be silently ignored, so it is rejected.
+UNSUPPORTED = frozenset(
+    ("output_to_file", "output_dir", "output_interval", "output_format", "restart_interval",
+     "async_output", "async_buffer_slots", "restart_file", "forcing_file", "forcing_x_origin",
+     "forcing_y_origin", "gauge_file", "gauge_output_interval", "compress_output",
+     "compress_level", "out_h_layer", "out_velocity", "out_salinity", "out_temperature",
+     "out_density", "out_w", "nesting_file", "nesting_x_origin", "nesting_y_origin"))
+
+_BC = ("wall", "open", "tidal", "nested", "inflow", "discharge", "clamped", "sponge", "chapman")
+ENUMS = {"bc_west": _BC, "bc_east": _BC, "bc_south": _BC, "bc_north": _BC,
+         "time_scheme": ("euler", "rk2", "rk3", "rk43"),
+         "remap_method": ("pcm", "plm", "ppm", "ppm_h4", "pqm"),
+         "vcoord_type": ("sigma", "zsigma", "zstar", "zstar_lite", "zstar_full",
+                         "zstar_sigma")}
+POSITIVE = ("nx", "ny", "dx", "dy", "t_end", "cfl", "nz_layers")
+INPUT_FILE_KEYS = ("bathymetry_file",)
+
+
+def _fortran_value(v):
+    """One Python value as namelist text."""
+    if isinstance(v, np.generic):
+        v = v.item()
+    if v is None:
+        raise ValueError("None is not a valid namelist value")
+    if isinstance(v, bool):
+        return ".true." if v else ".false."
+    if isinstance(v, str):
+        return '"' + v.replace('"', '""') + '"'
+    if isinstance(v, (list, tuple, np.ndarray)):
+        return ", ".join(_fortran_value(x) for x in v)
+    if isinstance(v, float):
+        if not math.isfinite(v):
+            raise ValueError(f"non-finite value {v!r} is not allowed")
+        return repr(v)
+    if isinstance(v, int):
+        return str(v)
+    raise ValueError(f"unsupported namelist value {v!r}")
+
+
+def kwargs_to_namelist(kwargs: dict) -> str:
+    """Validate keyword arguments and render them as namelist text."""
+    by_group: dict[str, list[str]] = {}
+    for key, value in kwargs.items():
+        if key in UNSUPPORTED:
+            raise ValueError(f"'{key}' is read by the Fortran driver executable, not the "
+                             "library API, so it would be silently ignored here")
+        if key not in PARAM_GROUP:
+            raise ValueError(f"Unknown parameter '{key}'. Valid parameters: "
+                             f"{sorted(PARAM_GROUP)}")
+        if isinstance(value, np.generic):
+            value = value.item()
+        if key in ENUMS and (not isinstance(value, str) or value.lower() not in ENUMS[key]):
+            raise ValueError(f"{key}={value!r} is not valid; choose one of {ENUMS[key]}")
+        if key in POSITIVE and not (isinstance(value, (int, float))
+                                    and not isinstance(value, bool) and value > 0):
+            raise ValueError(f"{key} must be a positive number, got {value!r}")
+        by_group.setdefault(PARAM_GROUP[key], []).append(f"  {key} = {_fortran_value(value)}")
+    out = ["! namelist written by rakali_b200"]
+    for group, lines in by_group.items():
+        out.append(f"&{group}")
+        out.extend(lines)
+        out.append("/")
+    return "\n".join(out) + "\n"
+
+
+def _view(address: int, count: int, owner) -> np.ndarray:
+    """numpy float64 view of library memory that keeps `owner` alive."""
+    buf = (ctypes.c_double * count).from_address(address)
+    buf._rakali_owner = owner  # noqa: SLF001 - the view's base chain holds the sim
+    return np.frombuffer(buf, dtype=np.float64)
+
+
+class _CudaArray:
+    """__cuda_array_interface__ exporter for a pitched device field."""
+
+    def __init__(self, ptr, shape, strides, owner):
+        self._owner = owner
+        self.__cuda_array_interface__ = {
+            "shape": shape, "strides": strides, "typestr": "<f8",
+            "data": (ptr, False), "version": 3}
+
+
+class Rakali:
+    """Structured 2D shallow-water simulation on one B200 (SSP-RK2, FP64).
+
+    >>> sim = Rakali(nx=200, ny=100, dx=10.0, dy=10.0, t_end=60.0, use_hllc=True)
+    >>> sim.advance(60.0)
+    >>> sim.h_phys.max()
+    """
+
+    def __init__(self, namelist=None, defer_init=False, **kwargs):
+        self._lib = _lib.load()
+        self._handle = ctypes.c_void_p()
+        self._alive = False
+        if namelist is not None and kwargs:
+            raise ValueError("Pass either a namelist file or keyword arguments, not both")
+        if namelist is not None:
+            path = Path(namelist)
+            if not path.is_file():
+                raise FileNotFoundError(f"Namelist file not found: {path}")
+            self._check_input_files(self._namelist_inputs(path.read_text()), path.resolve().parent)
+            raw = str(path.resolve()).encode()
+            fn = self._lib.rki_create if defer_init else self._lib.rki_create_from_namelist
+            rc = fn(raw, len(raw), ctypes.byref(self._handle))
+        elif kwargs:
+            self._check_input_files({k: v for k, v in kwargs.items() if k in INPUT_FILE_KEYS},
+                                    Path.cwd())
+            text = kwargs_to_namelist(kwargs).encode()
+            fn = (self._lib.rki_create_from_string if defer_init
+                  else self._lib.rki_create_from_namelist_string)
+            rc = fn(text, len(text), ctypes.byref(self._handle))
+        else:
+            raise ValueError("Pass a namelist file or keyword arguments")
+        if rc != 0:
+            raise RuntimeError(f"Failed to create simulation (rc={rc}): "
+                               f"{_lib.last_error(self._lib)}")
+        self._finalised = not defer_init
+        self._alive = True
+        self._query_grid()
+
+    # --- construction helpers -------------------------------------------
+    @staticmethod
+    def _namelist_inputs(text: str) -> dict:
+        import re
+        out = {}
+        for m in re.finditer(r'^\s*(bathymetry_file)\s*=\s*["\']([^"\']*)["\']', text,
+                             re.IGNORECASE | re.MULTILINE):
+            out[m.group(1).lower()] = m.group(2)
+        return out
+
+    @staticmethod
+    def _check_input_files(entries: dict, base: Path):
+        for key, value in entries.items():
+            if not value:
+                continue
+            p = Path(str(value))
+            if not p.is_absolute():
+                p = Path(base) / p
+            if not p.is_file():
+                raise FileNotFoundError(f"{key} = {value!r} not found (looked for {p})")
+
+    _kwargs_to_namelist = staticmethod(kwargs_to_namelist)
+
+    def _query_grid(self):
+        nx, ny, ng = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        dx, dy = ctypes.c_double(), ctypes.c_double()
+        self._lib.rki_get_grid_info(self._handle, ctypes.byref(nx), ctypes.byref(ny),
+                                    ctypes.byref(ng), ctypes.byref(dx), ctypes.byref(dy))
+        self._nx, self._ny, self._ng = nx.value, ny.value, ng.value
+        self._dx, self._dy = dx.value, dy.value
+
+    # --- lifecycle --------------------------------------------------------
+    def _destroy_handle(self):
+        if getattr(self, "_alive", False):
+            self._alive = False
+            self._lib.rki_destroy(ctypes.byref(self._handle))
+
+    def close(self):
+        """Release the solver handle (idempotent)."""
+        self._destroy_handle()
+
+    destroy = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self._destroy_handle()
+        return False
+
+    def __del__(self):
+        try:
+            self._destroy_handle()
+        except Exception:
+            pass
+
+    def _check_alive(self):
+        if not self._alive:
+            raise RuntimeError("Simulation has been destroyed")
+
+    def _check_ready(self):
+        self._check_alive()
+        if not self._finalised:
+            raise RuntimeError("Simulation not finalised. Call finalize() after "
+                               "set_bathymetry() / set_initial_h().")
+
+    def _rc(self, rc, what):
+        if rc != 0:
+            raise RuntimeError(f"{what} failed (rc={rc}): {_lib.last_error(self._lib)}")
+
+    def finalize(self):
+        """Complete two-phase setup (bed ghosts, initial condition, BCs, upload)."""
+        self._check_alive()
+        if self._finalised:
+            raise RuntimeError("Simulation already finalised")
+        self._rc(self._lib.rki_finalize(self._handle), "Finalize")
+        self._finalised = True
+
+    def prepare(self):
+        """Alias of :meth:`finalize`."""
+        self.finalize()
+
+    # --- fields -----------------------------------------------------------
+    def _field(self, name):
+        self._check_alive()
+        ptr = ctypes.c_void_p()
+        nx, ny = ctypes.c_int(), ctypes.c_int()
+        rc = getattr(self._lib, f"rki_get_{name}_ptr")(self._handle, ctypes.byref(ptr),
+                                                       ctypes.byref(nx), ctypes.byref(ny))
+        self._rc(rc, f"rki_get_{name}_ptr")
+        arr = _view(ptr.value, nx.value * ny.value, self)
+        return arr.reshape((nx.value, ny.value), order="F")
+
+    def _phys(self, a):
+        g = self._ng
+        return a[g:-g, g:-g]
+
+    h = property(lambda self: self._field("h"), doc="Water depth (with ghosts).")
+    hu = property(lambda self: self._field("hu"), doc="x-momentum (with ghosts).")
+    hv = property(lambda self: self._field("hv"), doc="y-momentum (with ghosts).")
+    b = property(lambda self: self._field("b"), doc="Bed elevation, positive up (with ghosts).")
+    h0 = property(lambda self: self._field("h0"), doc="RK2 save of h (start of the last step).")
+    hu0 = property(lambda self: self._field("hu0"), doc="RK2 save of hu.")
+    hv0 = property(lambda self: self._field("hv0"), doc="RK2 save of hv.")
+    h_phys = property(lambda self: self._phys(self.h), doc="Water depth, interior only.")
+    hu_phys = property(lambda self: self._phys(self.hu), doc="x-momentum, interior only.")
+    hv_phys = property(lambda self: self._phys(self.hv), doc="y-momentum, interior only.")
+    b_phys = property(lambda self: self._phys(self.b), doc="Bed elevation, interior only.")
+
+    @property
+    def time(self):
+        self._check_alive()
+        return self._lib.rki_get_time(self._handle)
+
+    @property
+    def dt(self):
+        self._check_alive()
+        return self._lib.rki_get_dt(self._handle)
+
+    @property
+    def step_count(self):
+        self._check_alive()
+        return self._lib.rki_get_step_count(self._handle)
+
+    @property
+    def nz(self):
+        self._check_alive()
+        return self._lib.rki_get_nz_ml(self._handle)
+
+    nx = property(lambda self: self._nx)
+    ny = property(lambda self: self._ny)
+    nghost = property(lambda self: self._ng)
+    dx = property(lambda self: self._dx)
+    dy = property(lambda self: self._dy)
+
+    @property
+    def manning_n(self):
+        self._check_alive()
+        return self._lib.rki_get_manning_n(self._handle)
+
+    @property
+    def coriolis_f(self):
+        self._check_alive()
+        return self._lib.rki_get_coriolis_f(self._handle)
+
+    @property
+    def clamped_elevation(self):
+        self._check_alive()
+        return self._lib.rki_get_clamped_elevation(self._handle)
+
+    # --- stepping ---------------------------------------------------------
+    def step(self, n=1):
+        """Take n steps (each capped at t_end); raises once t_end is reached."""
+        self._check_ready()
+        t0 = self.time
+        self._rc(self._lib.rki_step(self._handle, int(n)), "Solver step")
+        if n > 0 and not self.time > t0:
+            raise RuntimeError(f"step() made no progress at t={self.time:g} s: the run has "
+                               "reached its t_end. Increase t_end when creating the simulation.")
+
+    def advance(self, target_time, callback=None, callback_interval=None, progress=False):
+        """Advance to ``target_time``; with a callback, in chunks with a host sync."""
+        self._check_ready()
+        target_time = float(target_time)
+        bar = None
+        if progress:
+            try:
+                from tqdm.auto import tqdm
+                bar = tqdm(total=max(target_time - self.time, 0.0), unit="s",
+                           desc=f"advance to t={target_time:.1f}s")
+            except ImportError:
+                import warnings
+                warnings.warn("progress=True requires tqdm", RuntimeWarning, stacklevel=2)
+        if callback is None and bar is None:
+            self._rc(self._lib.rki_advance(self._handle, target_time), "Advance")
+            return
+        if callback_interval is None:
+            frac = 10.0 if callback is not None else 100.0
+            callback_interval = max((target_time - self.time) / frac, TIME_EPS)
+        if callback_interval <= 0:
+            raise ValueError("callback_interval must be positive")
+        try:
+            t_now = last = self.time
+            while t_now < target_time - TIME_EPS:
+                t_next = min(t_now + callback_interval, target_time)
+                self._rc(self._lib.rki_advance(self._handle, t_next), "Advance")
+                self._lib.rki_sync_host(self._handle)
+                if callback is not None:
+                    callback(self)
+                t_now = self.time
+                if bar is not None:
+                    bar.update(t_now - last)
+                    last = t_now
+        finally:
+            if bar is not None:
+                bar.close()
+
+    def sync_host(self):
+        """Refresh the host copies of h, hu, hv (device state stays canonical)."""
+        self._check_alive()
+        self._lib.rki_sync_host(self._handle)
+
+    # --- setters ----------------------------------------------------------
+    def _shape(self, a, label):
+        a = np.asarray(a, dtype=np.float64)
+        if a.shape != (self._nx, self._ny):
+            raise ValueError(f"{label}: expected shape ({self._nx}, {self._ny}), got {a.shape}")
+        return np.asfortranarray(a)
+
+    def _set(self, fn, label, *arrays):
+        self._check_alive()
+        fs = [self._shape(a, label) for a in arrays]
+        ptrs = [f.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) for f in fs]
+        self._rc(getattr(self._lib, fn)(self._handle, *ptrs, self._nx, self._ny), label)
+
+    def set_bathymetry(self, b):
+        self._set("rki_set_bathymetry", "set_bathymetry", b)
+
+    def set_initial_h(self, h):
+        self._set("rki_set_initial_h", "set_initial_h", h)
+
+    def set_h(self, h):
+        self._set("rki_set_h", "set_h", h)
+
+    def set_hu(self, hu):
+        self._set("rki_set_hu", "set_hu", hu)
+
+    def set_hv(self, hv):
+        self._set("rki_set_hv", "set_hv", hv)
+
+    def set_wind(self, wx, wy):
+        self._set("rki_set_wind", "set_wind", wx, wy)
+
+    def set_atm_pressure(self, p):
+        self._set("rki_set_atm_pressure", "set_atm_pressure", p)
+
+    def set_precipitation(self, p):
+        self._set("rki_set_precipitation", "set_precipitation", p)
+
+    def set_heat_flux(self, q):
+        self._set("rki_set_heat_flux", "set_heat_flux", q)
+
+    def set_evap_minus_precip(self, ep):
+        self._set("rki_set_evap_minus_precip", "set_evap_minus_precip", ep)
+
+    def _scalar(self, fn, label, value):
+        self._check_alive()
+        v = float(value)
+        if not math.isfinite(v):
+            raise ValueError(f"{label} must be finite, got {value!r}")
+        self._rc(getattr(self._lib, fn)(self._handle, v), label)
+
+    def set_inflow_velocity(self, v):
+        self._scalar("rki_set_inflow_velocity", "inflow_velocity", v)
+
+    def set_inflow_salinity(self, s):
+        self._scalar("rki_set_inflow_salinity", "inflow_salinity", s)
+
+    def set_inflow_temperature(self, t):
+        self._scalar("rki_set_inflow_temperature", "inflow_temperature", t)
+
+    def set_discharge_flux(self, q):
+        self._scalar("rki_set_discharge_flux", "discharge_flux", q)
+
+    def set_clamped_elevation(self, eta):
+        self._scalar("rki_set_clamped_elevation", "clamped_elevation", eta)
+
+    def set_use_hllc(self, enable=True):
+        self._check_alive()
+        self._rc(self._lib.rki_set_use_hllc(self._handle, int(bool(enable))), "set_use_hllc")
+
+    def set_use_ppm_tracer(self, enable=True):
+        self._check_alive()
+        self._rc(self._lib.rki_set_use_ppm_tracer(self._handle, int(bool(enable))),
+                 "set_use_ppm_tracer")
+
+    def set_tidal_constituents(self, amp, phase, omega):
+        self._check_alive()
+        a, p, w = (np.ascontiguousarray(np.atleast_1d(x), dtype=np.float64)
+                   for x in (amp, phase, omega))
+        if not (a.shape == p.shape == w.shape) or a.ndim != 1:
+            raise ValueError("amp, phase and omega must be 1-D arrays of equal length")
+        dp = ctypes.POINTER(ctypes.c_double)
+        self._rc(self._lib.rki_set_tidal_constituents(
+            self._handle, a.ctypes.data_as(dp), p.ctypes.data_as(dp), w.ctypes.data_as(dp),
+            int(a.size)), "set_tidal_constituents")
+
+    def save_restart(self, filename):
+        self._check_alive()
+        raw = str(filename).encode()
+        self._rc(self._lib.rki_save_restart(self._handle, raw, len(raw)), "save_restart")
+
+    # --- additions --------------------------------------------------------
+    def mass_budget(self):
+        """(mass_out, mass_src): boundary outflow and source volume since creation."""
+        self._check_ready()
+        out = (ctypes.c_double * 3)()
+        self._rc(self._lib.rkb_get_mass_budget(self._handle, out), "mass_budget")
+        return out[0], out[1]
+
+    def device_fields(self):
+        """Zero-copy torch CUDA views (h, hu, hv, b) of the device state, with ghosts.
+
+        Valid until the next step (the state alternates between two buffers).
+        """
+        import torch
+        self._check_ready()
+        ptrs = (ctypes.c_void_p * 4)()
+        pitch = ctypes.c_int()
+        self._rc(self._lib.rkb_get_device_fields(self._handle, ptrs, ctypes.byref(pitch)),
+                 "device_fields")
+        shape = (self._nx + 2 * self._ng, self._ny + 2 * self._ng)
+        strides = (8, 8 * pitch.value)
+        return tuple(torch.as_tensor(_CudaArray(p, shape, strides, self), device="cuda")
+                     for p in ptrs)
+
+    def set_tile(self, tile: int):
+        """Tile shape of the fused stage kernel (0: 32x8, 1: 32x16, 2: 64x4, 3: 16x16)."""
+        self._check_alive()
+        self._rc(self._lib.rkb_set_tile(self._handle, int(tile)), "set_tile")
+
+
+def validate_namelist(text: str):
+    """(rc, message) of the library's namelist validation; needs no GPU."""
+    lib = _lib.load()
+    raw = text.encode()
+    buf = ctypes.create_string_buffer(512)
+    rc = lib.rkb_validate_namelist(raw, len(raw), buf, len(buf))
+    return rc, buf.value.decode()
+
+
+__all__ = ["Rakali", "kwargs_to_namelist", "validate_namelist"]
+
+if os.environ.get("RAKALI_B200_EAGER_LOAD"):
+    _lib.load()

@@ -1,0 +1,166 @@
+// Shared definitions for the B200 structured shallow-water step.
+//
+// Layout: every field is a pitched, column-major (Fortran order) array of
+// nx_total x ny_total cells, ghosts included; element (i, j) (0-based) lives
+// at a[i + j * pitch] with pitch >= nx_total a multiple of 32 elements, so
+// every row starts on a 256-byte boundary.
+//
+// The FP64 path is compiled with --fmad=false and evaluates every expression
+// in the reference's left-to-right order, so its results are bit-identical
+// to the Fortran arithmetic wherever only +, -, *, / and sqrt are involved
+// (IEEE-754 correctly rounded on both CPU and GPU).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace rkb {
+
+// src/core/rki_constants.F90:38-157
+constexpr double kG = 9.80665;
+constexpr double kRho = 1035.0;
+constexpr double kDry = 1.0e-6;
+constexpr double kThin = 1.0e-3;
+constexpr double kFroude = 50.0;
+// DESING_EPS = 1.5e-4; the reference folds DESING_EPS**4 at compile time.
+constexpr double kEps4 = 5.062499999999998e-16;
+constexpr double kSqrt2 = 1.4142135623730951;
+constexpr double kTwoPi = 6.283185307179586;
+constexpr double kHalfG = 0.5 * kG;  // exact: halving is exact
+
+constexpr int kMaxTidal = 10;
+
+// Boundary tags, src/core/structured/rki_boundary_types.F90:19-36.
+enum BcType : int {
+  kWall = 1, kOpen = 2, kTidal = 3, kNested = 4, kInflow = 5,
+  kDischarge = 6, kClamped = 7, kSponge = 8, kChapman = 9
+};
+
+struct Grid {
+  int nxt, nyt, ng;  // totals including ghosts, ghost width
+  int pitch;         // elements between consecutive j
+  double dx, dy;
+  __host__ __device__ int nx_phys() const { return nxt - 2 * ng; }
+  __host__ __device__ int ny_phys() const { return nyt - 2 * ng; }
+  __host__ __device__ size_t at(int i, int j) const { return (size_t)i + (size_t)j * (size_t)pitch; }
+};
+
+// Boundary parameters (bc_params_t, rki_boundary_types.F90:38-100), kept in
+// device memory so setters can change them without re-capturing graphs.
+struct BcParams {
+  int type[4];  // west, east, south, north
+  int n_tidal;
+  int sponge_width;
+  double tidal_amplitude, tidal_period;
+  double amp[kMaxTidal], phase[kMaxTidal], omega[kMaxTidal];
+  double inflow_velocity, discharge_flux, clamped_elevation;
+  double sponge_strength, sponge_h_ref;
+};
+
+// Physics / time-control scalars (state_t + config_t fields the step reads).
+struct Physics {
+  double cfl, dt_fixed, t_end, ssp_coeff;
+  double manning_n, coriolis_f;
+  int cfl_interval;
+  int forcing_active;
+  int use_hllc;
+  int pad_;
+};
+
+// Device-resident clock and reductions of one simulation.  Fields marked
+// (step) are written inside a step; the others change only at the end of a
+// step (by the last block of the final stage kernel) or from the host.
+struct StepCtl {
+  double t;            // h%t_current
+  double dt_prev;      // state%dt as of the start of the step
+  double dt;           // (step) this step's dt
+  double target;       // advance target (mode 0)
+  double mass_out, mass_src;
+  double precip_sum;   // sum of precipitation over the interior (host-set)
+  double msx, msy;     // max over wet cells of (|u|+c) along x and y (current state)
+  unsigned long long msx_next, msy_next;  // (step) atomicMax accumulators (bit patterns)
+  int step_count;
+  int cur;             // ping-pong buffer holding U^n
+  int active;          // (step) 1 when this step runs
+  int mode;            // 0: advance to target, 1: fixed step count
+  int remaining;       // steps left in mode 1
+  int ms_valid;        // msx/msy describe the current state
+  unsigned int done_blocks;  // last-block counter of the final stage kernel
+  unsigned int ms_done_blocks;
+  int steps_run;       // steps executed since the host last cleared it
+  int pad_;
+};
+
+// ---------------------------------------------------------------------------
+// Small FP64 helpers in the reference's evaluation order.
+// ---------------------------------------------------------------------------
+
+__host__ __device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
+__host__ __device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
+// Fortran max(0, x) for non-NaN x.
+__host__ __device__ __forceinline__ double pos(double x) { return x > 0.0 ? x : 0.0; }
+
+// minmod, rki_kernel_flux.F90:380-393
+__device__ __forceinline__ double minmod(double a, double b) {
+  if (a * b <= 0.0) return 0.0;
+  return fabs(a) < fabs(b) ? a : b;
+}
+
+// Clamp + KP07 desingularisation + Froude backstop
+// (rki_kernel_fused.F90:93-119 and :441-463).
+__device__ __forceinline__ void protect(double& h, double& u, double& v) {
+  if (h < 0.0) {
+    h = 0.0; u = 0.0; v = 0.0;
+  } else if (h < kDry) {
+    u = 0.0; v = 0.0;
+  } else {
+    double h2 = h * h;
+    double h4 = h2 * h2;
+    if (h4 < kEps4) {
+      double r = sqrt(h4 + kEps4);
+      double uu = kSqrt2 * h * u / r;
+      double vv = kSqrt2 * h * v / r;
+      u = h * uu;
+      v = h * vv;
+    }
+    double sp2 = (u * u + v * v) / (h * h);
+    double fr2 = kFroude * kFroude * kG * h;
+    if (sp2 > fr2) {
+      double sc = sqrt(fr2 / sp2);
+      u = u * sc;
+      v = v * sc;
+    }
+  }
+}
+
+// Wave speed terms of compute_timestep (rki_kernel_timestep.F90:52-66):
+// returns (|u|_KP07 + sqrt(g h)) along x and y, before the division by dx/dy.
+__device__ __forceinline__ void wave_speed(double h, double hu, double hv, double& sx, double& sy) {
+  sx = 0.0;
+  sy = 0.0;
+  if (h > kDry) {
+    double c = sqrt(kG * h);
+    double h2 = h * h;
+    double den = sqrt(h2 * h2 + kEps4);
+    double ua = fabs(hu) * kSqrt2 * h / den;
+    double va = fabs(hv) * kSqrt2 * h / den;
+    sx = ua + c;
+    sy = va + c;
+  }
+}
+
+// dt from the maximum wave speed (rki_kernel_timestep.F90:68-72), the SSP
+// factor and the cap (rki_solver.F90:731-748).  Dividing the maxima by dx/dy
+// once is exact: x -> fl(x/d) is monotone for d > 0.
+__host__ __device__ inline double cfl_dt(double msx, double msy, const Grid& g, double cfl) {
+  double ms = dmax(msx / g.dx, msy / g.dy);
+  if (ms > 0.0) return cfl / ms;
+  return cfl * dmin(g.dx, g.dy) / sqrt(kG * kDry);
+}
+
+// Non-negative doubles order like their bit patterns.
+__device__ __forceinline__ void atomic_max_pos(unsigned long long* addr, double v) {
+  if (v > 0.0) atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+}  // namespace rkb

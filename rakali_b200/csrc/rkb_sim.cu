@@ -1,0 +1,647 @@
+// Host driver of one structured simulation (see rkb_sim.hpp).
+#include "rkb_sim.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace rkb {
+
+namespace {
+
+size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
+
+#define RKB_TRY(expr)                      \
+  do {                                     \
+    cudaError_t e_ = (expr);               \
+    if (e_ != cudaSuccess) return -1;      \
+  } while (0)
+
+}  // namespace
+
+Sim::~Sim() {
+  for (auto& ge : graphs_) {
+    if (ge.exec) cudaGraphExecDestroy(ge.exec);
+    if (ge.graph) cudaGraphDestroy(ge.graph);
+  }
+  graphs_.clear();
+  free_device();
+  for (auto& p : hf_) {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+  }
+  if (hctl_) cudaFreeHost(hctl_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+int Sim::create(const std::string& text, std::string& err) {
+  Config c;
+  if (!parse_namelist(text, c, err)) return -2;
+  int rc = validate(c, err);
+  if (rc != 0) return rc;
+  cfg = c;
+  g.ng = cfg.nghost;
+  g.nxt = cfg.nx + 2 * cfg.nghost;
+  g.nyt = cfg.ny + 2 * cfg.nghost;
+  g.pitch = (int)round_up((size_t)g.nxt, 32);
+  g.dx = cfg.dx;
+  g.dy = cfg.dy;
+  ncell_ = (size_t)g.nxt * (size_t)g.nyt;
+
+  if (cudaGetDevice(&device_) != cudaSuccess) {
+    err = "no CUDA device available";
+    return -1;
+  }
+  for (auto& p : hf_) {
+    if (cudaMallocHost((void**)&p, ncell_ * sizeof(double)) != cudaSuccess) {
+      err = "pinned host allocation failed";
+      return -1;
+    }
+    std::memset(p, 0, ncell_ * sizeof(double));
+  }
+  if (cudaMallocHost((void**)&hctl_, sizeof(StepCtl)) != cudaSuccess) {
+    err = "pinned host allocation failed";
+    return -1;
+  }
+  std::memset(hctl_, 0, sizeof(StepCtl));
+
+  // Physics and time control (state_init_from_config, rki_state.F90:134-301)
+  phys = Physics{};
+  phys.cfl = cfg.cfl;
+  phys.dt_fixed = cfg.dt_fixed;
+  phys.t_end = cfg.t_end;
+  phys.cfl_interval = cfg.cfl_interval;
+  phys.manning_n = cfg.manning_n;
+  phys.coriolis_f = cfg.coriolis_f;
+  phys.use_hllc = cfg.use_hllc ? 1 : 0;
+  phys.forcing_active = 0;
+  phys.ssp_coeff = scheme_code(cfg.time_scheme) == 4 ? 2.0 : 1.0;
+  params_dirty = true;
+  t_current_ = 0.0;
+  dt_ = 0.0;
+  step_count_ = 0;
+  is_initialised = true;
+  is_finalised = false;
+  return 0;
+}
+
+// init_from_config (src/core/rki_init.F90:196-216) on the host arrays.
+void Sim::init_condition() {
+  const int nxt = g.nxt, nyt = g.nyt, ng = g.ng;
+  double* h = hf_[0];
+  double* hu = hf_[1];
+  double* hv = hf_[2];
+  double* b = hf_[3];
+  auto at = [&](int i, int j) { return (size_t)i + (size_t)j * (size_t)nxt; };
+  bool has_b = false;
+  for (size_t k = 0; k < ncell_ && !has_b; ++k) has_b = b[k] != 0.0;
+  const std::string& ic = cfg.init_condition;
+  if (ic == "still_water") {
+    for (size_t k = 0; k < ncell_; ++k) {
+      h[k] = std::max(cfg.eta_initial - b[k], 0.0);
+      hu[k] = 0.0;
+      hv[k] = 0.0;
+    }
+  } else if (ic == "gaussian_hump") {
+    const double xc = (double)cfg.nx * g.dx * 0.5 + cfg.hump_x_offset;
+    const double yc = (double)cfg.ny * g.dy * 0.5 + cfg.hump_y_offset;
+    const double s2 = 2.0 * (cfg.hump_sigma * cfg.hump_sigma);
+    for (int j = 0; j < nyt; ++j)
+      for (int i = 0; i < nxt; ++i) {
+        const double x = ((double)(i + 1 - ng) - 0.5) * g.dx;
+        const double y = ((double)(j + 1 - ng) - 0.5) * g.dy;
+        const double r2 = (x - xc) * (x - xc) + (y - yc) * (y - yc);
+        const size_t q = at(i, j);
+        if (!has_b) b[q] = 0.0;
+        h[q] = cfg.h0 + cfg.hump_amplitude * std::exp(-r2 / s2);
+        hu[q] = 0.0;
+        hv[q] = 0.0;
+      }
+  } else if (ic == "castro_dam_break") {
+    const double x0 = -0.5 * (double)cfg.nx * g.dx;
+    const double y0 = -0.5 * (double)cfg.ny * g.dy;
+    for (int j = 0; j < nyt; ++j)
+      for (int i = 0; i < nxt; ++i) {
+        const double x = x0 + ((double)(i + 1 - ng) - 0.5) * g.dx;
+        const double y = y0 + ((double)(j + 1 - ng) - 0.5) * g.dy;
+        const size_t q = at(i, j);
+        b[q] = -(1.0 - 0.4 * std::exp(-x * x - y * y));
+        h[q] = (x * x + y * y <= 0.36) ? 3.0 - b[q] : 1.0 - b[q];
+        hu[q] = 0.0;
+        hv[q] = 0.0;
+      }
+  } else {  // dam_break
+    const int mid_x = ng + cfg.nx / 2;
+    for (int j = 0; j < nyt; ++j)
+      for (int i = 0; i < nxt; ++i) {
+        const size_t q = at(i, j);
+        if (!has_b) b[q] = 0.0;
+        hu[q] = 0.0;
+        hv[q] = 0.0;
+        h[q] = (i + 1 <= mid_x) ? 2.0 : 1.0;
+      }
+  }
+}
+
+int Sim::finalize(std::string& err) {
+  const int nxt = g.nxt, nyt = g.nyt, ng = g.ng;
+  double* b = hf_[3];
+  auto at = [&](int i, int j) { return (size_t)i + (size_t)j * (size_t)nxt; };
+  // fill_bathymetry_ghosts_array (src/io/rki_bathymetry.F90:165-196)
+  for (int j = 0; j < nyt; ++j)
+    for (int i = 0; i < ng; ++i) {
+      b[at(i, j)] = b[at(ng, j)];
+      b[at(ng + cfg.nx + i, j)] = b[at(ng + cfg.nx - 1, j)];
+    }
+  for (int j = 0; j < ng; ++j)
+    for (int i = 0; i < nxt; ++i) {
+      b[at(i, j)] = b[at(i, ng)];
+      b[at(i, ng + cfg.ny + j)] = b[at(i, ng + cfg.ny - 1)];
+    }
+  if (!user_set_h) init_condition();
+
+  // bc_init_from_config (rki_boundary_types.F90:132-154)
+  bc = BcParams{};
+  bc.type[0] = bc_code(cfg.bc_west);
+  bc.type[1] = bc_code(cfg.bc_east);
+  bc.type[2] = bc_code(cfg.bc_south);
+  bc.type[3] = bc_code(cfg.bc_north);
+  bc.tidal_amplitude = cfg.tidal_amplitude;
+  bc.tidal_period = cfg.tidal_period;
+  bc.n_tidal = cfg.n_tidal_constituents;
+  for (int k = 0; k < kMaxTidal; ++k) {
+    bc.amp[k] = cfg.tidal_amp[k];
+    bc.phase[k] = cfg.tidal_phase[k];
+    bc.omega[k] = cfg.tidal_omega[k];
+  }
+  bc.inflow_velocity = cfg.inflow_velocity;
+  bc.discharge_flux = cfg.discharge_flux;
+  bc.clamped_elevation = cfg.clamped_elevation;
+  bc.sponge_width = cfg.sponge_width;
+  bc.sponge_strength = cfg.sponge_strength;
+  bc.sponge_h_ref = cfg.sponge_h_ref;
+  // bc_init_chapman (rki_boundary_types.F90:156-202)
+  eta_old_[0].assign(nyt, 0.0);
+  eta_old_[1].assign(nyt, 0.0);
+  eta_old_[2].assign(nxt, 0.0);
+  eta_old_[3].assign(nxt, 0.0);
+  const double* h = hf_[0];
+  if (bc.type[0] == kChapman || bc.type[1] == kChapman)
+    for (int j = 0; j < nyt; ++j) {
+      eta_old_[0][j] = h[at(ng, j)] + b[at(ng, j)];
+      eta_old_[1][j] = h[at(nxt - ng - 1, j)] + b[at(nxt - ng - 1, j)];
+    }
+  if (bc.type[2] == kChapman || bc.type[3] == kChapman)
+    for (int i = 0; i < nxt; ++i) {
+      eta_old_[2][i] = h[at(i, ng)] + b[at(i, ng)];
+      eta_old_[3][i] = h[at(i, nyt - ng - 1)] + b[at(i, nyt - ng - 1)];
+    }
+  params_dirty = true;
+
+  int rc = alloc_device(err);
+  if (rc != 0) return rc;
+  for (int w = 0; w < 4; ++w)
+    RKB_TRY(cudaMemcpyAsync(args_.eta_old[w], eta_old_[w].data(),
+                            eta_old_[w].size() * sizeof(double), cudaMemcpyHostToDevice,
+                            stream_));
+  rc = upload_state();
+  if (rc != 0) return rc;
+  RKB_TRY(cudaStreamSynchronize(stream_));
+  on_device_ = true;
+  host_is_current_ = false;
+  is_finalised = true;
+  return 0;
+}
+
+int Sim::alloc_device(std::string& err) {
+  if (dmem_) return 0;
+  if (cudaSetDevice(device_) != cudaSuccess) { err = "cudaSetDevice failed"; return -1; }
+  if (!stream_ && cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking) != cudaSuccess) {
+    err = "stream creation failed";
+    return -1;
+  }
+  const size_t field = round_up((size_t)g.pitch * (size_t)g.nyt, 64);  // doubles
+  size_t npart = 0;
+  for (int t = 0; t < kNumTiles; ++t) npart = std::max(npart, partials_doubles(g, t));
+  npart = round_up(npart, 64);
+  const size_t neta = round_up(2 * (size_t)g.nyt + 2 * (size_t)g.nxt, 64);
+  const size_t ctl_bytes = round_up(sizeof(StepCtl), 256) + round_up(sizeof(Physics), 256) +
+                           round_up(sizeof(BcParams), 256);
+  const size_t bytes = (10 * field + npart + neta) * sizeof(double) + ctl_bytes;
+  if (cudaMalloc(&dmem_, bytes) != cudaSuccess) {
+    dmem_ = nullptr;
+    err = "device allocation failed";
+    return -1;
+  }
+  if (cudaMemsetAsync(dmem_, 0, bytes, stream_) != cudaSuccess) return -1;
+  double* p = (double*)dmem_;
+  auto take = [&](size_t n) {
+    double* q = p;
+    p += n;
+    return q;
+  };
+  args_.g = g;
+  args_.U0 = {take(field), take(field), take(field)};
+  args_.U1 = {take(field), take(field), take(field)};
+  args_.S = {take(field), take(field), take(field)};
+  args_.b = take(field);
+  args_.partials = take(npart);
+  double* eo = take(neta);
+  args_.eta_old[0] = eo;
+  args_.eta_old[1] = eo + g.nyt;
+  args_.eta_old[2] = eo + 2 * g.nyt;
+  args_.eta_old[3] = eo + 2 * g.nyt + g.nxt;
+  char* cp = (char*)p;
+  args_.ctl = (StepCtl*)cp;
+  cp += round_up(sizeof(StepCtl), 256);
+  args_.phys = (const Physics*)cp;
+  cp += round_up(sizeof(Physics), 256);
+  args_.bc = (const BcParams*)cp;
+  args_.fo = Forcing{nullptr, nullptr, nullptr, nullptr};
+  args_.tile = tile;
+  args_.hllc = phys.use_hllc;
+  cur_ = 0;
+  return 0;
+}
+
+void Sim::free_device() {
+  if (dmem_) cudaFree(dmem_);
+  dmem_ = nullptr;
+  for (double* f : {const_cast<double*>(args_.fo.wind_x), const_cast<double*>(args_.fo.wind_y),
+                    const_cast<double*>(args_.fo.atm), const_cast<double*>(args_.fo.precip)})
+    if (f) cudaFree(f);
+  args_.fo = Forcing{nullptr, nullptr, nullptr, nullptr};
+}
+
+// Host arrays -> device (solver_enter_data): h, hu, hv into the current
+// buffer, the bed, and the forcing fields when active.
+int Sim::upload_state() {
+  const size_t wbytes = (size_t)g.nxt * sizeof(double);
+  const size_t dpitch = (size_t)g.pitch * sizeof(double);
+  FieldSet F = cur_ ? args_.U1 : args_.U0;
+  double* dst[4] = {F.h, F.hu, F.hv, args_.b};
+  for (int k = 0; k < 4; ++k)
+    RKB_TRY(cudaMemcpy2DAsync(dst[k], dpitch, hf_[k], wbytes, wbytes, g.nyt,
+                              cudaMemcpyHostToDevice, stream_));
+  if (phys.forcing_active && upload_forcing() != 0) return -1;
+  hctl_->ms_valid = 0;
+  RKB_TRY(cudaMemcpyAsync(&args_.ctl->ms_valid, &hctl_->ms_valid, sizeof(int),
+                          cudaMemcpyHostToDevice, stream_));
+  params_dirty = true;
+  return 0;
+}
+
+// Forcing fields -> device (solver_update_forcing, rki_solver.F90:421-434) and
+// the precipitation sum the mass budget adds each stage.
+int Sim::upload_forcing() {
+  const size_t wbytes = (size_t)g.nxt * sizeof(double);
+  const size_t dpitch = (size_t)g.pitch * sizeof(double);
+  if (!args_.fo.wind_x) {
+    double* f[4];
+    for (int k = 0; k < 4; ++k)
+      RKB_TRY(cudaMalloc((void**)&f[k], (size_t)g.pitch * g.nyt * sizeof(double)));
+    args_.fo = Forcing{f[0], f[1], f[2], f[3]};
+    for (auto& ge : graphs_) {  // graphs hold the old (null) forcing pointers
+      if (ge.exec) cudaGraphExecDestroy(ge.exec);
+      if (ge.graph) cudaGraphDestroy(ge.graph);
+    }
+    graphs_.clear();
+  }
+  const double* dstf[4] = {args_.fo.wind_x, args_.fo.wind_y, args_.fo.atm, args_.fo.precip};
+  for (int k = 0; k < 4; ++k)
+    RKB_TRY(cudaMemcpy2DAsync(const_cast<double*>(dstf[k]), dpitch, forcing_[k].data(), wbytes,
+                              wbytes, g.nyt, cudaMemcpyHostToDevice, stream_));
+  double acc = 0.0;
+  for (int j = g.ng; j < g.nyt - g.ng; ++j)
+    for (int i = g.ng; i < g.nxt - g.ng; ++i) acc = acc + forcing_[3][(size_t)i + (size_t)j * g.nxt];
+  hctl_->precip_sum = acc;
+  RKB_TRY(cudaMemcpyAsync(&args_.ctl->precip_sum, &hctl_->precip_sum, sizeof(double),
+                          cudaMemcpyHostToDevice, stream_));
+  return cudaStreamSynchronize(stream_) == cudaSuccess ? 0 : -1;
+}
+
+int Sim::upload_params() {
+  if (!params_dirty) return 0;
+  // The stream is synchronised after every run, so the pinned staging copies
+  // are free to reuse.
+  static_assert(sizeof(Physics) + sizeof(BcParams) < 4096, "param staging");
+  RKB_TRY(cudaMemcpyAsync(const_cast<Physics*>(args_.phys), &phys, sizeof(Physics),
+                          cudaMemcpyHostToDevice, stream_));
+  RKB_TRY(cudaMemcpyAsync(const_cast<BcParams*>(args_.bc), &bc, sizeof(BcParams),
+                          cudaMemcpyHostToDevice, stream_));
+  RKB_TRY(cudaStreamSynchronize(stream_));
+  args_.hllc = phys.use_hllc;
+  args_.tile = tile;
+  RKB_TRY(configure_kernels(args_.tile, args_.hllc));
+  params_dirty = false;
+  return 0;
+}
+
+int Sim::ensure_device() {
+  if (cudaSetDevice(device_) != cudaSuccess) return -1;
+  if (!on_device_) {
+    if (upload_state() != 0) return -1;
+    on_device_ = true;
+  }
+  host_is_current_ = false;
+  return 0;
+}
+
+// Device -> host of h, hu, hv (solver_update_host); with `full`, also the
+// bed and the RK2 save arrays (solver_exit_data).
+static int pull(const StepArgs& a, int cur, bool stepped, bool full, double* const* hf,
+                const Grid& g, cudaStream_t s) {
+  const size_t wbytes = (size_t)g.nxt * sizeof(double);
+  const size_t spitch = (size_t)g.pitch * sizeof(double);
+  FieldSet F = cur ? a.U1 : a.U0;
+  const double* src[4] = {F.h, F.hu, F.hv, a.b};
+  const int n = full ? 4 : 3;
+  for (int k = 0; k < n; ++k)
+    if (cudaMemcpy2DAsync(hf[k], wbytes, src[k], spitch, wbytes, g.nyt, cudaMemcpyDeviceToHost, s) !=
+        cudaSuccess)
+      return -1;
+  if (full && stepped) {
+    // RK2 save arrays: interior of U^n from the other buffer; the reference
+    // never writes their ghosts in the fused RK2 path (left at zero here).
+    FieldSet O = cur ? a.U0 : a.U1;
+    const double* so[3] = {O.h, O.hu, O.hv};
+    const size_t off_d = (size_t)g.ng + (size_t)g.ng * (size_t)g.pitch;
+    const size_t off_h = (size_t)g.ng + (size_t)g.ng * (size_t)g.nxt;
+    for (int k = 0; k < 3; ++k)
+      if (cudaMemcpy2DAsync(hf[4 + k] + off_h, wbytes, so[k] + off_d, spitch,
+                            (size_t)g.nx_phys() * sizeof(double), g.ny_phys(),
+                            cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return -1;
+  }
+  return cudaStreamSynchronize(s) == cudaSuccess ? 0 : -1;
+}
+
+void Sim::ensure_host() {
+  if (host_is_current_) return;
+  if (on_device_) {
+    cudaSetDevice(device_);
+    pull(args_, cur_, stepped_, true, hf_, g, stream_);
+    on_device_ = false;
+    host_is_current_ = true;
+  }
+}
+
+void Sim::sync_host() {
+  if (is_initialised && on_device_ && !host_is_current_) {
+    cudaSetDevice(device_);
+    pull(args_, cur_, stepped_, false, hf_, g, stream_);
+    host_is_current_ = true;
+  }
+}
+
+void Sim::sync_from_device() {
+  if (is_initialised && on_device_) {
+    cudaSetDevice(device_);
+    pull(args_, cur_, stepped_, true, hf_, g, stream_);
+    on_device_ = false;
+    host_is_current_ = true;
+  }
+}
+
+double* Sim::field_ptr(int which) {
+  ensure_host();
+  return hf_[which];
+}
+
+int Sim::set_interior(int which, const double* data, int nx, int ny) {
+  if (nx != cfg.nx || ny != cfg.ny) return -2;
+  const bool state_field = which <= 2;
+  const bool pre_final = (which == 3) || (which == 10);  // bathymetry, initial h
+  if (pre_final) {
+    if (on_device_) ensure_host();
+  } else if (state_field) {
+    // refresh_host (rki_api.F90:126-135)
+    if (is_initialised && !host_is_current_ && on_device_) sync_host();
+  }
+  const int f = which == 10 ? 0 : which;
+  double* dst = hf_[f];
+  for (int j = 0; j < ny; ++j)
+    std::memcpy(dst + (size_t)g.ng + (size_t)(g.ng + j) * g.nxt, data + (size_t)j * nx,
+                (size_t)nx * sizeof(double));
+  if (which == 3) {
+    user_set_bathymetry = true;
+    if (is_finalised) {
+      double* b = dst;
+      auto at = [&](int i, int j) { return (size_t)i + (size_t)j * (size_t)g.nxt; };
+      for (int j = 0; j < g.nyt; ++j)
+        for (int i = 0; i < g.ng; ++i) {
+          b[at(i, j)] = b[at(g.ng, j)];
+          b[at(g.ng + cfg.nx + i, j)] = b[at(g.ng + cfg.nx - 1, j)];
+        }
+      for (int j = 0; j < g.ng; ++j)
+        for (int i = 0; i < g.nxt; ++i) {
+          b[at(i, j)] = b[at(i, g.ng)];
+          b[at(i, g.ng + cfg.ny + j)] = b[at(i, g.ng + cfg.ny - 1)];
+        }
+    }
+  }
+  if (which == 10 || which == 0) user_set_h = true;
+  if (state_field && on_device_) {
+    // push_state_to_device (rki_api.F90:137-143)
+    const size_t wbytes = (size_t)g.nxt * sizeof(double);
+    const size_t dpitch = (size_t)g.pitch * sizeof(double);
+    FieldSet F = cur_ ? args_.U1 : args_.U0;
+    double* dstd[3] = {F.h, F.hu, F.hv};
+    for (int k = 0; k < 3; ++k)
+      if (cudaMemcpy2DAsync(dstd[k], dpitch, hf_[k], wbytes, wbytes, g.nyt,
+                            cudaMemcpyHostToDevice, stream_) != cudaSuccess)
+        return -1;
+    hctl_->ms_valid = 0;
+    if (cudaMemcpyAsync(&args_.ctl->ms_valid, &hctl_->ms_valid, sizeof(int),
+                        cudaMemcpyHostToDevice, stream_) != cudaSuccess)
+      return -1;
+    if (cudaStreamSynchronize(stream_) != cudaSuccess) return -1;
+    host_is_current_ = false;
+  }
+  return 0;
+}
+
+int Sim::set_forcing(int which, const double* data, int nx, int ny) {
+  if (nx != cfg.nx || ny != cfg.ny) return -2;
+  if (forcing_[0].empty()) {
+    // state%forcing arrays: uniform config wind stress, zero elsewhere
+    forcing_[0].assign(ncell_, cfg.wind_stress_x);
+    forcing_[1].assign(ncell_, cfg.wind_stress_y);
+    for (int k = 2; k < 6; ++k) forcing_[k].assign(ncell_, 0.0);
+  }
+  double* dst = forcing_[which].data();
+  for (int j = 0; j < ny; ++j)
+    std::memcpy(dst + (size_t)g.ng + (size_t)(g.ng + j) * g.nxt, data + (size_t)j * nx,
+                (size_t)nx * sizeof(double));
+  if (which <= 3) {
+    phys.forcing_active = 1;
+    params_dirty = true;
+  }
+  if (on_device_ && which <= 3) return upload_forcing();
+  return 0;
+}
+
+void Sim::pull_ctl() {
+  cudaMemcpyAsync(hctl_, args_.ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, stream_);
+  cudaStreamSynchronize(stream_);
+  t_current_ = hctl_->t;
+  dt_ = hctl_->dt_prev;
+  step_count_ = hctl_->step_count;
+  cur_ = hctl_->cur;
+}
+
+cudaGraphExec_t Sim::graph_for(int steps) {
+  for (auto& ge : graphs_)
+    if (ge.steps == steps && ge.hllc == args_.hllc && ge.tile == args_.tile) return ge.exec;
+  GraphEntry ge{steps, args_.hllc, args_.tile, nullptr, nullptr};
+  if (cudaStreamSynchronize(stream_) != cudaSuccess) return nullptr;
+  if (cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    return nullptr;
+  for (int k = 0; k < steps; ++k) launch_step(args_, stream_);
+  if (cudaStreamEndCapture(stream_, &ge.graph) != cudaSuccess) return nullptr;
+  if (cudaGraphInstantiate(&ge.exec, ge.graph, 0) != cudaSuccess) return nullptr;
+  graphs_.push_back(ge);
+  return ge.exec;
+}
+
+int Sim::prepare_run(int mode, double target, int nsteps) {
+  if (ensure_device() != 0) return -1;
+  if (upload_params() != 0) return -1;
+  // the kernels read the control block; set the run mode
+  hctl_->mode = mode;
+  hctl_->target = target;
+  hctl_->remaining = nsteps;
+  RKB_TRY(cudaMemcpyAsync(&args_.ctl->target, &hctl_->target, sizeof(double),
+                          cudaMemcpyHostToDevice, stream_));
+  RKB_TRY(cudaMemcpyAsync(&args_.ctl->mode, &hctl_->mode, sizeof(int), cudaMemcpyHostToDevice,
+                          stream_));
+  RKB_TRY(cudaMemcpyAsync(&args_.ctl->remaining, &hctl_->remaining, sizeof(int),
+                          cudaMemcpyHostToDevice, stream_));
+  // CFL maxima of the current state if no step epilogue has produced them
+  RKB_TRY(cudaMemcpyAsync(&hctl_->ms_valid, &args_.ctl->ms_valid, sizeof(int),
+                          cudaMemcpyDeviceToHost, stream_));
+  RKB_TRY(cudaStreamSynchronize(stream_));
+  if (!hctl_->ms_valid) RKB_TRY(launch_max_speed(args_, stream_));
+  return 0;
+}
+
+int Sim::run(int mode, double target, int nsteps) {
+  if (prepare_run(mode, target, nsteps) != 0) return -1;
+
+  if (mode == 1) {
+    int left = nsteps;
+    while (left > 0) {
+      int k = 1;
+      while (k * 2 <= left && k * 2 <= steps_per_graph_cap) k *= 2;
+      cudaGraphExec_t ge = graph_for(k);
+      if (!ge) return -1;
+      RKB_TRY(cudaGraphLaunch(ge, stream_));
+      left -= k;
+    }
+    pull_ctl();
+  } else {
+    pull_ctl();
+    while (t_current_ < target - 1.0e-10) {
+      int k = 1;
+      if (dt_ > 0.0) {
+        const double est = std::ceil((target - t_current_) / dt_ * 1.02) + 1.0;
+        while (k < est && k < steps_per_graph_cap) k *= 2;
+      }
+      cudaGraphExec_t ge = graph_for(k);
+      if (!ge) return -1;
+      RKB_TRY(cudaGraphLaunch(ge, stream_));
+      const double t_before = t_current_;
+      const int steps_before = step_count_;
+      pull_ctl();
+      if (!(t_current_ > t_before) && step_count_ == steps_before) return -1;  // no progress
+    }
+  }
+  if (cudaGetLastError() != cudaSuccess) return -1;
+  stepped_ = true;
+  host_is_current_ = false;
+  return 0;
+}
+
+int Sim::time_steps(int n, double* ms) {
+  if (n <= 0) return -2;
+  if (prepare_run(1, 0.0, n) != 0) return -1;
+  // capture the graphs first so instantiation stays outside the timed region
+  for (int k = 1; k <= steps_per_graph_cap; k *= 2)
+    if (k <= n && !graph_for(k)) return -1;
+  cudaEvent_t e0, e1;
+  RKB_TRY(cudaEventCreate(&e0));
+  RKB_TRY(cudaEventCreate(&e1));
+  RKB_TRY(cudaEventRecord(e0, stream_));
+  int left = n;
+  while (left > 0) {
+    int k = 1;
+    while (k * 2 <= left && k * 2 <= steps_per_graph_cap) k *= 2;
+    RKB_TRY(cudaGraphLaunch(graph_for(k), stream_));
+    left -= k;
+  }
+  RKB_TRY(cudaEventRecord(e1, stream_));
+  RKB_TRY(cudaEventSynchronize(e1));
+  float f = 0.0f;
+  RKB_TRY(cudaEventElapsedTime(&f, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = f;
+  pull_ctl();
+  stepped_ = true;
+  host_is_current_ = false;
+  return 0;
+}
+
+int Sim::profile_steps(int n, double out[5]) {
+  if (n <= 0) return -2;
+  if (prepare_run(1, 0.0, n) != 0) return -1;
+  cudaEvent_t ev[5];
+  for (auto& e : ev) RKB_TRY(cudaEventCreate(&e));
+  double acc[4] = {0, 0, 0, 0};
+  for (int s = 0; s < n; ++s) {
+    RKB_TRY(cudaEventRecord(ev[0], stream_));
+    RKB_TRY(launch_bc(args_, 1, stream_));
+    RKB_TRY(cudaEventRecord(ev[1], stream_));
+    RKB_TRY(launch_stage_only(args_, 1, stream_));
+    RKB_TRY(cudaEventRecord(ev[2], stream_));
+    RKB_TRY(launch_bc(args_, 2, stream_));
+    RKB_TRY(cudaEventRecord(ev[3], stream_));
+    RKB_TRY(launch_stage_only(args_, 2, stream_));
+    RKB_TRY(cudaEventRecord(ev[4], stream_));
+    RKB_TRY(cudaEventSynchronize(ev[4]));
+    for (int k = 0; k < 4; ++k) {
+      float f = 0.0f;
+      RKB_TRY(cudaEventElapsedTime(&f, ev[k], ev[k + 1]));
+      acc[k] += f;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (int k = 0; k < 4; ++k) out[k] = acc[k] / n;
+  out[4] = (double)launches_per_step(args_);
+  pull_ctl();
+  stepped_ = true;
+  host_is_current_ = false;
+  return 0;
+}
+
+int Sim::step(int n) {
+  if (n <= 0) return 0;
+  return run(1, 0.0, n);
+}
+
+int Sim::advance(double target) {
+  if (!(t_current_ < target - 1.0e-10)) return 0;
+  return run(0, target, 0);
+}
+
+void Sim::mass_budget(double out[3]) {
+  if (dmem_) {
+    cudaMemcpyAsync(hctl_, args_.ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, stream_);
+    cudaStreamSynchronize(stream_);
+  }
+  out[0] = hctl_->mass_out;
+  out[1] = hctl_->mass_src;
+  out[2] = 0.0;
+}
+
+}  // namespace rkb

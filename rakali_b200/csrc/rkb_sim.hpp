@@ -1,0 +1,105 @@
+// One structured simulation: host mirror, device state and the step driver.
+//
+// The host side mirrors the reference handle's state machine
+// (src/api/rki_api.F90:48-150, on_device / host_is_current) so the zero-copy
+// field views behave the same: reading a field pointer brings the device
+// state home, and the next step uploads whatever the caller left in it.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "rkb_config.hpp"
+#include "rkb_kernels.h"
+
+namespace rkb {
+
+class Sim {
+ public:
+  Sim() = default;
+  ~Sim();
+  Sim(const Sim&) = delete;
+  Sim& operator=(const Sim&) = delete;
+
+  // rki_create / rki_create_from_string: parse, validate, allocate host state.
+  int create(const std::string& namelist_text, std::string& err);
+  // rki_finalize: ghost-fill the bed, initial condition, BCs, device upload.
+  int finalize(std::string& err);
+
+  int step(int n);                 // rki_step
+  // n steps bracketed by CUDA events on the simulation's stream; *ms = elapsed.
+  int time_steps(int n, double* ms);
+  // n steps launched one kernel at a time with events between launches;
+  // out[k] = mean ms of launch k of a step (bc1, stage1, bc2, stage2 in order,
+  // the boundary launches summed), out[4] = launches per step.
+  int profile_steps(int n, double out[5]);
+  int advance(double target_time);  // rki_advance
+
+  // Field access (F-order host arrays with ghosts).  `which`: 0 h, 1 hu,
+  // 2 hv, 3 b, 4 h0, 5 hu0, 6 hv0.
+  double* field_ptr(int which);
+  int set_interior(int which, const double* data, int nx, int ny);  // setters
+  int set_forcing(int which, const double* data, int nx, int ny);   // 0 wx, 1 wy, 2 atm, 3 precip
+  void sync_host();          // rki_sync_host
+  void sync_from_device();   // rki_sync_from_device
+
+  // bookkeeping the API reads
+  double time() const { return t_current_; }
+  double dt() const { return dt_; }
+  int step_count() const { return step_count_; }
+  void mass_budget(double out[3]);
+
+  Config cfg;
+  Grid g{};
+  bool is_initialised = false, is_finalised = false;
+  bool user_set_bathymetry = false, user_set_h = false;
+  BcParams bc{};
+  Physics phys{};
+  bool params_dirty = true;
+  int tile = kTile32x8;
+  int steps_per_graph_cap = 256;
+
+  // Device pointers for the torch / kernel-level paths.
+  StepArgs device_args() const { return args_; }
+  int current_buffer() const { return cur_; }
+  cudaStream_t stream() const { return stream_; }
+  int ensure_device();
+  void ensure_host();
+
+ private:
+  int alloc_device(std::string& err);
+  void free_device();
+  int upload_state();
+  int upload_params();
+  int upload_forcing();
+  int run(int mode, double target, int nsteps);
+  int prepare_run(int mode, double target, int nsteps);
+  cudaGraphExec_t graph_for(int steps);
+  void pull_ctl();
+  void init_condition();
+
+  size_t ncell_ = 0;
+  double* hf_[7] = {};  // pinned host fields
+  std::vector<double> forcing_[6];  // wind_x, wind_y, atm, precip, heat_flux, e-p (contiguous)
+  std::vector<double> eta_old_[4];
+  bool forcing_dev_ = false;
+
+  int device_ = 0;
+  cudaStream_t stream_ = nullptr;
+  void* dmem_ = nullptr;
+  StepArgs args_{};
+  StepCtl* hctl_ = nullptr;  // pinned
+  bool on_device_ = false, host_is_current_ = false, stepped_ = false;
+  int cur_ = 0;
+  double t_current_ = 0.0, dt_ = 0.0;
+  int step_count_ = 0;
+
+  struct GraphEntry {
+    int steps, hllc, tile;
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+  };
+  std::vector<GraphEntry> graphs_;
+};
+
+}  // namespace rkb

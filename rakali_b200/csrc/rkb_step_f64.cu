@@ -1,0 +1,784 @@
+// FP64 kernels of the structured SSP-RK2 step (sm_100a).
+//
+// One step is four launches, all reading their clock from the device-side
+// StepCtl so a whole chunk of steps can be captured once in a CUDA graph:
+//
+//   bc_we / bc_sn (stage 1, time t)   ghost fill of U^n          rki_boundary.F90:40-218
+//   stage<1>                          U^n -> U*                  rki_kernel_flux.F90 + rki_kernel_fused.F90:164-303
+//   bc_we / bc_sn (stage 2, t + dt)   ghost fill of U*           (ghosts also copied into the U^{n+1} buffer)
+//   stage<2>                          U*, U^n -> U^{n+1}         rki_kernel_fused.F90:305-471
+//
+// The CFL reduction (rki_kernel_timestep.F90:16-74) is folded into the
+// stage-2 epilogue; the first launch of the next step turns it into dt.
+// The boundary mass-out sums (rki_solver.F90:507-537) are per-block partials
+// reduced in a fixed order by the last block of stage 2.
+#include "rkb_face.cuh"
+#include "rkb_kernels.h"
+
+namespace rkb {
+
+// ---------------------------------------------------------------------------
+// Step control
+// ---------------------------------------------------------------------------
+
+// Decide whether this step runs and its dt (rki_api.F90:385-410 loop test,
+// rki_solver.F90:731-748).  Reads only fields that stay fixed during a step,
+// so every thread of the first launch computes the same answer.
+__device__ __forceinline__ bool step_begin(const StepCtl* c, const Physics* p, const Grid& g,
+                                           double& dt) {
+  double dt_max;
+  bool active;
+  if (c->mode == 0) {
+    active = c->t < c->target - 1.0e-10;
+    dt_max = c->target - c->t;
+  } else {
+    active = c->remaining > 0;
+    dt_max = p->t_end - c->t;
+  }
+  dt = c->dt_prev;
+  if (!active) return false;
+  if (p->dt_fixed > 0.0) {
+    dt = dmin(p->dt_fixed, dt_max);
+  } else if (c->step_count % p->cfl_interval == 0 || c->dt_prev <= 0.0) {
+    dt = cfl_dt(c->msx, c->msy, g, p->cfl) * p->ssp_coeff;
+    dt = dmin(dt, dt_max);
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Boundary conditions (rki_boundary.F90:40-552)
+// ---------------------------------------------------------------------------
+
+struct Edge {
+  int ig0, jg0, din, djn, dit, djt, n_tan;
+  double sgn;
+  bool normal_u;
+};
+
+// Edge geometry of rki_boundary.F90:75-84 in 0-based indices.
+__device__ __forceinline__ Edge make_edge(int w, const Grid& g) {
+  Edge e;
+  switch (w) {
+    case 0: e = {g.ng - 1, 0, -1, 0, 0, 1, g.nyt, -1.0, true}; break;
+    case 1: e = {g.nxt - g.ng, 0, 1, 0, 0, 1, g.nyt, 1.0, true}; break;
+    case 2: e = {0, g.ng - 1, 0, -1, 1, 0, g.nxt, -1.0, false}; break;
+    default: e = {0, g.nyt - g.ng, 0, 1, 1, 0, g.nxt, 1.0, false}; break;
+  }
+  return e;
+}
+
+__device__ __forceinline__ double tidal_eta(const BcParams* bc, double time) {
+  double eta = 0.0;
+  if (bc->n_tidal > 0) {
+    for (int n = 0; n < bc->n_tidal; ++n)
+      eta = eta + bc->amp[n] * cos(bc->omega[n] * time - bc->phase[n]);
+  } else if (bc->tidal_period > 0.0) {
+    eta = bc->tidal_amplitude * sin(kTwoPi * time / bc->tidal_period);
+  }
+  return eta;
+}
+
+// One thread per tangential position t of an edge, looping over the ghost
+// layers k (so the Chapman surface refresh of position t is race-free).
+// The kernel fills edges [e0, e0 + gridDim.y).  Ghost values go to `h/hu/hv`
+// and, when `h2` is non-null, also to a second buffer.
+__global__ void k_bc(Grid g, StepCtl* ctl, const Physics* phys, const BcParams* bc, int stage,
+                     int e0, FieldSet U0, FieldSet U1, FieldSet S, double* __restrict__ b,
+                     double* eta_old_w, double* eta_old_e, double* eta_old_s, double* eta_old_n,
+                     int first_launch) {
+  double dt;
+  bool active = step_begin(ctl, phys, g, dt);
+  if (first_launch) {
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+      ctl->active = active ? 1 : 0;
+      ctl->dt = dt;
+    }
+  }
+  if (!active) return;
+  const int w = e0 + blockIdx.y;
+  const int type = bc->type[w];
+  if (type == kNested) return;
+  const Edge e = make_edge(w, g);
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= e.n_tan) return;
+
+  const double time = stage == 1 ? ctl->t : ctl->t + dt;
+  const int cur = ctl->cur;
+  FieldSet F = stage == 1 ? (cur ? U1 : U0) : S;
+  double* h2 = nullptr;
+  double* hu2 = nullptr;
+  double* hv2 = nullptr;
+  if (stage == 2) {
+    FieldSet N = cur ? U0 : U1;
+    h2 = N.h; hu2 = N.hu; hv2 = N.hv;
+  }
+  double* h = F.h;
+  double* hu = F.hu;
+  double* hv = F.hv;
+
+  // ghost (k) and first interior cell along the inward normal
+  const int ii = e.ig0 + t * e.dit - e.din;
+  const int ji = e.jg0 + t * e.djt - e.djn;
+
+  auto put = [&](int ig, int jg, double vh, double vu, double vv) {
+    const size_t q = g.at(ig, jg);
+    h[q] = vh; hu[q] = vu; hv[q] = vv;
+    if (h2) { h2[q] = vh; hu2[q] = vu; hv2[q] = vv; }
+  };
+
+  if (type == kWall || type == kSponge) {
+    // bc_wall_edge :220-291 (bed and surface mirrored, normal momentum negated)
+    for (int k = 1; k <= g.ng; ++k) {
+      const int ig = e.ig0 + (k - 1) * e.din + t * e.dit;
+      const int jg = e.jg0 + (k - 1) * e.djn + t * e.djt;
+      const int im = ig - (2 * k - 1) * e.din;
+      const int jm = jg - (2 * k - 1) * e.djn;
+      const size_t m = g.at(im, jm);
+      const double bm = b[m];
+      b[g.at(ig, jg)] = bm;
+      const double vh = pos(h[m] + bm - bm);
+      double vu, vv;
+      if (e.normal_u) { vu = -hu[m]; vv = hv[m]; } else { vv = -hv[m]; vu = hu[m]; }
+      put(ig, jg, vh, vu, vv);
+    }
+    return;
+  }
+
+  const size_t qi = g.at(ii, ji);
+  const double hi = h[qi];
+  const double qu = hu[qi];
+  const double qv = hv[qi];
+  if (type == kOpen || type == kTidal) {
+    // bc_flather_edge :293-345
+    const bool prescribe = type == kTidal;
+    const double eta_ext = prescribe ? tidal_eta(bc, time) : 0.0;
+    const double ei = hi + b[qi];
+    const double hmax = dmax(hi, 1.0e-6);
+    const double c = sqrt(kG * hmax);
+    for (int k = 1; k <= g.ng; ++k) {
+      const int ig = e.ig0 + (k - 1) * e.din + t * e.dit;
+      const int jg = e.jg0 + (k - 1) * e.djn + t * e.djt;
+      const double hg = prescribe ? pos(eta_ext - b[g.at(ig, jg)]) : hi;
+      if (e.normal_u)
+        put(ig, jg, hg, hg * (qu / hmax + e.sgn * c * (ei - eta_ext) / hmax), qv);
+      else
+        put(ig, jg, hg, qu, hg * (qv / hmax + e.sgn * c * (ei - eta_ext) / hmax));
+    }
+  } else if (type == kInflow) {
+    // bc_inflow_edge :347-390
+    const double in_sgn = -e.sgn;
+    for (int k = 1; k <= g.ng; ++k) {
+      const int ig = e.ig0 + (k - 1) * e.din + t * e.dit;
+      const int jg = e.jg0 + (k - 1) * e.djn + t * e.djt;
+      if (e.normal_u)
+        put(ig, jg, hi, in_sgn * hi * bc->inflow_velocity, qv);
+      else
+        put(ig, jg, hi, qu, in_sgn * hi * bc->inflow_velocity);
+    }
+  } else if (type == kDischarge) {
+    // bc_disch_edge :392-434
+    const double in_sgn = -e.sgn;
+    for (int k = 1; k <= g.ng; ++k) {
+      const int ig = e.ig0 + (k - 1) * e.din + t * e.dit;
+      const int jg = e.jg0 + (k - 1) * e.djn + t * e.djt;
+      if (e.normal_u)
+        put(ig, jg, hi, in_sgn * bc->discharge_flux, qv);
+      else
+        put(ig, jg, hi, qu, in_sgn * bc->discharge_flux);
+    }
+  } else if (type == kClamped) {
+    // bc_clamped_edge :436-469
+    for (int k = 1; k <= g.ng; ++k) {
+      const int ig = e.ig0 + (k - 1) * e.din + t * e.dit;
+      const int jg = e.jg0 + (k - 1) * e.djn + t * e.djt;
+      put(ig, jg, pos(bc->clamped_elevation - b[g.at(ig, jg)]), qu, qv);
+    }
+  } else if (type == kChapman) {
+    // bc_chapman_edge :471-552; every layer reads the surface stored before
+    // this call, then position t's surface is refreshed once.
+    double* eo = w == 0 ? eta_old_w : w == 1 ? eta_old_e : w == 2 ? eta_old_s : eta_old_n;
+    const double dd = e.normal_u ? g.dx : g.dy;
+    // The reference fills the ghosts once more before computing dt
+    // (rki_solver.F90:719); for Chapman that extra call refreshes the stored
+    // surface to the current interior one, which stage 1 then sees.
+    const double ei0 = hi + b[qi];
+    const double eov = stage == 1 ? ei0 : eo[t];
+    const double ei = hi + b[qi];
+    const double hmax = dmax(hi, 1.0e-6);
+    const double c = sqrt(kG * hmax);
+    const int i2 = ii - e.din;
+    const int j2 = ji - e.djn;
+    double eg;
+    if (dt > 0.0) {
+      const double detadt = (ei - eov) / dt;
+      double detadx = 0.0;
+      if (i2 >= 0 && i2 < g.nxt && j2 >= 0 && j2 < g.nyt) {
+        const size_t q2 = g.at(i2, j2);
+        detadx = (h[q2] + b[q2] - ei) / dd;
+      }
+      double cp = fabs(detadx) > 1.0e-10 ? -detadt / detadx : 0.0;
+      cp = pos(dmin(cp, c));
+      eg = eov - cp * dt / dd * (eov - ei);
+    } else {
+      eg = ei;
+    }
+    for (int k = 1; k <= g.ng; ++k) {
+      const int ig = e.ig0 + (k - 1) * e.din + t * e.dit;
+      const int jg = e.jg0 + (k - 1) * e.djn + t * e.djt;
+      const double hg = pos(eg - b[g.at(ig, jg)]);
+      if (e.normal_u)
+        put(ig, jg, hg, hg * (qu / hmax + e.sgn * c * (ei - eg) / hmax), qv);
+      else
+        put(ig, jg, hg, qu, hg * (qv / hmax + e.sgn * c * (ei - eg) / hmax));
+    }
+    eo[t] = ei;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// CFL reduction over the current state (used when no stage-2 epilogue has
+// produced it yet: after create or after the host changed the state).
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) {
+    double w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = w > v ? w : v;
+  }
+  return v;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = v + __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__global__ void k_max_speed(Grid g, StepCtl* ctl, FieldSet U0, FieldSet U1) {
+  const FieldSet F = ctl->cur ? U1 : U0;
+  const int nxp = g.nx_phys(), nyp = g.ny_phys();
+  const long long n = (long long)nxp * nyp;
+  double mx = 0.0, my = 0.0;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int i = g.ng + (int)(k % nxp);
+    const int j = g.ng + (int)(k / nxp);
+    const size_t q = g.at(i, j);
+    double sx, sy;
+    wave_speed(F.h[q], F.hu[q], F.hv[q], sx, sy);
+    if (sx > mx) mx = sx;
+    if (sy > my) my = sy;
+  }
+  mx = warp_max(mx);
+  my = warp_max(my);
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_pos(&ctl->msx_next, mx);
+    atomic_max_pos(&ctl->msy_next, my);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned int done = atomicAdd(&ctl->ms_done_blocks, 1u);
+    if (done == gridDim.x - 1) {
+      __threadfence();
+      volatile StepCtl* vc = ctl;
+      ctl->msx = __longlong_as_double((long long)vc->msx_next);
+      ctl->msy = __longlong_as_double((long long)vc->msy_next);
+      ctl->msx_next = 0ull;
+      ctl->msy_next = 0ull;
+      ctl->ms_valid = 1;
+      ctl->ms_done_blocks = 0u;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Fused stage kernel
+// ---------------------------------------------------------------------------
+
+// Shared-memory plan of one TX x TY tile (doubles):
+//   tile  5 x (TX+4)(TY+4)   h, hu, hv, b, eta with a 2-cell halo
+//   sx    3 x (TX+2) TY      limited x-slopes of eta, hu, hv
+//   sy    3 x TX (TY+2)      limited y-slopes
+//   fx    6 x (TX+1) TY      x-face fluxes + well-balanced terms
+//   fy    6 x TX (TY+1)      y-face fluxes + well-balanced terms
+template <int TX, int TY>
+struct StageSmem {
+  static constexpr int TW = TX + 4, TH = TY + 4;
+  static constexpr int NT = TW * TH;
+  static constexpr int NSX = (TX + 2) * TY;
+  static constexpr int NSY = TX * (TY + 2);
+  static constexpr int NFX = (TX + 1) * TY;
+  static constexpr int NFY = TX * (TY + 1);
+  static constexpr int DOUBLES = 5 * NT + 3 * NSX + 3 * NSY + 6 * NFX + 6 * NFY;
+  static constexpr size_t BYTES = sizeof(double) * (size_t)DOUBLES;
+};
+
+// Pointwise sources after the Euler update: Manning friction, wind,
+// pressure gradient, Coriolis, precipitation (rki_kernel_fused.F90:121-154).
+__device__ __forceinline__ void sources(double& h, double& u, double& v, const Physics* p, double dt,
+                                        double n_sq, double cosf, double sinf, bool has_cor,
+                                        const Grid& g, int i, int j, const Forcing& fo) {
+  if (h > kDry) {
+    if (p->manning_n > 0.0) {
+      const double uu = u / h;
+      const double vv = v / h;
+      const double speed = sqrt(uu * uu + vv * vv);
+      const double cf = kG * n_sq / pow(h, 1.0 / 3.0);
+      const double den = 1.0 + dt * cf * speed / h;
+      u = u / den;
+      v = v / den;
+    }
+    if (p->forcing_active) {
+      const size_t q = g.at(i, j);
+      u = u + dt * fo.wind_x[q] / kRho;
+      v = v + dt * fo.wind_y[q] / kRho;
+      const double dpdx = (fo.atm[g.at(i + 1, j)] - fo.atm[g.at(i - 1, j)]) / (2.0 * g.dx);
+      const double dpdy = (fo.atm[g.at(i, j + 1)] - fo.atm[g.at(i, j - 1)]) / (2.0 * g.dy);
+      u = u - dt * h * dpdx / kRho;
+      v = v - dt * h * dpdy / kRho;
+    }
+    if (has_cor) {
+      const double uo = u, vo = v;
+      u = uo * cosf + vo * sinf;
+      v = -(uo * sinf) + vo * cosf;
+    }
+  }
+  if (p->forcing_active) h = h + dt * fo.precip[g.at(i, j)];
+}
+
+// Sponge relaxation of interior cell (i, j) (rki_kernel_sponge.F90:16-88).
+__device__ __forceinline__ void sponge(double& h, double& u, double& v, const BcParams* bc,
+                                       const Grid& g, int i, int j, double dt) {
+  const int sw = bc->sponge_width;
+  if (sw <= 0 || bc->sponge_strength <= 0.0) return;
+  const int i0 = g.ng, i1 = g.nxt - g.ng - 1, j0 = g.ng, j1 = g.nyt - g.ng - 1;
+  int dmn = sw + 1;
+  if (bc->type[0] == kSponge && i - i0 < sw && i - i0 < dmn) dmn = i - i0;
+  if (bc->type[1] == kSponge && i1 - i < sw && i1 - i < dmn) dmn = i1 - i;
+  if (bc->type[2] == kSponge && j - j0 < sw && j - j0 < dmn) dmn = j - j0;
+  if (bc->type[3] == kSponge && j1 - j < sw && j1 - j < dmn) dmn = j1 - j;
+  if (dmn < sw) {
+    const double ratio = (double)(sw - dmn) / (double)sw;
+    const double alpha = bc->sponge_strength * ratio * ratio;
+    h = h - dt * alpha * (h - bc->sponge_h_ref);
+    u = u - dt * alpha * u;
+    v = v - dt * alpha * v;
+  }
+}
+
+// STAGE 1: U^n (buffer cur) -> U* (scratch S).
+// STAGE 2: U* (S) and U^n (buffer cur) -> U^{n+1} (buffer cur^1).
+// STAGE 0: flux divergence only (kernel-level API): writes flux/mass-flux
+//          arrays from `in`, no update.
+template <int TX, int TY, bool HLLC, int STAGE>
+__global__ void __launch_bounds__(TX * TY)
+    k_stage(Grid g, StepCtl* ctl, const Physics* phys, const BcParams* bcp, FieldSet U0,
+            FieldSet U1, FieldSet S, const double* __restrict__ b, Forcing fo,
+            double* __restrict__ partials, FluxOut fl) {
+  using SM = StageSmem<TX, TY>;
+  constexpr int TW = SM::TW;
+  constexpr int NTH = TX * TY;
+  extern __shared__ double smem[];
+  double* th = smem;
+  double* tu = th + SM::NT;
+  double* tv = tu + SM::NT;
+  double* tb = tv + SM::NT;
+  double* te = tb + SM::NT;
+  double* sxe = te + SM::NT;
+  double* sxu = sxe + SM::NSX;
+  double* sxv = sxu + SM::NSX;
+  double* sye = sxv + SM::NSX;
+  double* syu = sye + SM::NSY;
+  double* syv = syu + SM::NSY;
+  double* fxa = syv + SM::NSY;  // 6 arrays of NFX: fh, fqx, fqy, wbR, hL2, pL2
+  double* fya = fxa + 6 * SM::NFX;
+
+  double dt = 0.0;
+  int cur = 0;
+  if (STAGE != 0) {
+    if (!ctl->active) return;
+    dt = ctl->dt;
+    cur = ctl->cur;
+  }
+  const FieldSet in = STAGE == 2 ? S : (cur ? U1 : U0);
+
+  const int tid = threadIdx.x;
+  const int gx0 = g.ng + blockIdx.x * TX;  // first interior cell of the tile
+  const int gy0 = g.ng + blockIdx.y * TY;
+
+  // 1. tile load with halo (ghost cells come from the BC launches)
+  for (int k = tid; k < SM::NT; k += NTH) {
+    const int x = k % TW, y = k / TW;
+    const int gi = gx0 - 2 + x, gj = gy0 - 2 + y;
+    double vh = 0.0, vu = 0.0, vv = 0.0, vb = 0.0;
+    if (gi < g.nxt && gj < g.nyt) {
+      const size_t q = g.at(gi, gj);
+      vh = in.h[q]; vu = in.hu[q]; vv = in.hv[q]; vb = b[q];
+    }
+    th[k] = vh; tu[k] = vu; tv[k] = vv; tb[k] = vb;
+    te[k] = vh + vb;
+  }
+  __syncthreads();
+
+  // 2. limited slopes: x for cells c in [-1, TX], y for rows r in [-1, TY]
+  for (int k = tid; k < SM::NSX + SM::NSY; k += NTH) {
+    if (k < SM::NSX) {
+      const int c = k % (TX + 2) - 1, r = k / (TX + 2);
+      const int q = (r + 2) * TW + (c + 2);
+      cell_slope(th[q - 1], th[q], th[q + 1], te[q - 1], te[q], te[q + 1], tu[q - 1], tu[q],
+                 tu[q + 1], tv[q - 1], tv[q], tv[q + 1], sxe[k], sxu[k], sxv[k]);
+    } else {
+      const int kk = k - SM::NSX;
+      const int c = kk % TX, r = kk / TX - 1;
+      const int q = (r + 2) * TW + (c + 2);
+      cell_slope(th[q - TW], th[q], th[q + TW], te[q - TW], te[q], te[q + TW], tu[q - TW], tu[q],
+                 tu[q + TW], tv[q - TW], tv[q], tv[q + TW], sye[kk], syu[kk], syv[kk]);
+    }
+  }
+  __syncthreads();
+
+  // 3. faces, each evaluated once
+  for (int k = tid; k < SM::NFX + SM::NFY; k += NTH) {
+    FaceOut o;
+    if (k < SM::NFX) {
+      const int c = k % (TX + 1), r = k / (TX + 1);  // face between c-1 and c
+      const int qL = (r + 2) * TW + (c + 1), qR = qL + 1;
+      const int sL = r * (TX + 2) + c, sR = sL + 1;  // slope index of cell c-1 and c
+      face_flux<0, HLLC>(te[qL] + 0.5 * sxe[sL], tu[qL] + 0.5 * sxu[sL], tv[qL] + 0.5 * sxv[sL],
+                         tb[qL], te[qR] - 0.5 * sxe[sR], tu[qR] - 0.5 * sxu[sR],
+                         tv[qR] - 0.5 * sxv[sR], tb[qR], o);
+      fxa[k] = o.fh;
+      fxa[SM::NFX + k] = o.fqx;
+      fxa[2 * SM::NFX + k] = o.fqy;
+      fxa[3 * SM::NFX + k] = o.wbR;
+      fxa[4 * SM::NFX + k] = o.hL2;
+      fxa[5 * SM::NFX + k] = o.pL2;
+    } else {
+      const int kk = k - SM::NFX;
+      const int c = kk % TX, r = kk / TX;  // face between rows r-1 and r
+      const int qB = (r + 1) * TW + (c + 2), qT = qB + TW;
+      const int sB = r * TX + c, sT = sB + TX;  // y-slope index of rows r-1 and r
+      face_flux<1, HLLC>(te[qB] + 0.5 * sye[sB], tu[qB] + 0.5 * syu[sB], tv[qB] + 0.5 * syv[sB],
+                         tb[qB], te[qT] - 0.5 * sye[sT], tu[qT] - 0.5 * syu[sT],
+                         tv[qT] - 0.5 * syv[sT], tb[qT], o);
+      fya[kk] = o.fh;
+      fya[SM::NFY + kk] = o.fqx;
+      fya[2 * SM::NFY + kk] = o.fqy;
+      fya[3 * SM::NFY + kk] = o.wbR;
+      fya[4 * SM::NFY + kk] = o.hL2;
+      fya[5 * SM::NFY + kk] = o.pL2;
+    }
+  }
+  __syncthreads();
+
+  // 4. cell update: one cell per thread
+  const int c = tid % TX, r = tid / TX;
+  const int i = gx0 + c, j = gy0 + r;
+  const bool valid = i < g.nxt - g.ng && j < g.nyt - g.ng;
+  const int fl_ = r * (TX + 1) + c, fr_ = fl_ + 1;
+  const int fb_ = r * TX + c, ft_ = fb_ + TX;
+  const double dx = g.dx, dy = g.dy;
+  const double o_fh = -((fxa[fr_] - fxa[fl_]) / dx) - (fya[ft_] - fya[fb_]) / dy;
+  const double o_fhu =
+      -((fxa[SM::NFX + fr_] - fxa[SM::NFX + fl_]) / dx) -
+      (fya[SM::NFY + ft_] - fya[SM::NFY + fb_]) / dy -
+      kHalfG * (fxa[3 * SM::NFX + fl_] - fxa[4 * SM::NFX + fr_] + fxa[5 * SM::NFX + fr_]) / dx;
+  const double o_fhv =
+      -((fxa[2 * SM::NFX + fr_] - fxa[2 * SM::NFX + fl_]) / dx) -
+      (fya[2 * SM::NFY + ft_] - fya[2 * SM::NFY + fb_]) / dy -
+      kHalfG * (fya[3 * SM::NFY + fb_] - fya[4 * SM::NFY + ft_] + fya[5 * SM::NFY + ft_]) / dy;
+
+  double part = 0.0, sponge_d = 0.0, wsx = 0.0, wsy = 0.0;
+  if (valid) {
+    const size_t q = g.at(i, j);
+    if (STAGE == 0) {
+      fl.flux_h[q] = o_fh;
+      fl.flux_hu[q] = o_fhu;
+      fl.flux_hv[q] = o_fhv;
+      if (fl.mflux_x) {
+        fl.mflux_x[q] = fxa[fr_];
+        if (i == g.ng) fl.mflux_x[q - 1] = fxa[fl_];
+      }
+      if (fl.mflux_y) {
+        fl.mflux_y[q] = fya[ft_];
+        if (j == g.ng) fl.mflux_y[q - g.pitch] = fya[fb_];
+      }
+    } else {
+      const int qc = (r + 2) * TW + (c + 2);
+      double a = th[qc], u = tu[qc], v = tv[qc];
+      a = a + dt * o_fh;
+      u = u + dt * o_fhu;
+      v = v + dt * o_fhv;
+      protect(a, u, v);
+      const double n_sq = phys->manning_n * phys->manning_n;
+      const bool has_cor = fabs(phys->coriolis_f) > 1.0e-20;
+      double cosf = 0.0, sinf = 0.0;
+      if (has_cor) {
+        cosf = cos(phys->coriolis_f * dt);
+        sinf = sin(phys->coriolis_f * dt);
+      }
+      sources(a, u, v, phys, dt, n_sq, cosf, sinf, has_cor, g, i, j, fo);
+      FieldSet out;
+      if (STAGE == 1) {
+        out = S;
+      } else {
+        // RK2 average with U^n and the second clamp (rki_kernel_fused.F90:435-463)
+        const FieldSet old = cur ? U1 : U0;
+        out = cur ? U0 : U1;
+        a = 0.5 * (old.h[q] + a);
+        u = 0.5 * (old.hu[q] + u);
+        v = 0.5 * (old.hv[q] + v);
+        protect(a, u, v);
+      }
+      const double h_pre_sponge = a;
+      sponge(a, u, v, bcp, g, i, j, dt);
+      out.h[q] = a;
+      out.hu[q] = u;
+      out.hv[q] = v;
+      part = o_fh;
+      sponge_d = a - h_pre_sponge;
+      if (STAGE == 2) wave_speed(a, u, v, wsx, wsy);
+    }
+  }
+  if (STAGE == 0) return;
+
+  // 5. block partials (fixed order) and the CFL maxima of the new state
+  part = warp_sum(part);
+  sponge_d = warp_sum(sponge_d);
+  if (STAGE == 2) {
+    wsx = warp_max(wsx);
+    wsy = warp_max(wsy);
+    if ((tid & 31) == 0) {
+      atomic_max_pos(&ctl->msx_next, wsx);
+      atomic_max_pos(&ctl->msy_next, wsy);
+    }
+  }
+  __shared__ double red[2][NTH / 32];
+  if ((tid & 31) == 0) {
+    red[0][tid >> 5] = part;
+    red[1][tid >> 5] = sponge_d;
+  }
+  __syncthreads();
+  const unsigned int nblocks = gridDim.x * gridDim.y;
+  const unsigned int bid = blockIdx.y * gridDim.x + blockIdx.x;
+  if (tid == 0) {
+    double s0 = 0.0, s1 = 0.0;
+    for (int w = 0; w < NTH / 32; ++w) {
+      s0 = s0 + red[0][w];
+      s1 = s1 + red[1][w];
+    }
+    double* P = partials + (size_t)(STAGE - 1) * 2 * nblocks;
+    P[bid] = s0;
+    P[nblocks + bid] = s1;
+  }
+  if (STAGE != 2) return;
+
+  // 6. last block closes the step
+  __shared__ bool last;
+  if (tid == 0) {
+    __threadfence();
+    last = atomicAdd(&ctl->done_blocks, 1u) == nblocks - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // fixed-order sums of the per-block partials, one warp per sum
+  const double area = g.dx * g.dy;
+  volatile double* VP = partials;
+  double sums[4];
+  for (int s = 0; s < 4; ++s) {
+    double acc = 0.0;
+    if (tid < 32)
+      for (unsigned int k = tid; k < nblocks; k += 32) acc = acc + VP[(size_t)s * nblocks + k];
+    sums[s] = warp_sum(acc);
+  }
+  if (tid == 0) {
+    volatile StepCtl* vc = ctl;
+    // mass budget in the reference's order: stage 1 then stage 2
+    double mo = ctl->mass_out;
+    mo = mo - 0.5 * dt * sums[0] * area;
+    mo = mo - 0.5 * dt * sums[2] * area;
+    ctl->mass_out = mo;
+    double ms = ctl->mass_src;
+    if (phys->forcing_active) ms = ms + 0.5 * dt * ctl->precip_sum * area;
+    ms = ms + 0.5 * sums[1] * area;
+    if (phys->forcing_active) ms = ms + 0.5 * dt * ctl->precip_sum * area;
+    ms = ms + 0.5 * sums[3] * area;
+    ctl->mass_src = ms;
+    ctl->msx = __longlong_as_double((long long)vc->msx_next);
+    ctl->msy = __longlong_as_double((long long)vc->msy_next);
+    ctl->msx_next = 0ull;
+    ctl->msy_next = 0ull;
+    ctl->ms_valid = 1;
+    ctl->t = ctl->t + dt;
+    ctl->dt_prev = dt;
+    ctl->step_count = ctl->step_count + 1;
+    ctl->remaining = ctl->remaining - 1;
+    ctl->steps_run = ctl->steps_run + 1;
+    ctl->cur = cur ^ 1;
+    ctl->done_blocks = 0u;
+  }
+}
+
+}  // namespace rkb
+
+// ---------------------------------------------------------------------------
+// Host launch wrappers
+// ---------------------------------------------------------------------------
+
+namespace rkb {
+
+const char* tile_name(int tile) {
+  switch (tile) {
+    case kTile32x8: return "32x8";
+    case kTile32x16: return "32x16";
+    case kTile64x4: return "64x4";
+    default: return "16x16";
+  }
+}
+
+void tile_dims(int tile, int& tx, int& ty) {
+  switch (tile) {
+    case kTile32x8: tx = 32; ty = 8; break;
+    case kTile32x16: tx = 32; ty = 16; break;
+    case kTile64x4: tx = 64; ty = 4; break;
+    default: tx = 16; ty = 16; break;
+  }
+}
+
+static dim3 stage_grid(const Grid& g, int tile) {
+  int tx, ty;
+  tile_dims(tile, tx, ty);
+  return dim3((unsigned)((g.nx_phys() + tx - 1) / tx), (unsigned)((g.ny_phys() + ty - 1) / ty));
+}
+
+size_t partials_doubles(const Grid& g, int tile) {
+  dim3 d = stage_grid(g, tile);
+  return 4 * (size_t)d.x * (size_t)d.y;
+}
+
+template <int TX, int TY, bool HLLC, int STAGE>
+static cudaError_t launch_stage_t(const StepArgs& a, FluxOut fl, cudaStream_t s) {
+  using SM = StageSmem<TX, TY>;
+  auto kern = k_stage<TX, TY, HLLC, STAGE>;
+  dim3 grid = stage_grid(a.g, a.tile);
+  kern<<<grid, TX * TY, SM::BYTES, s>>>(a.g, a.ctl, a.phys, a.bc, a.U0, a.U1, a.S, a.b, a.fo,
+                                        a.partials, fl);
+  return cudaGetLastError();
+}
+
+template <int TX, int TY, bool HLLC>
+static cudaError_t configure_t() {
+  cudaError_t e = cudaSuccess;
+  const int bytes = (int)StageSmem<TX, TY>::BYTES;
+  e = cudaFuncSetAttribute(k_stage<TX, TY, HLLC, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_stage<TX, TY, HLLC, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_stage<TX, TY, HLLC, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  return e;
+}
+
+cudaError_t configure_kernels(int tile, int hllc) {
+  const bool h = hllc != 0;
+  switch (tile) {
+    case kTile32x8: return h ? configure_t<32, 8, true>() : configure_t<32, 8, false>();
+    case kTile32x16: return h ? configure_t<32, 16, true>() : configure_t<32, 16, false>();
+    case kTile64x4: return h ? configure_t<64, 4, true>() : configure_t<64, 4, false>();
+    default: return h ? configure_t<16, 16, true>() : configure_t<16, 16, false>();
+  }
+}
+
+template <int STAGE>
+static cudaError_t launch_stage(const StepArgs& a, FluxOut fl, cudaStream_t s) {
+  const bool h = a.hllc != 0;
+  switch (a.tile) {
+    case kTile32x8:
+      return h ? launch_stage_t<32, 8, true, STAGE>(a, fl, s) : launch_stage_t<32, 8, false, STAGE>(a, fl, s);
+    case kTile32x16:
+      return h ? launch_stage_t<32, 16, true, STAGE>(a, fl, s) : launch_stage_t<32, 16, false, STAGE>(a, fl, s);
+    case kTile64x4:
+      return h ? launch_stage_t<64, 4, true, STAGE>(a, fl, s) : launch_stage_t<64, 4, false, STAGE>(a, fl, s);
+    default:
+      return h ? launch_stage_t<16, 16, true, STAGE>(a, fl, s) : launch_stage_t<16, 16, false, STAGE>(a, fl, s);
+  }
+}
+
+cudaError_t launch_bc(const StepArgs& a, int stage, cudaStream_t s) {
+  const Grid& g = a.g;
+  const int tpb = 128;
+  // Opposite edges may run in one launch only when neither reads cells the
+  // other writes, i.e. when the interior is at least max(nghost, 2) wide.
+  const bool pair_x = g.nx_phys() >= (g.ng > 2 ? g.ng : 2);
+  const bool pair_y = g.ny_phys() >= (g.ng > 2 ? g.ng : 2);
+  int first = stage == 1 ? 1 : 0;
+  auto go = [&](int e0, int count, int n_tan) {
+    dim3 grid((unsigned)((n_tan + tpb - 1) / tpb), (unsigned)count);
+    k_bc<<<grid, tpb, 0, s>>>(g, a.ctl, a.phys, a.bc, stage, e0, a.U0, a.U1, a.S, a.b,
+                              a.eta_old[0], a.eta_old[1], a.eta_old[2], a.eta_old[3], first);
+    first = 0;
+  };
+  if (pair_x) {
+    go(0, 2, g.nyt);
+  } else {
+    go(0, 1, g.nyt);
+    go(1, 1, g.nyt);
+  }
+  if (pair_y) {
+    go(2, 2, g.nxt);
+  } else {
+    go(2, 1, g.nxt);
+    go(3, 1, g.nxt);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_step(const StepArgs& a, cudaStream_t s) {
+  FluxOut none{};
+  cudaError_t e = launch_bc(a, 1, s);
+  if (e != cudaSuccess) return e;
+  e = launch_stage<1>(a, none, s);
+  if (e != cudaSuccess) return e;
+  e = launch_bc(a, 2, s);
+  if (e != cudaSuccess) return e;
+  return launch_stage<2>(a, none, s);
+}
+
+cudaError_t launch_stage_only(const StepArgs& a, int stage, cudaStream_t s) {
+  FluxOut none{};
+  return stage == 1 ? launch_stage<1>(a, none, s) : launch_stage<2>(a, none, s);
+}
+
+int launches_per_step(const StepArgs& a) {
+  const Grid& g = a.g;
+  const int need = g.ng > 2 ? g.ng : 2;
+  const int bc = (g.nx_phys() >= need ? 1 : 2) + (g.ny_phys() >= need ? 1 : 2);
+  return 2 * bc + 2;
+}
+
+cudaError_t launch_max_speed(const StepArgs& a, cudaStream_t s) {
+  const long long n = (long long)a.g.nx_phys() * a.g.ny_phys();
+  long long blocks = (n + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  if (blocks < 1) blocks = 1;
+  k_max_speed<<<(unsigned)blocks, 256, 0, s>>>(a.g, a.ctl, a.U0, a.U1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_flux(const Grid& g, int hllc, FieldSet in, const double* b, FluxOut out,
+                        int tile, cudaStream_t s) {
+  StepArgs a{};
+  a.g = g;
+  a.U0 = in;
+  a.U1 = in;
+  a.S = in;
+  a.b = const_cast<double*>(b);
+  a.tile = tile;
+  a.hllc = hllc;
+  cudaError_t e = configure_kernels(tile, hllc);
+  if (e != cudaSuccess) return e;
+  return launch_stage<0>(a, out, s);
+}
+
+}  // namespace rkb

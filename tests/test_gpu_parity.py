@@ -1,0 +1,292 @@
+"""GPU parity of the B200 step against the CPU oracle, through the C ABI.
+
+FP64 tolerance: the north-star bar is 1e-12 relative.  Cases that use only
++ - * / sqrt are expected to be bit-identical (the kernels keep the
+reference's operation order and are built with --fmad=false); cases with
+friction (pow) or tidal forcing (cos/sin) may differ by libm rounding and
+are held to 1e-12.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from tests.helpers import G, compare_state, gaussian_bed, hump_depth, max_rel_diff, pair
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-12
+
+
+def test_config1_dam_break_bit_exact():
+    """200 x 100 dam break, dx = 10 m, HLLC, CFL 0.5, walls, 60 s."""
+    cfg = dict(nx=200, ny=100, dx=10.0, dy=10.0, t_end=60.0, cfl=0.5, use_hllc=True,
+               bc_west="wall", bc_east="wall", bc_south="wall", bc_north="wall")
+    sim, orc = pair(cfg)
+    with sim:
+        sim.advance(60.0)
+        orc.advance(60.0)
+        assert sim.step_count == orc.step_count
+        assert sim.time == orc.time
+        assert sim.dt == orc.dt
+        d = compare_state(sim, orc, rtol=0.0)
+        compare_state(sim, orc, rtol=0.0, fields=("h0", "hu0", "hv0"))
+        m0 = 0.5 * (2.0 + 1.0) * 200 * 100 * 100.0
+        assert abs(sim.h_phys.sum() * 100.0 - m0) / m0 < 1e-12
+        assert d["h"] == 0.0
+
+
+@pytest.mark.parametrize("hllc", [False, True])
+@pytest.mark.parametrize("nghost", [2, 3])
+def test_wet_dry_islands_with_friction(hllc, nghost):
+    """Config-2 family at 192 x 160: emergent islands, hump, Manning n = 0.025."""
+    nx, ny, dx = 192, 160, 5.0
+    b = gaussian_bed(nx, ny, dx, dx, 32, seed=7, width=(20.0, 120.0))
+    h = hump_depth(b, dx, dx, width=80.0)
+    assert (h == 0.0).sum() > 50  # dry islands present
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, manning_n=0.025,
+               use_hllc=hllc, nghost=nghost)
+    sim, orc = pair(cfg, bathymetry=b, initial_h=h)
+    with sim:
+        sim.step(60)
+        orc.step(60)
+        assert sim.step_count == orc.step_count == 60
+        assert abs(sim.time - orc.time) <= 1e-12 * orc.time
+        compare_state(sim, orc, rtol=RTOL)
+
+
+def test_lake_at_rest_emergent_island_1e13():
+    """Flat surface over an irregular bed with dry islands stays at rest."""
+    nx, ny, dx = 160, 128, 5.0
+    b = gaussian_bed(nx, ny, dx, dx, 32, seed=3, width=(20.0, 120.0))
+    h = np.asfortranarray(np.maximum(0.0 - b, 0.0))
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, manning_n=0.025)
+    sim, orc = pair(cfg, bathymetry=b, initial_h=h)
+    with sim:
+        sim.step(200)
+        hp = sim.h_phys
+        wet = hp > 0.0
+        eta = hp + sim.b_phys
+        assert np.abs(eta[wet]).max() <= 1e-13
+        # momentum round-off stays far below the reference's 1e-12 * H * sqrt(g H)
+        assert np.abs(sim.hu_phys).max() <= 1e-11 and np.abs(sim.hv_phys).max() <= 1e-11
+        orc.step(200)
+        compare_state(sim, orc, rtol=RTOL)
+
+
+@pytest.mark.parametrize("edges", [
+    dict(bc_west="tidal", tidal_amplitude=0.5, tidal_period=600.0),
+    dict(bc_west="open", bc_east="open", bc_south="open", bc_north="open"),
+    dict(bc_west="inflow", inflow_velocity=0.3, bc_east="open"),
+    dict(bc_west="discharge", discharge_flux=0.8, bc_east="clamped", clamped_elevation=0.1),
+    dict(bc_west="chapman", bc_north="chapman"),
+    dict(bc_west="sponge", bc_east="sponge", sponge_width=6, sponge_strength=0.01,
+         sponge_h_ref=10.0),
+    dict(bc_west="nested", bc_south="open"),
+])
+def test_boundary_types(edges):
+    nx, ny, dx = 96, 64, 10.0
+    b = np.asfortranarray(np.tile(np.linspace(-12.0, -8.0, nx)[:, None], (1, ny)))
+    h = hump_depth(b, dx, dx, amp=0.4, width=60.0)
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, manning_n=0.02, **edges)
+    sim, orc = pair(cfg, bathymetry=b, initial_h=h)
+    with sim:
+        sim.advance(120.0)
+        orc.advance(120.0)
+        assert sim.step_count == orc.step_count
+        compare_state(sim, orc, rtol=RTOL)
+
+
+def test_multi_constituent_tide_setter():
+    nx, ny, dx = 80, 48, 20.0
+    b = np.asfortranarray(np.tile(np.linspace(-20.0, 2.0, nx)[:, None], (1, ny)))
+    h = np.asfortranarray(np.maximum(0.0 - b, 0.0))
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, manning_n=0.02,
+               bc_west="tidal")
+    sim, orc = pair(cfg, bathymetry=b, initial_h=h)
+    amp, ph, om = [0.8, 0.2], [0.3, -1.1], [2 * math.pi / 300.0, 2 * math.pi / 170.0]
+    with sim:
+        sim.set_tidal_constituents(amp, ph, om)
+        orc.set_tidal_constituents(amp, ph, om)
+        sim.advance(200.0)
+        orc.advance(200.0)
+        compare_state(sim, orc, rtol=RTOL)
+
+
+def test_forcing_wind_pressure_rain_coriolis():
+    nx, ny, dx = 64, 48, 50.0
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, manning_n=0.03,
+               coriolis_f=1.0e-4, init_condition="still_water", eta_initial=0.0)
+    b = gaussian_bed(nx, ny, dx, dx, 6, seed=11, base=-5.0, amp=(-2.0, 6.0),
+                     width=(100.0, 400.0))
+    sim, orc = pair(cfg, bathymetry=b)
+    rng = np.random.default_rng(5)
+    wx = rng.uniform(0.0, 0.3, (nx, ny))
+    wy = rng.uniform(-0.1, 0.1, (nx, ny))
+    p = rng.uniform(-50.0, 50.0, (nx, ny))  # anomaly: the ghosts stay at 0
+    rain = np.full((nx, ny), 1.0e-5)
+    with sim:
+        sim.set_wind(wx, wy)
+        sim.set_atm_pressure(p)
+        sim.set_precipitation(rain)
+        g = orc.ng
+        for name, arr in (("wind_x", wx), ("wind_y", wy), ("atm", p), ("precip", rain)):
+            orc.arrays[name][g:-g, g:-g] = arr
+        orc.s.forcing_active = 1
+        sim.step(40)
+        orc.step(40)
+        compare_state(sim, orc, rtol=RTOL)
+        mo, ms = sim.mass_budget()
+        assert abs(ms - orc.s.mass_src) <= 1e-10 * abs(orc.s.mass_src)
+
+
+def test_closed_basin_mass_and_budget():
+    """Walls only: mass conserved to round-off, boundary outflux ~ 0."""
+    nx, ny, dx = 128, 96, 10.0
+    b = gaussian_bed(nx, ny, dx, dx, 12, seed=2, width=(30.0, 200.0))
+    h = hump_depth(b, dx, dx, amp=0.5, width=100.0)
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45)
+    sim, orc = pair(cfg, bathymetry=b, initial_h=h)
+    with sim:
+        m0 = sim.h_phys.sum()
+        sim.step(300)
+        m1 = sim.h_phys.sum()
+        assert abs(m1 - m0) <= 1e-12 * m0
+        mo, _ = sim.mass_budget()
+        orc.step(300)
+        assert abs(mo - orc.s.mass_out) <= 1e-9 * max(1.0, abs(orc.s.mass_out))
+
+
+def test_cfl_interval_and_dt_fixed():
+    nx, ny, dx = 64, 64, 10.0
+    for extra in (dict(cfl_interval=5), dict(dt_fixed=0.4)):
+        cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=30.0, cfl=0.45, **extra)
+        sim, orc = pair(cfg)
+        with sim:
+            sim.advance(25.0)
+            orc.advance(25.0)
+            assert sim.step_count == orc.step_count
+            assert sim.dt == orc.dt
+            compare_state(sim, orc, rtol=0.0)
+
+
+def test_step_clamps_to_t_end_like_reference():
+    cfg = dict(nx=8, ny=8, dx=1.0, dy=1.0, t_end=0.2)
+    sim, orc = pair(cfg)
+    with sim:
+        sim.step(2000)
+        orc.step(2000)
+        assert sim.time == pytest.approx(0.2)
+        assert sim.time == orc.time
+        compare_state(sim, orc, rtol=0.0)
+        with pytest.raises(RuntimeError, match="t_end"):
+            sim.step(1)
+
+
+def test_tiles_agree():
+    nx, ny, dx = 150, 70, 5.0
+    b = gaussian_bed(nx, ny, dx, dx, 10, seed=9, width=(20.0, 80.0))
+    h = hump_depth(b, dx, dx, width=40.0)
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, use_hllc=True)
+    ref = None
+    for tile in range(4):
+        sim, _ = pair(cfg, bathymetry=b, initial_h=h)
+        with sim:
+            sim.set_tile(tile)
+            sim.step(25)
+            cur = sim.h.copy(), sim.hu.copy(), sim.hv.copy()
+        if ref is None:
+            ref = cur
+        else:
+            for a, r in zip(cur, ref):
+                assert np.array_equal(a, r)
+
+
+# ---------------------------------------------------------------------------
+# kernel-level entry points (device arrays through torch)
+# ---------------------------------------------------------------------------
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(np.asfortranarray(a).T)).cuda()
+
+
+def _host(t):
+    return np.asfortranarray(t.cpu().numpy().T)
+
+
+@pytest.mark.parametrize("hllc", [False, True])
+def test_kernel_flux_matches_oracle(hllc):
+    from oracle import oracle as orc
+    from rakali_b200 import _lib
+    lib = _lib.load()
+    nx, ny, ng = 70, 45, 2
+    rng = np.random.default_rng(1)
+    b = gaussian_bed(nx + 2 * ng, ny + 2 * ng, 1.0, 1.0, 5, seed=4, base=-1.0, amp=(-0.5, 1.5),
+                     width=(3.0, 10.0))
+    h = np.asfortranarray(np.maximum(0.3 * rng.random(b.shape) - b, 0.0))
+    h[h < 2e-3] *= rng.random((h < 2e-3).sum())  # thin films near the fronts
+    hu = np.asfortranarray(rng.normal(0, 0.3, b.shape) * h)
+    hv = np.asfortranarray(rng.normal(0, 0.3, b.shape) * h)
+    exp = orc.compute_flux(h, hu, hv, b, ng, 1.0, 1.0, hllc=hllc)
+    dh, dhu, dhv, db = (_dev(a) for a in (h, hu, hv, b))
+    outs = [_dev(np.zeros_like(h)) for _ in range(5)]
+    rc = lib.rkb_compute_flux(int(hllc), dh.data_ptr(), dhu.data_ptr(), dhv.data_ptr(),
+                              db.data_ptr(), *(o.data_ptr() for o in outs), h.shape[0],
+                              h.shape[1], ng, h.shape[0], 1.0, 1.0)
+    assert rc == 0
+    s = (slice(ng, -ng), slice(ng, -ng))
+    for got, want in zip(outs[:3], exp[:3]):
+        assert np.array_equal(_host(got)[s], want[s])
+    # mass fluxes: right/top faces of the interior plus the first left/bottom face
+    assert np.array_equal(_host(outs[3])[ng - 1:-ng, ng:-ng], exp[3][ng - 1:-ng, ng:-ng])
+    assert np.array_equal(_host(outs[4])[ng:-ng, ng - 1:-ng], exp[4][ng:-ng, ng - 1:-ng])
+
+
+def test_kernel_flux_known_answers():
+    """test_flux.F90:66-148 (dam break) and :185-229 (lake at rest) on the GPU."""
+    from rakali_b200 import _lib
+    lib = _lib.load()
+
+    def run(h, hu, hv, b, ng=2):
+        ins = [_dev(a) for a in (h, hu, hv, b)]
+        outs = [_dev(np.zeros_like(h)) for _ in range(5)]
+        rc = lib.rkb_compute_flux(0, *(t.data_ptr() for t in ins), *(o.data_ptr() for o in outs),
+                                  h.shape[0], h.shape[1], ng, h.shape[0], 1.0, 1.0)
+        assert rc == 0
+        return [_host(o) for o in outs]
+
+    nx, ny = 16, 8
+    h = np.full((nx, ny), 1.0, order="F")
+    h[: nx // 2, :] = 2.0
+    z = np.zeros((nx, ny), order="F")
+    fh = run(h, z, z, z)[0]
+    im = nx // 2 - 1
+    for j in range(2, ny - 2):
+        assert abs(fh[im, j] + math.sqrt(G / 2)) < 1e-12
+        assert abs(fh[im, j] + fh[im + 1, j]) < 1e-13
+    i = np.arange(1, 15)[:, None]
+    j = np.arange(1, 15)[None, :]
+    b = np.asfortranarray(0.5 * np.exp(-0.5 * ((i - 7) ** 2 + (j - 7) ** 2).astype(float)))
+    hh = np.asfortranarray(np.maximum(0.0, 2.0 - b))
+    out = run(hh, np.zeros_like(b), np.zeros_like(b), b)
+    assert max(np.abs(o[2:-2, 2:-2]).max() for o in out[:3]) < 1e-10
+
+
+def test_kernel_timestep_matches_oracle():
+    from oracle import oracle as orc
+    from rakali_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(2)
+    shape = (38, 27)
+    h = np.asfortranarray(rng.random(shape) * 2.0)
+    h[h < 0.2] = 0.0
+    hu = np.asfortranarray(rng.normal(0, 1, shape))
+    hv = np.asfortranarray(rng.normal(0, 1, shape))
+    dt_ref, _ = orc.compute_timestep(h, hu, hv, 3, 2.0, 3.0, 0.45)
+    ins = [_dev(a) for a in (h, hu, hv)]
+    import ctypes
+    out = ctypes.c_double()
+    rc = lib.rkb_compute_timestep(*(t.data_ptr() for t in ins), shape[0], shape[1], 3, shape[0],
+                                  2.0, 3.0, 0.45, ctypes.byref(out))
+    assert rc == 0
+    assert out.value == dt_ref
