@@ -192,7 +192,7 @@ def run_b200(args, rank, world, local_rank, dist):
     from rakali_b200 import workloads as wl
 
     torch.cuda.set_device(local_rank)
-    n = N_CELLS_SIDE
+    n = args.side
     b, h = wl.config2(n=n, seed=2024 + rank)
     sim = Rakali(defer_init=True, nx=n, ny=n, **wl.CONFIG2_KW)
     sim.set_bathymetry(b)
@@ -270,7 +270,7 @@ def run_b200(args, rank, world, local_rank, dist):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "structured SSP-RK2 wet/dry step, 4096x4096 per GPU, dx=5 m, "
+        "config": {"workload": f"structured SSP-RK2 wet/dry step, {n}x{n} per GPU, dx=5 m, "
                                "32-Gaussian bed, 0.5 m hump, Manning 0.025, walls, FP64 "
                                "(parity build)",
                    "cells_per_gpu": cells, "tile": "32x8", "parallelism": f"replicas{world}",
@@ -294,6 +294,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--side", type=int, default=N_CELLS_SIDE,
+                    help="grid side (smaller sides are for profiler captures only)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

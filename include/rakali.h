@@ -149,6 +149,11 @@ int rkb_time_steps(void *handle, int n, double *ms);
  * out5[4] = kernel launches per step. */
 int rkb_profile_steps(void *handle, int n, double *out5);
 
+/* Correctly rounded h**fl(1/3) and sin/cos, the host builds of the device
+ * functions the step uses for the friction, tidal and Coriolis terms. */
+double rkb_cr_pow_third(double h);
+void rkb_cr_sincos(double x, double *sn, double *cs);
+
 /*
  * Kernel-level entry points on caller-owned DEVICE arrays, Fortran order
  * with leading dimension `ld` (>= nx_total).  All run on the current

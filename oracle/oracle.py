@@ -132,6 +132,9 @@ def lib():
         L.orc_apply_bc.argtypes = [_DP] * 4 + [ctypes.c_int] * 3 + [ctypes.POINTER(_Bc)]
         L.orc_tidal_eta.argtypes = [ctypes.POINTER(_Bc)]
         L.orc_tidal_eta.restype = ctypes.c_double
+        L.orc_cr_pow_third.argtypes = [ctypes.c_double]
+        L.orc_cr_pow_third.restype = ctypes.c_double
+        L.orc_cr_sincos.argtypes = [ctypes.c_double, _DP, _DP]
         L.orc_set_threads.argtypes = [ctypes.c_int]
         L.orc_set_threads.restype = ctypes.c_int
         _lib = L

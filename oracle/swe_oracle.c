@@ -365,7 +365,7 @@ static void sources(double *ph, double *pu, double *pv, int nx, int i, int j, do
       double uu = u / h;
       double vv = v / h;
       double speed = sqrt(uu * uu + vv * vv);
-      double cf = G * n_sq / pow(h, 1.0 / 3.0);
+      double cf = G * n_sq / orc_cr_pow_third(h);
       double den = 1.0 + dt * cf * speed / h;
       u = u / den;
       v = v / den;
@@ -400,8 +400,8 @@ static src_consts make_src(double manning_n, double coriolis_f, double dt) {
   c.n_sq = manning_n * manning_n;
   c.has_fric = manning_n > 0.0;
   c.has_cor = fabs(coriolis_f) > 1.0e-20;
-  c.cosf = c.has_cor ? cos(coriolis_f * dt) : 0.0;
-  c.sinf = c.has_cor ? sin(coriolis_f * dt) : 0.0;
+  c.cosf = c.has_cor ? orc_cr_cos(coriolis_f * dt) : 0.0;
+  c.sinf = c.has_cor ? orc_cr_sin(coriolis_f * dt) : 0.0;
   return c;
 }
 
@@ -544,7 +544,7 @@ void orc_apply_friction(double *h, double *hu, double *hv, int nx, int ny, int n
         double v = AT(hv, i, j) / hval;
         double speed = sqrt(u * u + v * v);
         if (has_fric) {
-          double cf = G * manning_n * manning_n / pow(hval, 1.0 / 3.0);
+          double cf = G * manning_n * manning_n / orc_cr_pow_third(hval);
           double den = 1.0 + dt * cf * speed / hval;
           AT(hu, i, j) = AT(hu, i, j) / den;
           AT(hv, i, j) = AT(hv, i, j) / den;
@@ -567,7 +567,7 @@ void orc_apply_friction(double *h, double *hu, double *hv, int nx, int ny, int n
 void orc_apply_coriolis(const double *h, double *hu, double *hv, int nx, int ny, int ng,
                         double dt, double f) {
   if (fabs(f) < 1.0e-20) return;
-  double cosf_ = cos(f * dt), sinf_ = sin(f * dt);
+  double cosf_ = orc_cr_cos(f * dt), sinf_ = orc_cr_sin(f * dt);
   for (int j = ng; j < ny - ng; ++j)
     for (int i = ng; i < nx - ng; ++i)
       if (AT(h, i, j) > DRY) {
@@ -804,9 +804,9 @@ double orc_tidal_eta(const orc_bc *bc) {
   double eta = 0.0;
   if (bc->n_tidal > 0) {
     for (int n = 0; n < bc->n_tidal; ++n)
-      eta = eta + bc->tidal_amp[n] * cos(bc->tidal_omega[n] * bc->time - bc->tidal_phase[n]);
+      eta = eta + bc->tidal_amp[n] * orc_cr_cos(bc->tidal_omega[n] * bc->time - bc->tidal_phase[n]);
   } else if (bc->tidal_period > 0.0) {
-    eta = bc->tidal_amplitude * sin(TWO_PI_C * bc->time / bc->tidal_period);
+    eta = bc->tidal_amplitude * orc_cr_sin(TWO_PI_C * bc->time / bc->tidal_period);
   }
   return eta;
 }

@@ -67,6 +67,13 @@ typedef struct {
 /* OpenMP thread count for timing runs; returns the count in effect. */
 int orc_set_threads(int n);
 
+/* Correctly rounded h**(1/3) (as h**fl(1/3)), sin, cos (crmath.c): the
+ * platform-independent values of the reference's libm calls. */
+double orc_cr_pow_third(double h);
+double orc_cr_sin(double x);
+double orc_cr_cos(double x);
+void orc_cr_sincos(double x, double *sn, double *cs);
+
 /* rki_kernel_flux.F90:17-102 (compute_flux_hll / compute_flux_hllc). */
 void orc_compute_flux(int use_hllc, const double *h, const double *hu, const double *hv,
                       const double *b, double *flux_h, double *flux_hu, double *flux_hv,

@@ -103,6 +103,8 @@ def load(path: str | None = None):
     _sig(lib, "rkb_get_tile", [H], I)
     _sig(lib, "rkb_time_steps", [H, I, DP], I)
     _sig(lib, "rkb_profile_steps", [H, I, DP], I)
+    _sig(lib, "rkb_cr_pow_third", [D], D)
+    _sig(lib, "rkb_cr_sincos", [D, DP, DP], None)
     _sig(lib, "rkb_compute_flux", [I, H, H, H, H, H, H, H, H, H, I, I, I, I, D, D], I)
     _sig(lib, "rkb_compute_timestep", [H, H, H, I, I, I, I, D, D, D, DP], I)
     if lib.rki_working_precision() != 8:

@@ -110,3 +110,15 @@ int rkb_compute_timestep(const double* h, const double* hu, const double* hv, in
 }
 
 }  // extern "C"
+
+// Host builds of the correctly rounded transcendental terms the kernels use
+// (rkb_crmath.cuh), exposed so the same code can be checked without a GPU.
+#include "rkb_crmath.cuh"
+
+extern "C" {
+
+double rkb_cr_pow_third(double h) { return rkb::cr_pow_third(h); }
+
+void rkb_cr_sincos(double x, double* sn, double* cs) { rkb::cr_sincos(x, *sn, *cs); }
+
+}  // extern "C"

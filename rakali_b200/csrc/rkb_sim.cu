@@ -283,6 +283,24 @@ int Sim::upload_state() {
   for (int k = 0; k < 4; ++k)
     RKB_TRY(cudaMemcpy2DAsync(dst[k], dpitch, hf_[k], wbytes, wbytes, g.nyt,
                               cudaMemcpyHostToDevice, stream_));
+  // The other state buffer and the stage scratch start as copies too: ghost
+  // cells that no boundary rule rewrites (nested edges) then keep their
+  // values in every buffer, as the reference's single array does.
+  const size_t fbytes = (size_t)g.pitch * (size_t)g.nyt * sizeof(double);
+  FieldSet O = cur_ ? args_.U0 : args_.U1;
+  double* copies[2][3] = {{O.h, O.hu, O.hv}, {args_.S.h, args_.S.hu, args_.S.hv}};
+  for (auto& c : copies)
+    for (int k = 0; k < 3; ++k)
+      RKB_TRY(cudaMemcpyAsync(c[k], dst[k], fbytes, cudaMemcpyDeviceToDevice, stream_));
+  if (stepped_) {
+    // the other buffer's interior is the RK2 save U^n (the h0 views)
+    const size_t off_d = (size_t)g.ng + (size_t)g.ng * (size_t)g.pitch;
+    const size_t off_h = (size_t)g.ng + (size_t)g.ng * (size_t)g.nxt;
+    for (int k = 0; k < 3; ++k)
+      RKB_TRY(cudaMemcpy2DAsync(copies[0][k] + off_d, dpitch, hf_[4 + k] + off_h, wbytes,
+                                (size_t)g.nx_phys() * sizeof(double), g.ny_phys(),
+                                cudaMemcpyHostToDevice, stream_));
+  }
   if (phys.forcing_active && upload_forcing() != 0) return -1;
   hctl_->ms_valid = 0;
   RKB_TRY(cudaMemcpyAsync(&args_.ctl->ms_valid, &hctl_->ms_valid, sizeof(int),

@@ -12,6 +12,7 @@
 // stage-2 epilogue; the first launch of the next step turns it into dt.
 // The boundary mass-out sums (rki_solver.F90:507-537) are per-block partials
 // reduced in a fixed order by the last block of stage 2.
+#include "rkb_crmath.cuh"
 #include "rkb_face.cuh"
 #include "rkb_kernels.h"
 
@@ -72,9 +73,9 @@ __device__ __forceinline__ double tidal_eta(const BcParams* bc, double time) {
   double eta = 0.0;
   if (bc->n_tidal > 0) {
     for (int n = 0; n < bc->n_tidal; ++n)
-      eta = eta + bc->amp[n] * cos(bc->omega[n] * time - bc->phase[n]);
+      eta = eta + bc->amp[n] * cr_cos(bc->omega[n] * time - bc->phase[n]);
   } else if (bc->tidal_period > 0.0) {
-    eta = bc->tidal_amplitude * sin(kTwoPi * time / bc->tidal_period);
+    eta = bc->tidal_amplitude * cr_sin(kTwoPi * time / bc->tidal_period);
   }
   return eta;
 }
@@ -324,7 +325,7 @@ __device__ __forceinline__ void sources(double& h, double& u, double& v, const P
       const double uu = u / h;
       const double vv = v / h;
       const double speed = sqrt(uu * uu + vv * vv);
-      const double cf = kG * n_sq / pow(h, 1.0 / 3.0);
+      const double cf = kG * n_sq / cr_pow_third(h);
       const double den = 1.0 + dt * cf * speed / h;
       u = u / den;
       v = v / den;
@@ -406,6 +407,16 @@ __global__ void __launch_bounds__(TX * TY)
   const int tid = threadIdx.x;
   const int gx0 = g.ng + blockIdx.x * TX;  // first interior cell of the tile
   const int gy0 = g.ng + blockIdx.y * TY;
+
+  // Coriolis rotation of this stage, cos/sin(f dt), correctly rounded once
+  // per block (rki_kernel_fused.F90:211-214)
+  __shared__ double rot[2];
+  if (STAGE != 0 && tid == 0) {
+    double sn = 0.0, cs = 0.0;
+    if (fabs(phys->coriolis_f) > 1.0e-20) cr_sincos(phys->coriolis_f * dt, sn, cs);
+    rot[0] = cs;
+    rot[1] = sn;
+  }
 
   // 1. tile load with halo (ghost cells come from the BC launches)
   for (int k = tid; k < SM::NT; k += NTH) {
@@ -513,12 +524,7 @@ __global__ void __launch_bounds__(TX * TY)
       protect(a, u, v);
       const double n_sq = phys->manning_n * phys->manning_n;
       const bool has_cor = fabs(phys->coriolis_f) > 1.0e-20;
-      double cosf = 0.0, sinf = 0.0;
-      if (has_cor) {
-        cosf = cos(phys->coriolis_f * dt);
-        sinf = sin(phys->coriolis_f * dt);
-      }
-      sources(a, u, v, phys, dt, n_sq, cosf, sinf, has_cor, g, i, j, fo);
+      sources(a, u, v, phys, dt, n_sq, rot[0], rot[1], has_cor, g, i, j, fo);
       FieldSet out;
       if (STAGE == 1) {
         out = S;

@@ -50,11 +50,12 @@ def pair(cfg: dict, bathymetry=None, initial_h=None):
     return sim, orc
 
 
-def max_rel_diff(a, b, floor=1.0):
-    """max |a - b| / max(|b|, floor)."""
+def max_rel_diff(a, b, floor=1.0e-6):
+    """Relative L-infinity error max|a - b| / max|b| (scale floored at `floor`)."""
     a = np.asarray(a)
     b = np.asarray(b)
-    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor)))
+    scale = max(float(np.max(np.abs(b))), floor)
+    return float(np.max(np.abs(a - b))) / scale
 
 
 def compare_state(sim, orc, rtol=0.0, ghosts=True, fields=("h", "hu", "hv", "b")):
