@@ -198,6 +198,7 @@ def run_b200(args, rank, world, local_rank, dist):
     sim.set_bathymetry(b)
     sim.set_initial_h(h)
     sim.finalize()
+    sim.set_tile(args.tile)
     lib = sim._lib
     cells = n * n
 
@@ -273,7 +274,7 @@ def run_b200(args, rank, world, local_rank, dist):
         "config": {"workload": f"structured SSP-RK2 wet/dry step, {n}x{n} per GPU, dx=5 m, "
                                "32-Gaussian bed, 0.5 m hump, Manning 0.025, walls, FP64 "
                                "(parity build)",
-                   "cells_per_gpu": cells, "tile": "32x8", "parallelism": f"replicas{world}",
+                   "cells_per_gpu": cells, "tile": args.tile, "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (3 x 134 MB per buffer)"},
         "e2e": e2e,
         "gpu_launches": launches * args.steps,
@@ -294,6 +295,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tile", type=int, default=4,
+                    help="stage-kernel variant (rkb_set_tile): 0-3 shared-memory tiles, "
+                         "4/5 marching strips of 64/32 rows")
     ap.add_argument("--side", type=int, default=N_CELLS_SIDE,
                     help="grid side (smaller sides are for profiler captures only)")
     args = ap.parse_args()

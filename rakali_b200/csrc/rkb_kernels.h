@@ -30,7 +30,11 @@ struct FluxOut {
 };
 
 // Tile shapes of the fused stage kernel (cells per block in x and y).
-enum TileShape : int { kTile32x8 = 0, kTile32x16 = 1, kTile64x4 = 2, kTile16x16 = 3, kNumTiles = 4 };
+enum TileShape : int {
+  kTile32x8 = 0, kTile32x16 = 1, kTile64x4 = 2, kTile16x16 = 3,  // shared-memory tiles
+  kMarch64 = 4, kMarch32 = 5,  // warp-per-strip marching kernel, 64 / 32 rows per warp
+  kNumTiles = 6
+};
 const char* tile_name(int tile);
 void tile_dims(int tile, int& tx, int& ty);
 

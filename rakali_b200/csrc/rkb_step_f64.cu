@@ -368,6 +368,48 @@ __device__ __forceinline__ void sponge(double& h, double& u, double& v, const Bc
   }
 }
 
+// Close a step (last block of the final stage kernel): fixed-order sums of
+// the per-block partials, the mass budget in the reference's order
+// (rki_solver.F90:507-657), the CFL maxima of the new state and the clock.
+__device__ void finalize_step(const Grid& g, StepCtl* ctl, const Physics* phys,
+                              double* partials, unsigned int nparts, double dt, int cur) {
+  const int tid = threadIdx.x;
+  const double area = g.dx * g.dy;
+  volatile double* VP = partials;
+  double sums[4];
+  for (int s = 0; s < 4; ++s) {
+    double acc = 0.0;
+    if (tid < 32)
+      for (unsigned int k = tid; k < nparts; k += 32) acc = acc + VP[(size_t)s * nparts + k];
+    sums[s] = warp_sum(acc);
+  }
+  if (tid == 0) {
+    volatile StepCtl* vc = ctl;
+    double mo = ctl->mass_out;
+    mo = mo - 0.5 * dt * sums[0] * area;
+    mo = mo - 0.5 * dt * sums[2] * area;
+    ctl->mass_out = mo;
+    double ms = ctl->mass_src;
+    if (phys->forcing_active) ms = ms + 0.5 * dt * ctl->precip_sum * area;
+    ms = ms + 0.5 * sums[1] * area;
+    if (phys->forcing_active) ms = ms + 0.5 * dt * ctl->precip_sum * area;
+    ms = ms + 0.5 * sums[3] * area;
+    ctl->mass_src = ms;
+    ctl->msx = __longlong_as_double((long long)vc->msx_next);
+    ctl->msy = __longlong_as_double((long long)vc->msy_next);
+    ctl->msx_next = 0ull;
+    ctl->msy_next = 0ull;
+    ctl->ms_valid = 1;
+    ctl->t = ctl->t + dt;
+    ctl->dt_prev = dt;
+    ctl->step_count = ctl->step_count + 1;
+    ctl->remaining = ctl->remaining - 1;
+    ctl->steps_run = ctl->steps_run + 1;
+    ctl->cur = cur ^ 1;
+    ctl->done_blocks = 0u;
+  }
+}
+
 // STAGE 1: U^n (buffer cur) -> U* (scratch S).
 // STAGE 2: U* (S) and U^n (buffer cur) -> U^{n+1} (buffer cur^1).
 // STAGE 0: flux divergence only (kernel-level API): writes flux/mass-flux
@@ -589,42 +631,215 @@ __global__ void __launch_bounds__(TX * TY)
   __syncthreads();
   if (!last) return;
   __threadfence();
-  // fixed-order sums of the per-block partials, one warp per sum
-  const double area = g.dx * g.dy;
-  volatile double* VP = partials;
-  double sums[4];
-  for (int s = 0; s < 4; ++s) {
-    double acc = 0.0;
-    if (tid < 32)
-      for (unsigned int k = tid; k < nblocks; k += 32) acc = acc + VP[(size_t)s * nblocks + k];
-    sums[s] = warp_sum(acc);
+  finalize_step(g, ctl, phys, partials, nblocks, dt, cur);
+}
+
+// ---------------------------------------------------------------------------
+// Marching stage kernel: one warp per 28-column strip, stepping up the rows.
+// ---------------------------------------------------------------------------
+//
+// Lane l of a warp owns column x0 - 2 + l; lanes 2..29 produce output cells,
+// lanes 0, 1, 30, 31 carry the x halo.  Each iteration handles one row j:
+// the y-face above it (the one below was computed in the previous
+// iteration), the x-face left of every lane (the right face comes from the
+// next lane by shuffle), then the cell update.  No shared memory and no
+// block barriers on the data path; each face is evaluated once except the
+// strip-boundary ones (x: 1 in 29, y: 1 per ROWS rows).
+
+constexpr int kMarchWarps = 4;   // strips per block
+constexpr int kMarchCols = 28;   // output columns per strip
+
+struct RowVals {
+  double h, u, v, b;
+};
+
+__device__ __forceinline__ RowVals load_row(const FieldSet& F, const double* __restrict__ b,
+                                            const Grid& g, int gi, int j, bool col_in) {
+  RowVals r{0.0, 0.0, 0.0, 0.0};
+  if (col_in) {
+    const size_t q = g.at(gi, j);
+    r.h = F.h[q];
+    r.u = F.hu[q];
+    r.v = F.hv[q];
+    r.b = b[q];
   }
-  if (tid == 0) {
-    volatile StepCtl* vc = ctl;
-    // mass budget in the reference's order: stage 1 then stage 2
-    double mo = ctl->mass_out;
-    mo = mo - 0.5 * dt * sums[0] * area;
-    mo = mo - 0.5 * dt * sums[2] * area;
-    ctl->mass_out = mo;
-    double ms = ctl->mass_src;
-    if (phys->forcing_active) ms = ms + 0.5 * dt * ctl->precip_sum * area;
-    ms = ms + 0.5 * sums[1] * area;
-    if (phys->forcing_active) ms = ms + 0.5 * dt * ctl->precip_sum * area;
-    ms = ms + 0.5 * sums[3] * area;
-    ctl->mass_src = ms;
-    ctl->msx = __longlong_as_double((long long)vc->msx_next);
-    ctl->msy = __longlong_as_double((long long)vc->msy_next);
-    ctl->msx_next = 0ull;
-    ctl->msy_next = 0ull;
-    ctl->ms_valid = 1;
-    ctl->t = ctl->t + dt;
-    ctl->dt_prev = dt;
-    ctl->step_count = ctl->step_count + 1;
-    ctl->remaining = ctl->remaining - 1;
-    ctl->steps_run = ctl->steps_run + 1;
-    ctl->cur = cur ^ 1;
-    ctl->done_blocks = 0u;
+  return r;
+}
+
+__device__ __forceinline__ void yslope(const RowVals& m, const RowVals& c, const RowVals& p,
+                                       double& se, double& su, double& sv) {
+  cell_slope(m.h, c.h, p.h, m.h + m.b, c.h + c.b, p.h + p.b, m.u, c.u, p.u, m.v, c.v, p.v, se,
+             su, sv);
+}
+
+template <bool HLLC>
+__device__ __forceinline__ void yface(const RowVals& lo, double sle, double slu, double slv,
+                                      const RowVals& hi, double she, double shu, double shv,
+                                      FaceOut& o) {
+  face_flux<1, HLLC>(lo.h + lo.b + 0.5 * sle, lo.u + 0.5 * slu, lo.v + 0.5 * slv, lo.b,
+                     hi.h + hi.b - 0.5 * she, hi.u - 0.5 * shu, hi.v - 0.5 * shv, hi.b, o);
+}
+
+template <bool HLLC, int STAGE, int ROWS>
+__global__ void __launch_bounds__(kMarchWarps * 32, 4)
+    k_march(Grid g, StepCtl* ctl, const Physics* phys, const BcParams* bcp, FieldSet U0,
+            FieldSet U1, FieldSet S, const double* __restrict__ b, Forcing fo,
+            double* __restrict__ partials) {
+  if (!ctl->active) return;
+  const double dt = ctl->dt;
+  const int cur = ctl->cur;
+  const FieldSet in = STAGE == 2 ? S : (cur ? U1 : U0);
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int strip = blockIdx.x * kMarchWarps + warp;
+  const int x0 = g.ng + strip * kMarchCols;
+  const int gi = x0 - 2 + lane;
+  const int y0 = g.ng + blockIdx.y * ROWS;
+  const int yend = min(y0 + ROWS, g.nyt - g.ng);
+  const bool col_in = gi < g.nxt;
+  const bool out_lane = lane >= 2 && lane < 2 + kMarchCols && gi < g.nxt - g.ng;
+  const double dx = g.dx, dy = g.dy;
+  const double n_sq = phys->manning_n * phys->manning_n;
+  const bool has_cor = fabs(phys->coriolis_f) > 1.0e-20;
+  double cosf = 0.0, sinf = 0.0;
+  if (has_cor) cr_sincos(phys->coriolis_f * dt, sinf, cosf);
+
+  double part = 0.0, sponge_d = 0.0, wsx = 0.0, wsy = 0.0;
+  if (x0 < g.nxt - g.ng && y0 < yend) {  // warp-uniform
+    // prologue: rows y0-2 .. y0+1, slopes of y0-1 and y0, face y0-1/2
+    RowVals A = load_row(in, b, g, gi, y0 - 2, col_in);
+    RowVals B = load_row(in, b, g, gi, y0 - 1, col_in);
+    RowVals C = load_row(in, b, g, gi, y0, col_in);
+    RowVals D = load_row(in, b, g, gi, y0 + 1, col_in);
+    double sBe, sBu, sBv, sCe, sCu, sCv;
+    yslope(A, B, C, sBe, sBu, sBv);
+    yslope(B, C, D, sCe, sCu, sCv);
+    FaceOut bot;
+    yface<HLLC>(B, sBe, sBu, sBv, C, sCe, sCu, sCv, bot);
+    RowVals E = load_row(in, b, g, gi, y0 + 2, col_in);
+    for (int j = y0; j < yend; ++j) {
+      // prefetch row j+3 (stays inside the array: j + 3 <= nyt - ng + 2)
+      RowVals Fn{0.0, 0.0, 0.0, 0.0};
+      if (j + 1 < yend) Fn = load_row(in, b, g, gi, j + 3, col_in);
+      double old_h = 0.0, old_u = 0.0, old_v = 0.0;
+      size_t q = 0;
+      if (out_lane) {
+        q = g.at(gi, j);
+        if (STAGE == 2) {
+          const FieldSet old = cur ? U1 : U0;
+          old_h = old.h[q];
+          old_u = old.hu[q];
+          old_v = old.hv[q];
+        }
+      }
+      // y-face above row j
+      double sDe, sDu, sDv;
+      yslope(C, D, E, sDe, sDu, sDv);
+      FaceOut top;
+      yface<HLLC>(C, sCe, sCu, sCv, D, sDe, sDu, sDv, top);
+      // x-slope of this lane's cell in row j (neighbours by shuffle)
+      const double ec = C.h + C.b;
+      const double hm = __shfl_up_sync(0xffffffffu, C.h, 1);
+      const double hp = __shfl_down_sync(0xffffffffu, C.h, 1);
+      const double em = __shfl_up_sync(0xffffffffu, ec, 1);
+      const double ep = __shfl_down_sync(0xffffffffu, ec, 1);
+      const double um = __shfl_up_sync(0xffffffffu, C.u, 1);
+      const double up = __shfl_down_sync(0xffffffffu, C.u, 1);
+      const double vm = __shfl_up_sync(0xffffffffu, C.v, 1);
+      const double vp = __shfl_down_sync(0xffffffffu, C.v, 1);
+      double sxe, sxu, sxv;
+      cell_slope(hm, C.h, hp, em, ec, ep, um, C.u, up, vm, C.v, vp, sxe, sxu, sxv);
+      // x-face left of this lane: left state = previous lane reconstructed right
+      const double re = ec + 0.5 * sxe, ru = C.u + 0.5 * sxu, rv = C.v + 0.5 * sxv;
+      const double le = __shfl_up_sync(0xffffffffu, re, 1);
+      const double lu = __shfl_up_sync(0xffffffffu, ru, 1);
+      const double lv = __shfl_up_sync(0xffffffffu, rv, 1);
+      const double lb = __shfl_up_sync(0xffffffffu, C.b, 1);
+      FaceOut xf;
+      face_flux<0, HLLC>(le, lu, lv, lb, ec - 0.5 * sxe, C.u - 0.5 * sxu, C.v - 0.5 * sxv, C.b,
+                         xf);
+      const double r_fh = __shfl_down_sync(0xffffffffu, xf.fh, 1);
+      const double r_fx = __shfl_down_sync(0xffffffffu, xf.fqx, 1);
+      const double r_fy = __shfl_down_sync(0xffffffffu, xf.fqy, 1);
+      const double r_h2 = __shfl_down_sync(0xffffffffu, xf.hL2, 1);
+      const double r_p2 = __shfl_down_sync(0xffffffffu, xf.pL2, 1);
+      if (out_lane) {
+        const double o_fh = -((r_fh - xf.fh) / dx) - (top.fh - bot.fh) / dy;
+        const double o_fhu = -((r_fx - xf.fqx) / dx) - (top.fqx - bot.fqx) / dy -
+                             kHalfG * (xf.wbR - r_h2 + r_p2) / dx;
+        const double o_fhv = -((r_fy - xf.fqy) / dx) - (top.fqy - bot.fqy) / dy -
+                             kHalfG * (bot.wbR - top.hL2 + top.pL2) / dy;
+        double a = C.h, u = C.u, v = C.v;
+        a = a + dt * o_fh;
+        u = u + dt * o_fhu;
+        v = v + dt * o_fhv;
+        protect(a, u, v);
+        sources(a, u, v, phys, dt, n_sq, cosf, sinf, has_cor, g, gi, j, fo);
+        FieldSet out;
+        if (STAGE == 1) {
+          out = S;
+        } else {
+          out = cur ? U0 : U1;
+          a = 0.5 * (old_h + a);
+          u = 0.5 * (old_u + u);
+          v = 0.5 * (old_v + v);
+          protect(a, u, v);
+        }
+        const double h_pre_sponge = a;
+        sponge(a, u, v, bcp, g, gi, j, dt);
+        out.h[q] = a;
+        out.hu[q] = u;
+        out.hv[q] = v;
+        part = part + o_fh;
+        sponge_d = sponge_d + (a - h_pre_sponge);
+        if (STAGE == 2) {
+          double sx, sy;
+          wave_speed(a, u, v, sx, sy);
+          if (sx > wsx) wsx = sx;
+          if (sy > wsy) wsy = sy;
+        }
+      }
+      // rotate the row window
+      C = D;
+      D = E;
+      E = Fn;
+      sCe = sDe;
+      sCu = sDu;
+      sCv = sDv;
+      bot = top;
+    }
   }
+
+  // per-warp partials (fixed order) and the CFL maxima of the new state
+  part = warp_sum(part);
+  sponge_d = warp_sum(sponge_d);
+  const unsigned int nblocks = gridDim.x * gridDim.y;
+  const unsigned int nw = nblocks * kMarchWarps;
+  const unsigned int wid = (blockIdx.y * gridDim.x + blockIdx.x) * kMarchWarps + warp;
+  if (STAGE == 2) {
+    wsx = warp_max(wsx);
+    wsy = warp_max(wsy);
+  }
+  if (lane == 0) {
+    double* P = partials + (size_t)(STAGE - 1) * 2 * nw;
+    P[wid] = part;
+    P[nw + wid] = sponge_d;
+    if (STAGE == 2) {
+      atomic_max_pos(&ctl->msx_next, wsx);
+      atomic_max_pos(&ctl->msy_next, wsy);
+    }
+  }
+  if (STAGE != 2) return;
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(&ctl->done_blocks, 1u) == nblocks - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  finalize_step(g, ctl, phys, partials, nw, dt, cur);
 }
 
 }  // namespace rkb
@@ -640,7 +855,9 @@ const char* tile_name(int tile) {
     case kTile32x8: return "32x8";
     case kTile32x16: return "32x16";
     case kTile64x4: return "64x4";
-    default: return "16x16";
+    case kTile16x16: return "16x16";
+    case kMarch64: return "march28x64";
+    default: return "march28x32";
   }
 }
 
@@ -649,9 +866,13 @@ void tile_dims(int tile, int& tx, int& ty) {
     case kTile32x8: tx = 32; ty = 8; break;
     case kTile32x16: tx = 32; ty = 16; break;
     case kTile64x4: tx = 64; ty = 4; break;
-    default: tx = 16; ty = 16; break;
+    case kTile16x16: tx = 16; ty = 16; break;
+    case kMarch64: tx = kMarchCols * kMarchWarps; ty = 64; break;
+    default: tx = kMarchCols * kMarchWarps; ty = 32; break;
   }
 }
+
+static bool is_march(int tile) { return tile == kMarch64 || tile == kMarch32; }
 
 static dim3 stage_grid(const Grid& g, int tile) {
   int tx, ty;
@@ -661,7 +882,8 @@ static dim3 stage_grid(const Grid& g, int tile) {
 
 size_t partials_doubles(const Grid& g, int tile) {
   dim3 d = stage_grid(g, tile);
-  return 4 * (size_t)d.x * (size_t)d.y;
+  const size_t parts = (size_t)d.x * (size_t)d.y * (is_march(tile) ? kMarchWarps : 1);
+  return 4 * parts;
 }
 
 template <int TX, int TY, bool HLLC, int STAGE>
@@ -671,6 +893,14 @@ static cudaError_t launch_stage_t(const StepArgs& a, FluxOut fl, cudaStream_t s)
   dim3 grid = stage_grid(a.g, a.tile);
   kern<<<grid, TX * TY, SM::BYTES, s>>>(a.g, a.ctl, a.phys, a.bc, a.U0, a.U1, a.S, a.b, a.fo,
                                         a.partials, fl);
+  return cudaGetLastError();
+}
+
+template <bool HLLC, int STAGE, int ROWS>
+static cudaError_t launch_march_t(const StepArgs& a, cudaStream_t s) {
+  dim3 grid = stage_grid(a.g, a.tile);
+  k_march<HLLC, STAGE, ROWS><<<grid, kMarchWarps * 32, 0, s>>>(a.g, a.ctl, a.phys, a.bc, a.U0,
+                                                              a.U1, a.S, a.b, a.fo, a.partials);
   return cudaGetLastError();
 }
 
@@ -692,7 +922,8 @@ cudaError_t configure_kernels(int tile, int hllc) {
     case kTile32x8: return h ? configure_t<32, 8, true>() : configure_t<32, 8, false>();
     case kTile32x16: return h ? configure_t<32, 16, true>() : configure_t<32, 16, false>();
     case kTile64x4: return h ? configure_t<64, 4, true>() : configure_t<64, 4, false>();
-    default: return h ? configure_t<16, 16, true>() : configure_t<16, 16, false>();
+    case kTile16x16: return h ? configure_t<16, 16, true>() : configure_t<16, 16, false>();
+    default: return cudaSuccess;  // marching kernels use no dynamic shared memory
   }
 }
 
@@ -706,9 +937,16 @@ static cudaError_t launch_stage(const StepArgs& a, FluxOut fl, cudaStream_t s) {
       return h ? launch_stage_t<32, 16, true, STAGE>(a, fl, s) : launch_stage_t<32, 16, false, STAGE>(a, fl, s);
     case kTile64x4:
       return h ? launch_stage_t<64, 4, true, STAGE>(a, fl, s) : launch_stage_t<64, 4, false, STAGE>(a, fl, s);
-    default:
+    case kTile16x16:
       return h ? launch_stage_t<16, 16, true, STAGE>(a, fl, s) : launch_stage_t<16, 16, false, STAGE>(a, fl, s);
+    default:
+      break;
   }
+  if (STAGE == 0) return cudaErrorInvalidValue;  // the flux-only entry uses the tiled kernels
+  constexpr int ST = STAGE == 0 ? 1 : STAGE;
+  if (a.tile == kMarch64)
+    return h ? launch_march_t<true, ST, 64>(a, s) : launch_march_t<false, ST, 64>(a, s);
+  return h ? launch_march_t<true, ST, 32>(a, s) : launch_march_t<false, ST, 32>(a, s);
 }
 
 cudaError_t launch_bc(const StepArgs& a, int stage, cudaStream_t s) {
