@@ -295,7 +295,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--tile", type=int, default=4,
+    ap.add_argument("--tile", type=int, default=1,
                     help="stage-kernel variant (rkb_set_tile): 0-3 shared-memory tiles, "
                          "4/5 marching strips of 64/32 rows")
     ap.add_argument("--side", type=int, default=N_CELLS_SIDE,
