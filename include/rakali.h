@@ -171,6 +171,21 @@ int rkb_compute_timestep(const double *h, const double *hu, const double *hv, in
                          int ny_total, int nghost, int ld, double dx, double dy, double cfl,
                          double *dt_out);
 
+/* No counterpart in the reference.  The same dt as rkb_compute_timestep for
+ * callers that cannot allocate device memory when they need it: a host
+ * application whose memory pool already owns the GPU, or a driver loop that
+ * must not block (cudaMalloc/cudaFree synchronise the device).  It allocates
+ * nothing: its scratch is a fixed array inside the library (2 doubles per
+ * interior row plus one, for at most 32768 interior rows; about 512 KB on
+ * every GPU that loads the library, held until exit).  More rows return -2
+ * with the reason in rki_last_error().  The first call on each device looks
+ * up the array's device address with that device current; make that first
+ * call before any stream capture.  Calls share the array, so calls that
+ * overlap on the GPU race; the result is read back before returning. */
+int rkb_compute_timestep_noalloc(const double *h, const double *hu, const double *hv,
+                                 int nx_total, int ny_total, int nghost, int ld, double dx,
+                                 double dy, double cfl, double *dt_out);
+
 #ifdef __cplusplus
 }
 #endif

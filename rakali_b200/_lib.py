@@ -107,6 +107,7 @@ def load(path: str | None = None):
     _sig(lib, "rkb_cr_sincos", [D, DP, DP], None)
     _sig(lib, "rkb_compute_flux", [I, H, H, H, H, H, H, H, H, H, I, I, I, I, D, D], I)
     _sig(lib, "rkb_compute_timestep", [H, H, H, I, I, I, I, D, D, D, DP], I)
+    _sig(lib, "rkb_compute_timestep_noalloc", [H, H, H, I, I, I, I, D, D, D, DP], I)
     if lib.rki_working_precision() != 8:
         raise RuntimeError("librakali.so must be the FP64 build")
     lib.wp_dtype = np.float64

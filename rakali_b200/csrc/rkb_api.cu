@@ -429,3 +429,8 @@ int rkb_get_tile(void* handle) {
 }
 
 }  // extern "C"
+
+namespace rkb {
+// Message for rki_last_error() from entry points defined in other files.
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace rkb

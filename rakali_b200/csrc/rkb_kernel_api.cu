@@ -122,3 +122,139 @@ double rkb_cr_pow_third(double h) { return rkb::cr_pow_third(h); }
 void rkb_cr_sincos(double x, double* sn, double* cs) { rkb::cr_sincos(x, *sn, *cs); }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free CFL timestep.
+//
+// Some callers of this library cannot allocate device memory at the point
+// where they need dt: a host application that has reserved the GPU's memory
+// for its own pool (the reference's OpenACC runtime maps all model arrays up
+// front), or a driver loop that must not block - cudaMalloc and cudaFree
+// synchronise the whole device.  rkb_compute_timestep_noalloc therefore does
+// its two-pass reduction in a fixed scratch array compiled into the library:
+// one slot pair per interior row, plus the result.
+//
+// Limits: ny_total - 2*nghost <= kNoAllocMaxRows rows.  The array is device
+// memory of every GPU that loads the library, held until the process exits.
+// Every call shares it and it keeps the last call's contents; the row pass
+// writes every slot it later reads, so nothing needs clearing.  Calls that
+// overlap on the GPU (other host threads, other streams) race on it.
+// ---------------------------------------------------------------------------
+
+#include <mutex>
+#include <string>
+
+namespace rkb {
+void set_last_error(const std::string& msg);  // rkb_api.cu
+namespace {
+
+constexpr int kNoAllocMaxRows = 32768;
+static __device__ __align__(256) double g_noalloc_scratch[2 * kNoAllocMaxRows + 2];
+
+// One warp per interior row: the row's maxima of (|u|+c) along x and y.
+__global__ void k_row_speed(Grid g, const double* __restrict__ h, const double* __restrict__ hu,
+                            const double* __restrict__ hv, double* scratch) {
+  const int lane = threadIdx.x & 31;
+  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int nyp = g.ny_phys();
+  if (row >= nyp) return;
+  const int j = g.ng + row;
+  double mx = 0.0, my = 0.0;
+  for (int i = g.ng + lane; i < g.nxt - g.ng; i += 32) {
+    const size_t q = g.at(i, j);
+    double sx, sy;
+    wave_speed(h[q], hu[q], hv[q], sx, sy);
+    if (sx > mx) mx = sx;
+    if (sy > my) my = sy;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double a = __shfl_xor_sync(0xffffffffu, mx, o);
+    const double b = __shfl_xor_sync(0xffffffffu, my, o);
+    mx = a > mx ? a : mx;
+    my = b > my ? b : my;
+  }
+  if (lane == 0) {
+    scratch[row] = mx;
+    scratch[kNoAllocMaxRows + row] = my;
+  }
+}
+
+// One block folds the row maxima and stores dt in the last slot.
+__global__ void k_rows_to_dt(Grid g, double cfl, double* scratch) {
+  const int nyp = g.ny_phys();
+  double mx = 0.0, my = 0.0;
+  for (int r = threadIdx.x; r < nyp; r += blockDim.x) {
+    const double a = scratch[r], b = scratch[kNoAllocMaxRows + r];
+    if (a > mx) mx = a;
+    if (b > my) my = b;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double a = __shfl_xor_sync(0xffffffffu, mx, o);
+    const double b = __shfl_xor_sync(0xffffffffu, my, o);
+    mx = a > mx ? a : mx;
+    my = b > my ? b : my;
+  }
+  __shared__ double wx[32], wy[32];
+  if ((threadIdx.x & 31) == 0) {
+    wx[threadIdx.x >> 5] = mx;
+    wy[threadIdx.x >> 5] = my;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+      if (wx[w] > mx) mx = wx[w];
+      if (wy[w] > my) my = wy[w];
+    }
+    scratch[2 * kNoAllocMaxRows] = cfl_dt(mx, my, g, cfl);
+  }
+}
+
+// Device address of the scratch array, looked up once per device with that
+// device current (the symbol's host-side name is not a device address).
+double* scratch_address(int device) {
+  static std::mutex mu;
+  static double* addr[64] = {};
+  if (device < 0 || device >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!addr[device]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) return nullptr;
+    addr[device] = static_cast<double*>(p);
+  }
+  return addr[device];
+}
+
+}  // namespace
+}  // namespace rkb
+
+extern "C" {
+
+int rkb_compute_timestep_noalloc(const double* h, const double* hu, const double* hv,
+                                 int nx_total, int ny_total, int nghost, int ld, double dx,
+                                 double dy, double cfl, double* dt_out) {
+  if (!rkb::grid_ok(nx_total, ny_total, nghost, ld) || !(dx > 0.0) || !(dy > 0.0)) return -2;
+  if (!h || !hu || !hv || !dt_out) return -2;
+  if (ny_total - 2 * nghost > rkb::kNoAllocMaxRows) {
+    rkb::set_last_error("rkb_compute_timestep_noalloc: " + std::to_string(ny_total - 2 * nghost) +
+                        " interior rows exceed the fixed scratch of " +
+                        std::to_string(rkb::kNoAllocMaxRows) + " rows");
+    return -2;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+  double* scratch = rkb::scratch_address(dev);
+  if (!scratch) return -1;
+  rkb::Grid g = rkb::make_grid(nx_total, ny_total, nghost, ld, dx, dy);
+  const int rows = g.ny_phys();
+  const int warps_per_block = 8;
+  rkb::k_row_speed<<<(rows + warps_per_block - 1) / warps_per_block, 32 * warps_per_block>>>(
+      g, h, hu, hv, scratch);
+  rkb::k_rows_to_dt<<<1, 1024>>>(g, cfl, scratch);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpy(dt_out, scratch + 2 * rkb::kNoAllocMaxRows, sizeof(double),
+                   cudaMemcpyDeviceToHost);
+  return e == cudaSuccess ? 0 : -1;
+}
+
+}  // extern "C"
