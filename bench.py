@@ -41,6 +41,12 @@ METRIC = "cell-updates/s on 1 B200: FP64 plain vs FP32, batched, fwd+adjoint, at
 BYTES_STAGE1 = 7 * 8
 BYTES_STAGE2 = 10 * 8
 BYTES_PER_CELL_UPDATE = BYTES_STAGE1 + BYTES_STAGE2
+# FP32 surface form: eta, hu, hv are 4-byte words, the bed stays 8 bytes:
+# stage 1 reads 3 x 4 + 8 and writes 3 x 4 (32 B); stage 2 reads 3 x 4 + 8 +
+# 3 x 4 and writes 3 x 4 (44 B): 76 B per cell-update.
+BYTES_STAGE1_32 = 3 * 4 + 8 + 3 * 4
+BYTES_STAGE2_32 = 3 * 4 + 8 + 3 * 4 + 3 * 4
+BYTES_PER_CELL_UPDATE_32 = BYTES_STAGE1_32 + BYTES_STAGE2_32
 
 
 def peaks():
@@ -119,9 +125,9 @@ def visible_gpu_index(local_rank: int) -> int:
     return local_rank
 
 
-def traffic_per_launch(n_cells: int):
+def traffic_per_launch(n_cells: int, precision: int = 64):
     """DRAM bytes per stage-2 launch from the committed ncu summary, scaled by cells."""
-    p = ROOT / "profiles" / "stage2_fp64_ncu.json"
+    p = ROOT / "profiles" / f"stage2_fp{precision}_ncu.json"
     if not p.is_file():
         return None
     d = json.loads(p.read_text())
@@ -199,6 +205,9 @@ def run_b200(args, rank, world, local_rank, dist):
     sim.set_initial_h(h)
     sim.finalize()
     sim.set_tile(args.tile)
+    if args.precision == 32:
+        sim.set_precision(32)
+        sim.set_sweep(args.sweep_cols, args.sweep_rows)
     lib = sim._lib
     cells = n * n
 
@@ -257,23 +266,29 @@ def run_b200(args, rank, world, local_rank, dist):
         sim.close()
         return 0
     hbm, peak_kind = peaks()
-    achieved = BYTES_STAGE2 * cells / (t_s2 * 1e-3) / 1e9
+    f32 = args.precision == 32
+    b_s2 = BYTES_STAGE2_32 if f32 else BYTES_STAGE2
+    b_cell = BYTES_PER_CELL_UPDATE_32 if f32 else BYTES_PER_CELL_UPDATE
+    achieved = b_s2 * cells / (t_s2 * 1e-3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": traffic_per_launch(cells),
-                "kernel": "k_stage<stage 2> (fused flux + update + RK2 average)",
+                "frac": achieved / hbm, "traffic": traffic_per_launch(cells, args.precision),
+                "kernel": ("k_sweep<stage 2> (FP32 surface form: flux + update + RK2 average)"
+                           if f32 else "k_stage<stage 2> (fused flux + update + RK2 average)"),
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                 if peak_kind == "measured" else "fallback 6650 GB/s",
                 "stage_ms": {"bc_stage1": t_bc1, "stage1": t_s1, "bc_stage2": t_bc2,
                              "stage2": t_s2},
-                "step_frac_of_hbm": BYTES_PER_CELL_UPDATE * value / world / 1e9 / hbm}
+                "bytes_per_cell_update": b_cell,
+                "step_frac_of_hbm": b_cell * value / world / 1e9 / hbm}
     line = {
         "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if f32 else "f64", "data": "synthetic",
         "config": {"workload": f"structured SSP-RK2 wet/dry step, {n}x{n} per GPU, dx=5 m, "
-                               "32-Gaussian bed, 0.5 m hump, Manning 0.025, walls, FP64 "
-                               "(parity build)",
+                               "32-Gaussian bed, 0.5 m hump, Manning 0.025, walls, "
+                               + ("FP32 surface form (FP64 bed differences, wet/dry tests "
+                                  "and mass sums)" if f32 else "FP64 (parity build)"),
                    "cells_per_gpu": cells, "tile": args.tile, "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (3 x 134 MB per buffer)"},
         "e2e": e2e,
@@ -298,6 +313,12 @@ def main():
     ap.add_argument("--tile", type=int, default=1,
                     help="stage-kernel variant (rkb_set_tile): 0-3 shared-memory tiles, "
                          "4/5 marching strips of 64/32 rows")
+    ap.add_argument("--precision", type=int, choices=(32, 64), default=64,
+                    help="64: FP64 depth form (reference arithmetic); 32: FP32 surface form")
+    ap.add_argument("--sweep-cols", type=int, choices=(0, 2, 4), default=0,
+                    help="FP32 form: columns per lane of the sweep kernel (0 = default)")
+    ap.add_argument("--sweep-rows", type=int, default=0,
+                    help="FP32 form: rows per warp sweep (0 = automatic)")
     ap.add_argument("--side", type=int, default=N_CELLS_SIDE,
                     help="grid side (smaller sides are for profiler captures only)")
     args = ap.parse_args()

@@ -141,6 +141,18 @@ int rkb_get_device_fields(void *handle, void **ptrs, int *pitch);
 int rkb_set_tile(void *handle, int tile);
 int rkb_get_tile(void *handle);
 
+/* Arithmetic form of the step: 64 = FP64 depth form (the reference's
+ * arithmetic, the default), 32 = FP32 surface form (eta = h + b, hu, hv in
+ * FP32; bed differences, wet/dry tests and mass sums in FP64).  May be called
+ * before or after rki_finalize; the host views and setters keep their FP64
+ * arrays in both forms.  -2 for any other value. */
+int rkb_set_precision(void *handle, int bits);
+int rkb_get_precision(void *handle);
+/* FP32 form: columns per lane of the sweep kernel (0 = default 2, or 2, 4)
+ * and rows each warp sweeps (0 = one wave of resident warps).  Results do
+ * not depend on either. */
+int rkb_set_sweep(void *handle, int cols_per_lane, int rows);
+
 /* Run n steps bracketed by CUDA events on the simulation's own stream;
  * *ms = device time of the n steps (state already resident). */
 int rkb_time_steps(void *handle, int n, double *ms);

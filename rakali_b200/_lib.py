@@ -101,6 +101,9 @@ def load(path: str | None = None):
     _sig(lib, "rkb_get_device_fields", [H, HP, IP], I)
     _sig(lib, "rkb_set_tile", [H, I], I)
     _sig(lib, "rkb_get_tile", [H], I)
+    _sig(lib, "rkb_set_precision", [H, I], I)
+    _sig(lib, "rkb_get_precision", [H], I)
+    _sig(lib, "rkb_set_sweep", [H, I, I], I)
     _sig(lib, "rkb_time_steps", [H, I, DP], I)
     _sig(lib, "rkb_profile_steps", [H, I, DP], I)
     _sig(lib, "rkb_cr_pow_third", [D], D)

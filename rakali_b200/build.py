@@ -4,8 +4,9 @@ Usage: python -m rakali_b200.build [--force] [--jobs N]
 
 The FP64 step and kernel-level translation units are compiled with
 --fmad=false so every a*b+c rounds twice, as the reference's arithmetic
-does; the host-only units are compiled by nvcc as well so the library links
-against the static CUDA runtime.
+does; the FP32 surface form uses contracted, flush-to-zero arithmetic; the
+host-only units are compiled by nvcc as well so the library links against
+the static CUDA runtime.
 """
 from __future__ import annotations
 
@@ -29,6 +30,10 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = {
     "rkb_step_f64.cu": ["--fmad=false"],
     "rkb_kernel_api.cu": ["--fmad=false"],
+    # FP32 surface form: contracted multiply-adds, flush-to-zero, approximate
+    # reciprocal and square root (the well-balanced products are written
+    # with explicit round-to-nearest intrinsics and are never contracted)
+    "rkb_step_f32.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
     "rkb_sim.cu": [],
     "rkb_api.cu": [],
     "rkb_config.cpp": [],

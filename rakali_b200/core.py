@@ -152,10 +152,12 @@ class Rakali:
     >>> sim.h_phys.max()
     """
 
-    def __init__(self, namelist=None, defer_init=False, **kwargs):
+    def __init__(self, namelist=None, defer_init=False, precision=64, **kwargs):
         self._lib = _lib.load()
         self._handle = ctypes.c_void_p()
         self._alive = False
+        if precision not in (32, 64):
+            raise ValueError(f"precision must be 32 or 64, got {precision!r}")
         if namelist is not None and kwargs:
             raise ValueError("Pass either a namelist file or keyword arguments, not both")
         if namelist is not None:
@@ -181,6 +183,8 @@ class Rakali:
         self._finalised = not defer_init
         self._alive = True
         self._query_grid()
+        if precision != 64:
+            self.set_precision(precision)
 
     # --- construction helpers -------------------------------------------
     @staticmethod
@@ -502,6 +506,24 @@ class Rakali:
         """Tile shape of the fused stage kernel (0: 32x8, 1: 32x16, 2: 64x4, 3: 16x16)."""
         self._check_alive()
         self._rc(self._lib.rkb_set_tile(self._handle, int(tile)), "set_tile")
+
+    @property
+    def precision(self) -> int:
+        """64: FP64 depth form (the reference's arithmetic); 32: FP32 surface form."""
+        self._check_alive()
+        return int(self._lib.rkb_get_precision(self._handle))
+
+    def set_precision(self, bits: int):
+        """Switch the step between the FP64 and the FP32 form (state carried over)."""
+        self._check_alive()
+        if bits not in (32, 64):
+            raise ValueError(f"precision must be 32 or 64, got {bits!r}")
+        self._rc(self._lib.rkb_set_precision(self._handle, int(bits)), "set_precision")
+
+    def set_sweep(self, cols_per_lane: int = 0, rows: int = 0):
+        """FP32 form: columns per lane (2 or 4; 0 = default) and rows per warp (0 = automatic)."""
+        self._check_alive()
+        self._rc(self._lib.rkb_set_sweep(self._handle, int(cols_per_lane), int(rows)), "set_sweep")
 
 
 def validate_namelist(text: str):

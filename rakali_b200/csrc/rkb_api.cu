@@ -181,7 +181,7 @@ int rki_step(void* handle, int n_steps) {
   if (!s) return kBadHandle;
   if (!s->is_finalised) return -1;
   int rc = s->step(n_steps);
-  return rc ? fail(rc, "device step failed") : 0;
+  return rc ? fail(rc, s->error_text().empty() ? "device step failed" : s->error_text()) : 0;
 }
 
 int rki_advance(void* handle, double target_time) {
@@ -189,7 +189,7 @@ int rki_advance(void* handle, double target_time) {
   if (!s) return kBadHandle;
   if (!s->is_finalised) return -1;
   int rc = s->advance(target_time);
-  return rc ? fail(rc, "device advance failed") : 0;
+  return rc ? fail(rc, s->error_text().empty() ? "device advance failed" : s->error_text()) : 0;
 }
 
 double rki_get_time(void* handle) {
@@ -387,6 +387,9 @@ int rkb_get_device_fields(void* handle, void** ptrs, int* pitch) {
   rkb::Sim* s = sim_of(handle);
   if (!s) return kBadHandle;
   if (!s->is_finalised) return -1;
+  if (s->precision() != 64)
+    return fail(-3, "device field views are FP64 depth-form arrays; the handle runs the FP32 "
+                    "surface form (rkb_set_precision(handle, 64) first)");
   if (s->ensure_device() != 0) return -1;
   rkb::StepArgs a = s->device_args();
   rkb::FieldSet F = s->current_buffer() ? a.U1 : a.U0;
@@ -426,6 +429,30 @@ int rkb_profile_steps(void* handle, int n, double* out5) {
 int rkb_get_tile(void* handle) {
   rkb::Sim* s = sim_of(handle);
   return s ? s->tile : kBadHandle;
+}
+
+int rkb_set_precision(void* handle, int bits) {
+  rkb::Sim* s = sim_of(handle);
+  if (!s) return kBadHandle;
+  if (bits != 32 && bits != 64) return fail(-2, "precision must be 32 or 64");
+  return s->set_precision(bits);
+}
+
+int rkb_get_precision(void* handle) {
+  rkb::Sim* s = sim_of(handle);
+  return s ? s->precision() : kBadHandle;
+}
+
+int rkb_set_sweep(void* handle, int cols_per_lane, int rows) {
+  rkb::Sim* s = sim_of(handle);
+  if (!s) return kBadHandle;
+  if (cols_per_lane != 0 && cols_per_lane != 2 && cols_per_lane != 4)
+    return fail(-2, "cols_per_lane must be 0 (default), 2 or 4");
+  if (rows < 0) return fail(-2, "rows must be >= 0 (0 selects the automatic value)");
+  s->sweep_cpl = cols_per_lane == 0 ? 2 : cols_per_lane;
+  s->sweep_rows = rows;
+  s->params_dirty = true;
+  return 0;
 }
 
 }  // extern "C"

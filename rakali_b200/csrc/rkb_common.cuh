@@ -88,7 +88,7 @@ struct StepCtl {
   unsigned int done_blocks;  // last-block counter of the final stage kernel
   unsigned int ms_done_blocks;
   int steps_run;       // steps executed since the host last cleared it
-  int pad_;
+  int error;           // nonzero: a bounded device-side wait gave up (FP32 sweep)
 };
 
 // ---------------------------------------------------------------------------

@@ -56,6 +56,57 @@ struct StepArgs {
 // Doubles of per-block partial storage the step kernels need.
 size_t partials_doubles(const Grid& g, int tile);
 
+// ---- FP32 surface form ----------------------------------------------------
+// State (eta = h + b, hu, hv) in FP32, bed in FP64 (rkb_step_f32.cu).
+struct FieldSet32 {
+  float* eta;
+  float* hu;
+  float* hv;
+};
+
+// Pointers of the surface form are offset so that element (i, j) is
+// p[i + j * g.pitch] and the first interior column of every row is
+// 128-byte aligned; the pitch also covers the right halo of the last strip.
+struct StepArgs32 {
+  Grid g;              // surface-form layout (pitch in elements)
+  StepCtl* ctl;
+  const Physics* phys;
+  const BcParams* bc;
+  FieldSet32 U0, U1, S;
+  double* b;           // bed, FP64, surface-form layout
+  Forcing fo;          // FP64 forcing fields, depth-form layout (pitch fpitch)
+  int fpitch;
+  double* partials;
+  double* eta_old[4];  // Chapman surfaces (FP64)
+  int hllc;
+  int cpl;             // columns per lane of the sweep (2 or 4)
+  int rows;            // rows per warp sweep
+  int nstrips, nrowblk;
+};
+
+// Strips and row blocks of the sweep for `rows` rows per warp and `cpl`
+// columns per lane (strips of 30 * cpl output columns).
+void sweep_shape(const Grid& g, int rows, int cpl, int& nstrips, int& nrowblk);
+// Columns of a row (counted from column 0) that the sweep's copies touch, for
+// any supported cpl: the surface-form pitch must cover it.
+size_t sweep_row_extent(const Grid& g);
+// Rows per sweep so that one wave of resident warps covers the grid.
+int auto_rows32(const Grid& g, int cpl);
+// Partial-sum doubles for any cpl and rows >= `rows`.
+size_t partials_doubles32(const Grid& g, int rows);
+cudaError_t configure_kernels32();
+int launches_per_step32(const StepArgs32& a);
+cudaError_t launch_step32(const StepArgs32& a, cudaStream_t s);
+cudaError_t launch_bc32(const StepArgs32& a, int stage, cudaStream_t s);
+cudaError_t launch_stage32_only(const StepArgs32& a, int stage, cudaStream_t s);
+cudaError_t launch_max_speed32(const StepArgs32& a, cudaStream_t s);
+// Conversions between the FP64 depth form and the FP32 surface form (every
+// cell, ghosts included); `bed_out` (may be null) receives the bed.
+cudaError_t launch_to_surface(const Grid& g64, const Grid& g32, FieldSet src, const double* b64,
+                              FieldSet32 dst, double* bed_out, cudaStream_t s);
+cudaError_t launch_to_depth(const Grid& g32, const Grid& g64, FieldSet32 src, const double* b32,
+                            FieldSet dst, double* bed_out, cudaStream_t s);
+
 // Set the shared-memory attributes of the stage kernels of one variant (call
 // before capturing them in a graph).
 cudaError_t configure_kernels(int tile, int hllc);

@@ -267,6 +267,8 @@ int Sim::alloc_device(std::string& err) {
 void Sim::free_device() {
   if (dmem_) cudaFree(dmem_);
   dmem_ = nullptr;
+  if (dmem32_) cudaFree(dmem32_);
+  dmem32_ = nullptr;
   for (double* f : {const_cast<double*>(args_.fo.wind_x), const_cast<double*>(args_.fo.wind_y),
                     const_cast<double*>(args_.fo.atm), const_cast<double*>(args_.fo.precip)})
     if (f) cudaFree(f);
@@ -302,6 +304,7 @@ int Sim::upload_state() {
                                 cudaMemcpyHostToDevice, stream_));
   }
   if (phys.forcing_active && upload_forcing() != 0) return -1;
+  if (precision_ == 32 && to_surface(false) != 0) return -1;
   hctl_->ms_valid = 0;
   RKB_TRY(cudaMemcpyAsync(&args_.ctl->ms_valid, &hctl_->ms_valid, sizeof(int),
                           cudaMemcpyHostToDevice, stream_));
@@ -394,11 +397,16 @@ static int pull(const StepArgs& a, int cur, bool stepped, bool full, double* con
   return cudaStreamSynchronize(s) == cudaSuccess ? 0 : -1;
 }
 
+int Sim::pull_state(bool full) {
+  if (precision_ == 32 && to_depth(full) != 0) return -1;
+  return pull(args_, cur_, stepped_, full, hf_, g, stream_);
+}
+
 void Sim::ensure_host() {
   if (host_is_current_) return;
   if (on_device_) {
     cudaSetDevice(device_);
-    pull(args_, cur_, stepped_, true, hf_, g, stream_);
+    pull_state(true);
     on_device_ = false;
     host_is_current_ = true;
   }
@@ -407,7 +415,7 @@ void Sim::ensure_host() {
 void Sim::sync_host() {
   if (is_initialised && on_device_ && !host_is_current_) {
     cudaSetDevice(device_);
-    pull(args_, cur_, stepped_, false, hf_, g, stream_);
+    pull_state(false);
     host_is_current_ = true;
   }
 }
@@ -415,7 +423,7 @@ void Sim::sync_host() {
 void Sim::sync_from_device() {
   if (is_initialised && on_device_) {
     cudaSetDevice(device_);
-    pull(args_, cur_, stepped_, true, hf_, g, stream_);
+    pull_state(true);
     on_device_ = false;
     host_is_current_ = true;
   }
@@ -469,6 +477,7 @@ int Sim::set_interior(int which, const double* data, int nx, int ny) {
       if (cudaMemcpy2DAsync(dstd[k], dpitch, hf_[k], wbytes, wbytes, g.nyt,
                             cudaMemcpyHostToDevice, stream_) != cudaSuccess)
         return -1;
+    if (precision_ == 32 && to_surface(true) != 0) return -1;
     hctl_->ms_valid = 0;
     if (cudaMemcpyAsync(&args_.ctl->ms_valid, &hctl_->ms_valid, sizeof(int),
                         cudaMemcpyHostToDevice, stream_) != cudaSuccess)
@@ -509,13 +518,21 @@ void Sim::pull_ctl() {
 }
 
 cudaGraphExec_t Sim::graph_for(int steps) {
+  const int rows = precision_ == 32 ? args32_.rows * 8 + args32_.cpl : 0;
   for (auto& ge : graphs_)
-    if (ge.steps == steps && ge.hllc == args_.hllc && ge.tile == args_.tile) return ge.exec;
-  GraphEntry ge{steps, args_.hllc, args_.tile, nullptr, nullptr};
+    if (ge.steps == steps && ge.hllc == args_.hllc && ge.tile == args_.tile &&
+        ge.prec == precision_ && ge.rows == rows)
+      return ge.exec;
+  GraphEntry ge{steps, args_.hllc, args_.tile, precision_, rows, nullptr, nullptr};
   if (cudaStreamSynchronize(stream_) != cudaSuccess) return nullptr;
   if (cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
     return nullptr;
-  for (int k = 0; k < steps; ++k) launch_step(args_, stream_);
+  for (int k = 0; k < steps; ++k) {
+    if (precision_ == 32)
+      launch_step32(args32_, stream_);
+    else
+      launch_step(args_, stream_);
+  }
   if (cudaStreamEndCapture(stream_, &ge.graph) != cudaSuccess) return nullptr;
   if (cudaGraphInstantiate(&ge.exec, ge.graph, 0) != cudaSuccess) return nullptr;
   graphs_.push_back(ge);
@@ -539,7 +556,12 @@ int Sim::prepare_run(int mode, double target, int nsteps) {
   RKB_TRY(cudaMemcpyAsync(&hctl_->ms_valid, &args_.ctl->ms_valid, sizeof(int),
                           cudaMemcpyDeviceToHost, stream_));
   RKB_TRY(cudaStreamSynchronize(stream_));
-  if (!hctl_->ms_valid) RKB_TRY(launch_max_speed(args_, stream_));
+  if (precision_ == 32) {
+    sync_args32();
+    if (!hctl_->ms_valid) RKB_TRY(launch_max_speed32(args32_, stream_));
+  } else if (!hctl_->ms_valid) {
+    RKB_TRY(launch_max_speed(args_, stream_));
+  }
   return 0;
 }
 
@@ -571,9 +593,11 @@ int Sim::run(int mode, double target, int nsteps) {
       const double t_before = t_current_;
       const int steps_before = step_count_;
       pull_ctl();
+      if (check_device_error() != 0) return -1;
       if (!(t_current_ > t_before) && step_count_ == steps_before) return -1;  // no progress
     }
   }
+  if (check_device_error() != 0) return -1;
   if (cudaGetLastError() != cudaSuccess) return -1;
   stepped_ = true;
   host_is_current_ = false;
@@ -605,6 +629,7 @@ int Sim::time_steps(int n, double* ms) {
   cudaEventDestroy(e1);
   *ms = f;
   pull_ctl();
+  if (check_device_error() != 0) return -1;
   stepped_ = true;
   host_is_current_ = false;
   return 0;
@@ -617,14 +642,15 @@ int Sim::profile_steps(int n, double out[5]) {
   for (auto& e : ev) RKB_TRY(cudaEventCreate(&e));
   double acc[4] = {0, 0, 0, 0};
   for (int s = 0; s < n; ++s) {
+    const bool f32 = precision_ == 32;
     RKB_TRY(cudaEventRecord(ev[0], stream_));
-    RKB_TRY(launch_bc(args_, 1, stream_));
+    RKB_TRY(f32 ? launch_bc32(args32_, 1, stream_) : launch_bc(args_, 1, stream_));
     RKB_TRY(cudaEventRecord(ev[1], stream_));
-    RKB_TRY(launch_stage_only(args_, 1, stream_));
+    RKB_TRY(f32 ? launch_stage32_only(args32_, 1, stream_) : launch_stage_only(args_, 1, stream_));
     RKB_TRY(cudaEventRecord(ev[2], stream_));
-    RKB_TRY(launch_bc(args_, 2, stream_));
+    RKB_TRY(f32 ? launch_bc32(args32_, 2, stream_) : launch_bc(args_, 2, stream_));
     RKB_TRY(cudaEventRecord(ev[3], stream_));
-    RKB_TRY(launch_stage_only(args_, 2, stream_));
+    RKB_TRY(f32 ? launch_stage32_only(args32_, 2, stream_) : launch_stage_only(args_, 2, stream_));
     RKB_TRY(cudaEventRecord(ev[4], stream_));
     RKB_TRY(cudaEventSynchronize(ev[4]));
     for (int k = 0; k < 4; ++k) {
@@ -635,11 +661,114 @@ int Sim::profile_steps(int n, double out[5]) {
   }
   for (auto& e : ev) cudaEventDestroy(e);
   for (int k = 0; k < 4; ++k) out[k] = acc[k] / n;
-  out[4] = (double)launches_per_step(args_);
+  out[4] = (double)(precision_ == 32 ? launches_per_step32(args32_) : launches_per_step(args_));
   pull_ctl();
+  if (check_device_error() != 0) return -1;
   stepped_ = true;
   host_is_current_ = false;
   return 0;
+}
+
+// ---------------------------------------------------------------------------
+// FP32 surface form
+// ---------------------------------------------------------------------------
+
+int Sim::set_precision(int p) {
+  if (p != 32 && p != 64) return -2;
+  if (p == precision_) return 0;
+  if (is_finalised && on_device_) ensure_host();  // state home in the old form
+  precision_ = p;
+  params_dirty = true;
+  return 0;
+}
+
+// Surface-form buffers: U0, U1, S (eta, hu, hv in FP32), the bed in FP64 and
+// the per-warp partials, in one allocation.  Rows start 128-byte aligned at
+// the first interior column; the pitch covers the last strip's right halo.
+int Sim::alloc_device32() {
+  if (dmem32_) return 0;
+  if (!stream_) return -1;
+  Grid g32 = g;
+  const int off = (32 - g.ng % 32) % 32;
+  const size_t need = (size_t)off + sweep_row_extent(g);
+  g32.pitch = (int)round_up(std::max(need, (size_t)off + (size_t)g.nxt), 32);
+  const size_t field = round_up((size_t)g32.pitch * (size_t)g.nyt, 64);  // elements
+  const size_t npart = round_up(partials_doubles32(g, 4), 64);
+  const size_t bytes = 9 * field * sizeof(float) + field * sizeof(double) + npart * sizeof(double);
+  if (cudaMalloc(&dmem32_, bytes) != cudaSuccess) {
+    dmem32_ = nullptr;
+    err_text_ = "device allocation of the FP32 surface form failed";
+    return -1;
+  }
+  if (cudaMemsetAsync(dmem32_, 0, bytes, stream_) != cudaSuccess) return -1;
+  float* fp = (float*)dmem32_;
+  auto f32 = [&](int k) { return fp + (size_t)k * field + off; };
+  args32_ = StepArgs32{};
+  args32_.g = g32;
+  args32_.U0 = {f32(0), f32(1), f32(2)};
+  args32_.U1 = {f32(3), f32(4), f32(5)};
+  args32_.S = {f32(6), f32(7), f32(8)};
+  double* dp = (double*)(fp + 9 * field);
+  args32_.b = dp + off;
+  args32_.partials = dp + field;
+  if (configure_kernels32() != cudaSuccess) return -1;
+  auto_rows_[0] = auto_rows32(g, 2);
+  auto_rows_[1] = auto_rows32(g, 4);
+  sync_args32();
+  return 0;
+}
+
+// Shared pointers and launch shape of the surface form (forcing fields may be
+// allocated late; the sweep rows may be overridden).
+void Sim::sync_args32() {
+  args32_.ctl = args_.ctl;
+  args32_.phys = args_.phys;
+  args32_.bc = args_.bc;
+  args32_.fo = args_.fo;
+  args32_.fpitch = g.pitch;
+  for (int w = 0; w < 4; ++w) args32_.eta_old[w] = args_.eta_old[w];
+  args32_.hllc = phys.use_hllc;
+  args32_.cpl = sweep_cpl == 4 ? 4 : 2;
+  int rows = sweep_rows > 0 ? sweep_rows : auto_rows_[args32_.cpl == 4 ? 1 : 0];
+  if (rows < 4) rows = 4;
+  args32_.rows = rows;
+  sweep_shape(g, rows, args32_.cpl, args32_.nstrips, args32_.nrowblk);
+}
+
+// FP64 staging buffers -> surface form: all three buffers (after an upload)
+// or the current one (after a setter).
+int Sim::to_surface(bool cur_only) {
+  if (alloc_device32() != 0) return -1;
+  const FieldSet src[3] = {args_.U0, args_.U1, args_.S};
+  const FieldSet32 dst[3] = {args32_.U0, args32_.U1, args32_.S};
+  for (int k = 0; k < 3; ++k) {
+    if (cur_only && k != cur_) continue;
+    RKB_TRY(launch_to_surface(g, args32_.g, src[k], args_.b, dst[k],
+                              k == (cur_only ? cur_ : 0) ? args32_.b : nullptr, stream_));
+  }
+  return 0;
+}
+
+// Surface form -> FP64 depth buffers ahead of a host read: the current state
+// and the bed, plus the RK2 save buffer when `full`.
+int Sim::to_depth(bool full) {
+  if (!dmem32_) return 0;
+  const FieldSet src64[2] = {args_.U0, args_.U1};
+  const FieldSet32 src32[2] = {args32_.U0, args32_.U1};
+  RKB_TRY(launch_to_depth(args32_.g, g, src32[cur_], args32_.b, src64[cur_], args_.b, stream_));
+  if (full && stepped_)
+    RKB_TRY(launch_to_depth(args32_.g, g, src32[cur_ ^ 1], args32_.b, src64[cur_ ^ 1], nullptr,
+                            stream_));
+  return 0;
+}
+
+int Sim::check_device_error() {
+  if (!hctl_->error) return 0;
+  err_text_ = "a bounded device-side wait for a bulk copy expired; the step was abandoned";
+  hctl_->error = 0;
+  cudaMemcpyAsync(&args_.ctl->error, &hctl_->error, sizeof(int), cudaMemcpyHostToDevice, stream_);
+  cudaStreamSynchronize(stream_);
+  return -1;
 }
 
 int Sim::step(int n) {

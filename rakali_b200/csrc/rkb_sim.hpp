@@ -58,6 +58,15 @@ class Sim {
   bool params_dirty = true;
   int tile = kTile32x16;  // fastest measured FP64 variant on B200
   int steps_per_graph_cap = 256;
+  int sweep_rows = 0;     // FP32 sweep: rows per warp (0: one wave of resident warps)
+  int sweep_cpl = 2;      // FP32 sweep: columns per lane (2 or 4)
+
+  // Arithmetic form of the step: 64 = FP64 depth form (the reference's
+  // arithmetic), 32 = FP32 surface form (rkb_step_f32.cu).  Switching brings
+  // the state home in the old form and uploads it in the new one.
+  int precision() const { return precision_; }
+  int set_precision(int p);
+  const std::string& error_text() const { return err_text_; }
 
   // Device pointers for the torch / kernel-level paths.
   StepArgs device_args() const { return args_; }
@@ -71,6 +80,12 @@ class Sim {
   void free_device();
   int upload_state();
   int upload_params();
+  int alloc_device32();
+  int to_surface(bool cur_only);
+  int to_depth(bool full);
+  int pull_state(bool full);
+  void sync_args32();
+  int check_device_error();
   int upload_forcing();
   int run(int mode, double target, int nsteps);
   int prepare_run(int mode, double target, int nsteps);
@@ -93,9 +108,16 @@ class Sim {
   int cur_ = 0;
   double t_current_ = 0.0, dt_ = 0.0;
   int step_count_ = 0;
+  int precision_ = 64;
+  std::string err_text_;
+
+  // FP32 surface form: one more allocation, same control/parameter blocks
+  void* dmem32_ = nullptr;
+  StepArgs32 args32_{};
+  int auto_rows_[2] = {0, 0};  // automatic rows for 2 and 4 columns per lane
 
   struct GraphEntry {
-    int steps, hllc, tile;
+    int steps, hllc, tile, prec, rows;
     cudaGraph_t graph;
     cudaGraphExec_t exec;
   };

@@ -1,0 +1,1110 @@
+// FP32 surface form of the structured SSP-RK2 step (sm_100a).
+//
+// State: the free surface eta = h + b and the momenta hu, hv in FP32; the bed
+// b in FP64.  Same scheme and step structure as the FP64 kernels
+// (rki_kernel_flux.F90:104-783, rki_kernel_fused.F90:164-471,
+// rki_boundary.F90:40-552, rki_kernel_timestep.F90:16-74), with:
+//
+//  * every difference against the bed in FP64: the depth h = eta - b of a
+//    cell, the reconstructed depths eta_face - b_cell and the Audusse
+//    hydrostatic depths eta_face - max(b_L, b_R); the wet/dry threshold tests
+//    are made on those FP64 values;
+//  * the domain sums (mass budget partials) in FP64;
+//  * the rest (slopes, Riemann fluxes, update, friction) in FP32.
+//
+// The momentum update never subtracts two hydrostatic pressures g/2 h^2: each
+// face returns its flux in excess of the left hydrostatic pressure and the
+// pressure jump g/2 (dh_hyd)(h_hyd,L + h_hyd,R) with dh_hyd an FP64
+// difference, and each cell adds its own reconstruction term g h s (s = the
+// limited surface slope); see face().  Lake at rest is exact: a flat wet
+// surface has zero slopes, both sides of a face then have the same
+// hydrostatic depth, so the jump, the excess flux and the cell term are all
+// exactly zero.  Dry cells store the bed rounded down (eta <= b), so they
+// read back as h <= 0.
+//
+// Data movement: one warp sweeps a strip of 124 columns up a range of rows.
+// Lane l (0..30) owns columns x0 + 4l .. x0 + 4l + 3; lane 31 owns the right
+// halo and the left halo (x0 - 2, x0 - 1) and computes the strip's right
+// edge face.  Rows arrive through a per-warp ring of shared-memory slots
+// filled by 1D bulk asynchronous copies (cp.async.bulk, completion on an
+// mbarrier); x-neighbours are exchanged with warp shuffles, y-neighbours
+// stay in registers.  No block barrier on the data path.  Every wait is
+// bounded in time; a wait that gives up sets StepCtl::error.
+#include <cstdint>
+
+#include "rkb_crmath.cuh"
+#include "rkb_kernels.h"
+#include "rkb_stepctl.cuh"
+
+namespace rkb {
+namespace {
+
+constexpr float kGf = 9.80665f;
+constexpr float kHalfGf = 0.5f * kGf;
+constexpr float kDryF = 1.0e-6f;
+constexpr float kEps4F = 5.062499999999998e-16f;
+constexpr float kSqrt2F = 1.41421356f;
+constexpr float kFroude2G = 50.0f * 50.0f * kGf;
+constexpr unsigned kFull = 0xffffffffu;
+
+// Strip geometry and shared-memory ring.  With C columns per lane, lanes
+// 0..29 own the strip's 30 C output columns, lane 30 the C columns right of
+// the strip and lane 31 the C columns left of it: the 32 lanes form a ring of
+// consecutive column groups (31 -> 0 -> 1 -> ... -> 30), so neighbour
+// exchanges are plain shuffles and every lane runs the same code.
+constexpr int kWarps = 4;  // warps (strips) per block
+constexpr int kNbuf = 5;   // ring slots per warp
+template <int C>
+struct Lay {
+  static constexpr int kStrip = 30 * C;                     // output columns
+  static constexpr int kSeg = (4 + 31 * C + 3) / 4 * 4;     // copied: [x0 - 4, x0 - 4 + kSeg)
+  // slot layout (bytes): eta, hu, hv (FP32, kSeg), b (FP64, kSeg); stage 2
+  // adds the RK2 save eta, hu, hv of the output columns (FP32, kStrip)
+  static constexpr int kOffE = 0;
+  static constexpr int kOffU = kOffE + 4 * kSeg;
+  static constexpr int kOffV = kOffU + 4 * kSeg;
+  static constexpr int kOffB = kOffV + 4 * kSeg;
+  static constexpr int kOffOE = kOffB + 8 * kSeg;
+  static constexpr int kOffOU = kOffOE + 4 * kStrip;
+  static constexpr int kOffOV = kOffOU + 4 * kStrip;
+  static constexpr int kSlot1 = kOffOE;
+  static constexpr int kSlot2 = kOffOV + 4 * kStrip;
+  static_assert(kStrip % 4 == 0 && kSeg % 4 == 0 && kSlot2 % 16 == 0,
+                "bulk copies need 16-byte aligned rows and slots");
+  static constexpr int slot(int stage) { return stage == 2 ? kSlot2 : kSlot1; }
+};
+constexpr long long kWaitCycles = 2000000000ll;  // ~1 s at B200 clocks
+
+// ---------------------------------------------------------------------------
+// PTX helpers: bulk copies, mbarriers, approximate FP32 math
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes,
+                                         uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Wait for a phase of `bar` for at most kWaitCycles; warp-uniform result.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  bool ok = mbar_try_wait(bar, parity);
+  if (!ok) {
+    const long long t0 = clock64();
+    while (!(ok = mbar_try_wait(bar, parity)))
+      if (clock64() - t0 > kWaitCycles) break;
+  }
+  return __all_sync(kFull, ok);
+}
+
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// Surface value of depth h over bed b; a dry cell stores the bed rounded
+// down so that it reads back as h <= 0.
+__device__ __forceinline__ float surface_of(double h, double b) {
+  return h > 0.0 ? __double2float_rn(h + b) : __double2float_rd(b);
+}
+
+// Cell flags: bit 0 h >= DRY_THRESHOLD, bit 1 h >= THIN_THRESHOLD (FP64 test).
+__device__ __forceinline__ unsigned cell_flags(float e, double b) {
+  const double h = (double)e - b;
+  return (h >= kDry ? 1u : 0u) | (h >= kThin ? 2u : 0u);
+}
+
+__device__ __forceinline__ float minmodf(float a, float b) {
+  if (a * b <= 0.0f) return 0.0f;
+  return fabsf(a) < fabsf(b) ? a : b;
+}
+
+struct Slope {
+  float e, u, v;
+};
+
+// Limited slope (rki_kernel_flux.F90:159-181): zero unless the cell is thick
+// and both neighbours are wet.
+__device__ __forceinline__ Slope slope(unsigned fm, unsigned fc, unsigned fp, float em, float ec,
+                                       float ep, float um, float uc, float up, float vm, float vc,
+                                       float vp) {
+  Slope s{0.0f, 0.0f, 0.0f};
+  if ((fc & 2u) && (fm & 1u) && (fp & 1u)) {
+    s.e = minmodf(ec - em, ep - ec);
+    s.u = minmodf(uc - um, up - uc);
+    s.v = minmodf(vc - vm, vp - vc);
+  }
+  return s;
+}
+
+// One face.  n = normal momentum, t = tangential momentum.
+//
+// The reference hands each cell the face flux F together with its
+// well-balanced terms, F - Q(h_hyd) + Q(h_face) with Q(h) = g/2 h^2
+// (rki_kernel_flux.F90:361-369).  In FP32 those are differences of numbers of
+// size g/2 h^2 (~490 in 10 m of water) whose rounding swamps the pressure
+// gradient, so the same sums are regrouped to subtract only small numbers:
+//
+//   en = F - Q(h_hyd,L)                  flux in excess of the left hydrostatic pressure
+//   dq = Q(h_hyd,R) - Q(h_hyd,L) = g/2 (h_hyd,R - h_hyd,L)(h_hyd,R + h_hyd,L)
+//
+// with the hydrostatic depth jump taken as an FP64 difference.  A cell with
+// faces l, r then gets  en_r - en_l + dq_l + [Q(h_face,r) - Q(h_face,l)],
+// the bracket being the cell's own reconstruction term (cell_pressure).
+struct FaceF {
+  float fh, en, dq, ft;
+};
+
+template <bool HLLC>
+__device__ __forceinline__ FaceF face(float eL, float nL, float tL, double bL, float eR, float nR,
+                                      float tR, double bR) {
+  const double bmax = bL > bR ? bL : bR;
+  const double eLd = (double)eL, eRd = (double)eR;
+  const double hLd = eLd - bL, hRd = eRd - bR;  // reconstructed depths
+  const double yLd = pos(eLd - bmax), yRd = pos(eRd - bmax);  // Audusse hydrostatic depths
+  const float hL = fmaxf(__double2float_rn(hLd), 0.0f);
+  const float hR = fmaxf(__double2float_rn(hRd), 0.0f);
+  const float yl = __double2float_rn(yLd);
+  const float yr = __double2float_rn(yRd);
+  const float dy = __double2float_rn(yRd - yLd);  // hydrostatic depth jump, FP64 difference
+  const bool wyl = yLd > kDry, wyr = yRd > kDry;
+  float ul = 0.0f, vl = 0.0f, ur = 0.0f, vr = 0.0f;
+  if (hLd > kDry) {
+    const float r = rcp_approx(hL);
+    ul = nL * r;
+    vl = tL * r;
+  }
+  if (hRd > kDry) {
+    const float r = rcp_approx(hR);
+    ur = nR * r;
+    vr = tR * r;
+  }
+  // HLL / HLLC on the hydrostatic states (rki_kernel_flux.F90:410-783)
+  const float qnl = yl * ul, qtl = yl * vl, qnr = yr * ur, qtr = yr * vr;
+  const float unl = wyl ? ul : 0.0f, utl = wyl ? vl : 0.0f;
+  const float unr = wyr ? ur : 0.0f, utr = wyr ? vr : 0.0f;
+  const float al = sqrt_approx(kGf * yl), ar = sqrt_approx(kGf * yr);
+  float sl, sr;
+  if (!wyr) {
+    sl = unl - al;
+    sr = unl + 2.0f * al;
+  } else if (!wyl) {
+    sl = unr - 2.0f * ar;
+    sr = unr + ar;
+  } else {
+    sl = fminf(unl - al, unr - ar);
+    sr = fmaxf(unl + al, unr + ar);
+  }
+  FaceF o;
+  o.dq = kHalfGf * dy * (yl + yr);
+  const float ln = qnl * unl, rn = qnr * unr;  // advective parts of the normal fluxes
+  const float lt = qnl * utl, rt = qnr * utr;
+  if (sl >= 0.0f) {
+    o.fh = qnl; o.en = ln; o.ft = lt;
+  } else if (sr <= 0.0f) {
+    o.fh = qnr; o.en = rn + o.dq; o.ft = rt;
+  } else {
+    // F = F_L - s_L (F_R - F_L - s_R (U_R - U_L)) / (s_R - s_L)
+    const float inv = rcp_approx(sr - sl);
+    o.fh = qnl - sl * ((qnr - qnl) - sr * dy) * inv;
+    o.en = ln - sl * (((rn - ln) + o.dq) - sr * (qnr - qnl)) * inv;
+    if (!HLLC) {
+      o.ft = lt - sl * ((rt - lt) - sr * (qtr - qtl)) * inv;
+    } else {
+      const float den = yr * (unr - sr) - yl * (unl - sl);
+      float ss;
+      if (fabsf(den) > kDryF)
+        ss = (sl * yr * (unr - sr) - sr * yl * (unl - sl)) * rcp_approx(den);
+      else
+        ss = 0.5f * (unl + unr);
+      o.ft = ss >= 0.0f ? o.fh * utl : o.fh * utr;
+    }
+  }
+  return o;
+}
+
+// Q(h_face,r) - Q(h_face,l) of a cell of depth hc whose limited surface slope
+// is s: its reconstructed depths are hc + s/2 and hc - s/2 (rki_kernel_flux.F90:
+// 186-224), so the difference is g hc s unless a face depth is clipped at 0.
+__device__ __forceinline__ float cell_pressure(float hc, float s) {
+  const float a = hc + 0.5f * s, c = hc - 0.5f * s;
+  if (a >= 0.0f && c >= 0.0f) return kGf * hc * s;
+  const float pa = fmaxf(a, 0.0f), pc = fmaxf(c, 0.0f);
+  return kHalfGf * (pa - pc) * (pa + pc);
+}
+
+// Clamp + KP07 + Froude backstop (rki_kernel_fused.F90:93-119) with the
+// threshold tests on the FP64 depth; returns that depth.
+__device__ __forceinline__ double protect(float& e, float& hu, float& hv, double b, float& h) {
+  const double hd = (double)e - b;
+  if (hd < 0.0) {
+    e = __double2float_rd(b);
+    hu = 0.0f;
+    hv = 0.0f;
+    h = 0.0f;
+    return 0.0;
+  }
+  h = __double2float_rn(hd);
+  if (hd < kDry) {
+    hu = 0.0f;
+    hv = 0.0f;
+    return hd;
+  }
+  const float h2 = h * h;
+  const float h4 = h2 * h2;
+  if (h4 < kEps4F) {
+    const float f = kSqrt2F * h2 * rsqrt_approx(h4 + kEps4F);
+    hu = hu * f;
+    hv = hv * f;
+  }
+  const float q2 = hu * hu + hv * hv;
+  const float lim = kFroude2G * h * h2;  // (Fr_max^2 g h) h^2
+  if (q2 > lim) {
+    const float sc = sqrt_approx(lim) * rsqrt_approx(q2);
+    hu = hu * sc;
+    hv = hv * sc;
+  }
+  return hd;
+}
+
+// (|u| + c) along x and y with the KP07 velocity (rki_kernel_timestep.F90:52-66).
+__device__ __forceinline__ void wave_speed32(double hd, float h, float hu, float hv, float& sx,
+                                             float& sy) {
+  sx = 0.0f;
+  sy = 0.0f;
+  if (hd > kDry) {
+    const float c = sqrt_approx(kGf * h);
+    const float h2 = h * h;
+    const float f = kSqrt2F * h * rsqrt_approx(h2 * h2 + kEps4F);
+    sx = fabsf(hu) * f + c;
+    sy = fabsf(hv) * f + c;
+  }
+}
+
+template <int C>
+struct Row {
+  float e[C], u[C], v[C];
+  float h[C];   // cell depth (FP64 difference, rounded)
+  double b[C];
+  unsigned f;   // 2 flag bits per column
+};
+
+__device__ __forceinline__ unsigned colf(unsigned f, int k) { return (f >> (2 * k)) & 3u; }
+
+template <int C>
+__device__ __forceinline__ void ld_f(const unsigned char* p, float (&o)[C]) {
+  if (C == 4) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    o[0] = t.x; o[1] = t.y; o[2 % C] = t.z; o[3 % C] = t.w;
+  } else {
+    const float2 t = *reinterpret_cast<const float2*>(p);
+    o[0] = t.x; o[1] = t.y;
+  }
+}
+
+template <int C>
+__device__ __forceinline__ void ld_d(const unsigned char* p, double (&o)[C]) {
+#pragma unroll
+  for (int k = 0; k < C; k += 2) {
+    const double2 t = *reinterpret_cast<const double2*>(p + 8 * k);
+    o[k] = t.x;
+    o[k + 1] = t.y;
+  }
+}
+
+// This lane's C columns of a row from its ring slot (`base` = first column's
+// index in the copied segment).
+template <int C>
+__device__ __forceinline__ void read_row(const unsigned char* slot, int base, Row<C>& r) {
+  using L = Lay<C>;
+  ld_f<C>(slot + L::kOffE + 4 * base, r.e);
+  ld_f<C>(slot + L::kOffU + 4 * base, r.u);
+  ld_f<C>(slot + L::kOffV + 4 * base, r.v);
+  ld_d<C>(slot + L::kOffB + 8 * base, r.b);
+  unsigned f = 0;
+#pragma unroll
+  for (int k = 0; k < C; ++k) {
+    const double hd = (double)r.e[k] - r.b[k];
+    r.h[k] = __double2float_rn(hd);
+    f |= ((hd >= kDry ? 1u : 0u) | (hd >= kThin ? 2u : 0u)) << (2 * k);
+  }
+  r.f = f;
+}
+
+template <int C>
+__device__ __forceinline__ void yslopes(const Row<C>& m, const Row<C>& c, const Row<C>& p,
+                                        Slope (&s)[C]) {
+#pragma unroll
+  for (int k = 0; k < C; ++k)
+    s[k] = slope(colf(m.f, k), colf(c.f, k), colf(p.f, k), m.e[k], c.e[k], p.e[k], m.u[k], c.u[k],
+                 p.u[k], m.v[k], c.v[k], p.v[k]);
+}
+
+// y-faces between rows lo and hi (normal momentum hv, tangential hu).
+template <bool HLLC, int C>
+__device__ __forceinline__ void yfaces(const Row<C>& lo, const Slope (&sl)[C], const Row<C>& hi,
+                                       const Slope (&sh)[C], FaceF (&f)[C]) {
+#pragma unroll
+  for (int k = 0; k < C; ++k)
+    f[k] = face<HLLC>(lo.e[k] + 0.5f * sl[k].e, lo.v[k] + 0.5f * sl[k].v, lo.u[k] + 0.5f * sl[k].u,
+                      lo.b[k], hi.e[k] - 0.5f * sh[k].e, hi.v[k] - 0.5f * sh[k].v,
+                      hi.u[k] - 0.5f * sh[k].u, hi.b[k]);
+}
+
+// What a cell keeps of the face below it: mass flux, tangential (hu) flux,
+// excess normal flux and hydrostatic pressure jump.
+struct BotFace {
+  float fh, ft, en, dq;
+};
+
+template <int C>
+__device__ __forceinline__ void st_f(float* p, const float (&v)[C]) {
+  if (C == 4)
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2 % C], v[3 % C]);
+  else
+    *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+}
+
+// ---------------------------------------------------------------------------
+// Stage kernel
+// ---------------------------------------------------------------------------
+// STAGE 1: U^n (buffer cur) -> U* (S).  STAGE 2: U*, U^n -> U^{n+1} (cur^1).
+template <int C, bool HLLC, int STAGE>
+__global__ void __launch_bounds__(kWarps * 32, C == 2 ? 4 : 2) k_sweep(StepArgs32 a) {
+  using L = Lay<C>;
+  constexpr int SLOT = L::slot(STAGE);
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) unsigned long long bars[kWarps][kNbuf];
+  __shared__ float rot[2];
+  StepCtl* ctl = a.ctl;
+  if (!ctl->active) return;
+  const Grid g = a.g;
+  const Physics* phys = a.phys;
+  const double dtd = ctl->dt;
+  const float dt = (float)dtd;
+  const int cur = ctl->cur;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) {
+    // Coriolis rotation cos/sin(f dt) (rki_kernel_fused.F90:211-214)
+    double sn = 0.0, cs = 1.0;
+    if (fabs(phys->coriolis_f) > 1.0e-20) cr_sincos(phys->coriolis_f * dtd, sn, cs);
+    rot[0] = (float)cs;
+    rot[1] = (float)sn;
+  }
+  __syncthreads();
+  const bool has_cor = fabs(phys->coriolis_f) > 1.0e-20;
+  const bool friction = phys->manning_n > 0.0;
+  const float gn2dt = (float)(kG * phys->manning_n * phys->manning_n) * dt;
+  const bool forcing = phys->forcing_active != 0;
+  const bool sponge_on = a.bc->sponge_width > 0 && a.bc->sponge_strength > 0.0;
+  const float rdx = (float)(1.0 / g.dx), rdy = (float)(1.0 / g.dy);
+  const float cosf_ = rot[0], sinf_ = rot[1];
+
+  const FieldSet32 in = STAGE == 2 ? a.S : (cur ? a.U1 : a.U0);
+  const FieldSet32 old = cur ? a.U1 : a.U0;
+  const FieldSet32 out = STAGE == 1 ? a.S : (cur ? a.U0 : a.U1);
+
+  const unsigned nw = gridDim.x * kWarps;
+  const unsigned gw = blockIdx.x * kWarps + warp;
+  double part = 0.0, sponge_d = 0.0;
+  float wsx = 0.0f, wsy = 0.0f;
+
+  if (gw < (unsigned)(a.nstrips * a.nrowblk)) {  // warp-uniform
+    const int strip = (int)(gw % (unsigned)a.nstrips);
+    const int rb = (int)(gw / (unsigned)a.nstrips);
+    const int x0 = g.ng + strip * L::kStrip;
+    const int y0 = g.ng + rb * a.rows;
+    const int yend = min(y0 + a.rows, g.nyt - g.ng);
+    const int r0 = y0 - 2, rlast = yend + 1;
+    const int li = lane == 31 ? -1 : lane;   // column group of this lane in the ring
+    const int base = 4 + C * li;             // its first column in the copied segment
+    const bool out_lane = lane < 30;
+    unsigned char* ring = smem + warp * (kNbuf * SLOT);
+    const uint32_t ring_s = smem_u32(ring);
+    const uint32_t bar0 = smem_u32(&bars[warp][0]);
+    if (lane == 0) {
+      for (int s = 0; s < kNbuf; ++s) mbar_init(bar0 + 8 * s, 1);
+      fence_mbar_init();
+    }
+    __syncwarp();
+
+    auto issue = [&](int r) {  // lane 0
+      const int s = (r - r0) % kNbuf;
+      const uint32_t dst = ring_s + s * SLOT, bar = bar0 + 8 * s;
+      const bool with_old = STAGE == 2 && r >= y0 && r < yend;
+      mbar_expect_tx(bar, with_old ? L::kSlot2 : L::kSlot1);
+      const size_t ro = (size_t)r * (size_t)g.pitch + (size_t)(x0 - 4);
+      bulk_g2s(dst + L::kOffE, in.eta + ro, 4 * L::kSeg, bar);
+      bulk_g2s(dst + L::kOffU, in.hu + ro, 4 * L::kSeg, bar);
+      bulk_g2s(dst + L::kOffV, in.hv + ro, 4 * L::kSeg, bar);
+      bulk_g2s(dst + L::kOffB, a.b + ro, 8 * L::kSeg, bar);
+      if (with_old) {
+        const size_t ro2 = ro + 4;
+        bulk_g2s(dst + L::kOffOE, old.eta + ro2, 4 * L::kStrip, bar);
+        bulk_g2s(dst + L::kOffOU, old.hu + ro2, 4 * L::kStrip, bar);
+        bulk_g2s(dst + L::kOffOV, old.hv + ro2, 4 * L::kStrip, bar);
+      }
+    };
+    auto slot_of = [&](int r) { return ring + ((r - r0) % kNbuf) * SLOT; };
+    auto wait_row = [&](int r) {
+      const int k = r - r0;
+      return mbar_wait(bar0 + 8 * (k % kNbuf), (uint32_t)((k / kNbuf) & 1));
+    };
+
+    int issued = min(r0 + kNbuf - 1, rlast);
+    if (lane == 0)
+      for (int r = r0; r <= issued; ++r) issue(r);
+
+    // prologue: rows y0-2 .. y0+1, slopes of y0-1 and y0, face y0-1/2
+    Row<C> A, B, Cr, D, E;
+    bool ok = true;
+    int waited = r0 - 1;  // last row whose copies have landed
+    auto take = [&](int r, Row<C>& R) {
+      if (!ok) return;
+      ok = wait_row(r);
+      if (ok) {
+        read_row<C>(slot_of(r), base, R);
+        waited = r;
+      }
+    };
+    take(r0, A);
+    take(r0 + 1, B);
+    take(y0, Cr);
+    take(y0 + 1, D);
+    Slope sC[C];
+    BotFace bot[C];
+    if (ok) {
+      Slope sB[C];
+      yslopes<C>(A, B, Cr, sB);
+      yslopes<C>(B, Cr, D, sC);
+      FaceF f[C];
+      yfaces<HLLC, C>(B, sB, Cr, sC, f);
+#pragma unroll
+      for (int k = 0; k < C; ++k) bot[k] = BotFace{f[k].fh, f[k].ft, f[k].en, f[k].dq};
+      __syncwarp();
+      if (lane == 0) {
+        fence_proxy_async();
+        for (int r = r0 + kNbuf; r <= min(r0 + kNbuf + 1, rlast); ++r) issue(r);
+      }
+      issued = min(r0 + kNbuf + 1, rlast);
+    }
+
+    const int src_r = (lane + 1) & 31, src_l = (lane + 31) & 31;
+    for (int j = y0; ok && j < yend; ++j) {
+      ok = wait_row(j + 2);
+      if (!ok) break;
+      waited = j + 2;
+      read_row<C>(slot_of(j + 2), base, E);
+      Slope sD[C];
+      yslopes<C>(Cr, D, E, sD);
+      FaceF top[C];
+      yfaces<HLLC, C>(Cr, sC, D, sD, top);
+
+      // ---- x direction on row j: neighbour columns by shuffle around the ring ----
+      const float pe = __shfl_sync(kFull, Cr.e[0], src_r);
+      const float pu = __shfl_sync(kFull, Cr.u[0], src_r);
+      const float pv = __shfl_sync(kFull, Cr.v[0], src_r);
+      const unsigned pf = __shfl_sync(kFull, Cr.f & 3u, src_r);
+      const float me = __shfl_sync(kFull, Cr.e[C - 1], src_l);
+      const float mu = __shfl_sync(kFull, Cr.u[C - 1], src_l);
+      const float mv = __shfl_sync(kFull, Cr.v[C - 1], src_l);
+      const unsigned mf = __shfl_sync(kFull, colf(Cr.f, C - 1), src_l);
+      Slope sx[C];
+#pragma unroll
+      for (int k = 0; k < C; ++k) {
+        const float em = k ? Cr.e[k - 1] : me, um = k ? Cr.u[k - 1] : mu, vm = k ? Cr.v[k - 1] : mv;
+        const unsigned fm = k ? colf(Cr.f, k - 1) : mf;
+        const float ep = k < C - 1 ? Cr.e[k + 1] : pe, up = k < C - 1 ? Cr.u[k + 1] : pu;
+        const float vp = k < C - 1 ? Cr.v[k + 1] : pv;
+        const unsigned fp = k < C - 1 ? colf(Cr.f, k + 1) : pf;
+        sx[k] = slope(fm, colf(Cr.f, k), fp, em, Cr.e[k], ep, um, Cr.u[k], up, vm, Cr.v[k], vp);
+      }
+      // left state of this lane's first x-face: the left lane's last column
+      const float le = __shfl_sync(kFull, Cr.e[C - 1] + 0.5f * sx[C - 1].e, src_l);
+      const float lu = __shfl_sync(kFull, Cr.u[C - 1] + 0.5f * sx[C - 1].u, src_l);
+      const float lv = __shfl_sync(kFull, Cr.v[C - 1] + 0.5f * sx[C - 1].v, src_l);
+      const double lb = __shfl_sync(kFull, Cr.b[C - 1], src_l);
+      FaceF xf[C];
+#pragma unroll
+      for (int k = 0; k < C; ++k) {
+        const float eL = k ? Cr.e[k - 1] + 0.5f * sx[k - 1].e : le;
+        const float uL = k ? Cr.u[k - 1] + 0.5f * sx[k - 1].u : lu;
+        const float vL = k ? Cr.v[k - 1] + 0.5f * sx[k - 1].v : lv;
+        const double bL = k ? Cr.b[k - 1] : lb;
+        xf[k] = face<HLLC>(eL, uL, vL, bL, Cr.e[k] - 0.5f * sx[k].e, Cr.u[k] - 0.5f * sx[k].u,
+                           Cr.v[k] - 0.5f * sx[k].v, Cr.b[k]);
+      }
+      // right face of the last column = the right lane's first face
+      const float rfh = __shfl_sync(kFull, xf[0].fh, src_r);
+      const float ren = __shfl_sync(kFull, xf[0].en, src_r);
+      const float rft = __shfl_sync(kFull, xf[0].ft, src_r);
+
+      // RK2 save of this row (stage 2), then release the slot of row j
+      float oe[C], ou[C], ov[C];
+      if (STAGE == 2) {
+#pragma unroll
+        for (int k = 0; k < C; ++k) { oe[k] = 0.0f; ou[k] = 0.0f; ov[k] = 0.0f; }
+        if (out_lane) {
+          const unsigned char* sj = slot_of(j);
+          ld_f<C>(sj + L::kOffOE + 4 * C * lane, oe);
+          ld_f<C>(sj + L::kOffOU + 4 * C * lane, ou);
+          ld_f<C>(sj + L::kOffOV + 4 * C * lane, ov);
+        }
+      }
+      __syncwarp();
+      if (j + kNbuf <= rlast) {
+        if (lane == 0) {
+          fence_proxy_async();
+          issue(j + kNbuf);
+        }
+        issued = j + kNbuf;
+      }
+
+      // ---- cell updates of row j ----
+      float ne[C], nu[C], nv[C];
+      const int ib = x0 + C * li;
+#pragma unroll
+      for (int k = 0; k < C; ++k) {
+        const float Rfh = k < C - 1 ? xf[k + 1].fh : rfh;
+        const float Ren = k < C - 1 ? xf[k + 1].en : ren;
+        const float Rft = k < C - 1 ? xf[k + 1].ft : rft;
+        const float px = cell_pressure(Cr.h[k], sx[k].e), py = cell_pressure(Cr.h[k], sC[k].e);
+        const float dE = -(Rfh - xf[k].fh) * rdx - (top[k].fh - bot[k].fh) * rdy;
+        const float dU = -(((Ren - xf[k].en) + xf[k].dq) + px) * rdx - (top[k].ft - bot[k].ft) * rdy;
+        const float dV = -(Rft - xf[k].ft) * rdx - (((top[k].en - bot[k].en) + bot[k].dq) + py) * rdy;
+        float e = Cr.e[k] + dt * dE;
+        float hu = Cr.u[k] + dt * dU;
+        float hv = Cr.v[k] + dt * dV;
+        const double bc = Cr.b[k];
+        float h;
+        const double hd = protect(e, hu, hv, bc, h);
+        const int i = ib + k;
+        const bool valid = out_lane && i < g.nxt - g.ng;  // forcing reads stay in bounds
+        if (hd > kDry) {
+          // Manning friction (rki_kernel_fused.F90:121-130): hu / (1 + dt g n^2 |q| h^-7/3)
+          if (friction) {
+            const float den = 1.0f + gn2dt * sqrt_approx(hu * hu + hv * hv) * __powf(h, -7.0f / 3.0f);
+            const float r = rcp_approx(den);
+            hu = hu * r;
+            hv = hv * r;
+          }
+          if (forcing && valid) {  // wind, pressure gradient (rki_kernel_fused.F90:131-146)
+            const size_t q = (size_t)i + (size_t)j * (size_t)a.fpitch;
+            hu = hu + dt * (float)(a.fo.wind_x[q] / kRho);
+            hv = hv + dt * (float)(a.fo.wind_y[q] / kRho);
+            const float dpdx = (float)((a.fo.atm[q + 1] - a.fo.atm[q - 1]) / (2.0 * g.dx));
+            const float dpdy = (float)((a.fo.atm[q + a.fpitch] - a.fo.atm[q - a.fpitch]) / (2.0 * g.dy));
+            hu = hu - dt * h * dpdx * (float)(1.0 / kRho);
+            hv = hv - dt * h * dpdy * (float)(1.0 / kRho);
+          }
+          if (has_cor) {
+            const float uo = hu, vo = hv;
+            hu = uo * cosf_ + vo * sinf_;
+            hv = -(uo * sinf_) + vo * cosf_;
+          }
+        }
+        if (forcing && valid) e = e + dt * (float)a.fo.precip[(size_t)i + (size_t)j * (size_t)a.fpitch];
+        double hfin = hd;
+        if (STAGE == 2) {  // RK2 average and second clamp (rki_kernel_fused.F90:435-463)
+          e = 0.5f * (oe[k] + e);
+          hu = 0.5f * (ou[k] + hu);
+          hv = 0.5f * (ov[k] + hv);
+          hfin = protect(e, hu, hv, bc, h);
+        }
+        if (sponge_on) {
+          const double alpha = sponge_alpha(a.bc, g, i, j);
+          if (alpha > 0.0) {
+            const float fa = dt * (float)alpha;
+            const float de = -fa * (fmaxf(h, 0.0f) - (float)a.bc->sponge_h_ref);
+            e = e + de;
+            hu = hu - fa * hu;
+            hv = hv - fa * hv;
+            if (valid) sponge_d += (double)de;
+            hfin = (double)e - bc;
+            h = fmaxf((float)hfin, 0.0f);
+          }
+        }
+        ne[k] = e;
+        nu[k] = hu;
+        nv[k] = hv;
+        if (valid) {
+          part += (double)dE;
+          if (STAGE == 2) {
+            float sx_, sy_;
+            wave_speed32(hfin, h, hu, hv, sx_, sy_);
+            wsx = fmaxf(wsx, sx_);
+            wsy = fmaxf(wsy, sy_);
+          }
+        }
+      }
+      if (out_lane) {
+        const size_t q = (size_t)j * (size_t)g.pitch + (size_t)ib;
+        if (ib + C - 1 < g.nxt - g.ng) {
+          st_f<C>(out.eta + q, ne);
+          st_f<C>(out.hu + q, nu);
+          st_f<C>(out.hv + q, nv);
+        } else {
+#pragma unroll
+          for (int k = 0; k < C; ++k)
+            if (ib + k < g.nxt - g.ng) {
+              out.eta[q + k] = ne[k];
+              out.hu[q + k] = nu[k];
+              out.hv[q + k] = nv[k];
+            }
+        }
+      }
+      // rotate the row window
+      Cr = D;
+      D = E;
+#pragma unroll
+      for (int k = 0; k < C; ++k) {
+        sC[k] = sD[k];
+        bot[k] = BotFace{top[k].fh, top[k].ft, top[k].en, top[k].dq};
+      }
+    }
+    if (!ok) {
+      // a copy did not arrive in time: flag it and let every copy this warp
+      // issued land (each wait bounded) before the shared memory goes away
+      if (lane == 0) atomicExch(&ctl->error, 1);
+      for (int r = waited + 1; r <= issued; ++r) wait_row(r);
+    }
+  }
+
+  // per-warp partials (fixed order), CFL maxima, last block closes the step
+  part = warp_sum(part);
+  sponge_d = warp_sum(sponge_d);
+  if (STAGE == 2) {
+    wsx = (float)warp_max((double)wsx);
+    wsy = (float)warp_max((double)wsy);
+  }
+  if (lane == 0) {
+    double* P = a.partials + (size_t)(STAGE - 1) * 2 * nw;
+    P[gw] = part;
+    P[nw + gw] = sponge_d;
+    if (STAGE == 2) {
+      atomic_max_pos(&ctl->msx_next, (double)wsx);
+      atomic_max_pos(&ctl->msy_next, (double)wsy);
+    }
+  }
+  if (STAGE != 2) return;
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(&ctl->done_blocks, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  finalize_step(g, ctl, phys, a.partials, nw, dtd, cur);
+}
+
+// ---------------------------------------------------------------------------
+// Boundary conditions in surface form (rki_boundary.F90:40-552)
+// ---------------------------------------------------------------------------
+// Same edge walk as the FP64 fill; depths are read as max(0, eta - b) in FP64
+// and ghost surfaces written as surface_of(h, b).  A wall ghost takes the
+// mirrored cell's surface unchanged (its bed is the mirrored bed).
+__global__ void k_bc32(StepArgs32 a, int stage, int e0, int first_launch) {
+  const Grid g = a.g;
+  StepCtl* ctl = a.ctl;
+  const BcParams* bc = a.bc;
+  double dt;
+  const bool active = step_begin(ctl, a.phys, g, dt);
+  if (first_launch && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+    ctl->active = active ? 1 : 0;
+    ctl->dt = dt;
+  }
+  if (!active) return;
+  const int w = e0 + blockIdx.y;
+  const int type = bc->type[w];
+  if (type == kNested) return;
+  const Edge e = make_edge(w, g);
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= e.n_tan) return;
+  const double time = stage == 1 ? ctl->t : ctl->t + dt;
+  const int cur = ctl->cur;
+  const FieldSet32 F = stage == 1 ? (cur ? a.U1 : a.U0) : a.S;
+  const FieldSet32 N = cur ? a.U0 : a.U1;
+  const bool both = stage == 2;
+  double* b = a.b;
+  auto depth = [&](size_t q) { return pos((double)F.eta[q] - b[q]); };
+  auto put = [&](int ig, int jg, double vh, double vu, double vv) {
+    const size_t q = g.at(ig, jg);
+    const float ve = surface_of(vh, b[q]);
+    const float fu = (float)vu, fv = (float)vv;
+    F.eta[q] = ve; F.hu[q] = fu; F.hv[q] = fv;
+    if (both) { N.eta[q] = ve; N.hu[q] = fu; N.hv[q] = fv; }
+  };
+  const int ii = e.ig0 + t * e.dit - e.din;
+  const int ji = e.jg0 + t * e.djt - e.djn;
+
+  if (type == kWall || type == kSponge) {
+    for (int k = 1; k <= g.ng; ++k) {
+      const int ig = e.ig0 + (k - 1) * e.din + t * e.dit;
+      const int jg = e.jg0 + (k - 1) * e.djn + t * e.djt;
+      const size_t m = g.at(ig - (2 * k - 1) * e.din, jg - (2 * k - 1) * e.djn);
+      const size_t q = g.at(ig, jg);
+      b[q] = b[m];
+      const float ve = F.eta[m];
+      const float fu = e.normal_u ? -F.hu[m] : F.hu[m];
+      const float fv = e.normal_u ? F.hv[m] : -F.hv[m];
+      F.eta[q] = ve; F.hu[q] = fu; F.hv[q] = fv;
+      if (both) { N.eta[q] = ve; N.hu[q] = fu; N.hv[q] = fv; }
+    }
+    return;
+  }
+  const size_t qi = g.at(ii, ji);
+  const double hi = depth(qi);
+  const double qu = (double)F.hu[qi];
+  const double qv = (double)F.hv[qi];
+  if (type == kOpen || type == kTidal) {
+    const bool prescribe = type == kTidal;
+    const double eta_ext = prescribe ? tidal_eta(bc, time) : 0.0;
+    const double ei = hi + b[qi];
+    const double hmax = dmax(hi, 1.0e-6);
+    const double c = sqrt(kG * hmax);
+    for (int k = 1; k <= g.ng; ++k) {
+      const int ig = e.ig0 + (k - 1) * e.din + t * e.dit;
+      const int jg = e.jg0 + (k - 1) * e.djn + t * e.djt;
+      const double hg = prescribe ? pos(eta_ext - b[g.at(ig, jg)]) : hi;
+      const double qn = hg * ((e.normal_u ? qu : qv) / hmax + e.sgn * c * (ei - eta_ext) / hmax);
+      if (e.normal_u) put(ig, jg, hg, qn, qv);
+      else put(ig, jg, hg, qu, qn);
+    }
+  } else if (type == kInflow || type == kDischarge) {
+    const double in_sgn = -e.sgn;
+    for (int k = 1; k <= g.ng; ++k) {
+      const int ig = e.ig0 + (k - 1) * e.din + t * e.dit;
+      const int jg = e.jg0 + (k - 1) * e.djn + t * e.djt;
+      const double qn = type == kInflow ? in_sgn * hi * bc->inflow_velocity
+                                        : in_sgn * bc->discharge_flux;
+      if (e.normal_u) put(ig, jg, hi, qn, qv);
+      else put(ig, jg, hi, qu, qn);
+    }
+  } else if (type == kClamped) {
+    for (int k = 1; k <= g.ng; ++k) {
+      const int ig = e.ig0 + (k - 1) * e.din + t * e.dit;
+      const int jg = e.jg0 + (k - 1) * e.djn + t * e.djt;
+      put(ig, jg, pos(bc->clamped_elevation - b[g.at(ig, jg)]), qu, qv);
+    }
+  } else if (type == kChapman) {
+    double* eo = a.eta_old[w];
+    const double dd = e.normal_u ? g.dx : g.dy;
+    const double ei = hi + b[qi];
+    const double eov = stage == 1 ? ei : eo[t];
+    const double hmax = dmax(hi, 1.0e-6);
+    const double c = sqrt(kG * hmax);
+    const int i2 = ii - e.din;
+    const int j2 = ji - e.djn;
+    double eg;
+    if (dt > 0.0) {
+      const double detadt = (ei - eov) / dt;
+      double detadx = 0.0;
+      if (i2 >= 0 && i2 < g.nxt && j2 >= 0 && j2 < g.nyt) {
+        const size_t q2 = g.at(i2, j2);
+        detadx = (depth(q2) + b[q2] - ei) / dd;
+      }
+      double cp = fabs(detadx) > 1.0e-10 ? -detadt / detadx : 0.0;
+      cp = pos(dmin(cp, c));
+      eg = eov - cp * dt / dd * (eov - ei);
+    } else {
+      eg = ei;
+    }
+    for (int k = 1; k <= g.ng; ++k) {
+      const int ig = e.ig0 + (k - 1) * e.din + t * e.dit;
+      const int jg = e.jg0 + (k - 1) * e.djn + t * e.djt;
+      const double hg = pos(eg - b[g.at(ig, jg)]);
+      const double qn = hg * ((e.normal_u ? qu : qv) / hmax + e.sgn * c * (ei - eg) / hmax);
+      if (e.normal_u) put(ig, jg, hg, qn, qv);
+      else put(ig, jg, hg, qu, qn);
+    }
+    eo[t] = ei;
+  }
+}
+
+// CFL maxima of the current state (before the first step, or after the host
+// changed the state).
+__global__ void k_max_speed32(StepArgs32 a) {
+  const Grid g = a.g;
+  StepCtl* ctl = a.ctl;
+  const FieldSet32 F = ctl->cur ? a.U1 : a.U0;
+  const int nxp = g.nx_phys(), nyp = g.ny_phys();
+  const long long n = (long long)nxp * nyp;
+  float mx = 0.0f, my = 0.0f;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const size_t q = g.at(g.ng + (int)(k % nxp), g.ng + (int)(k / nxp));
+    const double hd = (double)F.eta[q] - a.b[q];
+    float sx, sy;
+    wave_speed32(hd, fmaxf((float)hd, 0.0f), F.hu[q], F.hv[q], sx, sy);
+    mx = fmaxf(mx, sx);
+    my = fmaxf(my, sy);
+  }
+  const double dmx = warp_max((double)mx), dmy = warp_max((double)my);
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_pos(&ctl->msx_next, dmx);
+    atomic_max_pos(&ctl->msy_next, dmy);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned int done = atomicAdd(&ctl->ms_done_blocks, 1u);
+    if (done == gridDim.x - 1) {
+      __threadfence();
+      volatile StepCtl* vc = ctl;
+      ctl->msx = __longlong_as_double((long long)vc->msx_next);
+      ctl->msy = __longlong_as_double((long long)vc->msy_next);
+      ctl->msx_next = 0ull;
+      ctl->msy_next = 0ull;
+      ctl->ms_valid = 1;
+      ctl->ms_done_blocks = 0u;
+    }
+  }
+}
+
+// FP64 (h, hu, hv) -> FP32 (eta, hu, hv), every cell incl. ghosts; with
+// `bed_out`, also copies the bed into the surface form's layout.
+__global__ void k_to_surface(Grid g64, Grid g32, FieldSet src, const double* __restrict__ b64,
+                             FieldSet32 dst, double* __restrict__ bed_out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i >= g64.nxt) return;
+  const size_t p = g64.at(i, j), q = g32.at(i, j);
+  const double b = b64[p];
+  dst.eta[q] = surface_of(src.h[p], b);
+  dst.hu[q] = (float)src.hu[p];
+  dst.hv[q] = (float)src.hv[p];
+  if (bed_out) bed_out[q] = b;
+}
+
+// FP32 surface form -> FP64 depth form (h = max(0, eta - b)); with
+// `bed_out`, also copies the bed back (wall fills mirror it into the ghosts).
+__global__ void k_to_depth(Grid g32, Grid g64, FieldSet32 src, const double* __restrict__ b32,
+                           FieldSet dst, double* __restrict__ bed_out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i >= g32.nxt) return;
+  const size_t q = g32.at(i, j), p = g64.at(i, j);
+  const double b = b32[q];
+  dst.h[p] = pos((double)src.eta[q] - b);
+  dst.hu[p] = (double)src.hu[q];
+  dst.hv[p] = (double)src.hv[q];
+  if (bed_out) bed_out[p] = b;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+
+template <int C>
+static void shape_t(const Grid& g, int rows, int& nstrips, int& nrowblk) {
+  nstrips = (g.nx_phys() + Lay<C>::kStrip - 1) / Lay<C>::kStrip;
+  nrowblk = (g.ny_phys() + rows - 1) / rows;
+}
+
+void sweep_shape(const Grid& g, int rows, int cpl, int& nstrips, int& nrowblk) {
+  if (cpl == 4)
+    shape_t<4>(g, rows, nstrips, nrowblk);
+  else
+    shape_t<2>(g, rows, nstrips, nrowblk);
+}
+
+// Columns (from column 0 of a row) the sweep's copies touch.
+template <int C>
+static size_t extent_t(const Grid& g) {
+  int ns, nr;
+  shape_t<C>(g, 1, ns, nr);
+  return (size_t)g.ng + (size_t)(ns - 1) * Lay<C>::kStrip - 4 + Lay<C>::kSeg;
+}
+
+size_t sweep_row_extent(const Grid& g) {
+  const size_t a = extent_t<2>(g), b = extent_t<4>(g);
+  return a > b ? a : b;
+}
+
+size_t partials_doubles32(const Grid& g, int rows) {
+  int ns, nr;
+  shape_t<2>(g, rows, ns, nr);  // the narrower strips give the most warps
+  const size_t blocks = ((size_t)ns * nr + kWarps - 1) / kWarps;
+  return 4 * blocks * kWarps;
+}
+
+template <int C, bool HLLC, int STAGE>
+static cudaError_t set_smem() {
+  const int bytes = kWarps * kNbuf * Lay<C>::slot(STAGE);
+  return cudaFuncSetAttribute(k_sweep<C, HLLC, STAGE>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+cudaError_t configure_kernels32() {
+  cudaError_t e = set_smem<2, false, 1>();
+  if (e == cudaSuccess) e = set_smem<2, false, 2>();
+  if (e == cudaSuccess) e = set_smem<2, true, 1>();
+  if (e == cudaSuccess) e = set_smem<2, true, 2>();
+  if (e == cudaSuccess) e = set_smem<4, false, 1>();
+  if (e == cudaSuccess) e = set_smem<4, false, 2>();
+  if (e == cudaSuccess) e = set_smem<4, true, 1>();
+  if (e == cudaSuccess) e = set_smem<4, true, 2>();
+  return e;
+}
+
+template <int C>
+static int auto_rows_t(const Grid& g) {
+  int per_sm = 0, sms = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<C, false, 2>, kWarps * 32,
+                                                    kWarps * kNbuf * Lay<C>::kSlot2) !=
+          cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  if (sms < 1) sms = 148;
+  int ns, nr;
+  shape_t<C>(g, 1, ns, nr);
+  const int warps = per_sm * sms * kWarps;
+  int nrb = warps / ns;
+  if (nrb < 1) nrb = 1;
+  int rows = (g.ny_phys() + nrb - 1) / nrb;
+  if (rows < 16) rows = 16;
+  return rows;
+}
+
+int auto_rows32(const Grid& g, int cpl) { return cpl == 4 ? auto_rows_t<4>(g) : auto_rows_t<2>(g); }
+
+template <int C, int STAGE>
+static cudaError_t launch_sweep_t(const StepArgs32& a, cudaStream_t s) {
+  const unsigned work = (unsigned)(a.nstrips * a.nrowblk);
+  const unsigned blocks = (work + kWarps - 1) / kWarps;
+  const size_t bytes = (size_t)kWarps * kNbuf * Lay<C>::slot(STAGE);
+  if (a.hllc)
+    k_sweep<C, true, STAGE><<<blocks, kWarps * 32, bytes, s>>>(a);
+  else
+    k_sweep<C, false, STAGE><<<blocks, kWarps * 32, bytes, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int STAGE>
+static cudaError_t launch_sweep(const StepArgs32& a, cudaStream_t s) {
+  return a.cpl == 4 ? launch_sweep_t<4, STAGE>(a, s) : launch_sweep_t<2, STAGE>(a, s);
+}
+
+cudaError_t launch_bc32(const StepArgs32& a, int stage, cudaStream_t s) {
+  const Grid& g = a.g;
+  const int tpb = 128;
+  const bool pair_x = g.nx_phys() >= (g.ng > 2 ? g.ng : 2);
+  const bool pair_y = g.ny_phys() >= (g.ng > 2 ? g.ng : 2);
+  int first = stage == 1 ? 1 : 0;
+  auto go = [&](int e0, int count, int n_tan) {
+    dim3 grid((unsigned)((n_tan + tpb - 1) / tpb), (unsigned)count);
+    k_bc32<<<grid, tpb, 0, s>>>(a, stage, e0, first);
+    first = 0;
+  };
+  if (pair_x) {
+    go(0, 2, g.nyt);
+  } else {
+    go(0, 1, g.nyt);
+    go(1, 1, g.nyt);
+  }
+  if (pair_y) {
+    go(2, 2, g.nxt);
+  } else {
+    go(2, 1, g.nxt);
+    go(3, 1, g.nxt);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_step32(const StepArgs32& a, cudaStream_t s) {
+  cudaError_t e = launch_bc32(a, 1, s);
+  if (e == cudaSuccess) e = launch_sweep<1>(a, s);
+  if (e == cudaSuccess) e = launch_bc32(a, 2, s);
+  if (e == cudaSuccess) e = launch_sweep<2>(a, s);
+  return e;
+}
+
+cudaError_t launch_stage32_only(const StepArgs32& a, int stage, cudaStream_t s) {
+  return stage == 1 ? launch_sweep<1>(a, s) : launch_sweep<2>(a, s);
+}
+
+int launches_per_step32(const StepArgs32& a) {
+  const Grid& g = a.g;
+  const int need = g.ng > 2 ? g.ng : 2;
+  const int bc = (g.nx_phys() >= need ? 1 : 2) + (g.ny_phys() >= need ? 1 : 2);
+  return 2 * bc + 2;
+}
+
+cudaError_t launch_max_speed32(const StepArgs32& a, cudaStream_t s) {
+  const long long n = (long long)a.g.nx_phys() * a.g.ny_phys();
+  long long blocks = (n + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  if (blocks < 1) blocks = 1;
+  k_max_speed32<<<(unsigned)blocks, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_to_surface(const Grid& g64, const Grid& g32, FieldSet src, const double* b64,
+                              FieldSet32 dst, double* bed_out, cudaStream_t s) {
+  dim3 grid((unsigned)((g64.nxt + 127) / 128), (unsigned)g64.nyt);
+  k_to_surface<<<grid, 128, 0, s>>>(g64, g32, src, b64, dst, bed_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_to_depth(const Grid& g32, const Grid& g64, FieldSet32 src, const double* b32,
+                            FieldSet dst, double* bed_out, cudaStream_t s) {
+  dim3 grid((unsigned)((g32.nxt + 127) / 128), (unsigned)g32.nyt);
+  k_to_depth<<<grid, 128, 0, s>>>(g32, g64, src, b32, dst, bed_out);
+  return cudaGetLastError();
+}
+
+}  // namespace rkb
