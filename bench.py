@@ -2,10 +2,17 @@
 
 Workload (per GPU): the 4096 x 4096 wet/dry configuration - dx = dy = 5 m, a
 bed of 32 seeded Gaussians (amplitudes U[-4, 12] m, widths U[50, 500] m), a
-0.5 m / 200 m hump at the centre, Manning n = 0.025, walls - advanced in
-FP64 through librakali.so.  One "step" is one full SSP-RK2 step of the grid.
+0.5 m / 200 m hump at the centre, Manning n = 0.025, walls - advanced through
+librakali.so.  One "step" is one full SSP-RK2 step of the grid.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--precision 64|32] [--one-form]
+
+The headline line is the FP64 depth form (the reference's arithmetic); the
+FP32 surface form is timed on the same handle right after and reported under
+"forms" with its free-surface error against the FP64 step after
+min(K, 500) steps and the FP64 step's own drift under a 1e-7 relative
+perturbation of h (the conditioning floor of this flow).
 
 N > 1 runs N independent replicas (one per rank, launched by torchrun): the
 step does not exchange data between instances, so scaling is weak and no
@@ -14,7 +21,8 @@ the max-over-ranks of the timed region.
 
 Timing: W untimed steps, then K steps bracketed by CUDA events recorded on
 the simulation's own stream (rkb_time_steps), max over ranks.  Each field is
-16.8 M cells x 8 B = 134 MB, so every step streams more than L2 holds.
+16.8 M cells x 8 B = 134 MB (FP64) or 67 MB (FP32), so every step streams
+more than L2 holds.
 """
 from __future__ import annotations
 
@@ -189,33 +197,20 @@ def run_reference(args, rank, world):
     return 0
 
 
-def run_b200(args, rank, world, local_rank, dist):
+def _form_numbers(sim, args, world, local_rank, dist, cells):
+    """Time one arithmetic form on the current state: device time of K steps,
+    per-kernel events and the end-to-end run through the public API."""
     import ctypes
 
     import torch
 
-    from rakali_b200 import Rakali
-    from rakali_b200 import workloads as wl
-
-    torch.cuda.set_device(local_rank)
-    n = args.side
-    b, h = wl.config2(n=n, seed=2024 + rank)
-    sim = Rakali(defer_init=True, nx=n, ny=n, **wl.CONFIG2_KW)
-    sim.set_bathymetry(b)
-    sim.set_initial_h(h)
-    sim.finalize()
-    sim.set_tile(args.tile)
-    if args.precision == 32:
-        sim.set_precision(32)
-        sim.set_sweep(args.sweep_cols, args.sweep_rows)
     lib = sim._lib
-    cells = n * n
 
     def device_steps(k):
         ms = ctypes.c_double()
         rc = lib.rkb_time_steps(sim._handle, int(k), ctypes.byref(ms))
         if rc != 0:
-            raise RuntimeError(f"rkb_time_steps failed rc={rc}")
+            raise RuntimeError(f"rkb_time_steps failed rc={rc}: {lib.rki_last_error()}")
         return ms.value
 
     device_steps(max(args.warmup, 3))
@@ -234,10 +229,8 @@ def run_b200(args, rank, world, local_rank, dist):
 
     # per-kernel device times (events between launches, same stream)
     prof = (ctypes.c_double * 5)()
-    rc = lib.rkb_profile_steps(sim._handle, 5, prof)
-    if rc != 0:
+    if lib.rkb_profile_steps(sim._handle, 5, prof) != 0:
         raise RuntimeError("rkb_profile_steps failed")
-    t_bc1, t_s1, t_bc2, t_s2, launches = prof[0], prof[1], prof[2], prof[3], int(prof[4])
 
     # end to end through the public API with host buffers: upload the state,
     # K steps, read the fields back (D2H) - wall clock around all of it.
@@ -252,54 +245,131 @@ def run_b200(args, rank, world, local_rank, dist):
     h_back = sim.h_phys
     _ = float(h_back[0, 0])
     e2e_s = time.perf_counter() - t0
-    nxt = n + 2 * sim.nghost
-    h2d = 3 * 8 * cells  # interior h, hu, hv
-    d2h = 7 * 8 * nxt * nxt  # h, hu, hv, b, h0, hu0, hv0 with ghosts
-    e2e = {"value": world * cells * args.steps / e2e_s, "unit": "cell-updates/s",
-           "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps}
     if dist is not None:
         t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e["value"] = world * cells * args.steps / float(t.item())
+        e2e_s = float(t.item())
+    n = int(round(cells ** 0.5))
+    nxt = n + 2 * sim.nghost
+    e2e = {"value": world * cells * args.steps / e2e_s, "unit": "cell-updates/s",
+           "h2d_bytes_per_step": 3 * 8 * cells / args.steps,   # interior h, hu, hv
+           "d2h_bytes_per_step": 7 * 8 * nxt * nxt / args.steps}  # h, hu, hv, b, h0, hu0, hv0
+    return {"value": value, "ms": ms, "e2e": e2e, "clocks": clk.summary(),
+            "stage_ms": {"bc_stage1": prof[0], "stage1": prof[1], "bc_stage2": prof[2],
+                         "stage2": prof[3]},
+            "launches_per_step": int(prof[4])}
 
-    if rank != 0:
-        sim.close()
-        return 0
+
+def _roofline(form, precision, cells, world):
     hbm, peak_kind = peaks()
-    f32 = args.precision == 32
+    f32 = precision == 32
     b_s2 = BYTES_STAGE2_32 if f32 else BYTES_STAGE2
     b_cell = BYTES_PER_CELL_UPDATE_32 if f32 else BYTES_PER_CELL_UPDATE
-    achieved = b_s2 * cells / (t_s2 * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": traffic_per_launch(cells, args.precision),
-                "kernel": ("k_sweep<stage 2> (FP32 surface form: flux + update + RK2 average)"
-                           if f32 else "k_stage<stage 2> (fused flux + update + RK2 average)"),
-                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
-                if peak_kind == "measured" else "fallback 6650 GB/s",
-                "stage_ms": {"bc_stage1": t_bc1, "stage1": t_s1, "bc_stage2": t_bc2,
-                             "stage2": t_s2},
-                "bytes_per_cell_update": b_cell,
-                "step_frac_of_hbm": b_cell * value / world / 1e9 / hbm}
+    achieved = b_s2 * cells / (form["stage_ms"]["stage2"] * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "traffic": traffic_per_launch(cells, precision),
+            "kernel": ("k_sweep<stage 2> (FP32 surface form: flux + update + RK2 average)"
+                       if f32 else "k_stage<stage 2> (fused flux + update + RK2 average)"),
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+            if peak_kind == "measured" else "fallback 6650 GB/s",
+            "stage_ms": form["stage_ms"], "bytes_per_cell_update": b_cell,
+            "step_frac_of_hbm": b_cell * form["value"] / world / 1e9 / hbm}
+
+
+def _fp32_error(b, h, n, steps):
+    """Free-surface error of the FP32 form against the FP64 step (which the
+    parity tests hold bit-identical to the oracle) after `steps` steps from the
+    same state, and the FP64 step's own drift when h is perturbed by 1e-7
+    relative noise (the conditioning floor of this configuration)."""
+    from rakali_b200 import Rakali
+    from rakali_b200 import workloads as wl
+
+    def run(hh, prec):
+        s = Rakali(defer_init=True, nx=n, ny=n, **wl.CONFIG2_KW)
+        s.set_bathymetry(b)
+        s.set_initial_h(hh)
+        s.finalize()
+        s.set_precision(prec)
+        s.step(steps)
+        out = s.h_phys.copy()
+        s.close()
+        return out
+
+    rng = np.random.default_rng(17)
+    hp = np.asfortranarray(h * (1.0 + 1.0e-7 * rng.standard_normal(h.shape)))
+    h64 = run(h, 64)
+    d32 = np.abs(run(h, 32) - h64)
+    dfl = np.abs(run(hp, 64) - h64)
+    return {"steps": steps, "unit": "m",
+            "max": float(d32.max()), "rms": float(np.sqrt(np.mean(d32 * d32))),
+            "p999": float(np.quantile(d32, 0.999)),
+            "fp64_floor_max": float(dfl.max()), "fp64_floor_rms": float(np.sqrt(np.mean(dfl * dfl))),
+            "note": "free surface vs the FP64 step; floor = FP64 step vs itself with h x (1 + 1e-7 noise)"}
+
+
+def run_b200(args, rank, world, local_rank, dist):
+    import torch
+
+    from rakali_b200 import Rakali
+    from rakali_b200 import workloads as wl
+
+    torch.cuda.set_device(local_rank)
+    n = args.side
+    b, h = wl.config2(n=n, seed=2024 + rank)
+    sim = Rakali(defer_init=True, nx=n, ny=n, **wl.CONFIG2_KW)
+    sim.set_bathymetry(b)
+    sim.set_initial_h(h)
+    sim.finalize()
+    sim.set_tile(args.tile)
+    sim.set_sweep(args.sweep_cols, args.sweep_rows)
+    cells = n * n
+
+    # the headline form first, then the other one on the same handle
+    head = args.precision
+    other = 32 if head == 64 else 64
+    forms = {}
+    for prec in (head, other) if args.both_forms else (head,):
+        sim.set_precision(prec)
+        forms[prec] = _form_numbers(sim, args, world, local_rank, dist, cells)
+        forms[prec]["roofline"] = _roofline(forms[prec], prec, cells, world)
+    sim.close()
+    err = None
+    if args.both_forms and rank == 0 and not args.no_accuracy:
+        err = _fp32_error(b, h, n, min(args.steps, 500))
+    if rank != 0:
+        return 0
+
+    f = forms[head]
+    desc = {64: "FP64 depth form (the reference's arithmetic, bit-identical to the oracle)",
+            32: "FP32 surface form (FP64 bed differences, wet/dry tests and mass sums)"}
     line = {
-        "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "metric": METRIC, "value": f["value"], "unit": "cell-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": f["ms"] / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32" if f32 else "f64", "data": "synthetic",
+        "dtype": "f32" if head == 32 else "f64", "data": "synthetic",
         "config": {"workload": f"structured SSP-RK2 wet/dry step, {n}x{n} per GPU, dx=5 m, "
-                               "32-Gaussian bed, 0.5 m hump, Manning 0.025, walls, "
-                               + ("FP32 surface form (FP64 bed differences, wet/dry tests "
-                                  "and mass sums)" if f32 else "FP64 (parity build)"),
-                   "cells_per_gpu": cells, "tile": args.tile, "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (3 x 134 MB per buffer)"},
-        "e2e": e2e,
-        "gpu_launches": launches * args.steps,
-        "roofline": roofline,
-        "clocks": clk.summary(),
+                               "32-Gaussian bed, 0.5 m hump, Manning 0.025, walls, " + desc[head],
+                   "cells_per_gpu": cells, "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (every field >= 67 MB, 7+ fields per stage)"},
+        "e2e": f["e2e"],
+        "gpu_launches": f["launches_per_step"] * args.steps,
+        "roofline": f["roofline"],
+        "clocks": f["clocks"],
     }
+    if len(forms) > 1:
+        line["forms"] = {}
+        for prec, fm in forms.items():
+            entry = {"dtype": "f32" if prec == 32 else "f64", "form": desc[prec],
+                     "value": fm["value"], "ms_per_step": fm["ms"] / args.steps,
+                     "e2e": fm["e2e"]["value"], "roofline_frac": fm["roofline"]["frac"],
+                     "roofline_achieved_gbs": fm["roofline"]["achieved"],
+                     "stage_ms": fm["stage_ms"], "clocks": fm["clocks"]}
+            if prec == 32 and err is not None:
+                entry["error_vs_fp64"] = err
+            line["forms"][f"fp{prec}"] = entry
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
     print(json.dumps(line), flush=True)
-    sim.close()
     return 0
 
 
@@ -314,7 +384,12 @@ def main():
                     help="stage-kernel variant (rkb_set_tile): 0-3 shared-memory tiles, "
                          "4/5 marching strips of 64/32 rows")
     ap.add_argument("--precision", type=int, choices=(32, 64), default=64,
-                    help="64: FP64 depth form (reference arithmetic); 32: FP32 surface form")
+                    help="headline form: 64 = FP64 depth form (reference arithmetic), "
+                         "32 = FP32 surface form")
+    ap.add_argument("--one-form", dest="both_forms", action="store_false",
+                    help="time only the headline form (default: both, the other under 'forms')")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the FP32-vs-FP64 error measurement")
     ap.add_argument("--sweep-cols", type=int, choices=(0, 2, 4), default=0,
                     help="FP32 form: columns per lane of the sweep kernel (0 = default)")
     ap.add_argument("--sweep-rows", type=int, default=0,

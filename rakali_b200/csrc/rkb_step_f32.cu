@@ -184,7 +184,14 @@ __device__ __forceinline__ Slope slope(unsigned fm, unsigned fc, unsigned fp, fl
   return s;
 }
 
-// One face.  n = normal momentum, t = tangential momentum.
+// One face.  n = normal momentum, t = tangential momentum; hL, hR are the
+// reconstructed depths max(0, h_cell +- s/2) of the two sides and bL, bR the
+// cell beds.
+//
+// The Audusse hydrostatic depths max(0, eta - max(b_L, b_R))
+// (rki_kernel_flux.F90:186-224) are FP64 differences: they are what keeps a
+// lake at rest at rest, and in FP64 a dry island whose top lies a hair above
+// the lake surface gets exactly zero depth on both sides of its shore faces.
 //
 // The reference hands each cell the face flux F together with its
 // well-balanced terms, F - Q(h_hyd) + Q(h_face) with Q(h) = g/2 h^2
@@ -193,86 +200,63 @@ __device__ __forceinline__ Slope slope(unsigned fm, unsigned fc, unsigned fp, fl
 // gradient, so the same sums are regrouped to subtract only small numbers:
 //
 //   en = F - Q(h_hyd,L)                  flux in excess of the left hydrostatic pressure
-//   dq = Q(h_hyd,R) - Q(h_hyd,L) = g/2 (h_hyd,R - h_hyd,L)(h_hyd,R + h_hyd,L)
+//   dq = Q(h_hyd,R) - Q(h_hyd,L) = g/2 dy (h_hyd,L + h_hyd,R)
 //
-// with the hydrostatic depth jump taken as an FP64 difference.  A cell with
-// faces l, r then gets  en_r - en_l + dq_l + [Q(h_face,r) - Q(h_face,l)],
-// the bracket being the cell's own reconstruction term (cell_pressure).
+// with dy = h_hyd,R - h_hyd,L = eta_R - eta_L while both sides are wet (the
+// bed cancels), else the difference of the clipped depths.  A cell with faces
+// l, r then gets  en_r - en_l + dq_l + [Q(h_face,r) - Q(h_face,l)], the
+// bracket being its own reconstruction term (cell_pressure).  At rest both
+// surfaces are equal, so dy, dq, the fluxes and the cell term are exactly 0.
 struct FaceF {
   float fh, en, dq, ft;
 };
 
 template <bool HLLC>
-__device__ __forceinline__ FaceF face(float eL, float nL, float tL, double bL, float eR, float nR,
-                                      float tR, double bR) {
+__device__ __forceinline__ FaceF face(float eL, float nL, float tL, float hL, double bL, float eR,
+                                      float nR, float tR, float hR, double bR) {
   const double bmax = bL > bR ? bL : bR;
-  const double eLd = (double)eL, eRd = (double)eR;
-  const double hLd = eLd - bL, hRd = eRd - bR;  // reconstructed depths
-  const double yLd = pos(eLd - bmax), yRd = pos(eRd - bmax);  // Audusse hydrostatic depths
-  const float hL = fmaxf(__double2float_rn(hLd), 0.0f);
-  const float hR = fmaxf(__double2float_rn(hRd), 0.0f);
-  const float yl = __double2float_rn(yLd);
-  const float yr = __double2float_rn(yRd);
-  const float dy = __double2float_rn(yRd - yLd);  // hydrostatic depth jump, FP64 difference
+  const double yLd = pos((double)eL - bmax), yRd = pos((double)eR - bmax);
+  const float yl = __double2float_rn(yLd), yr = __double2float_rn(yRd);
+  const float dy = (yl > 0.0f && yr > 0.0f) ? eR - eL : yr - yl;
   const bool wyl = yLd > kDry, wyr = yRd > kDry;
-  float ul = 0.0f, vl = 0.0f, ur = 0.0f, vr = 0.0f;
-  if (hLd > kDry) {
-    const float r = rcp_approx(hL);
-    ul = nL * r;
-    vl = tL * r;
-  }
-  if (hRd > kDry) {
-    const float r = rcp_approx(hR);
-    ur = nR * r;
-    vr = tR * r;
-  }
+  const float rl = rcp_approx(fmaxf(hL, kDryF)), rr = rcp_approx(fmaxf(hR, kDryF));
+  const float ul = hL > kDryF ? nL * rl : 0.0f, vl = hL > kDryF ? tL * rl : 0.0f;
+  const float ur = hR > kDryF ? nR * rr : 0.0f, vr = hR > kDryF ? tR * rr : 0.0f;
   // HLL / HLLC on the hydrostatic states (rki_kernel_flux.F90:410-783)
   const float qnl = yl * ul, qtl = yl * vl, qnr = yr * ur, qtr = yr * vr;
   const float unl = wyl ? ul : 0.0f, utl = wyl ? vl : 0.0f;
   const float unr = wyr ? ur : 0.0f, utr = wyr ? vr : 0.0f;
   const float al = sqrt_approx(kGf * yl), ar = sqrt_approx(kGf * yr);
-  float sl, sr;
-  if (!wyr) {
-    sl = unl - al;
-    sr = unl + 2.0f * al;
-  } else if (!wyl) {
-    sl = unr - 2.0f * ar;
-    sr = unr + ar;
-  } else {
-    sl = fminf(unl - al, unr - ar);
-    sr = fmaxf(unl + al, unr + ar);
-  }
+  const float sl = !wyr ? unl - al : (!wyl ? unr - 2.0f * ar : fminf(unl - al, unr - ar));
+  const float sr = !wyr ? unl + 2.0f * al : (!wyl ? unr + ar : fmaxf(unl + al, unr + ar));
   FaceF o;
   o.dq = kHalfGf * dy * (yl + yr);
   const float ln = qnl * unl, rn = qnr * unr;  // advective parts of the normal fluxes
   const float lt = qnl * utl, rt = qnr * utr;
-  if (sl >= 0.0f) {
-    o.fh = qnl; o.en = ln; o.ft = lt;
-  } else if (sr <= 0.0f) {
-    o.fh = qnr; o.en = rn + o.dq; o.ft = rt;
+  // F = F_L - s_L (F_R - F_L - s_R (U_R - U_L)) / (s_R - s_L) when s_L < 0 < s_R
+  const float inv = rcp_approx(sr - sl);
+  const float mfh = qnl - sl * ((qnr - qnl) - sr * dy) * inv;
+  const float men = ln - sl * (((rn - ln) + o.dq) - sr * (qnr - qnl)) * inv;
+  float mft;
+  if (!HLLC) {
+    mft = lt - sl * ((rt - lt) - sr * (qtr - qtl)) * inv;
   } else {
-    // F = F_L - s_L (F_R - F_L - s_R (U_R - U_L)) / (s_R - s_L)
-    const float inv = rcp_approx(sr - sl);
-    o.fh = qnl - sl * ((qnr - qnl) - sr * dy) * inv;
-    o.en = ln - sl * (((rn - ln) + o.dq) - sr * (qnr - qnl)) * inv;
-    if (!HLLC) {
-      o.ft = lt - sl * ((rt - lt) - sr * (qtr - qtl)) * inv;
-    } else {
-      const float den = yr * (unr - sr) - yl * (unl - sl);
-      float ss;
-      if (fabsf(den) > kDryF)
-        ss = (sl * yr * (unr - sr) - sr * yl * (unl - sl)) * rcp_approx(den);
-      else
-        ss = 0.5f * (unl + unr);
-      o.ft = ss >= 0.0f ? o.fh * utl : o.fh * utr;
-    }
+    const float den = yr * (unr - sr) - yl * (unl - sl);
+    const float ss = fabsf(den) > kDryF
+                         ? (sl * yr * (unr - sr) - sr * yl * (unl - sl)) * rcp_approx(den)
+                         : 0.5f * (unl + unr);
+    mft = ss >= 0.0f ? mfh * utl : mfh * utr;
   }
+  const bool up = sl >= 0.0f, down = sr <= 0.0f;  // supercritical to the right / left
+  o.fh = up ? qnl : (down ? qnr : mfh);
+  o.en = up ? ln : (down ? rn + o.dq : men);
+  o.ft = up ? lt : (down ? rt : mft);
   return o;
 }
 
 // Q(h_face,r) - Q(h_face,l) of a cell of depth hc whose limited surface slope
-// is s: its reconstructed depths are hc + s/2 and hc - s/2 (rki_kernel_flux.F90:
-// 186-224), so the difference is g hc s unless a face depth is clipped at 0.
+// is s: its reconstructed depths are hc + s/2 and hc - s/2 (clipped at 0), so
+// the difference is g hc s unless a face depth is clipped.
 __device__ __forceinline__ float cell_pressure(float hc, float s) {
   const float a = hc + 0.5f * s, c = hc - 0.5f * s;
   if (a >= 0.0f && c >= 0.0f) return kGf * hc * s;
@@ -331,12 +315,10 @@ __device__ __forceinline__ void wave_speed32(double hd, float h, float hu, float
 template <int C>
 struct Row {
   float e[C], u[C], v[C];
-  float h[C];   // cell depth (FP64 difference, rounded)
+  float h[C];     // cell depth (FP64 difference, rounded)
   double b[C];
-  unsigned f;   // 2 flag bits per column
+  unsigned f[C];  // bit 0: h >= DRY_THRESHOLD, bit 1: h >= THIN_THRESHOLD (FP64 tests)
 };
-
-__device__ __forceinline__ unsigned colf(unsigned f, int k) { return (f >> (2 * k)) & 3u; }
 
 template <int C>
 __device__ __forceinline__ void ld_f(const unsigned char* p, float (&o)[C]) {
@@ -368,14 +350,12 @@ __device__ __forceinline__ void read_row(const unsigned char* slot, int base, Ro
   ld_f<C>(slot + L::kOffU + 4 * base, r.u);
   ld_f<C>(slot + L::kOffV + 4 * base, r.v);
   ld_d<C>(slot + L::kOffB + 8 * base, r.b);
-  unsigned f = 0;
 #pragma unroll
   for (int k = 0; k < C; ++k) {
     const double hd = (double)r.e[k] - r.b[k];
     r.h[k] = __double2float_rn(hd);
-    f |= ((hd >= kDry ? 1u : 0u) | (hd >= kThin ? 2u : 0u)) << (2 * k);
+    r.f[k] = (hd >= kDry ? 1u : 0u) | (hd >= kThin ? 2u : 0u);
   }
-  r.f = f;
 }
 
 template <int C>
@@ -383,8 +363,8 @@ __device__ __forceinline__ void yslopes(const Row<C>& m, const Row<C>& c, const 
                                         Slope (&s)[C]) {
 #pragma unroll
   for (int k = 0; k < C; ++k)
-    s[k] = slope(colf(m.f, k), colf(c.f, k), colf(p.f, k), m.e[k], c.e[k], p.e[k], m.u[k], c.u[k],
-                 p.u[k], m.v[k], c.v[k], p.v[k]);
+    s[k] = slope(m.f[k], c.f[k], p.f[k], m.e[k], c.e[k], p.e[k], m.u[k], c.u[k], p.u[k], m.v[k],
+                 c.v[k], p.v[k]);
 }
 
 // y-faces between rows lo and hi (normal momentum hv, tangential hu).
@@ -394,8 +374,9 @@ __device__ __forceinline__ void yfaces(const Row<C>& lo, const Slope (&sl)[C], c
 #pragma unroll
   for (int k = 0; k < C; ++k)
     f[k] = face<HLLC>(lo.e[k] + 0.5f * sl[k].e, lo.v[k] + 0.5f * sl[k].v, lo.u[k] + 0.5f * sl[k].u,
-                      lo.b[k], hi.e[k] - 0.5f * sh[k].e, hi.v[k] - 0.5f * sh[k].v,
-                      hi.u[k] - 0.5f * sh[k].u, hi.b[k]);
+                      fmaxf(lo.h[k] + 0.5f * sl[k].e, 0.0f), lo.b[k], hi.e[k] - 0.5f * sh[k].e,
+                      hi.v[k] - 0.5f * sh[k].v, hi.u[k] - 0.5f * sh[k].u,
+                      fmaxf(hi.h[k] - 0.5f * sh[k].e, 0.0f), hi.b[k]);
 }
 
 // What a cell keeps of the face below it: mass flux, tangential (hu) flux,
@@ -476,8 +457,10 @@ __global__ void __launch_bounds__(kWarps * 32, C == 2 ? 4 : 2) k_sweep(StepArgs3
     }
     __syncwarp();
 
-    auto issue = [&](int r) {  // lane 0
-      const int s = (r - r0) % kNbuf;
+    // Ring bookkeeping without divisions: rows r0, r0+1, ... go to slots 0, 1,
+    // ..., kNbuf-1, 0, ...; bit s of `ph` is the parity of the next completion
+    // to wait for on slot s.
+    auto issue = [&](int r, int s) {  // lane 0
       const uint32_t dst = ring_s + s * SLOT, bar = bar0 + 8 * s;
       const bool with_old = STAGE == 2 && r >= y0 && r < yend;
       mbar_expect_tx(bar, with_old ? L::kSlot2 : L::kSlot1);
@@ -493,15 +476,20 @@ __global__ void __launch_bounds__(kWarps * 32, C == 2 ? 4 : 2) k_sweep(StepArgs3
         bulk_g2s(dst + L::kOffOV, old.hv + ro2, 4 * L::kStrip, bar);
       }
     };
-    auto slot_of = [&](int r) { return ring + ((r - r0) % kNbuf) * SLOT; };
-    auto wait_row = [&](int r) {
-      const int k = r - r0;
-      return mbar_wait(bar0 + 8 * (k % kNbuf), (uint32_t)((k / kNbuf) & 1));
+    auto nxt = [](int s) { return s + 1 == kNbuf ? 0 : s + 1; };
+    uint32_t ph = 0;
+    int ws = 0;  // slot of the next row to wait for
+    auto wait_next = [&]() {
+      const bool r_ok = mbar_wait(bar0 + 8 * ws, (ph >> ws) & 1u);
+      ph ^= 1u << ws;
+      const int s_done = ws;
+      ws = nxt(ws);
+      return r_ok ? s_done : -1;
     };
 
     int issued = min(r0 + kNbuf - 1, rlast);
     if (lane == 0)
-      for (int r = r0; r <= issued; ++r) issue(r);
+      for (int r = r0; r <= issued; ++r) issue(r, r - r0);
 
     // prologue: rows y0-2 .. y0+1, slopes of y0-1 and y0, face y0-1/2
     Row<C> A, B, Cr, D, E;
@@ -509,9 +497,10 @@ __global__ void __launch_bounds__(kWarps * 32, C == 2 ? 4 : 2) k_sweep(StepArgs3
     int waited = r0 - 1;  // last row whose copies have landed
     auto take = [&](int r, Row<C>& R) {
       if (!ok) return;
-      ok = wait_row(r);
+      const int sl = wait_next();
+      ok = sl >= 0;
       if (ok) {
-        read_row<C>(slot_of(r), base, R);
+        read_row<C>(ring + sl * SLOT, base, R);
         waited = r;
       }
     };
@@ -532,17 +521,19 @@ __global__ void __launch_bounds__(kWarps * 32, C == 2 ? 4 : 2) k_sweep(StepArgs3
       __syncwarp();
       if (lane == 0) {
         fence_proxy_async();
-        for (int r = r0 + kNbuf; r <= min(r0 + kNbuf + 1, rlast); ++r) issue(r);
+        for (int r = r0 + kNbuf; r <= min(r0 + kNbuf + 1, rlast); ++r) issue(r, r - r0 - kNbuf);
       }
       issued = min(r0 + kNbuf + 1, rlast);
     }
 
     const int src_r = (lane + 1) & 31, src_l = (lane + 31) & 31;
+    int sj = 2;  // slot of row j
     for (int j = y0; ok && j < yend; ++j) {
-      ok = wait_row(j + 2);
+      const int sn = wait_next();  // row j + 2
+      ok = sn >= 0;
       if (!ok) break;
       waited = j + 2;
-      read_row<C>(slot_of(j + 2), base, E);
+      read_row<C>(ring + sn * SLOT, base, E);
       Slope sD[C];
       yslopes<C>(Cr, D, E, sD);
       FaceF top[C];
@@ -552,25 +543,26 @@ __global__ void __launch_bounds__(kWarps * 32, C == 2 ? 4 : 2) k_sweep(StepArgs3
       const float pe = __shfl_sync(kFull, Cr.e[0], src_r);
       const float pu = __shfl_sync(kFull, Cr.u[0], src_r);
       const float pv = __shfl_sync(kFull, Cr.v[0], src_r);
-      const unsigned pf = __shfl_sync(kFull, Cr.f & 3u, src_r);
+      const unsigned pf = __shfl_sync(kFull, Cr.f[0], src_r);
       const float me = __shfl_sync(kFull, Cr.e[C - 1], src_l);
       const float mu = __shfl_sync(kFull, Cr.u[C - 1], src_l);
       const float mv = __shfl_sync(kFull, Cr.v[C - 1], src_l);
-      const unsigned mf = __shfl_sync(kFull, colf(Cr.f, C - 1), src_l);
+      const unsigned mf = __shfl_sync(kFull, Cr.f[C - 1], src_l);
       Slope sx[C];
 #pragma unroll
       for (int k = 0; k < C; ++k) {
         const float em = k ? Cr.e[k - 1] : me, um = k ? Cr.u[k - 1] : mu, vm = k ? Cr.v[k - 1] : mv;
-        const unsigned fm = k ? colf(Cr.f, k - 1) : mf;
+        const unsigned fm = k ? Cr.f[k - 1] : mf;
         const float ep = k < C - 1 ? Cr.e[k + 1] : pe, up = k < C - 1 ? Cr.u[k + 1] : pu;
         const float vp = k < C - 1 ? Cr.v[k + 1] : pv;
-        const unsigned fp = k < C - 1 ? colf(Cr.f, k + 1) : pf;
-        sx[k] = slope(fm, colf(Cr.f, k), fp, em, Cr.e[k], ep, um, Cr.u[k], up, vm, Cr.v[k], vp);
+        const unsigned fp = k < C - 1 ? Cr.f[k + 1] : pf;
+        sx[k] = slope(fm, Cr.f[k], fp, em, Cr.e[k], ep, um, Cr.u[k], up, vm, Cr.v[k], vp);
       }
       // left state of this lane's first x-face: the left lane's last column
       const float le = __shfl_sync(kFull, Cr.e[C - 1] + 0.5f * sx[C - 1].e, src_l);
       const float lu = __shfl_sync(kFull, Cr.u[C - 1] + 0.5f * sx[C - 1].u, src_l);
       const float lv = __shfl_sync(kFull, Cr.v[C - 1] + 0.5f * sx[C - 1].v, src_l);
+      const float lh = __shfl_sync(kFull, fmaxf(Cr.h[C - 1] + 0.5f * sx[C - 1].e, 0.0f), src_l);
       const double lb = __shfl_sync(kFull, Cr.b[C - 1], src_l);
       FaceF xf[C];
 #pragma unroll
@@ -578,9 +570,11 @@ __global__ void __launch_bounds__(kWarps * 32, C == 2 ? 4 : 2) k_sweep(StepArgs3
         const float eL = k ? Cr.e[k - 1] + 0.5f * sx[k - 1].e : le;
         const float uL = k ? Cr.u[k - 1] + 0.5f * sx[k - 1].u : lu;
         const float vL = k ? Cr.v[k - 1] + 0.5f * sx[k - 1].v : lv;
+        const float hL = k ? fmaxf(Cr.h[k - 1] + 0.5f * sx[k - 1].e, 0.0f) : lh;
         const double bL = k ? Cr.b[k - 1] : lb;
-        xf[k] = face<HLLC>(eL, uL, vL, bL, Cr.e[k] - 0.5f * sx[k].e, Cr.u[k] - 0.5f * sx[k].u,
-                           Cr.v[k] - 0.5f * sx[k].v, Cr.b[k]);
+        xf[k] = face<HLLC>(eL, uL, vL, hL, bL, Cr.e[k] - 0.5f * sx[k].e, Cr.u[k] - 0.5f * sx[k].u,
+                           Cr.v[k] - 0.5f * sx[k].v, fmaxf(Cr.h[k] - 0.5f * sx[k].e, 0.0f),
+                           Cr.b[k]);
       }
       // right face of the last column = the right lane's first face
       const float rfh = __shfl_sync(kFull, xf[0].fh, src_r);
@@ -593,20 +587,21 @@ __global__ void __launch_bounds__(kWarps * 32, C == 2 ? 4 : 2) k_sweep(StepArgs3
 #pragma unroll
         for (int k = 0; k < C; ++k) { oe[k] = 0.0f; ou[k] = 0.0f; ov[k] = 0.0f; }
         if (out_lane) {
-          const unsigned char* sj = slot_of(j);
-          ld_f<C>(sj + L::kOffOE + 4 * C * lane, oe);
-          ld_f<C>(sj + L::kOffOU + 4 * C * lane, ou);
-          ld_f<C>(sj + L::kOffOV + 4 * C * lane, ov);
+          const unsigned char* pj = ring + sj * SLOT;
+          ld_f<C>(pj + L::kOffOE + 4 * C * lane, oe);
+          ld_f<C>(pj + L::kOffOU + 4 * C * lane, ou);
+          ld_f<C>(pj + L::kOffOV + 4 * C * lane, ov);
         }
       }
       __syncwarp();
       if (j + kNbuf <= rlast) {
         if (lane == 0) {
           fence_proxy_async();
-          issue(j + kNbuf);
+          issue(j + kNbuf, sj);
         }
         issued = j + kNbuf;
       }
+      sj = nxt(sj);
 
       // ---- cell updates of row j ----
       float ne[C], nu[C], nv[C];
@@ -714,7 +709,7 @@ __global__ void __launch_bounds__(kWarps * 32, C == 2 ? 4 : 2) k_sweep(StepArgs3
       // a copy did not arrive in time: flag it and let every copy this warp
       // issued land (each wait bounded) before the shared memory goes away
       if (lane == 0) atomicExch(&ctl->error, 1);
-      for (int r = waited + 1; r <= issued; ++r) wait_row(r);
+      for (int r = waited + 1; r <= issued; ++r) wait_next();
     }
   }
 
