@@ -153,6 +153,26 @@ int rkb_get_precision(void *handle);
  * not depend on either. */
 int rkb_set_sweep(void *handle, int cols_per_lane, int rows);
 
+/* Batches of independent simulations (ensembles of uneven sizes): every
+ * member is advanced by one launch per phase covering all members, chunks of
+ * steps captured in CUDA graphs; each member keeps its own dt, clock,
+ * boundary parameters and host views.  Members must be finalised, share the
+ * Riemann solver and be at least max(nghost, 2) cells wide; a simulation
+ * belongs to one batch at most.  `precision` (64 or 32) is applied to every
+ * member.  Destroying a member makes later calls on the batch return -1. */
+int rkb_batch_create(void **handles, int n, int precision, void **batch);
+void rkb_batch_destroy(void **batch);
+int rkb_batch_step(void *batch, int n_steps);
+int rkb_batch_advance(void *batch, double target_time);
+/* n steps of every member between CUDA events on the batch's stream. */
+int rkb_batch_time_steps(void *batch, int n, double *ms);
+/* Times each candidate kernel shape (FP64: the four tiles; FP32: 2 or 4
+ * columns per lane x rows per warp sweep) for trial_steps steps on the live
+ * state, restores the state exactly, keeps the fastest shape. */
+int rkb_batch_autotune(void *batch, int trial_steps, double *best_ms_per_step);
+/* Kernel shape in use: FP64 (tile, 0); FP32 (columns per lane, rows). */
+int rkb_batch_variant(void *batch, int *a, int *b);
+
 /* Run n steps bracketed by CUDA events on the simulation's own stream;
  * *ms = device time of the n steps (state already resident). */
 int rkb_time_steps(void *handle, int n, double *ms);

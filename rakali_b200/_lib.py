@@ -104,6 +104,13 @@ def load(path: str | None = None):
     _sig(lib, "rkb_set_precision", [H, I], I)
     _sig(lib, "rkb_get_precision", [H], I)
     _sig(lib, "rkb_set_sweep", [H, I, I], I)
+    _sig(lib, "rkb_batch_create", [HP, I, I, HP], I)
+    _sig(lib, "rkb_batch_destroy", [HP], None)
+    _sig(lib, "rkb_batch_step", [H, I], I)
+    _sig(lib, "rkb_batch_advance", [H, D], I)
+    _sig(lib, "rkb_batch_time_steps", [H, I, DP], I)
+    _sig(lib, "rkb_batch_autotune", [H, I, DP], I)
+    _sig(lib, "rkb_batch_variant", [H, IP, IP], I)
     _sig(lib, "rkb_time_steps", [H, I, DP], I)
     _sig(lib, "rkb_profile_steps", [H, I, DP], I)
     _sig(lib, "rkb_cr_pow_third", [D], D)

@@ -35,6 +35,7 @@ UNITS = {
     # with explicit round-to-nearest intrinsics and are never contracted)
     "rkb_step_f32.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
     "rkb_sim.cu": [],
+    "rkb_batch.cu": [],
     "rkb_api.cu": [],
     "rkb_config.cpp": [],
 }

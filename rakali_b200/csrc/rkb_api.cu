@@ -13,6 +13,7 @@
 #include <string>
 
 #include "../../include/rakali.h"
+#include "rkb_batch.hpp"
 #include "rkb_sim.hpp"
 
 namespace {
@@ -27,6 +28,7 @@ constexpr unsigned kMagic = 0x72616B53u;  // 'rakS'
 
 std::mutex g_mu;
 std::set<Handle*> g_live;
+std::set<rkb::Batch*> g_batches;
 thread_local std::string g_err;
 
 Handle* resolve(void* p) {
@@ -170,6 +172,7 @@ void rki_destroy(void** handle) {
     g_live.erase(it);
     h = p;
   }
+  if (h->sim->batch) static_cast<rkb::Batch*>(h->sim->batch)->detach(h->sim);
   delete h->sim;
   h->magic = 0;
   delete h;
@@ -429,6 +432,91 @@ int rkb_profile_steps(void* handle, int n, double* out5) {
 int rkb_get_tile(void* handle) {
   rkb::Sim* s = sim_of(handle);
   return s ? s->tile : kBadHandle;
+}
+
+// ---- batches ----------------------------------------------------------------
+
+static rkb::Batch* batch_of(void* p) {
+  if (!p) return nullptr;
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto* b = static_cast<rkb::Batch*>(p);
+  return g_batches.count(b) ? b : nullptr;
+}
+
+int rkb_batch_create(void** handles, int n, int precision, void** batch) {
+  if (!batch) return fail(kBadHandle, "null batch slot");
+  *batch = nullptr;
+  if (!handles || n <= 0) return fail(-2, "a batch needs at least one simulation");
+  std::vector<rkb::Sim*> sims;
+  for (int i = 0; i < n; ++i) {
+    rkb::Sim* s = sim_of(handles[i]);
+    if (!s) return fail(kBadHandle, "invalid simulation handle in the batch");
+    sims.push_back(s);
+  }
+  auto* b = new rkb::Batch();
+  std::string err;
+  const int rc = b->create(sims, precision, err);
+  if (rc != 0) {
+    delete b;
+    return fail(rc, err);
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_batches.insert(b);
+  }
+  *batch = b;
+  g_err.clear();
+  return 0;
+}
+
+void rkb_batch_destroy(void** batch) {
+  if (!batch || !*batch) return;
+  rkb::Batch* b = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto* p = static_cast<rkb::Batch*>(*batch);
+    if (!g_batches.count(p)) return;
+    g_batches.erase(p);
+    b = p;
+  }
+  delete b;
+  *batch = nullptr;
+}
+
+int rkb_batch_step(void* batch, int n_steps) {
+  rkb::Batch* b = batch_of(batch);
+  if (!b) return kBadHandle;
+  const int rc = b->step(n_steps);
+  return rc ? fail(rc, b->error().empty() ? "batch step failed" : b->error()) : 0;
+}
+
+int rkb_batch_advance(void* batch, double target_time) {
+  rkb::Batch* b = batch_of(batch);
+  if (!b) return kBadHandle;
+  const int rc = b->advance(target_time);
+  return rc ? fail(rc, b->error().empty() ? "batch advance failed" : b->error()) : 0;
+}
+
+int rkb_batch_time_steps(void* batch, int n, double* ms) {
+  rkb::Batch* b = batch_of(batch);
+  if (!b) return kBadHandle;
+  if (!ms) return -2;
+  const int rc = b->time_steps(n, ms);
+  return rc ? fail(rc, b->error().empty() ? "batch timing failed" : b->error()) : 0;
+}
+
+int rkb_batch_autotune(void* batch, int trial_steps, double* best_ms_per_step) {
+  rkb::Batch* b = batch_of(batch);
+  if (!b) return kBadHandle;
+  const int rc = b->autotune(trial_steps, best_ms_per_step);
+  return rc ? fail(rc, b->error().empty() ? "batch autotune failed" : b->error()) : 0;
+}
+
+int rkb_batch_variant(void* batch, int* a, int* b_) {
+  rkb::Batch* b = batch_of(batch);
+  if (!b) return kBadHandle;
+  b->variant(a, b_);
+  return 0;
 }
 
 int rkb_set_precision(void* handle, int bits) {

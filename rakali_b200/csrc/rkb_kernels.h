@@ -123,6 +123,38 @@ int launches_per_step(const StepArgs& a);
 // Queue the CFL reduction of the current state (fills ctl->msx/msy).
 cudaError_t launch_max_speed(const StepArgs& a, cudaStream_t s);
 
+// ---- batches of independent simulations --------------------------------
+// One launch per phase covers every simulation: `args` holds each
+// simulation's StepArgs (device array) and `map` gives each block of the stage
+// launch its simulation and its tile / warp-group index within it.  All
+// simulations of a batch share the kernel variant (tile or columns per lane,
+// HLL / HLLC) and are at least max(nghost, 2) cells wide.
+struct BatchLaunch {
+  const StepArgs* args;
+  const int2* map;
+  int n;        // simulations
+  int blocks;   // blocks of one stage launch
+  int max_nxt, max_nyt;
+  int tile, hllc;
+};
+int batch_stage_blocks(const Grid& g, int tile);
+cudaError_t configure_batch(int tile, int hllc);
+cudaError_t launch_step_batch(const BatchLaunch& bl, cudaStream_t s);
+
+struct BatchLaunch32 {
+  const StepArgs32* args;
+  const int2* map;
+  int n;
+  int blocks;
+  int max_nxt, max_nyt;
+  int cpl, hllc;
+};
+int batch_sweep_blocks(const StepArgs32& a);
+cudaError_t configure_batch32();
+cudaError_t launch_step32_batch(const BatchLaunch32& bl, cudaStream_t s);
+cudaError_t launch_stage32_batch(const BatchLaunch32& bl, int stage, cudaStream_t s);
+cudaError_t launch_bc32_batch(const BatchLaunch32& bl, int stage, cudaStream_t s);
+
 // Kernel-level entry points (device pointers, pitched arrays).
 cudaError_t launch_flux(const Grid& g, int hllc, FieldSet in, const double* b, FluxOut out,
                         int tile, cudaStream_t s);

@@ -771,6 +771,68 @@ int Sim::check_device_error() {
   return -1;
 }
 
+// ---------------------------------------------------------------------------
+// Batch membership
+// ---------------------------------------------------------------------------
+
+int Sim::batch_prepare(int mode, double target, int nsteps) {
+  if (prepare_run(mode, target, nsteps) != 0) return -1;
+  return cudaStreamSynchronize(stream_) == cudaSuccess ? 0 : -1;
+}
+
+int Sim::batch_finish() {
+  pull_ctl();
+  if (check_device_error() != 0) return -1;
+  stepped_ = true;
+  host_is_current_ = false;
+  return 0;
+}
+
+// The state goes home (fields, RK2 save, bed, clock); trial steps may then run
+// on the device; restore() re-uploads exactly that state and clock.  The FP32
+// surface form round-trips through the FP64 host arrays bit for bit.
+int Sim::snapshot() {
+  if (ensure_device() != 0) return -1;
+  ensure_host();
+  pull_ctl();
+  snap_ctl_ = *hctl_;
+  for (int w = 0; w < 4; ++w)  // Chapman surfaces change with every boundary fill
+    RKB_TRY(cudaMemcpyAsync(eta_old_[w].data(), args_.eta_old[w],
+                            eta_old_[w].size() * sizeof(double), cudaMemcpyDeviceToHost,
+                            stream_));
+  RKB_TRY(cudaStreamSynchronize(stream_));
+  snap_cur_ = cur_;
+  snap_t_ = t_current_;
+  snap_dt_ = dt_;
+  snap_steps_ = step_count_;
+  snap_stepped_ = stepped_;
+  return 0;
+}
+
+int Sim::restore() {
+  if (cudaSetDevice(device_) != cudaSuccess) return -1;
+  *hctl_ = snap_ctl_;
+  hctl_->done_blocks = 0u;
+  hctl_->ms_done_blocks = 0u;
+  hctl_->msx_next = 0ull;
+  hctl_->msy_next = 0ull;
+  hctl_->error = 0;
+  RKB_TRY(cudaMemcpyAsync(args_.ctl, hctl_, sizeof(StepCtl), cudaMemcpyHostToDevice, stream_));
+  for (int w = 0; w < 4; ++w)
+    RKB_TRY(cudaMemcpyAsync(args_.eta_old[w], eta_old_[w].data(),
+                            eta_old_[w].size() * sizeof(double), cudaMemcpyHostToDevice,
+                            stream_));
+  RKB_TRY(cudaStreamSynchronize(stream_));
+  cur_ = snap_cur_;
+  t_current_ = snap_t_;
+  dt_ = snap_dt_;
+  step_count_ = snap_steps_;
+  stepped_ = snap_stepped_;
+  on_device_ = false;  // the next run uploads the host arrays, which hold the snapshot
+  host_is_current_ = true;
+  return 0;
+}
+
 int Sim::step(int n) {
   if (n <= 0) return 0;
   return run(1, 0.0, n);

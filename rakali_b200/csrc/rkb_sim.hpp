@@ -68,6 +68,19 @@ class Sim {
   int set_precision(int p);
   const std::string& error_text() const { return err_text_; }
 
+  // ---- membership of a batch (rkb_batch.cu) ----
+  // Set up a run of the device clock (mode 0: advance to `target`, mode 1:
+  // `nsteps` steps) without launching steps: state and parameters resident,
+  // CFL maxima current, kernel arguments in sync.
+  int batch_prepare(int mode, double target, int nsteps);
+  // After a batch ran steps on this simulation: read the device clock back.
+  int batch_finish();
+  // Trial runs (autotuning) on the live state: bring it home, then put it back.
+  int snapshot();
+  int restore();
+  StepArgs32 device_args32() const { return args32_; }
+  void* batch = nullptr;  // the batch this simulation belongs to (at most one)
+
   // Device pointers for the torch / kernel-level paths.
   StepArgs device_args() const { return args_; }
   int current_buffer() const { return cur_; }
@@ -115,6 +128,10 @@ class Sim {
   void* dmem32_ = nullptr;
   StepArgs32 args32_{};
   int auto_rows_[2] = {0, 0};  // automatic rows for 2 and 4 columns per lane
+  StepCtl snap_ctl_{};
+  int snap_cur_ = 0, snap_steps_ = 0;
+  double snap_t_ = 0.0, snap_dt_ = 0.0;
+  bool snap_stepped_ = false;
 
   struct GraphEntry {
     int steps, hllc, tile, prec, rows;

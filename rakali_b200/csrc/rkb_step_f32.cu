@@ -397,8 +397,9 @@ __device__ __forceinline__ void st_f(float* p, const float (&v)[C]) {
 // Stage kernel
 // ---------------------------------------------------------------------------
 // STAGE 1: U^n (buffer cur) -> U* (S).  STAGE 2: U*, U^n -> U^{n+1} (cur^1).
+// Block `blk` of the `nblk` blocks that cover one simulation.
 template <int C, bool HLLC, int STAGE>
-__global__ void __launch_bounds__(kWarps * 32, C == 2 ? 4 : 2) k_sweep(StepArgs32 a) {
+__device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, unsigned nblk) {
   using L = Lay<C>;
   constexpr int SLOT = L::slot(STAGE);
   extern __shared__ __align__(128) unsigned char smem[];
@@ -433,8 +434,8 @@ __global__ void __launch_bounds__(kWarps * 32, C == 2 ? 4 : 2) k_sweep(StepArgs3
   const FieldSet32 old = cur ? a.U1 : a.U0;
   const FieldSet32 out = STAGE == 1 ? a.S : (cur ? a.U0 : a.U1);
 
-  const unsigned nw = gridDim.x * kWarps;
-  const unsigned gw = blockIdx.x * kWarps + warp;
+  const unsigned nw = nblk * kWarps;
+  const unsigned gw = blk * kWarps + warp;
   double part = 0.0, sponge_d = 0.0;
   float wsx = 0.0f, wsy = 0.0f;
 
@@ -734,12 +735,30 @@ __global__ void __launch_bounds__(kWarps * 32, C == 2 ? 4 : 2) k_sweep(StepArgs3
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
-    last = atomicAdd(&ctl->done_blocks, 1u) == gridDim.x - 1;
+    last = atomicAdd(&ctl->done_blocks, 1u) == nblk - 1;
   }
   __syncthreads();
   if (!last) return;
   __threadfence();
   finalize_step(g, ctl, phys, a.partials, nw, dtd, cur);
+}
+
+template <int C, bool HLLC, int STAGE>
+__global__ void __launch_bounds__(kWarps * 32, C == 2 ? 4 : 2) k_sweep(StepArgs32 a) {
+  sweep_body<C, HLLC, STAGE>(a, blockIdx.x, gridDim.x);
+}
+
+// Every simulation of a batch in one launch: map[blockIdx.x] = (simulation,
+// block index within that simulation's sweep).
+template <int C, bool HLLC, int STAGE>
+__global__ void __launch_bounds__(kWarps * 32, C == 2 ? 4 : 2)
+    k_sweep_batch(const StepArgs32* __restrict__ args, const int2* __restrict__ map) {
+  __shared__ StepArgs32 sa;
+  const int2 m = map[blockIdx.x];
+  if (threadIdx.x == 0) sa = args[m.x];
+  __syncthreads();
+  const unsigned nblk = (unsigned)((sa.nstrips * sa.nrowblk + kWarps - 1) / kWarps);
+  sweep_body<C, HLLC, STAGE>(sa, (unsigned)m.y, nblk);
 }
 
 // ---------------------------------------------------------------------------
@@ -748,22 +767,21 @@ __global__ void __launch_bounds__(kWarps * 32, C == 2 ? 4 : 2) k_sweep(StepArgs3
 // Same edge walk as the FP64 fill; depths are read as max(0, eta - b) in FP64
 // and ghost surfaces written as surface_of(h, b).  A wall ghost takes the
 // mirrored cell's surface unchanged (its bed is the mirrored bed).
-__global__ void k_bc32(StepArgs32 a, int stage, int e0, int first_launch) {
-  const Grid g = a.g;
+__device__ __forceinline__ void bc32_body(const StepArgs32& a, int stage, int w, int t,
+                                          bool writer) {
+  const Grid& g = a.g;
   StepCtl* ctl = a.ctl;
   const BcParams* bc = a.bc;
   double dt;
   const bool active = step_begin(ctl, a.phys, g, dt);
-  if (first_launch && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+  if (writer) {
     ctl->active = active ? 1 : 0;
     ctl->dt = dt;
   }
   if (!active) return;
-  const int w = e0 + blockIdx.y;
   const int type = bc->type[w];
   if (type == kNested) return;
   const Edge e = make_edge(w, g);
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= e.n_tan) return;
   const double time = stage == 1 ? ctl->t : ctl->t + dt;
   const int cur = ctl->cur;
@@ -864,6 +882,20 @@ __global__ void k_bc32(StepArgs32 a, int stage, int e0, int first_launch) {
     }
     eo[t] = ei;
   }
+}
+
+__global__ void k_bc32(StepArgs32 a, int stage, int e0, int first_launch) {
+  bc32_body(a, stage, e0 + (int)blockIdx.y, (int)(blockIdx.x * blockDim.x + threadIdx.x),
+            first_launch && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0);
+}
+
+__global__ void k_bc32_batch(const StepArgs32* __restrict__ args, int stage, int e0,
+                             int first_launch) {
+  __shared__ StepArgs32 sa;
+  if (threadIdx.x == 0) sa = args[blockIdx.z];
+  __syncthreads();
+  bc32_body(sa, stage, e0 + (int)blockIdx.y, (int)(blockIdx.x * blockDim.x + threadIdx.x),
+            first_launch && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0);
 }
 
 // CFL maxima of the current state (before the first step, or after the host
@@ -1100,6 +1132,61 @@ cudaError_t launch_to_depth(const Grid& g32, const Grid& g64, FieldSet32 src, co
   dim3 grid((unsigned)((g32.nxt + 127) / 128), (unsigned)g32.nyt);
   k_to_depth<<<grid, 128, 0, s>>>(g32, g64, src, b32, dst, bed_out);
   return cudaGetLastError();
+}
+
+// ---- batches ----------------------------------------------------------------
+
+int batch_sweep_blocks(const StepArgs32& a) { return (a.nstrips * a.nrowblk + kWarps - 1) / kWarps; }
+
+template <int C, bool HLLC>
+static cudaError_t set_smem_batch() {
+  cudaError_t e = cudaFuncSetAttribute(k_sweep_batch<C, HLLC, 1>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kWarps * kNbuf * Lay<C>::slot(1));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_sweep_batch<C, HLLC, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kWarps * kNbuf * Lay<C>::slot(2));
+  return e;
+}
+
+cudaError_t configure_batch32() {
+  cudaError_t e = set_smem_batch<2, false>();
+  if (e == cudaSuccess) e = set_smem_batch<2, true>();
+  if (e == cudaSuccess) e = set_smem_batch<4, false>();
+  if (e == cudaSuccess) e = set_smem_batch<4, true>();
+  return e;
+}
+
+template <int C, int STAGE>
+static cudaError_t launch_sweep_batch_t(const BatchLaunch32& bl, cudaStream_t s) {
+  const size_t bytes = (size_t)kWarps * kNbuf * Lay<C>::slot(STAGE);
+  if (bl.hllc)
+    k_sweep_batch<C, true, STAGE><<<(unsigned)bl.blocks, kWarps * 32, bytes, s>>>(bl.args, bl.map);
+  else
+    k_sweep_batch<C, false, STAGE><<<(unsigned)bl.blocks, kWarps * 32, bytes, s>>>(bl.args, bl.map);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_stage32_batch(const BatchLaunch32& bl, int stage, cudaStream_t s) {
+  if (stage == 1) return bl.cpl == 4 ? launch_sweep_batch_t<4, 1>(bl, s) : launch_sweep_batch_t<2, 1>(bl, s);
+  return bl.cpl == 4 ? launch_sweep_batch_t<4, 2>(bl, s) : launch_sweep_batch_t<2, 2>(bl, s);
+}
+
+cudaError_t launch_bc32_batch(const BatchLaunch32& bl, int stage, cudaStream_t s) {
+  const int tpb = 128;
+  const dim3 gx((unsigned)((bl.max_nyt + tpb - 1) / tpb), 2, (unsigned)bl.n);
+  k_bc32_batch<<<gx, tpb, 0, s>>>(bl.args, stage, 0, stage == 1 ? 1 : 0);
+  const dim3 gy((unsigned)((bl.max_nxt + tpb - 1) / tpb), 2, (unsigned)bl.n);
+  k_bc32_batch<<<gy, tpb, 0, s>>>(bl.args, stage, 2, 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_step32_batch(const BatchLaunch32& bl, cudaStream_t s) {
+  cudaError_t e = launch_bc32_batch(bl, 1, s);
+  if (e == cudaSuccess) e = launch_stage32_batch(bl, 1, s);
+  if (e == cudaSuccess) e = launch_bc32_batch(bl, 2, s);
+  if (e == cudaSuccess) e = launch_stage32_batch(bl, 2, s);
+  return e;
 }
 
 }  // namespace rkb

@@ -23,29 +23,32 @@ namespace rkb {
 // Boundary conditions (rki_boundary.F90:40-552)
 // ---------------------------------------------------------------------------
 
-// One thread per tangential position t of an edge, looping over the ghost
+// One thread per tangential position t of edge w, looping over the ghost
 // layers k (so the Chapman surface refresh of position t is race-free).
-// The kernel fills edges [e0, e0 + gridDim.y).  Ghost values go to `h/hu/hv`
-// and, when `h2` is non-null, also to a second buffer.
-__global__ void k_bc(Grid g, StepCtl* ctl, const Physics* phys, const BcParams* bc, int stage,
-                     int e0, FieldSet U0, FieldSet U1, FieldSet S, double* __restrict__ b,
-                     double* eta_old_w, double* eta_old_e, double* eta_old_s, double* eta_old_n,
-                     int first_launch) {
+// Ghost values go to the stage's input buffer and, in stage 2, also to the
+// buffer that receives U^{n+1}.  `writer` marks the one thread of the step's
+// first boundary launch that publishes this step's active flag and dt.
+__device__ __forceinline__ void bc_body(const StepArgs& a, int stage, int w, int t, bool writer) {
+  const Grid& g = a.g;
+  StepCtl* ctl = a.ctl;
+  const BcParams* bc = a.bc;
+  double* __restrict__ b = a.b;
   double dt;
-  bool active = step_begin(ctl, phys, g, dt);
-  if (first_launch) {
-    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
-      ctl->active = active ? 1 : 0;
-      ctl->dt = dt;
-    }
+  bool active = step_begin(ctl, a.phys, g, dt);
+  if (writer) {
+    ctl->active = active ? 1 : 0;
+    ctl->dt = dt;
   }
   if (!active) return;
-  const int w = e0 + blockIdx.y;
   const int type = bc->type[w];
   if (type == kNested) return;
   const Edge e = make_edge(w, g);
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= e.n_tan) return;
+  const FieldSet U0 = a.U0, U1 = a.U1, S = a.S;
+  double* eta_old_w = a.eta_old[0];
+  double* eta_old_e = a.eta_old[1];
+  double* eta_old_s = a.eta_old[2];
+  double* eta_old_n = a.eta_old[3];
 
   const double time = stage == 1 ? ctl->t : ctl->t + dt;
   const int cur = ctl->cur;
@@ -180,6 +183,21 @@ __global__ void k_bc(Grid g, StepCtl* ctl, const Physics* phys, const BcParams* 
   }
 }
 
+// Edges [e0, e0 + gridDim.y) of one simulation.
+__global__ void k_bc(StepArgs a, int stage, int e0, int first_launch) {
+  bc_body(a, stage, e0 + (int)blockIdx.y, (int)(blockIdx.x * blockDim.x + threadIdx.x),
+          first_launch && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0);
+}
+
+// The same edges of every simulation of a batch (blockIdx.z = simulation).
+__global__ void k_bc_batch(const StepArgs* __restrict__ args, int stage, int e0, int first_launch) {
+  __shared__ StepArgs sa;
+  if (threadIdx.x == 0) sa = args[blockIdx.z];
+  __syncthreads();
+  bc_body(sa, stage, e0 + (int)blockIdx.y, (int)(blockIdx.x * blockDim.x + threadIdx.x),
+          first_launch && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0);
+}
+
 // ---------------------------------------------------------------------------
 // CFL reduction over the current state (used when no stage-2 epilogue has
 // produced it yet: after create or after the host changed the state).
@@ -293,11 +311,14 @@ __device__ __forceinline__ void sponge(double& h, double& u, double& v, const Bc
 // STAGE 2: U* (S) and U^n (buffer cur) -> U^{n+1} (buffer cur^1).
 // STAGE 0: flux divergence only (kernel-level API): writes flux/mass-flux
 //          arrays from `in`, no update.
+// Tile (bx, by) of a gx x gy tiling of one simulation.
 template <int TX, int TY, bool HLLC, int STAGE>
-__global__ void __launch_bounds__(TX * TY)
-    k_stage(Grid g, StepCtl* ctl, const Physics* phys, const BcParams* bcp, FieldSet U0,
-            FieldSet U1, FieldSet S, const double* __restrict__ b, Forcing fo,
-            double* __restrict__ partials, FluxOut fl) {
+__device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Physics* phys,
+                                           const BcParams* bcp, const FieldSet& U0,
+                                           const FieldSet& U1, const FieldSet& S,
+                                           const double* __restrict__ b, const Forcing& fo,
+                                           double* __restrict__ partials, const FluxOut& fl,
+                                           unsigned bx, unsigned by, unsigned gx, unsigned gy) {
   using SM = StageSmem<TX, TY>;
   constexpr int TW = SM::TW;
   constexpr int NTH = TX * TY;
@@ -326,8 +347,8 @@ __global__ void __launch_bounds__(TX * TY)
   const FieldSet in = STAGE == 2 ? S : (cur ? U1 : U0);
 
   const int tid = threadIdx.x;
-  const int gx0 = g.ng + blockIdx.x * TX;  // first interior cell of the tile
-  const int gy0 = g.ng + blockIdx.y * TY;
+  const int gx0 = g.ng + (int)bx * TX;  // first interior cell of the tile
+  const int gy0 = g.ng + (int)by * TY;
 
   // Coriolis rotation of this stage, cos/sin(f dt), correctly rounded once
   // per block (rki_kernel_fused.F90:211-214)
@@ -487,8 +508,8 @@ __global__ void __launch_bounds__(TX * TY)
     red[1][tid >> 5] = sponge_d;
   }
   __syncthreads();
-  const unsigned int nblocks = gridDim.x * gridDim.y;
-  const unsigned int bid = blockIdx.y * gridDim.x + blockIdx.x;
+  const unsigned int nblocks = gx * gy;
+  const unsigned int bid = by * gx + bx;
   if (tid == 0) {
     double s0 = 0.0, s1 = 0.0;
     for (int w = 0; w < NTH / 32; ++w) {
@@ -511,6 +532,32 @@ __global__ void __launch_bounds__(TX * TY)
   if (!last) return;
   __threadfence();
   finalize_step(g, ctl, phys, partials, nblocks, dt, cur);
+}
+
+template <int TX, int TY, bool HLLC, int STAGE>
+__global__ void __launch_bounds__(TX * TY)
+    k_stage(Grid g, StepCtl* ctl, const Physics* phys, const BcParams* bcp, FieldSet U0,
+            FieldSet U1, FieldSet S, const double* __restrict__ b, Forcing fo,
+            double* __restrict__ partials, FluxOut fl) {
+  stage_body<TX, TY, HLLC, STAGE>(g, ctl, phys, bcp, U0, U1, S, b, fo, partials, fl, blockIdx.x,
+                                  blockIdx.y, gridDim.x, gridDim.y);
+}
+
+// Every simulation of a batch in one launch: map[blockIdx.x] = (simulation,
+// tile index within that simulation's tiling).
+template <int TX, int TY, bool HLLC, int STAGE>
+__global__ void __launch_bounds__(TX * TY)
+    k_stage_batch(const StepArgs* __restrict__ args, const int2* __restrict__ map) {
+  __shared__ StepArgs sa;
+  const int2 m = map[blockIdx.x];
+  if (threadIdx.x == 0) sa = args[m.x];
+  __syncthreads();
+  const unsigned gx = (unsigned)((sa.g.nx_phys() + TX - 1) / TX);
+  const unsigned gy = (unsigned)((sa.g.ny_phys() + TY - 1) / TY);
+  const FluxOut none{};
+  stage_body<TX, TY, HLLC, STAGE>(sa.g, sa.ctl, sa.phys, sa.bc, sa.U0, sa.U1, sa.S, sa.b, sa.fo,
+                                  sa.partials, none, (unsigned)m.y % gx, (unsigned)m.y / gx, gx,
+                                  gy);
 }
 
 // ---------------------------------------------------------------------------
@@ -838,8 +885,7 @@ cudaError_t launch_bc(const StepArgs& a, int stage, cudaStream_t s) {
   int first = stage == 1 ? 1 : 0;
   auto go = [&](int e0, int count, int n_tan) {
     dim3 grid((unsigned)((n_tan + tpb - 1) / tpb), (unsigned)count);
-    k_bc<<<grid, tpb, 0, s>>>(g, a.ctl, a.phys, a.bc, stage, e0, a.U0, a.U1, a.S, a.b,
-                              a.eta_old[0], a.eta_old[1], a.eta_old[2], a.eta_old[3], first);
+    k_bc<<<grid, tpb, 0, s>>>(a, stage, e0, first);
     first = 0;
   };
   if (pair_x) {
@@ -887,6 +933,78 @@ cudaError_t launch_max_speed(const StepArgs& a, cudaStream_t s) {
   if (blocks < 1) blocks = 1;
   k_max_speed<<<(unsigned)blocks, 256, 0, s>>>(a.g, a.ctl, a.U0, a.U1);
   return cudaGetLastError();
+}
+
+// ---- batches: every simulation of a batch in one launch per phase ----
+
+int batch_stage_blocks(const Grid& g, int tile) {
+  const dim3 d = stage_grid(g, tile);
+  return (int)(d.x * d.y);
+}
+
+template <int TX, int TY, bool HLLC>
+static cudaError_t configure_batch_t() {
+  const int bytes = (int)StageSmem<TX, TY>::BYTES;
+  cudaError_t e = cudaFuncSetAttribute(k_stage_batch<TX, TY, HLLC, 1>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_stage_batch<TX, TY, HLLC, 2>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  return e;
+}
+
+cudaError_t configure_batch(int tile, int hllc) {
+  const bool h = hllc != 0;
+  switch (tile) {
+    case kTile32x8: return h ? configure_batch_t<32, 8, true>() : configure_batch_t<32, 8, false>();
+    case kTile32x16: return h ? configure_batch_t<32, 16, true>() : configure_batch_t<32, 16, false>();
+    case kTile64x4: return h ? configure_batch_t<64, 4, true>() : configure_batch_t<64, 4, false>();
+    case kTile16x16: return h ? configure_batch_t<16, 16, true>() : configure_batch_t<16, 16, false>();
+    default: return cudaErrorInvalidValue;  // batches use the shared-memory tiles
+  }
+}
+
+template <int TX, int TY, bool HLLC, int STAGE>
+static cudaError_t launch_stage_batch_t(const BatchLaunch& bl, cudaStream_t s) {
+  k_stage_batch<TX, TY, HLLC, STAGE><<<(unsigned)bl.blocks, TX * TY, StageSmem<TX, TY>::BYTES, s>>>(
+      bl.args, bl.map);
+  return cudaGetLastError();
+}
+
+template <int STAGE>
+static cudaError_t launch_stage_batch(const BatchLaunch& bl, cudaStream_t s) {
+  const bool h = bl.hllc != 0;
+  switch (bl.tile) {
+    case kTile32x8:
+      return h ? launch_stage_batch_t<32, 8, true, STAGE>(bl, s) : launch_stage_batch_t<32, 8, false, STAGE>(bl, s);
+    case kTile32x16:
+      return h ? launch_stage_batch_t<32, 16, true, STAGE>(bl, s) : launch_stage_batch_t<32, 16, false, STAGE>(bl, s);
+    case kTile64x4:
+      return h ? launch_stage_batch_t<64, 4, true, STAGE>(bl, s) : launch_stage_batch_t<64, 4, false, STAGE>(bl, s);
+    case kTile16x16:
+      return h ? launch_stage_batch_t<16, 16, true, STAGE>(bl, s) : launch_stage_batch_t<16, 16, false, STAGE>(bl, s);
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+// W/E edges of every simulation, then S/N (every simulation of a batch is at
+// least max(nghost, 2) cells wide, so opposite edges never overlap).
+cudaError_t launch_bc_batch(const BatchLaunch& bl, int stage, cudaStream_t s) {
+  const int tpb = 128;
+  const dim3 gx((unsigned)((bl.max_nyt + tpb - 1) / tpb), 2, (unsigned)bl.n);
+  k_bc_batch<<<gx, tpb, 0, s>>>(bl.args, stage, 0, stage == 1 ? 1 : 0);
+  const dim3 gy((unsigned)((bl.max_nxt + tpb - 1) / tpb), 2, (unsigned)bl.n);
+  k_bc_batch<<<gy, tpb, 0, s>>>(bl.args, stage, 2, 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_step_batch(const BatchLaunch& bl, cudaStream_t s) {
+  cudaError_t e = launch_bc_batch(bl, 1, s);
+  if (e == cudaSuccess) e = launch_stage_batch<1>(bl, s);
+  if (e == cudaSuccess) e = launch_bc_batch(bl, 2, s);
+  if (e == cudaSuccess) e = launch_stage_batch<2>(bl, s);
+  return e;
 }
 
 cudaError_t launch_flux(const Grid& g, int hllc, FieldSet in, const double* b, FluxOut out,

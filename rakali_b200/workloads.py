@@ -55,3 +55,45 @@ def config2(n=4096, dx=5.0, seed=2024, hump=True):
 
 CONFIG2_KW = dict(dx=5.0, dy=5.0, t_end=1.0e9, cfl=0.45, manning_n=0.025,
                   bc_west="wall", bc_east="wall", bc_south="wall", bc_north="wall")
+
+
+M2_PERIOD = 44712.0  # s
+
+
+def ensemble_members(n_inst=256, seed=7, size=(64, 1024), dx=10.0, manning_n=0.02):
+    """Configurations of the batched ensemble: per member (nx, ny) uniform in
+    [size[0], size[1]], a planar bed from -20 m at the west edge to +2 m at the
+    east edge, still water at eta = 0 (the east part starts dry), a tidal west
+    edge driven by one M2 constituent (amplitude U[0.5, 2] m, phase U[0, 2 pi)),
+    walls elsewhere, Manning n = 0.02.
+
+    Returns a list of dicts: ``kw`` (namelist keywords), ``b`` (interior bed),
+    ``h`` (initial depth), ``tide`` ((amp,), (phase,), (omega,)).
+    """
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_inst):
+        nx, ny = (int(v) for v in rng.integers(size[0], size[1] + 1, 2))
+        amp = float(rng.uniform(0.5, 2.0))
+        phase = float(rng.uniform(0.0, 2.0 * np.pi))
+        x = (np.arange(nx) + 0.5) / nx
+        b = np.asfortranarray(np.repeat((-20.0 + 22.0 * x)[:, None], ny, axis=1))
+        h = np.asfortranarray(np.maximum(0.0 - b, 0.0))
+        kw = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1.0e9, cfl=0.45, manning_n=manning_n,
+                  bc_west="tidal", bc_east="wall", bc_south="wall", bc_north="wall")
+        out.append(dict(kw=kw, b=b, h=h,
+                        tide=((amp,), (phase,), (2.0 * np.pi / M2_PERIOD,))))
+    return out
+
+
+def build_member(m, precision=64):
+    """A finalised ``Rakali`` for one ``ensemble_members`` entry."""
+    from .core import Rakali
+    s = Rakali(defer_init=True, **m["kw"])
+    s.set_bathymetry(m["b"])
+    s.set_initial_h(m["h"])
+    s.finalize()
+    s.set_tidal_constituents(*m["tide"])
+    if precision != 64:
+        s.set_precision(precision)
+    return s
