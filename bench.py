@@ -307,6 +307,50 @@ def _fp32_error(b, h, n, steps):
             "note": "free surface vs the FP64 step; floor = FP64 step vs itself with h x (1 + 1e-7 noise)"}
 
 
+def run_ensemble(args, world, local_rank, dist):
+    """The batched ensemble: 256 members of uneven sizes (U[64, 1024] cells a
+    side, planar bed -20 m -> +2 m, M2 tide at the west edge with seeded
+    amplitude and phase, walls, n = 0.02), autotuned, then timed over
+    `ensemble_steps` steps in each form."""
+    import torch
+
+    from rakali_b200 import workloads as wl
+    from rakali_b200.ensemble import Ensemble
+
+    torch.cuda.set_device(local_rank)
+    rank = int(os.environ.get("RANK", "0"))
+    t_setup = time.perf_counter()
+    members = wl.ensemble_members(n_inst=args.ensemble_members, seed=7 + rank)
+    sims = [wl.build_member(m) for m in members]
+    cells = sum(s.nx * s.ny for s in sims)
+    setup_s = time.perf_counter() - t_setup
+    out = {"workload": f"{len(sims)} independent members, {cells} cells in total "
+                       "(nx, ny ~ U[64, 1024], dx = 10 m, planar bed -20 -> +2 m, M2 tide "
+                       "west with seeded amplitude/phase, walls, n = 0.02)",
+           "members": len(sims), "cells_per_gpu": cells, "setup_s": setup_s, "forms": {}}
+    for prec in (64, 32):
+        with Ensemble(sims, precision=prec) as ens:
+            best = ens.autotune(trial_steps=3)
+            ens.step(max(args.warmup, 3))
+            if dist is not None:
+                dist.barrier()
+            with ClockSampler(visible_gpu_index(local_rank)) as clk:
+                ms = ens.time_steps(args.ensemble_steps)
+            if dist is not None:
+                t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                ms = float(t.item())
+            out["forms"][f"fp{prec}"] = {
+                "value": world * cells * args.ensemble_steps / (ms * 1e-3),
+                "unit": "cell-updates/s", "steps": args.ensemble_steps,
+                "ms_per_step": ms / args.ensemble_steps, "variant": list(ens.variant),
+                "autotune_best_ms_per_step": best, "clocks": clk.summary(),
+                "launches_per_step": 6}
+    for s in sims:
+        s.close()
+    return out
+
+
 def run_b200(args, rank, world, local_rank, dist):
     import torch
 
@@ -333,6 +377,7 @@ def run_b200(args, rank, world, local_rank, dist):
         forms[prec] = _form_numbers(sim, args, world, local_rank, dist, cells)
         forms[prec]["roofline"] = _roofline(forms[prec], prec, cells, world)
     sim.close()
+    ens = run_ensemble(args, world, local_rank, dist) if args.ensemble_steps > 0 else None
     err = None
     if args.both_forms and rank == 0 and not args.no_accuracy:
         err = _fp32_error(b, h, n, min(args.steps, 500))
@@ -369,6 +414,8 @@ def run_b200(args, rank, world, local_rank, dist):
             line["forms"][f"fp{prec}"] = entry
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
+    if args.ensemble_steps > 0:
+        line["ensemble"] = ens
     print(json.dumps(line), flush=True)
     return 0
 
@@ -388,6 +435,10 @@ def main():
                          "32 = FP32 surface form")
     ap.add_argument("--one-form", dest="both_forms", action="store_false",
                     help="time only the headline form (default: both, the other under 'forms')")
+    ap.add_argument("--ensemble-steps", type=int, default=2000,
+                    help="steps of the batched 256-member ensemble run after the single-grid "
+                         "forms (0 skips it)")
+    ap.add_argument("--ensemble-members", type=int, default=256)
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the FP32-vs-FP64 error measurement")
     ap.add_argument("--sweep-cols", type=int, choices=(0, 2, 4), default=0,
