@@ -173,6 +173,35 @@ int rkb_batch_autotune(void *batch, int trial_steps, double *best_ms_per_step);
 /* Kernel shape in use: FP64 (tile, 0); FP32 (columns per lane, rows). */
 int rkb_batch_variant(void *batch, int *a, int *b);
 
+/* Gauge-misfit adjoint of the FP64 step (walls, HLL or HLLC, Manning
+ * friction with a per-cell n field).  J = sum over steps 1..n_steps and the
+ * gauges of (h + b - obs)^2 on a fixed dt sequence; gradients by
+ * hand-written reverse kernels with sqrt(n_steps) checkpointing.  Interior
+ * arrays are (nx, ny) Fortran order on the host; gauges are interior
+ * (i, j), 0-based, distinct; obs is (n_steps, n_gauges) row-major. */
+int rkb_adjoint_create(int nx, int ny, int nghost, double dx, double dy, double cfl, int use_hllc,
+                       int n_steps, const double *h0, const double *hu0, const double *hv0,
+                       const int *gauge_i, const int *gauge_j, int n_gauges, void **adj);
+void rkb_adjoint_destroy(void **adj);
+int rkb_adjoint_set_obs(void *adj, const double *obs);
+int rkb_adjoint_set_dt(void *adj, const double *dts);
+int rkb_adjoint_get_dt(void *adj, double *dts);
+/* Forward run: record_dt != 0 takes CFL steps and stores them (else the
+ * stored sequence is replayed).  n_field may be NULL (uniform n_scalar).
+ * eta_gauges (optional) receives (n_steps, n_gauges) surfaces. */
+int rkb_adjoint_forward(void *adj, const double *b, const double *n_field, double n_scalar,
+                        int record_dt, double *J, double *eta_gauges);
+/* J and dJ/db, dJ/dn (interior (nx, ny) arrays) on the stored dt sequence. */
+int rkb_adjoint_gradient(void *adj, const double *b, const double *n_field, double n_scalar,
+                         double *J, double *grad_b, double *grad_n);
+int rkb_adjoint_checkpoint_interval(void *adj);
+/* Host builds of the face flux / cell update and their adjoints (for
+ * finite-difference checks without a GPU). */
+void rkb_test_face_flux(int dir, int hllc, const double *in8, double *out6);
+void rkb_test_face_adj(int dir, int hllc, const double *in8, const double *gout6, double *gin8);
+void rkb_test_cell(const double *in4, double dt, double *out3);
+void rkb_test_cell_adj(const double *in4, double dt, const double *gout3, double *gin4);
+
 /* Run n steps bracketed by CUDA events on the simulation's own stream;
  * *ms = device time of the n steps (state already resident). */
 int rkb_time_steps(void *handle, int n, double *ms);

@@ -111,6 +111,18 @@ def load(path: str | None = None):
     _sig(lib, "rkb_batch_time_steps", [H, I, DP], I)
     _sig(lib, "rkb_batch_autotune", [H, I, DP], I)
     _sig(lib, "rkb_batch_variant", [H, IP, IP], I)
+    _sig(lib, "rkb_adjoint_create", [I, I, I, D, D, D, I, I, DP, DP, DP, IP, IP, I, HP], I)
+    _sig(lib, "rkb_adjoint_destroy", [HP], None)
+    _sig(lib, "rkb_adjoint_set_obs", [H, DP], I)
+    _sig(lib, "rkb_adjoint_set_dt", [H, DP], I)
+    _sig(lib, "rkb_adjoint_get_dt", [H, DP], I)
+    _sig(lib, "rkb_adjoint_forward", [H, DP, DP, D, I, DP, DP], I)
+    _sig(lib, "rkb_adjoint_gradient", [H, DP, DP, D, DP, DP, DP], I)
+    _sig(lib, "rkb_adjoint_checkpoint_interval", [H], I)
+    _sig(lib, "rkb_test_face_flux", [I, I, DP, DP], None)
+    _sig(lib, "rkb_test_face_adj", [I, I, DP, DP, DP], None)
+    _sig(lib, "rkb_test_cell", [DP, D, DP], None)
+    _sig(lib, "rkb_test_cell_adj", [DP, D, DP, DP], None)
     _sig(lib, "rkb_time_steps", [H, I, DP], I)
     _sig(lib, "rkb_profile_steps", [H, I, DP], I)
     _sig(lib, "rkb_cr_pow_third", [D], D)

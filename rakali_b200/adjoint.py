@@ -1,0 +1,172 @@
+"""Gradients of a gauge misfit with respect to the bed and the Manning-n field.
+
+``GaugeMisfit`` wraps the hand-written adjoint of the FP64 step in
+librakali.so (rkb_adjoint_*): J = sum over steps 1..N and gauge cells of
+(eta - eta_obs)^2, eta = h + b, for the SSP-RK2 step with wall boundaries,
+HLL or HLLC fluxes and Manning friction with a per-cell n field, on a fixed dt
+sequence (``record_dt`` takes CFL steps once and stores them; every later run
+replays them, so J is a piecewise-smooth function of b and n).  The adjoint
+uses sqrt(N)-step checkpointing with recompute.
+
+``misfit(problem, b, n)`` is the ``torch.autograd.Function`` front end: it
+returns J as a 0-d float64 tensor and back-propagates dJ/db, dJ/dn.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+_DP = ctypes.POINTER(ctypes.c_double)
+_IP = ctypes.POINTER(ctypes.c_int)
+
+
+def _f(a, shape):
+    a = np.asfortranarray(np.asarray(a, dtype=np.float64))
+    if a.shape != shape:
+        raise ValueError(f"expected shape {shape}, got {a.shape}")
+    return a
+
+
+class GaugeMisfit:
+    """The misfit problem: initial state, gauges, observations, dt sequence."""
+
+    def __init__(self, nx, ny, dx, dy, h0, gauges, n_steps, hu0=None, hv0=None, nghost=2,
+                 cfl=0.45, use_hllc=False):
+        self._lib = _lib.load()
+        self.nx, self.ny, self.n_steps = int(nx), int(ny), int(n_steps)
+        shape = (self.nx, self.ny)
+        h0 = _f(h0, shape)
+        hu0 = _f(np.zeros(shape) if hu0 is None else hu0, shape)
+        hv0 = _f(np.zeros(shape) if hv0 is None else hv0, shape)
+        gi = np.ascontiguousarray([int(g[0]) for g in gauges], dtype=np.int32)
+        gj = np.ascontiguousarray([int(g[1]) for g in gauges], dtype=np.int32)
+        self.n_gauges = len(gi)
+        self._a = ctypes.c_void_p()
+        rc = self._lib.rkb_adjoint_create(self.nx, self.ny, int(nghost), float(dx), float(dy),
+                                          float(cfl), int(bool(use_hllc)), self.n_steps,
+                                          h0.ctypes.data_as(_DP), hu0.ctypes.data_as(_DP),
+                                          hv0.ctypes.data_as(_DP), gi.ctypes.data_as(_IP),
+                                          gj.ctypes.data_as(_IP), self.n_gauges,
+                                          ctypes.byref(self._a))
+        if rc != 0:
+            raise RuntimeError(f"adjoint setup failed (rc={rc}): {_lib.last_error(self._lib)}")
+        self.set_observations(np.zeros((self.n_steps, self.n_gauges)))
+
+    def _rc(self, rc, what):
+        if rc != 0:
+            raise RuntimeError(f"{what} failed (rc={rc}): {_lib.last_error(self._lib)}")
+
+    def _fields(self, b, n):
+        shape = (self.nx, self.ny)
+        b = _f(b, shape)
+        if n is None or np.ndim(n) == 0:
+            return b, None, float(0.0 if n is None else n)
+        return b, _f(n, shape), 0.0
+
+    def set_observations(self, obs):
+        obs = np.ascontiguousarray(obs, dtype=np.float64)
+        if obs.shape != (self.n_steps, self.n_gauges):
+            raise ValueError(f"observations must be ({self.n_steps}, {self.n_gauges})")
+        self._rc(self._lib.rkb_adjoint_set_obs(self._a, obs.ctypes.data_as(_DP)), "set_observations")
+
+    @property
+    def dt(self):
+        out = np.zeros(self.n_steps)
+        self._rc(self._lib.rkb_adjoint_get_dt(self._a, out.ctypes.data_as(_DP)), "dt")
+        return out
+
+    def set_dt(self, dts):
+        dts = np.ascontiguousarray(dts, dtype=np.float64)
+        if dts.shape != (self.n_steps,):
+            raise ValueError(f"dt must have {self.n_steps} entries")
+        self._rc(self._lib.rkb_adjoint_set_dt(self._a, dts.ctypes.data_as(_DP)), "set_dt")
+
+    def _forward(self, b, n, record):
+        b, nf, ns = self._fields(b, n)
+        J = ctypes.c_double()
+        eta = np.zeros((self.n_steps, self.n_gauges))
+        self._rc(self._lib.rkb_adjoint_forward(
+            self._a, b.ctypes.data_as(_DP), nf.ctypes.data_as(_DP) if nf is not None else None, ns,
+            int(record), ctypes.byref(J), eta.ctypes.data_as(_DP)), "forward")
+        return J.value, eta
+
+    def record_dt(self, b, n=None):
+        """Forward run with CFL steps; stores the dt sequence; returns (J, eta_gauges)."""
+        return self._forward(b, n, True)
+
+    def forward(self, b, n=None):
+        """(J, eta_gauges (n_steps, n_gauges)) on the stored dt sequence."""
+        return self._forward(b, n, False)
+
+    def gradient(self, b, n=None):
+        """(J, dJ/db, dJ/dn), the gradients as (nx, ny) arrays."""
+        b, nf, ns = self._fields(b, n)
+        J = ctypes.c_double()
+        gb = np.zeros((self.nx, self.ny), order="F")
+        gn = np.zeros((self.nx, self.ny), order="F")
+        self._rc(self._lib.rkb_adjoint_gradient(
+            self._a, b.ctypes.data_as(_DP), nf.ctypes.data_as(_DP) if nf is not None else None, ns,
+            ctypes.byref(J), gb.ctypes.data_as(_DP), gn.ctypes.data_as(_DP)), "gradient")
+        return J.value, gb, gn
+
+    @property
+    def checkpoint_interval(self):
+        return int(self._lib.rkb_adjoint_checkpoint_interval(self._a))
+
+    def close(self):
+        if getattr(self, "_a", None):
+            self._lib.rkb_adjoint_destroy(ctypes.byref(self._a))
+            self._a = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _function():
+    import torch
+
+    class _Misfit(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, b, n, problem):
+            bn = b.detach().to("cpu", torch.float64).numpy()
+            nn = n.detach().to("cpu", torch.float64).numpy()
+            if ctx.needs_input_grad[0] or ctx.needs_input_grad[1]:
+                J, gb, gn = problem.gradient(bn, nn)
+                ctx.save_for_backward(torch.from_numpy(np.ascontiguousarray(gb)).to(b.device),
+                                      torch.from_numpy(np.ascontiguousarray(gn)).to(n.device))
+            else:
+                J, _ = problem.forward(bn, nn)
+            return torch.tensor(J, dtype=torch.float64, device=b.device)
+
+        @staticmethod
+        def backward(ctx, gJ):
+            gb, gn = ctx.saved_tensors
+            return gJ * gb, gJ * gn, None
+
+    return _Misfit
+
+
+_MISFIT = None
+
+
+def misfit(problem: GaugeMisfit, b, n):
+    """J(b, n) as a differentiable float64 tensor (b, n: (nx, ny) tensors)."""
+    global _MISFIT
+    if _MISFIT is None:
+        _MISFIT = _function()
+    return _MISFIT.apply(b, n, problem)
+
+
+__all__ = ["GaugeMisfit", "misfit"]

@@ -101,14 +101,14 @@ __host__ __device__ __forceinline__ double dmin(double a, double b) { return a <
 __host__ __device__ __forceinline__ double pos(double x) { return x > 0.0 ? x : 0.0; }
 
 // minmod, rki_kernel_flux.F90:380-393
-__device__ __forceinline__ double minmod(double a, double b) {
+__host__ __device__ __forceinline__ double minmod(double a, double b) {
   if (a * b <= 0.0) return 0.0;
   return fabs(a) < fabs(b) ? a : b;
 }
 
 // Clamp + KP07 desingularisation + Froude backstop
 // (rki_kernel_fused.F90:93-119 and :441-463).
-__device__ __forceinline__ void protect(double& h, double& u, double& v) {
+__host__ __device__ __forceinline__ void protect(double& h, double& u, double& v) {
   if (h < 0.0) {
     h = 0.0; u = 0.0; v = 0.0;
   } else if (h < kDry) {
@@ -135,7 +135,7 @@ __device__ __forceinline__ void protect(double& h, double& u, double& v) {
 
 // Wave speed terms of compute_timestep (rki_kernel_timestep.F90:52-66):
 // returns (|u|_KP07 + sqrt(g h)) along x and y, before the division by dx/dy.
-__device__ __forceinline__ void wave_speed(double h, double hu, double hv, double& sx, double& sy) {
+__host__ __device__ __forceinline__ void wave_speed(double h, double hu, double hv, double& sx, double& sy) {
   sx = 0.0;
   sy = 0.0;
   if (h > kDry) {

@@ -20,7 +20,7 @@ struct FaceOut {
   double wbR, hL2, pL2;
 };
 
-__device__ __forceinline__ void velocity(double h, double qx, double qy, double& u, double& v) {
+__host__ __device__ __forceinline__ void velocity(double h, double qx, double qy, double& u, double& v) {
   if (h > kDry) {
     u = qx / h;
     v = qy / h;
@@ -33,7 +33,7 @@ __device__ __forceinline__ void velocity(double h, double qx, double qy, double&
 // HLL / HLLC in direction DIR (0: x, normal momentum qx; 1: y, normal qy).
 // hll_flux_x/y rki_kernel_flux.F90:410-582, hllc_flux_x/y :584-783.
 template <int DIR, bool HLLC>
-__device__ __forceinline__ void riemann(double hl, double qxl, double qyl, double hr, double qxr,
+__host__ __device__ __forceinline__ void riemann(double hl, double qxl, double qyl, double hr, double qxr,
                                         double qyr, double& fh, double& fqx, double& fqy) {
   double ul, vl, ur, vr;
   velocity(hl, qxl, qyl, ul, vl);
@@ -112,7 +112,7 @@ __device__ __forceinline__ void riemann(double hl, double qxl, double qyl, doubl
 // One face from the reconstructed side values (eta, hu, hv) and the beds.
 // The Audusse step follows rki_kernel_flux.F90:186-224.
 template <int DIR, bool HLLC>
-__device__ __forceinline__ void face_flux(double eL, double qxL, double qyL, double bL, double eR,
+__host__ __device__ __forceinline__ void face_flux(double eL, double qxL, double qyL, double bL, double eR,
                                           double qxR, double qyR, double bR, FaceOut& o) {
   const double hL = pos(eL - bL);
   const double hR = pos(eR - bR);
@@ -130,7 +130,7 @@ __device__ __forceinline__ void face_flux(double eL, double qxL, double qyL, dou
 
 // Limited slope of one cell along one direction (rki_kernel_flux.F90:159-181):
 // zero near wet/dry fronts, else minmod of the one-sided differences.
-__device__ __forceinline__ void cell_slope(double hm, double hc, double hp, double em, double ec,
+__host__ __device__ __forceinline__ void cell_slope(double hm, double hc, double hp, double em, double ec,
                                            double ep, double um, double uc, double up, double vm,
                                            double vc, double vp, double& se, double& su,
                                            double& sv) {

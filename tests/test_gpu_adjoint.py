@@ -1,0 +1,134 @@
+"""Adjoint of the FP64 step (GPU): gauge-misfit gradients w.r.t. bed and Manning n.
+
+* the adjoint's forward is the production step: with a uniform n field and
+  the recorded CFL dt sequence its gauge surfaces are bit-identical to
+  Rakali's FP64 step;
+* dJ/db and dJ/dn equal torch.autograd through the plain FP64 torch
+  transcription (tests/torch_step.py, itself pinned to the oracle) to 1e-8
+  relative;
+* directional derivatives match central finite differences on random smooth
+  directions to 1e-6 relative.  J is piecewise smooth, and at a lake at rest
+  it is not differentiable with respect to b at all: the minmod limiter sits
+  at (0, 0), where a bed perturbation e d gives slopes e minmod(d_a, d_b),
+  not linear in d, so no gradient (this adjoint's or autograd's) matches
+  finite differences there.  The finite-difference case therefore starts
+  from a surface with nonzero gradients everywhere;
+* the torch.autograd.Function front end back-propagates the same gradient.
+"""
+import numpy as np
+import pytest
+
+from rakali_b200.adjoint import GaugeMisfit, misfit
+from tests.helpers import gaussian_bed, hump_depth
+
+pytestmark = pytest.mark.gpu
+
+
+def _problem(nx, ny, steps, n_gauges, seed, hllc=False, dx=10.0, generic=False):
+    rng = np.random.default_rng(seed)
+    b = gaussian_bed(nx, ny, dx, dx, 8, seed=seed, base=-6.0, amp=(-2.0, 3.0), width=(30.0, 90.0))
+    h = hump_depth(b, dx, dx, amp=0.3, width=60.0)
+    if generic:  # a surface with nonzero gradients everywhere (no resting water)
+        x = (np.arange(nx) + 0.5) * dx
+        y = (np.arange(ny) + 0.5) * dx
+        X, Y = np.meshgrid(x, y, indexing="ij")
+        surf = 0.02 * np.sin(X / 37.0 + 0.3) * np.cos(Y / 23.0 + 0.7) + 0.01 * np.sin((X + 2 * Y) / 51.0)
+        h = np.asfortranarray(np.where(h > 0, np.maximum(h + surf, 0.0), 0.0))
+    cells = rng.choice(nx * ny, size=n_gauges, replace=False)
+    gauges = [(int(c % nx), int(c // nx)) for c in cells]
+    p = GaugeMisfit(nx, ny, dx, dx, h, gauges, steps, use_hllc=hllc)
+    n = np.full((nx, ny), 0.025)
+    p.record_dt(b, n)
+    # observations: the forward run of a perturbed bed
+    noise = 0.2 * np.asfortranarray(gaussian_bed(nx, ny, dx, dx, 5, seed=seed + 1, base=0.0,
+                                                 amp=(-1.0, 1.0), width=(40.0, 120.0)))
+    _, obs = p.forward(b + noise, n)
+    p.set_observations(obs)
+    return p, b, h, n, gauges, obs
+
+
+def test_forward_matches_production_step():
+    from rakali_b200 import Rakali
+    nx, ny, dx, steps = 40, 32, 10.0, 25
+    b = gaussian_bed(nx, ny, dx, dx, 8, seed=2, base=-6.0, amp=(-2.0, 3.0), width=(30.0, 90.0))
+    h = hump_depth(b, dx, dx, amp=0.3, width=60.0)
+    gauges = [(3, 4), (20, 16), (39, 31), (10, 25)]
+    p = GaugeMisfit(nx, ny, dx, dx, h, gauges, steps)
+    _, eta = p.record_dt(b, np.full((nx, ny), 0.025))
+    sim = Rakali(defer_init=True, nx=nx, ny=ny, dx=dx, dy=dx, nghost=2, t_end=1e6, cfl=0.45,
+                 manning_n=0.025)
+    sim.set_bathymetry(b)
+    sim.set_initial_h(h)
+    sim.finalize()
+    with sim:
+        for k in range(steps):
+            sim.step(1)
+            assert sim.dt == p.dt[k]
+            e = sim.h_phys + sim.b_phys
+            for m, (i, j) in enumerate(gauges):
+                assert e[i, j] == eta[k, m]
+    p.close()
+
+
+def test_uniform_field_equals_scalar():
+    p, b, h, n, _, _ = _problem(24, 20, 10, 5, seed=3)
+    J1, _ = p.forward(b, n)
+    J2, _ = p.forward(b, 0.025)
+    assert J1 == J2
+    p.close()
+
+
+@pytest.mark.parametrize("hllc", [False, True])
+def test_gradient_matches_torch_autograd(hllc):
+    import torch
+
+    from tests import torch_step as ts
+    nx, ny, steps = 28, 22, 14
+    p, b, h, n, gauges, obs = _problem(nx, ny, steps, 6, seed=5, hllc=hllc)
+    J, gb, gn = p.gradient(b, n)
+    obs = torch.from_numpy(obs)
+    bt = torch.tensor(b, dtype=torch.float64, requires_grad=True)
+    nt = torch.tensor(n, dtype=torch.float64, requires_grad=True)
+    z = torch.zeros((nx, ny), dtype=torch.float64)
+    Jt = ts.misfit(bt, nt, torch.from_numpy(h), z, z, gauges, obs, list(p.dt), 2, 10.0, 10.0,
+                   hllc=hllc)
+    Jt.backward()
+    assert abs(float(Jt) - J) <= 1e-10 * abs(J)
+    for got, ref in ((gb, bt.grad.numpy()), (gn, nt.grad.numpy())):
+        scale = float(np.abs(ref).max())
+        assert scale > 0.0
+        assert float(np.abs(got - ref).max()) <= 1e-8 * scale
+    p.close()
+
+
+def test_gradient_matches_central_differences():
+    nx, ny, steps = 40, 32, 29  # 29 steps: checkpoint segments of 6, the last one short
+    p, b, h, n, _, _ = _problem(nx, ny, steps, 10, seed=7, generic=True)
+    assert p.checkpoint_interval == 6
+    J, gb, gn = p.gradient(b, n)
+    rng = np.random.default_rng(11)
+    for k in range(5):
+        db = np.asfortranarray(gaussian_bed(nx, ny, 10.0, 10.0, 3, seed=100 + k, base=0.0,
+                                            amp=(-1.0, 1.0), width=(50.0, 150.0)))
+        dn = np.asfortranarray(0.005 * rng.standard_normal((nx, ny)))
+        eps = 1e-6
+        Jp, _ = p.forward(b + eps * db, n + eps * dn)
+        Jm, _ = p.forward(b - eps * db, n - eps * dn)
+        fd = (Jp - Jm) / (2 * eps)
+        ad = float(np.sum(gb * db) + np.sum(gn * dn))
+        assert abs(fd - ad) <= 1e-6 * max(abs(fd), 1e-12), (k, fd, ad)
+    p.close()
+
+
+def test_autograd_function_backward():
+    import torch
+    p, b, h, n, _, _ = _problem(24, 20, 12, 5, seed=9)
+    J, gb, gn = p.gradient(b, n)
+    bt = torch.tensor(b, dtype=torch.float64, requires_grad=True)
+    nt = torch.tensor(n, dtype=torch.float64, requires_grad=True)
+    Jt = misfit(p, bt, nt)
+    assert float(Jt) == J
+    (3.0 * Jt).backward()
+    assert np.array_equal(bt.grad.numpy(), 3.0 * gb)
+    assert np.array_equal(nt.grad.numpy(), 3.0 * gn)
+    p.close()

@@ -1,0 +1,207 @@
+"""Plain FP64 torch transcription of the structured step (test reference).
+
+The same SSP-RK2 step as the CUDA adjoint's forward (wall boundaries,
+hydrostatic/minmod reconstruction, HLL/HLLC, clamp/KP07/Froude backstop,
+Manning friction with a per-cell n field; rki_kernel_flux.F90,
+rki_kernel_fused.F90, rki_boundary.F90) written with whole-array torch
+operations, so torch.autograd can differentiate a gauge misfit through it.
+Branches are torch.where selections with the same conditions; every
+division and square root is guarded so the untaken branch produces no NaN
+gradient; ties of min/max and kinks of max(0, x) take the same side as the
+CUDA adjoint.  Used at small sizes only.
+"""
+from __future__ import annotations
+
+import torch
+
+G = 9.80665
+HALF_G = 0.5 * G
+DRY = 1.0e-6
+THIN = 1.0e-3
+EPS4 = 5.062499999999998e-16
+SQRT2 = 1.4142135623730951
+FROUDE = 50.0
+
+
+def pos(x):
+    return torch.where(x > 0.0, x, torch.zeros_like(x))
+
+
+def sdiv(a, b, mask):
+    return torch.where(mask, a / torch.where(mask, b, torch.ones_like(b)), torch.zeros_like(a))
+
+
+def ssqrt(x):
+    m = x > 0.0
+    return torch.where(m, torch.sqrt(torch.where(m, x, torch.ones_like(x))), torch.zeros_like(x))
+
+
+def minmod(a, b):
+    return torch.where(a * b <= 0.0, torch.zeros_like(a), torch.where(a.abs() < b.abs(), a, b))
+
+
+def velocity(h, qx, qy):
+    m = h > DRY
+    return sdiv(qx, h, m), sdiv(qy, h, m)
+
+
+def riemann(d, hllc, hl, qxl, qyl, hr, qxr, qyr):
+    ul, vl = velocity(hl, qxl, qyl)
+    ur, vr = velocity(hr, qxr, qyr)
+    al, ar = ssqrt(G * pos(hl)), ssqrt(G * pos(hr))
+    nl, nr = (ul, ur) if d == 0 else (vl, vr)
+    dryr, dryl = hr <= DRY, hl <= DRY
+    a1, a2, b1, b2 = nl - al, nr - ar, nl + al, nr + ar
+    sl = torch.where(dryr, nl - al, torch.where(dryl, nr - 2.0 * ar, torch.where(a1 < a2, a1, a2)))
+    sr = torch.where(dryr, nl + 2.0 * al, torch.where(dryl, nr + ar, torch.where(b1 > b2, b1, b2)))
+    if d == 0:
+        L = (qxl, qxl * ul + HALF_G * hl * hl, qxl * vl)
+        R = (qxr, qxr * ur + HALF_G * hr * hr, qxr * vr)
+    else:
+        L = (qyl, qxl * vl, qyl * vl + HALF_G * hl * hl)
+        R = (qyr, qxr * vr, qyr * vr + HALF_G * hr * hr)
+    UL, UR = (hl, qxl, qyl), (hr, qxr, qyr)
+    sub = (sl < 0.0) & (sr > 0.0)
+    inv = sdiv(torch.ones_like(sl), sr - sl, sub)
+    hll = [(sr * L[k] - sl * R[k] + sl * sr * (UR[k] - UL[k])) * inv for k in range(3)]
+    if hllc:
+        t = 2 if d == 0 else 1
+        un_l, un_r = (ul, ur) if d == 0 else (vl, vr)
+        ut_l, ut_r = (vl, vr) if d == 0 else (ul, ur)
+        den = hr * (un_r - sr) - hl * (un_l - sl)
+        big = den.abs() > DRY
+        ss = torch.where(big, sdiv(sl * hr * (un_r - sr) - sr * hl * (un_l - sl), den, big),
+                         0.5 * (un_l + un_r))
+        hll[t] = torch.where(ss >= 0.0, hll[0] * ut_l, hll[0] * ut_r)
+    out = []
+    for k in range(3):
+        out.append(torch.where(sl >= 0.0, L[k], torch.where(sr <= 0.0, R[k], hll[k])))
+    return out
+
+
+def face_flux(d, hllc, eL, qxL, qyL, bL, eR, qxR, qyR, bR):
+    hL, hR = pos(eL - bL), pos(eR - bR)
+    bmax = torch.where(bL > bR, bL, bR)
+    hyl, hyr = pos(hL + bL - bmax), pos(hR + bR - bmax)
+    ul, vl = velocity(hL, qxL, qyL)
+    ur, vr = velocity(hR, qxR, qyR)
+    fh, fqx, fqy = riemann(d, hllc, hyl, hyl * ul, hyl * vl, hyr, hyr * ur, hyr * vr)
+    return fh, fqx, fqy, hyr * hyr - hR * hR, hyl * hyl, hL * hL
+
+
+def protect(h, u, v):
+    neg, wet = h < 0.0, h >= DRY
+    h2 = h * h
+    h4 = h2 * h2
+    kp = wet & (h4 < EPS4)
+    r = torch.sqrt(h4 + EPS4)
+    u1 = torch.where(kp, h * (SQRT2 * h * u / r), u)
+    v1 = torch.where(kp, h * (SQRT2 * h * v / r), v)
+    sp2 = sdiv(u1 * u1 + v1 * v1, h * h, wet)
+    fr2 = FROUDE * FROUDE * G * h
+    fro = wet & (sp2 > fr2)
+    sc = ssqrt(sdiv(fr2, sp2, fro))
+    u2 = torch.where(fro, u1 * sc, u1)
+    v2 = torch.where(fro, v1 * sc, v1)
+    z = torch.zeros_like(h)
+    return (torch.where(neg, z, h), torch.where(wet, u2, z), torch.where(wet, v2, z))
+
+
+def friction(h, u, v, n, dt):
+    m = (h > DRY) & (n > 0.0)
+    uu, vv = sdiv(u, h, m), sdiv(v, h, m)
+    speed = ssqrt(uu * uu + vv * vv)
+    hs = torch.where(m, h, torch.ones_like(h))
+    cf = G * n * n / hs ** (1.0 / 3.0)
+    den = 1.0 + dt * cf * speed / hs
+    return torch.where(m, u / den, u), torch.where(m, v / den, v)
+
+
+def walls(h, hu, hv, b, ng):
+    h, hu, hv, b = h.clone(), hu.clone(), hv.clone(), b.clone()
+    nxt, nyt = h.shape
+    for k in range(1, ng + 1):  # west / east
+        for ig, im in ((ng - k, ng + k - 1), (nxt - ng + k - 1, nxt - ng - k)):
+            b[ig, :] = b[im, :]
+            h[ig, :] = pos(h[im, :] + b[im, :] - b[im, :])
+            hu[ig, :] = -hu[im, :]
+            hv[ig, :] = hv[im, :]
+    for k in range(1, ng + 1):  # south / north
+        for jg, jm in ((ng - k, ng + k - 1), (nyt - ng + k - 1, nyt - ng - k)):
+            b[:, jg] = b[:, jm]
+            h[:, jg] = pos(h[:, jm] + b[:, jm] - b[:, jm])
+            hv[:, jg] = -hv[:, jm]
+            hu[:, jg] = hu[:, jm]
+    return h, hu, hv, b
+
+
+def _slopes(h, e, hu, hv, dim, ng):
+    """Limited slopes of cells ng-1 .. n-ng along `dim` (rki_kernel_flux.F90:159-181)."""
+    n = h.shape[dim]
+    m = lambda x: x.narrow(dim, ng - 2, n - 2 * ng + 2)
+    c = lambda x: x.narrow(dim, ng - 1, n - 2 * ng + 2)
+    p = lambda x: x.narrow(dim, ng, n - 2 * ng + 2)
+    gate = ~((c(h) < THIN) | (m(h) < DRY) | (p(h) < DRY))
+    z = torch.zeros_like(c(e))
+    return tuple(torch.where(gate, minmod(c(x) - m(x), p(x) - c(x)), z) for x in (e, hu, hv))
+
+
+def stage(h, hu, hv, b, n, dt, ng, dx, dy, hllc, base=None):
+    """One stage on states with ghosts; returns interior (h, hu, hv)."""
+    nxt, nyt = h.shape
+    e = h + b
+    inner_y = slice(ng, nyt - ng)
+    inner_x = slice(ng, nxt - ng)
+    # x direction: slopes of columns ng-1 .. nxt-ng over the interior rows
+    sx = _slopes(h[:, inner_y], e[:, inner_y], hu[:, inner_y], hv[:, inner_y], 0, ng)
+    c = lambda x: x[ng - 1:nxt - ng + 1, inner_y]
+    L = lambda x, s: (c(x) + 0.5 * s)[:-1]
+    R = lambda x, s: (c(x) - 0.5 * s)[1:]
+    fx = face_flux(0, hllc, L(e, sx[0]), L(hu, sx[1]), L(hv, sx[2]), c(b)[:-1],
+                   R(e, sx[0]), R(hu, sx[1]), R(hv, sx[2]), c(b)[1:])
+    sy = _slopes(h[inner_x, :], e[inner_x, :], hu[inner_x, :], hv[inner_x, :], 1, ng)
+    cy = lambda x: x[inner_x, ng - 1:nyt - ng + 1]
+    B = lambda x, s: (cy(x) + 0.5 * s)[:, :-1]
+    T = lambda x, s: (cy(x) - 0.5 * s)[:, 1:]
+    fy = face_flux(1, hllc, B(e, sy[0]), B(hu, sy[1]), B(hv, sy[2]), cy(b)[:, :-1],
+                   T(e, sy[0]), T(hu, sy[1]), T(hv, sy[2]), cy(b)[:, 1:])
+    l_, r_ = slice(0, -1), slice(1, None)
+    o_fh = -((fx[0][r_] - fx[0][l_]) / dx) - (fy[0][:, r_] - fy[0][:, l_]) / dy
+    o_fhu = (-((fx[1][r_] - fx[1][l_]) / dx) - (fy[1][:, r_] - fy[1][:, l_]) / dy
+             - HALF_G * (fx[3][l_] - fx[4][r_] + fx[5][r_]) / dx)
+    o_fhv = (-((fx[2][r_] - fx[2][l_]) / dx) - (fy[2][:, r_] - fy[2][:, l_]) / dy
+             - HALF_G * (fy[3][:, l_] - fy[4][:, r_] + fy[5][:, r_]) / dy)
+    a = h[inner_x, inner_y] + dt * o_fh
+    u = hu[inner_x, inner_y] + dt * o_fhu
+    v = hv[inner_x, inner_y] + dt * o_fhv
+    a, u, v = protect(a, u, v)
+    u, v = friction(a, u, v, n, dt)
+    if base is not None:
+        a, u, v = protect(0.5 * (base[0] + a), 0.5 * (base[1] + u), 0.5 * (base[2] + v))
+    return a, u, v
+
+
+def embed(inner, ng):
+    out = torch.zeros(inner.shape[0] + 2 * ng, inner.shape[1] + 2 * ng, dtype=inner.dtype)
+    out[ng:-ng, ng:-ng] = inner
+    return out
+
+
+def misfit(b, n, h0, hu0, hv0, gauges, obs, dts, ng, dx, dy, hllc=False):
+    """J = sum over steps and gauges of (h + b - obs)^2; b, n, h0 interior tensors."""
+    bf = embed(b, ng)
+    h, hu, hv = embed(h0, ng), embed(hu0, ng), embed(hv0, ng)
+    gi = torch.as_tensor([g[0] for g in gauges])
+    gj = torch.as_tensor([g[1] for g in gauges])
+    J = torch.zeros((), dtype=torch.float64)
+    for k, dt in enumerate(dts):
+        h, hu, hv, bf = walls(h, hu, hv, bf, ng)
+        base = (h[ng:-ng, ng:-ng], hu[ng:-ng, ng:-ng], hv[ng:-ng, ng:-ng])
+        a, u, v = stage(h, hu, hv, bf, n, dt, ng, dx, dy, hllc)
+        hs, hus, hvs = embed(a, ng), embed(u, ng), embed(v, ng)
+        hs, hus, hvs, bf = walls(hs, hus, hvs, bf, ng)
+        a, u, v = stage(hs, hus, hvs, bf, n, dt, ng, dx, dy, hllc, base=base)
+        h, hu, hv = embed(a, ng), embed(u, ng), embed(v, ng)
+        eta = a[gi, gj] + b[gi, gj]
+        J = J + ((eta - obs[k]) ** 2).sum()
+    return J
