@@ -195,6 +195,8 @@ int rkb_adjoint_forward(void *adj, const double *b, const double *n_field, doubl
 int rkb_adjoint_gradient(void *adj, const double *b, const double *n_field, double n_scalar,
                          double *J, double *grad_b, double *grad_n);
 int rkb_adjoint_checkpoint_interval(void *adj);
+/* Device milliseconds of the last forward / gradient call (CUDA events). */
+double rkb_adjoint_last_ms(void *adj);
 /* Host builds of the face flux / cell update and their adjoints (for
  * finite-difference checks without a GPU). */
 void rkb_test_face_flux(int dir, int hllc, const double *in8, double *out6);

@@ -116,6 +116,11 @@ class GaugeMisfit:
     def checkpoint_interval(self):
         return int(self._lib.rkb_adjoint_checkpoint_interval(self._a))
 
+    @property
+    def last_ms(self) -> float:
+        """Device milliseconds of the last forward / gradient call."""
+        return float(self._lib.rkb_adjoint_last_ms(self._a))
+
     def close(self):
         if getattr(self, "_a", None):
             self._lib.rkb_adjoint_destroy(ctypes.byref(self._a))

@@ -471,6 +471,8 @@ __global__ void k_add(Grid g, FieldSet a, FieldSet b) {  // interior a += b
 class Adjoint {
  public:
   ~Adjoint() {
+    for (auto& e : ev_)
+      if (e) cudaEventDestroy(e);
     if (mem_) cudaFree(mem_);
     if (obs_d_) cudaFree(obs_d_);
     if (stream_) cudaStreamDestroy(stream_);
@@ -593,6 +595,7 @@ class Adjoint {
               double* eta_out) {
     if (!record && !have_dt_) return -2;
     if (upload_params(b, n, n_scalar) != 0) return -1;
+    if (mark(0) != 0) return -1;
     if (copy(U_, ck_[0]) != 0) return -1;
     std::vector<double> r((size_t)nsteps_ * ngauge_);
     for (int k = 0; k < nsteps_; ++k) {
@@ -608,6 +611,7 @@ class Adjoint {
       }
     }
     if (record) have_dt_ = true;
+    if (mark(1) != 0) return -1;
     ADJ_TRY(cudaMemcpyAsync(r.data(), r_, r.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_));
     ADJ_TRY(cudaStreamSynchronize(stream_));
     double acc = 0.0;
@@ -626,6 +630,7 @@ class Adjoint {
     if (!have_dt_) return -2;
     if (upload_params(b, n, n_scalar) != 0) return -1;
     const size_t f = (size_t)g_.pitch * g_.nyt;
+    if (mark(0) != 0) return -1;
     // forward with checkpoints
     if (copy(U_, ck_[0]) != 0) return -1;
     for (int k = 0; k < nsteps_; ++k) {
@@ -662,6 +667,7 @@ class Adjoint {
     }
     // bed ghosts mirror interior cells: fold their adjoints in (S/N then W/E)
     walls_adj(gV_, true);
+    if (mark(1) != 0) return -1;
     ADJ_TRY(cudaStreamSynchronize(stream_));
     double acc = 0.0;
     for (double x : r) acc += x * x;
@@ -680,8 +686,23 @@ class Adjoint {
   }
 
   int checkpoint_interval() const { return K_; }
+  // Device milliseconds of the last forward / gradient run (CUDA events on
+  // the adjoint's stream, from the initial state to the last kernel).
+  double last_ms() {
+    float f = 0.0f;
+    if (!ev_[0] || cudaEventSynchronize(ev_[1]) != cudaSuccess ||
+        cudaEventElapsedTime(&f, ev_[0], ev_[1]) != cudaSuccess)
+      return -1.0;
+    return f;
+  }
 
  private:
+  int mark(int k) {
+    if (!ev_[k] && cudaEventCreate(&ev_[k]) != cudaSuccess) return -1;
+    return cudaEventRecord(ev_[k], stream_) == cudaSuccess ? 0 : -1;
+  }
+  cudaEvent_t ev_[2] = {nullptr, nullptr};
+
   dim3 blocks(int x0, int x1, int y0, int y1) const {  // cover [x0, x1] x [y0, y1]
     return dim3((unsigned)((x1 - x0 + kBX) / kBX), (unsigned)((y1 - y0 + kBY) / kBY));
   }
@@ -894,6 +915,10 @@ int rkb_adjoint_gradient(void* adj, const double* b, const double* n_field, doub
 
 int rkb_adjoint_checkpoint_interval(void* adj) {
   return adj ? static_cast<rkb::Adjoint*>(adj)->checkpoint_interval() : -2;
+}
+
+double rkb_adjoint_last_ms(void* adj) {
+  return adj ? static_cast<rkb::Adjoint*>(adj)->last_ms() : -1.0;
 }
 
 // Host builds of the face and cell derivatives, for finite-difference checks.

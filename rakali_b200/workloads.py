@@ -97,3 +97,31 @@ def build_member(m, precision=64):
     if precision != 64:
         s.set_precision(precision)
     return s
+
+
+def adjoint_problem(n=1024, steps=500, n_gauges=64, dx=10.0, seed=31):
+    """The gradient workload: (nx = ny = n), bed of 16 seeded Gaussians on a
+    -10 m base, a 0.5 m / 200 m hump at the centre on top of a 2-3 cm smooth
+    surface undulation (so the water moves everywhere: a lake exactly at rest
+    makes the limiter non-differentiable), Manning n = 0.025 as a field, 64
+    seeded distinct gauge cells, and the smooth 0.2 m-amplitude bed noise
+    whose forward run provides the observations.
+
+    Returns dict(b, h, n, gauges, noise, dx, steps).
+    """
+    rng = np.random.default_rng(seed)
+    b = gaussian_bed(n, n, dx, dx, 16, seed)
+    x = (np.arange(n) + 0.5) * dx
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    L = n * dx
+    surf = (0.02 * np.sin(2 * np.pi * X / (0.37 * L) + 0.3) * np.cos(2 * np.pi * Y / (0.23 * L) + 0.7)
+            + 0.01 * np.sin(2 * np.pi * (X + 2 * Y) / (0.51 * L)))
+    h = hump_depth(b, dx, dx, amp=0.5, width=200.0)
+    h = np.asfortranarray(np.where(h > 0, np.maximum(h + surf, 0.0), 0.0))
+    cells = rng.choice(n * n, size=n_gauges, replace=False)
+    gauges = [(int(c % n), int(c // n)) for c in cells]
+    noise = gaussian_bed(n, n, dx, dx, 24, seed + 1, base=0.0, amp=(-1.0, 1.0),
+                         width=(100.0, 800.0))
+    noise = np.asfortranarray(0.2 * noise / np.abs(noise).max())
+    return dict(b=b, h=h, n=np.full((n, n), 0.025, order="F"), gauges=gauges, noise=noise,
+                dx=dx, steps=steps)

@@ -132,3 +132,23 @@ def test_autograd_function_backward():
     assert np.array_equal(bt.grad.numpy(), 3.0 * gb)
     assert np.array_equal(nt.grad.numpy(), 3.0 * gn)
     p.close()
+
+
+def test_gradient_matches_torch_autograd_128():
+    """The north-star size for the autograd comparison: 128 x 128, 30 steps, 16 gauges."""
+    import torch
+
+    from tests import torch_step as ts
+    nx = ny = 128
+    p, b, h, n, gauges, obs = _problem(nx, ny, 30, 16, seed=13)
+    J, gb, gn = p.gradient(b, n)
+    bt = torch.tensor(b, dtype=torch.float64, requires_grad=True)
+    nt = torch.tensor(n, dtype=torch.float64, requires_grad=True)
+    z = torch.zeros((nx, ny), dtype=torch.float64)
+    Jt = ts.misfit(bt, nt, torch.from_numpy(h), z, z, gauges, torch.from_numpy(obs), list(p.dt),
+                   2, 10.0, 10.0)
+    Jt.backward()
+    assert abs(float(Jt) - J) <= 1e-10 * abs(J)
+    for got, ref in ((gb, bt.grad.numpy()), (gn, nt.grad.numpy())):
+        assert float(np.abs(got - ref).max()) <= 1e-8 * float(np.abs(ref).max())
+    p.close()
