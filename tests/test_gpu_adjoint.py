@@ -135,12 +135,17 @@ def test_autograd_function_backward():
 
 
 def test_gradient_matches_torch_autograd_128():
-    """The north-star size for the autograd comparison: 128 x 128, 30 steps, 16 gauges."""
+    """The north-star size for the autograd comparison: 128 x 128, 30 steps, 16 gauges.
+
+    The transcription agrees with the CUDA forward to ~1e-12, not bit for bit;
+    on resting water the limiter and wave-speed branches are decided by
+    rounding-level differences, so the two would differentiate different
+    pieces there.  The case starts from a moving surface."""
     import torch
 
     from tests import torch_step as ts
     nx = ny = 128
-    p, b, h, n, gauges, obs = _problem(nx, ny, 30, 16, seed=13)
+    p, b, h, n, gauges, obs = _problem(nx, ny, 30, 16, seed=13, generic=True)
     J, gb, gn = p.gradient(b, n)
     bt = torch.tensor(b, dtype=torch.float64, requires_grad=True)
     nt = torch.tensor(n, dtype=torch.float64, requires_grad=True)
