@@ -426,7 +426,8 @@ int rkb_profile_steps(void* handle, int n, double* out5) {
   if (!s) return kBadHandle;
   if (!s->is_finalised) return -1;
   if (!out5) return -2;
-  return s->profile_steps(n, out5);
+  const int rc = s->profile_steps(n, out5);
+  return rc == 0 ? 0 : fail(rc, s->error_text());
 }
 
 int rkb_get_tile(void* handle) {
@@ -523,7 +524,8 @@ int rkb_set_precision(void* handle, int bits) {
   rkb::Sim* s = sim_of(handle);
   if (!s) return kBadHandle;
   if (bits != 32 && bits != 64) return fail(-2, "precision must be 32 or 64");
-  return s->set_precision(bits);
+  const int rc = s->set_precision(bits);
+  return rc == 0 ? 0 : fail(rc, s->error_text());
 }
 
 int rkb_get_precision(void* handle) {

@@ -61,6 +61,7 @@ int Batch::create(const std::vector<Sim*>& sims, int precision, std::string& err
     if (!s->is_finalised) { err = "every member must be finalised"; return -1; }
     if (s->batch) { err = "a simulation can belong to one batch only"; return -2; }
     if (s->phys.use_hllc != hllc_) { err = "members must share the Riemann solver (HLL or HLLC)"; return -2; }
+    if (s->phys.scheme != 2) { err = "batches run the SSP-RK2 scheme only"; return -2; }
     const int need = s->g.ng > 2 ? s->g.ng : 2;
     if (s->g.nx_phys() < need || s->g.ny_phys() < need) {
       err = "members must be at least max(nghost, 2) cells wide";

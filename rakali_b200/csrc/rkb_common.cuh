@@ -64,7 +64,14 @@ struct Physics {
   int cfl_interval;
   int forcing_active;
   int use_hllc;
+  // time_scheme: 2 = SSP-RK2 (the fused two-stage path); 1 euler, 3 rk3,
+  // 4 rk43 run the generic Shu-Osher stages (rki_timestepper.F90:60-100):
+  // stage k updates with beta[k] dt at time t + c[k] dt, then (alpha[k] != 0)
+  // blends alpha[k] U^n + (1 - alpha[k]) U.
+  int scheme;
+  int n_stages;
   int pad_;
+  double alpha[4], beta[4], c[4];
 };
 
 // Device-resident clock and reductions of one simulation.  Fields marked

@@ -51,6 +51,8 @@ struct StepArgs {
   double* eta_old[4];
   int tile;
   int hllc;
+  int scheme;    // time scheme: 2 SSP-RK2 (fused stages), 1 euler, 3 rk3, 4 rk43
+  int n_stages;  // stages of the generic schemes
 };
 
 // Doubles of per-block partial storage the step kernels need.

@@ -11,6 +11,45 @@ namespace {
 
 size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
 
+// Shu-Osher coefficients of the time schemes (rki_timestepper.F90:60-100):
+// stage k steps beta_k dt from X_k at time t + c_k dt, then mixes alpha_k U^n
+// + (1 - alpha_k) X_k+1 when alpha_k != 0.  ssp_coeff scales the CFL step.
+void fill_scheme(Physics& p, int code) {
+  for (int k = 0; k < 4; ++k) p.alpha[k] = p.beta[k] = p.c[k] = 0.0;
+  p.scheme = code;
+  p.ssp_coeff = 1.0;
+  switch (code) {
+    case 1:
+      p.n_stages = 1;
+      p.beta[0] = 1.0;
+      break;
+    case 3:
+      p.n_stages = 3;
+      p.alpha[1] = 0.75;
+      p.alpha[2] = 1.0 / 3.0;
+      p.beta[0] = p.beta[1] = p.beta[2] = 1.0;
+      p.c[1] = 1.0;
+      p.c[2] = 0.5;
+      break;
+    case 4:
+      p.n_stages = 4;
+      p.ssp_coeff = 2.0;
+      p.alpha[2] = 2.0 / 3.0;
+      p.beta[0] = p.beta[1] = p.beta[2] = p.beta[3] = 0.5;
+      p.c[1] = 0.5;
+      p.c[2] = 1.0;
+      p.c[3] = 0.5;
+      break;
+    default:
+      p.scheme = 2;
+      p.n_stages = 2;
+      p.alpha[1] = 0.5;
+      p.beta[0] = p.beta[1] = 1.0;
+      p.c[1] = 1.0;
+      break;
+  }
+}
+
 #define RKB_TRY(expr)                      \
   do {                                     \
     cudaError_t e_ = (expr);               \
@@ -75,7 +114,7 @@ int Sim::create(const std::string& text, std::string& err) {
   phys.coriolis_f = cfg.coriolis_f;
   phys.use_hllc = cfg.use_hllc ? 1 : 0;
   phys.forcing_active = 0;
-  phys.ssp_coeff = scheme_code(cfg.time_scheme) == 4 ? 2.0 : 1.0;
+  fill_scheme(phys, scheme_code(cfg.time_scheme));
   params_dirty = true;
   t_current_ = 0.0;
   dt_ = 0.0;
@@ -260,6 +299,8 @@ int Sim::alloc_device(std::string& err) {
   args_.fo = Forcing{nullptr, nullptr, nullptr, nullptr};
   args_.tile = tile;
   args_.hllc = phys.use_hllc;
+  args_.scheme = phys.scheme;
+  args_.n_stages = phys.n_stages;
   cur_ = 0;
   return 0;
 }
@@ -353,6 +394,8 @@ int Sim::upload_params() {
   RKB_TRY(cudaStreamSynchronize(stream_));
   args_.hllc = phys.use_hllc;
   args_.tile = tile;
+  args_.scheme = phys.scheme;
+  args_.n_stages = phys.n_stages;
   RKB_TRY(configure_kernels(args_.tile, args_.hllc));
   params_dirty = false;
   return 0;
@@ -381,7 +424,16 @@ static int pull(const StepArgs& a, int cur, bool stepped, bool full, double* con
     if (cudaMemcpy2DAsync(hf[k], wbytes, src[k], spitch, wbytes, g.nyt, cudaMemcpyDeviceToHost, s) !=
         cudaSuccess)
       return -1;
-  if (full && stepped) {
+  if (full && stepped && a.scheme != 2) {
+    // generic schemes: the save arrays are whole copies of U^n, ghosts
+    // included (solver_save_state), which is the other buffer
+    FieldSet O = cur ? a.U0 : a.U1;
+    const double* so[3] = {O.h, O.hu, O.hv};
+    for (int k = 0; k < 3; ++k)
+      if (cudaMemcpy2DAsync(hf[4 + k], wbytes, so[k], spitch, wbytes, g.nyt,
+                            cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return -1;
+  } else if (full && stepped) {
     // RK2 save arrays: interior of U^n from the other buffer; the reference
     // never writes their ghosts in the fused RK2 path (left at zero here).
     FieldSet O = cur ? a.U0 : a.U1;
@@ -637,6 +689,10 @@ int Sim::time_steps(int n, double* ms) {
 
 int Sim::profile_steps(int n, double out[5]) {
   if (n <= 0) return -2;
+  if (phys.scheme != 2) {
+    err_text_ = "stage timing covers the two fused SSP-RK2 stages only";
+    return -2;
+  }
   if (prepare_run(1, 0.0, n) != 0) return -1;
   cudaEvent_t ev[5];
   for (auto& e : ev) RKB_TRY(cudaEventCreate(&e));
@@ -676,6 +732,10 @@ int Sim::profile_steps(int n, double out[5]) {
 int Sim::set_precision(int p) {
   if (p != 32 && p != 64) return -2;
   if (p == precision_) return 0;
+  if (p == 32 && phys.scheme != 2) {
+    err_text_ = "the FP32 surface form runs the SSP-RK2 scheme only";
+    return -2;
+  }
   if (is_finalised && on_device_) ensure_host();  // state home in the old form
   precision_ = p;
   params_dirty = true;

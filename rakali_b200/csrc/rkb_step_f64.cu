@@ -23,11 +23,26 @@ namespace rkb {
 // Boundary conditions (rki_boundary.F90:40-552)
 // ---------------------------------------------------------------------------
 
+// Buffers of the generic Shu-Osher stages: stage k reads X_k and writes
+// X_{k+1}; X_0 = U^n (buffer cur), the last stage writes buffer cur^1, and
+// the others alternate with the scratch S so no stage writes its own input.
+__device__ __forceinline__ FieldSet generic_out(const FieldSet& U0, const FieldSet& U1,
+                                                const FieldSet& S, int k, int nst, int cur) {
+  return ((nst - 1 - k) % 2 == 0) ? (cur ? U0 : U1) : S;
+}
+__device__ __forceinline__ FieldSet generic_in(const FieldSet& U0, const FieldSet& U1,
+                                               const FieldSet& S, int k, int nst, int cur) {
+  return k == 0 ? (cur ? U1 : U0) : generic_out(U0, U1, S, k - 1, nst, cur);
+}
+
 // One thread per tangential position t of edge w, looping over the ghost
 // layers k (so the Chapman surface refresh of position t is race-free).
-// Ghost values go to the stage's input buffer and, in stage 2, also to the
-// buffer that receives U^{n+1}.  `writer` marks the one thread of the step's
-// first boundary launch that publishes this step's active flag and dt.
+// Ghost values go to the stage's input buffer and, in RK2 stage 2 and the
+// last generic stage, also to the buffer that receives U^{n+1} (its ghosts
+// then hold the last fill, as the reference's single array does).  `stage` is
+// 1 or 2 (SSP-RK2) or 10 + k (generic stage k, time t + c_k dt).  `writer`
+// marks the one thread of the step's first boundary launch that publishes
+// this step's active flag and dt.
 __device__ __forceinline__ void bc_body(const StepArgs& a, int stage, int w, int t, bool writer) {
   const Grid& g = a.g;
   StepCtl* ctl = a.ctl;
@@ -50,15 +65,27 @@ __device__ __forceinline__ void bc_body(const StepArgs& a, int stage, int w, int
   double* eta_old_s = a.eta_old[2];
   double* eta_old_n = a.eta_old[3];
 
-  const double time = stage == 1 ? ctl->t : ctl->t + dt;
   const int cur = ctl->cur;
-  FieldSet F = stage == 1 ? (cur ? U1 : U0) : S;
+  double time;
+  FieldSet F;
   double* h2 = nullptr;
   double* hu2 = nullptr;
   double* hv2 = nullptr;
-  if (stage == 2) {
-    FieldSet N = cur ? U0 : U1;
-    h2 = N.h; hu2 = N.hu; hv2 = N.hv;
+  if (stage >= 10) {
+    const int k = stage - 10, nst = a.phys->n_stages;
+    time = ctl->t + a.phys->c[k] * dt;
+    F = generic_in(U0, U1, S, k, nst, cur);
+    if (k == nst - 1) {
+      FieldSet N = cur ? U0 : U1;
+      h2 = N.h; hu2 = N.hu; hv2 = N.hv;
+    }
+  } else {
+    time = stage == 1 ? ctl->t : ctl->t + dt;
+    F = stage == 1 ? (cur ? U1 : U0) : S;
+    if (stage == 2) {
+      FieldSet N = cur ? U0 : U1;
+      h2 = N.h; hu2 = N.hu; hv2 = N.hv;
+    }
   }
   double* h = F.h;
   double* hu = F.hu;
@@ -148,9 +175,9 @@ __device__ __forceinline__ void bc_body(const StepArgs& a, int stage, int w, int
     const double dd = e.normal_u ? g.dx : g.dy;
     // The reference fills the ghosts once more before computing dt
     // (rki_solver.F90:719); for Chapman that extra call refreshes the stored
-    // surface to the current interior one, which stage 1 then sees.
+    // surface to the current interior one, which the first stage then sees.
     const double ei0 = hi + b[qi];
-    const double eov = stage == 1 ? ei0 : eo[t];
+    const double eov = (stage == 1 || stage == 10) ? ei0 : eo[t];
     const double ei = hi + b[qi];
     const double hmax = dmax(hi, 1.0e-6);
     const double c = sqrt(kG * hmax);
@@ -311,6 +338,10 @@ __device__ __forceinline__ void sponge(double& h, double& u, double& v, const Bc
 // STAGE 2: U* (S) and U^n (buffer cur) -> U^{n+1} (buffer cur^1).
 // STAGE 0: flux divergence only (kernel-level API): writes flux/mass-flux
 //          arrays from `in`, no update.
+// STAGE 3: generic Shu-Osher stage gk of an n-stage scheme
+//          (rki_solver.F90:861-926): X_gk -> X_gk+1 with step beta_gk dt,
+//          then the SSP combination with U^n when alpha_gk != 0.  The last
+//          stage closes the step without the boundary mass budget.
 // Tile (bx, by) of a gx x gy tiling of one simulation.
 template <int TX, int TY, bool HLLC, int STAGE>
 __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Physics* phys,
@@ -318,7 +349,8 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
                                            const FieldSet& U1, const FieldSet& S,
                                            const double* __restrict__ b, const Forcing& fo,
                                            double* __restrict__ partials, const FluxOut& fl,
-                                           unsigned bx, unsigned by, unsigned gx, unsigned gy) {
+                                           unsigned bx, unsigned by, unsigned gx, unsigned gy,
+                                           int gk = 0) {
   using SM = StageSmem<TX, TY>;
   constexpr int TW = SM::TW;
   constexpr int NTH = TX * TY;
@@ -344,7 +376,12 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
     dt = ctl->dt;
     cur = ctl->cur;
   }
-  const FieldSet in = STAGE == 2 ? S : (cur ? U1 : U0);
+  const double step_dt = dt;
+  const int nst = STAGE == 3 ? phys->n_stages : 0;
+  if (STAGE == 3) dt = phys->beta[gk] * dt;  // the stage's own step
+  const FieldSet in = STAGE == 3   ? generic_in(U0, U1, S, gk, nst, cur)
+                      : STAGE == 2 ? S
+                                   : (cur ? U1 : U0);
 
   const int tid = threadIdx.x;
   const int gx0 = g.ng + (int)bx * TX;  // first interior cell of the tile
@@ -470,6 +507,18 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
       FieldSet out;
       if (STAGE == 1) {
         out = S;
+      } else if (STAGE == 3) {
+        out = generic_out(U0, U1, S, gk, nst, cur);
+        // SSP combination with U^n and its clamp (rki_kernel_update.F90:152-208)
+        const double an = phys->alpha[gk];
+        if (an != 0.0) {
+          const FieldSet old = cur ? U1 : U0;
+          const double ap = 1.0 - an;
+          a = an * old.h[q] + ap * a;
+          u = an * old.hu[q] + ap * u;
+          v = an * old.hv[q] + ap * v;
+          protect(a, u, v);
+        }
       } else {
         // RK2 average with U^n and the second clamp (rki_kernel_fused.F90:435-463)
         const FieldSet old = cur ? U1 : U0;
@@ -486,15 +535,15 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
       out.hv[q] = v;
       part = o_fh;
       sponge_d = a - h_pre_sponge;
-      if (STAGE == 2) wave_speed(a, u, v, wsx, wsy);
+      if (STAGE == 2 || (STAGE == 3 && gk == nst - 1)) wave_speed(a, u, v, wsx, wsy);
     }
   }
   if (STAGE == 0) return;
+  if (STAGE == 3 && gk != nst - 1) return;  // block-uniform
 
   // 5. block partials (fixed order) and the CFL maxima of the new state
-  part = warp_sum(part);
-  sponge_d = warp_sum(sponge_d);
-  if (STAGE == 2) {
+  constexpr bool kBudget = STAGE != 3;
+  if (STAGE != 1) {
     wsx = warp_max(wsx);
     wsy = warp_max(wsy);
     if ((tid & 31) == 0) {
@@ -502,25 +551,29 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
       atomic_max_pos(&ctl->msy_next, wsy);
     }
   }
-  __shared__ double red[2][NTH / 32];
-  if ((tid & 31) == 0) {
-    red[0][tid >> 5] = part;
-    red[1][tid >> 5] = sponge_d;
-  }
-  __syncthreads();
   const unsigned int nblocks = gx * gy;
-  const unsigned int bid = by * gx + bx;
-  if (tid == 0) {
-    double s0 = 0.0, s1 = 0.0;
-    for (int w = 0; w < NTH / 32; ++w) {
-      s0 = s0 + red[0][w];
-      s1 = s1 + red[1][w];
+  if (kBudget) {
+    part = warp_sum(part);
+    sponge_d = warp_sum(sponge_d);
+    __shared__ double red[2][NTH / 32];
+    if ((tid & 31) == 0) {
+      red[0][tid >> 5] = part;
+      red[1][tid >> 5] = sponge_d;
     }
-    double* P = partials + (size_t)(STAGE - 1) * 2 * nblocks;
-    P[bid] = s0;
-    P[nblocks + bid] = s1;
+    __syncthreads();
+    const unsigned int bid = by * gx + bx;
+    if (tid == 0) {
+      double s0 = 0.0, s1 = 0.0;
+      for (int w = 0; w < NTH / 32; ++w) {
+        s0 = s0 + red[0][w];
+        s1 = s1 + red[1][w];
+      }
+      double* P = partials + (size_t)(STAGE - 1) * 2 * nblocks;
+      P[bid] = s0;
+      P[nblocks + bid] = s1;
+    }
   }
-  if (STAGE != 2) return;
+  if (STAGE == 1) return;
 
   // 6. last block closes the step
   __shared__ bool last;
@@ -531,16 +584,16 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
   __syncthreads();
   if (!last) return;
   __threadfence();
-  finalize_step(g, ctl, phys, partials, nblocks, dt, cur);
+  finalize_step(g, ctl, phys, partials, nblocks, step_dt, cur, kBudget);
 }
 
 template <int TX, int TY, bool HLLC, int STAGE>
 __global__ void __launch_bounds__(TX * TY)
     k_stage(Grid g, StepCtl* ctl, const Physics* phys, const BcParams* bcp, FieldSet U0,
             FieldSet U1, FieldSet S, const double* __restrict__ b, Forcing fo,
-            double* __restrict__ partials, FluxOut fl) {
+            double* __restrict__ partials, FluxOut fl, int gk) {
   stage_body<TX, TY, HLLC, STAGE>(g, ctl, phys, bcp, U0, U1, S, b, fo, partials, fl, blockIdx.x,
-                                  blockIdx.y, gridDim.x, gridDim.y);
+                                  blockIdx.y, gridDim.x, gridDim.y, gk);
 }
 
 // Every simulation of a batch in one launch: map[blockIdx.x] = (simulation,
@@ -813,12 +866,12 @@ size_t partials_doubles(const Grid& g, int tile) {
 }
 
 template <int TX, int TY, bool HLLC, int STAGE>
-static cudaError_t launch_stage_t(const StepArgs& a, FluxOut fl, cudaStream_t s) {
+static cudaError_t launch_stage_t(const StepArgs& a, FluxOut fl, cudaStream_t s, int gk) {
   using SM = StageSmem<TX, TY>;
   auto kern = k_stage<TX, TY, HLLC, STAGE>;
   dim3 grid = stage_grid(a.g, a.tile);
   kern<<<grid, TX * TY, SM::BYTES, s>>>(a.g, a.ctl, a.phys, a.bc, a.U0, a.U1, a.S, a.b, a.fo,
-                                        a.partials, fl);
+                                        a.partials, fl, gk);
   return cudaGetLastError();
 }
 
@@ -839,6 +892,8 @@ static cudaError_t configure_t() {
     e = cudaFuncSetAttribute(k_stage<TX, TY, HLLC, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_stage<TX, TY, HLLC, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_stage<TX, TY, HLLC, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   return e;
 }
 
@@ -849,27 +904,29 @@ cudaError_t configure_kernels(int tile, int hllc) {
     case kTile32x16: return h ? configure_t<32, 16, true>() : configure_t<32, 16, false>();
     case kTile64x4: return h ? configure_t<64, 4, true>() : configure_t<64, 4, false>();
     case kTile16x16: return h ? configure_t<16, 16, true>() : configure_t<16, 16, false>();
-    default: return cudaSuccess;  // marching kernels use no dynamic shared memory
+    // marching kernels use no dynamic shared memory; the generic stages run
+    // on 32x16 tiles under them
+    default: return h ? configure_t<32, 16, true>() : configure_t<32, 16, false>();
   }
 }
 
 template <int STAGE>
-static cudaError_t launch_stage(const StepArgs& a, FluxOut fl, cudaStream_t s) {
+static cudaError_t launch_stage(const StepArgs& a, FluxOut fl, cudaStream_t s, int gk = 0) {
   const bool h = a.hllc != 0;
   switch (a.tile) {
     case kTile32x8:
-      return h ? launch_stage_t<32, 8, true, STAGE>(a, fl, s) : launch_stage_t<32, 8, false, STAGE>(a, fl, s);
+      return h ? launch_stage_t<32, 8, true, STAGE>(a, fl, s, gk) : launch_stage_t<32, 8, false, STAGE>(a, fl, s, gk);
     case kTile32x16:
-      return h ? launch_stage_t<32, 16, true, STAGE>(a, fl, s) : launch_stage_t<32, 16, false, STAGE>(a, fl, s);
+      return h ? launch_stage_t<32, 16, true, STAGE>(a, fl, s, gk) : launch_stage_t<32, 16, false, STAGE>(a, fl, s, gk);
     case kTile64x4:
-      return h ? launch_stage_t<64, 4, true, STAGE>(a, fl, s) : launch_stage_t<64, 4, false, STAGE>(a, fl, s);
+      return h ? launch_stage_t<64, 4, true, STAGE>(a, fl, s, gk) : launch_stage_t<64, 4, false, STAGE>(a, fl, s, gk);
     case kTile16x16:
-      return h ? launch_stage_t<16, 16, true, STAGE>(a, fl, s) : launch_stage_t<16, 16, false, STAGE>(a, fl, s);
+      return h ? launch_stage_t<16, 16, true, STAGE>(a, fl, s, gk) : launch_stage_t<16, 16, false, STAGE>(a, fl, s, gk);
     default:
       break;
   }
-  if (STAGE == 0) return cudaErrorInvalidValue;  // the flux-only entry uses the tiled kernels
-  constexpr int ST = STAGE == 0 ? 1 : STAGE;
+  if (STAGE == 0 || STAGE == 3) return cudaErrorInvalidValue;  // tiled kernels only
+  constexpr int ST = STAGE == 1 ? 1 : 2;
   if (a.tile == kMarch64)
     return h ? launch_march_t<true, ST, 64>(a, s) : launch_march_t<false, ST, 64>(a, s);
   return h ? launch_march_t<true, ST, 32>(a, s) : launch_march_t<false, ST, 32>(a, s);
@@ -882,7 +939,7 @@ cudaError_t launch_bc(const StepArgs& a, int stage, cudaStream_t s) {
   // other writes, i.e. when the interior is at least max(nghost, 2) wide.
   const bool pair_x = g.nx_phys() >= (g.ng > 2 ? g.ng : 2);
   const bool pair_y = g.ny_phys() >= (g.ng > 2 ? g.ng : 2);
-  int first = stage == 1 ? 1 : 0;
+  int first = (stage == 1 || stage == 10) ? 1 : 0;
   auto go = [&](int e0, int count, int n_tan) {
     dim3 grid((unsigned)((n_tan + tpb - 1) / tpb), (unsigned)count);
     k_bc<<<grid, tpb, 0, s>>>(a, stage, e0, first);
@@ -903,7 +960,24 @@ cudaError_t launch_bc(const StepArgs& a, int stage, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// Generic Shu-Osher schemes (euler, rk3, rk43): per stage k a boundary fill
+// at t + c_k dt and one stage<3> launch; the marching tiles have no generic
+// form, so those stages run on 32x16 tiles.
+static cudaError_t launch_step_generic(const StepArgs& a, cudaStream_t s) {
+  FluxOut none{};
+  StepArgs ga = a;
+  if (is_march(ga.tile)) ga.tile = kTile32x16;
+  for (int k = 0; k < a.n_stages; ++k) {
+    cudaError_t e = launch_bc(ga, 10 + k, s);
+    if (e != cudaSuccess) return e;
+    e = launch_stage<3>(ga, none, s, k);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t launch_step(const StepArgs& a, cudaStream_t s) {
+  if (a.scheme != 2) return launch_step_generic(a, s);
   FluxOut none{};
   cudaError_t e = launch_bc(a, 1, s);
   if (e != cudaSuccess) return e;
@@ -923,6 +997,7 @@ int launches_per_step(const StepArgs& a) {
   const Grid& g = a.g;
   const int need = g.ng > 2 ? g.ng : 2;
   const int bc = (g.nx_phys() >= need ? 1 : 2) + (g.ny_phys() >= need ? 1 : 2);
+  if (a.scheme != 2) return a.n_stages * (bc + 1);
   return 2 * bc + 2;
 }
 

@@ -97,20 +97,22 @@ __device__ __forceinline__ double warp_sum(double v) {
 // Close a step (last block of the final stage kernel): fixed-order sums of
 // the per-block partials, the mass budget in the reference's order
 // (rki_solver.F90:507-657), the CFL maxima of the new state and the clock.
+// `budget` false: the generic Shu-Osher schemes, which do not accumulate the
+// boundary mass budget (rki_solver.F90:861-926).
 static __device__ void finalize_step(const Grid& g, StepCtl* ctl, const Physics* phys,
-                              double* partials, unsigned int nparts, double dt, int cur) {
+                              double* partials, unsigned int nparts, double dt, int cur,
+                              bool budget = true) {
   const int tid = threadIdx.x;
   const double area = g.dx * g.dy;
   volatile double* VP = partials;
   double sums[4];
   for (int s = 0; s < 4; ++s) {
     double acc = 0.0;
-    if (tid < 32)
+    if (tid < 32 && budget)
       for (unsigned int k = tid; k < nparts; k += 32) acc = acc + VP[(size_t)s * nparts + k];
     sums[s] = warp_sum(acc);
   }
-  if (tid == 0) {
-    volatile StepCtl* vc = ctl;
+  if (tid == 0 && budget) {
     double mo = ctl->mass_out;
     mo = mo - 0.5 * dt * sums[0] * area;
     mo = mo - 0.5 * dt * sums[2] * area;
@@ -121,6 +123,9 @@ static __device__ void finalize_step(const Grid& g, StepCtl* ctl, const Physics*
     if (phys->forcing_active) ms = ms + 0.5 * dt * ctl->precip_sum * area;
     ms = ms + 0.5 * sums[3] * area;
     ctl->mass_src = ms;
+  }
+  if (tid == 0) {
+    volatile StepCtl* vc = ctl;
     ctl->msx = __longlong_as_double((long long)vc->msx_next);
     ctl->msy = __longlong_as_double((long long)vc->msy_next);
     ctl->msx_next = 0ull;

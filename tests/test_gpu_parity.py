@@ -183,6 +183,110 @@ def test_step_clamps_to_t_end_like_reference():
             sim.step(1)
 
 
+# ---------------------------------------------------------------------------
+# generic Shu-Osher schemes (euler, rk3, rk43): rki_solver.F90:861-926
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("scheme", ["euler", "rk3", "rk43"])
+@pytest.mark.parametrize("hllc", [False, True])
+def test_generic_schemes_wet_dry_friction(scheme, hllc):
+    """Islands, hump, Manning n: every stage, the SSP mixes, dt (x2 for rk43)."""
+    nx, ny, dx = 120, 96, 5.0
+    b = gaussian_bed(nx, ny, dx, dx, 20, seed=17, width=(20.0, 100.0))
+    h = hump_depth(b, dx, dx, width=60.0)
+    assert (h == 0.0).sum() > 20
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, manning_n=0.025,
+               use_hllc=hllc, time_scheme=scheme)
+    sim, orc = pair(cfg, bathymetry=b, initial_h=h)
+    with sim:
+        sim.step(40)
+        orc.step(40)
+        assert sim.step_count == orc.step_count == 40
+        assert sim.time == orc.time
+        assert sim.dt == orc.dt
+        compare_state(sim, orc, rtol=0.0)
+        compare_state(sim, orc, rtol=0.0, fields=("h0", "hu0", "hv0"))
+
+
+@pytest.mark.parametrize("scheme", ["euler", "rk3", "rk43"])
+@pytest.mark.parametrize("edges", [
+    dict(bc_west="tidal", tidal_amplitude=0.5, tidal_period=300.0, bc_east="chapman"),
+    dict(bc_west="sponge", bc_east="sponge", sponge_width=6, sponge_strength=0.01,
+         sponge_h_ref=10.0, bc_south="open", bc_north="inflow", inflow_velocity=0.2),
+])
+def test_generic_schemes_boundaries(scheme, edges):
+    """Stage times t + c_k dt reach the tide; sponge and Chapman per stage."""
+    nx, ny, dx = 96, 64, 10.0
+    b = np.asfortranarray(np.tile(np.linspace(-12.0, -8.0, nx)[:, None], (1, ny)))
+    h = hump_depth(b, dx, dx, amp=0.4, width=60.0)
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, manning_n=0.02,
+               time_scheme=scheme, **edges)
+    sim, orc = pair(cfg, bathymetry=b, initial_h=h)
+    with sim:
+        sim.advance(90.0)
+        orc.advance(90.0)
+        assert sim.step_count == orc.step_count
+        assert sim.time == orc.time
+        compare_state(sim, orc, rtol=0.0)
+
+
+@pytest.mark.parametrize("scheme", ["euler", "rk3", "rk43"])
+def test_generic_schemes_forcing_coriolis(scheme):
+    """Wind, pressure, rain and the Coriolis rotation by f * beta_k dt."""
+    nx, ny, dx = 48, 40, 50.0
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, manning_n=0.03,
+               coriolis_f=1.0e-4, init_condition="still_water", eta_initial=0.0,
+               time_scheme=scheme)
+    b = gaussian_bed(nx, ny, dx, dx, 6, seed=12, base=-5.0, amp=(-2.0, 6.0),
+                     width=(100.0, 400.0))
+    sim, orc = pair(cfg, bathymetry=b)
+    rng = np.random.default_rng(8)
+    wx = rng.uniform(0.0, 0.3, (nx, ny))
+    wy = rng.uniform(-0.1, 0.1, (nx, ny))
+    p = rng.uniform(-50.0, 50.0, (nx, ny))
+    rain = np.full((nx, ny), 1.0e-5)
+    with sim:
+        sim.set_wind(wx, wy)
+        sim.set_atm_pressure(p)
+        sim.set_precipitation(rain)
+        g = orc.ng
+        for name, arr in (("wind_x", wx), ("wind_y", wy), ("atm", p), ("precip", rain)):
+            orc.arrays[name][g:-g, g:-g] = arr
+        orc.s.forcing_active = 1
+        sim.step(30)
+        orc.step(30)
+        compare_state(sim, orc, rtol=0.0)
+
+
+def test_generic_scheme_graph_chunks_and_fixed_dt():
+    """Many steps per graph launch, other tiles and a fixed dt give the same bits."""
+    nx, ny, dx = 80, 72, 5.0
+    b = gaussian_bed(nx, ny, dx, dx, 12, seed=21, width=(20.0, 80.0))
+    h = hump_depth(b, dx, dx, width=50.0)
+    for tile, extra in ((0, dict(cfl_interval=3)), (4, dict(dt_fixed=0.05))):
+        cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, time_scheme="rk3", **extra)
+        sim, orc = pair(cfg, bathymetry=b, initial_h=h)
+        with sim:
+            sim.set_tile(tile)  # 4: a marching tile, whose generic stages run on 32x16 tiles
+            sim.step(150)
+            orc.step(150)
+            assert sim.dt == orc.dt
+            compare_state(sim, orc, rtol=0.0)
+
+
+def test_generic_schemes_refuse_fp32_and_batches():
+    from rakali_b200 import Rakali
+    from rakali_b200.ensemble import Ensemble
+    cfg = dict(nx=32, ny=32, dx=1.0, dy=1.0, t_end=10.0, time_scheme="rk3")
+    with Rakali(**cfg) as sim:
+        with pytest.raises(RuntimeError, match="SSP-RK2"):
+            sim.set_precision(32)
+        assert sim.precision == 64
+        with pytest.raises(RuntimeError, match="SSP-RK2"):
+            Ensemble([sim])
+        sim.step(3)  # still usable
+
+
 def test_tiles_agree():
     nx, ny, dx = 150, 70, 5.0
     b = gaussian_bed(nx, ny, dx, dx, 10, seed=9, width=(20.0, 80.0))
