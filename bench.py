@@ -427,6 +427,106 @@ def run_adjoint(args):
     return out
 
 
+def run_config5(args):
+    """FP32 forward + FP32 adjoint of 64 independent 2048^2 gradient problems
+    (the 1024^2 gradient workload's family at 2048^2, one seed per member),
+    500 steps, batched: every kernel launch covers a group of members sized to
+    the free device memory.  Reports throughput of the forward and of forward +
+    adjoint, the cost multiple, the FP64 mass drift of the FP32 forward, and
+    member 0's J and gradient against the FP64 adjoint of the same member on
+    the same dt sequence and observations, beside the FP64 gradient's own
+    sensitivity to a 1e-7 |b|max bed perturbation."""
+    import torch
+
+    from rakali_b200 import workloads as wl
+    from rakali_b200.adjoint import GaugeMisfitBatch
+
+    nm, n, steps = args.c5_members, args.c5_side, args.c5_steps
+    dx = 10.0
+    pitch = (n + 4 + 31) // 32 * 32
+    per_member = 4 * pitch * (n + 4) * 240  # bytes: ~240 FP32 fields (states, tapes, checkpoints)
+    free, _ = torch.cuda.mem_get_info()
+    group = nm
+    while group > 1 and group * per_member > 0.7 * free:
+        group //= 2
+    fwd_ms = grad_ms = 0.0
+    drift = 0.0
+    ref = None
+    for g0 in range(0, nm, group):
+        ms = list(range(g0, min(nm, g0 + group)))
+        probs = [wl.adjoint_problem(n=n, steps=steps, dx=dx, seed=1000 + m) for m in ms]
+        b = np.array([p["b"] for p in probs])
+        h = np.array([p["h"] for p in probs])
+        nf = np.array([p["n"] for p in probs])
+        noise = np.array([p["noise"] for p in probs])
+        gauges = [p["gauges"] for p in probs]
+        del probs
+        with GaugeMisfitBatch(len(ms), n, n, dx, dx, h, gauges, steps, precision=32) as pb:
+            pb.record_dt(b, nf)
+            _, obs = pb.forward(b + noise, nf)
+            pb.set_observations(obs)
+            J, _ = pb.forward(b, nf)
+            fwd_ms += pb.last_ms
+            mass = pb.mass
+            drift = max(drift, float(np.max(np.abs(mass[1] - mass[0]) / mass[0])))
+            _, gb, gn = pb.gradient(b, nf)
+            grad_ms += pb.last_ms
+            if ref is None:
+                ref = dict(b=b[0], h=h[0], n=nf[0], gauges=gauges[0], dt=pb.dt[0], obs=obs[:, 0, :],
+                           J=float(J[0]), gb=gb[0], gn=gn[0],
+                           checkpoint_interval=pb.checkpoint_interval)
+        del b, h, nf, noise, gb, gn
+    cells = nm * n * n * steps
+    # member 0 in FP64 on the same dt sequence and observations
+    shape = (1, n, n)
+    with GaugeMisfitBatch(1, n, n, dx, dx, ref["h"][None], [ref["gauges"]], steps,
+                          precision=64) as p64:
+        p64.set_dt(ref["dt"][None])
+        p64.set_observations(ref["obs"][:, None, :])
+        J64, gb64, gn64 = p64.gradient(ref["b"][None], ref["n"][None])
+        rng = np.random.default_rng(9)
+        pert = 1e-7 * float(np.abs(ref["b"]).max()) * rng.standard_normal(shape)
+        _, gbf, gnf = p64.gradient(ref["b"][None] + pert, ref["n"][None])
+
+    def rel(a, r):
+        return float(np.linalg.norm(a - r) / np.linalg.norm(r))
+
+    dd, dd_floor = [], []
+    for k in range(8):
+        db = wl.gaussian_bed(n, n, dx, dx, 3, 700 + k, base=0.0, amp=(-1.0, 1.0),
+                             width=(200.0, 1500.0))
+        dn = wl.gaussian_bed(n, n, dx, dx, 3, 800 + k, base=0.0, amp=(-0.01, 0.01),
+                             width=(200.0, 1500.0))
+        d64 = float(np.sum(gb64[0] * db) + np.sum(gn64[0] * dn))
+        d32 = float(np.sum(ref["gb"] * db) + np.sum(ref["gn"] * dn))
+        dfl = float(np.sum(gbf[0] * db) + np.sum(gnf[0] * dn))
+        dd.append(abs(d32 - d64) / abs(d64))
+        dd_floor.append(abs(dfl - d64) / abs(d64))
+    return {
+        "workload": f"{nm} members x {n}x{n}, dx = {dx} m, 16-Gaussian bed per member "
+                    f"(seeds 1000..{1000 + nm - 1}), 0.5 m hump on a smooth undulation, "
+                    f"Manning n field 0.025, walls, {steps} steps, 64 gauges per member; "
+                    "FP32 forward + FP32 adjoint, FP64 misfit and mass sums",
+        "members_per_launch": group,
+        "checkpoint_interval": ref["checkpoint_interval"],
+        "forward_ms": fwd_ms, "forward_plus_adjoint_ms": grad_ms,
+        "forward_cell_updates_per_s": cells / (fwd_ms * 1e-3),
+        "forward_plus_adjoint_cell_updates_per_s": cells / (grad_ms * 1e-3),
+        "cost_multiple_of_forward": grad_ms / fwd_ms,
+        "mass_drift_rel_max": drift,
+        "vs_fp64_member0": {
+            "J_rel_err": abs(ref["J"] - float(J64[0])) / abs(float(J64[0])),
+            "grad_b_rel_l2": rel(ref["gb"], gb64[0]), "grad_n_rel_l2": rel(ref["gn"], gn64[0]),
+            "directional_rel_err_median": float(np.median(dd)),
+            "directional_rel_err_max": float(np.max(dd)),
+            "fp64_floor": {"bed_noise_rel": 1e-7,
+                           "grad_b_rel_l2": rel(gbf[0], gb64[0]),
+                           "grad_n_rel_l2": rel(gnf[0], gn64[0]),
+                           "directional_rel_err_median": float(np.median(dd_floor)),
+                           "directional_rel_err_max": float(np.max(dd_floor))}},
+    }
+
+
 def run_b200(args, rank, world, local_rank, dist):
     import torch
 
@@ -494,6 +594,8 @@ def run_b200(args, rank, world, local_rank, dist):
         line["ensemble"] = ens
     if world == 1 and args.adjoint_steps > 0:
         line["adjoint"] = run_adjoint(args)
+    if world == 1 and args.config5:
+        line["adjoint_fp32_batched"] = run_config5(args)
     print(json.dumps(line), flush=True)
     return 0
 
@@ -524,6 +626,12 @@ def main():
                     help="random directions of the finite-difference check")
     ap.add_argument("--adjoint-fd-steps", type=int, default=100,
                     help="steps of the finite-difference check (the gradient's first steps)")
+    ap.add_argument("--config5", action="store_true",
+                    help="also run the batched FP32 forward + adjoint (64 x 2048^2, 500 steps; "
+                         "a few minutes)")
+    ap.add_argument("--c5-members", type=int, default=64)
+    ap.add_argument("--c5-side", type=int, default=2048)
+    ap.add_argument("--c5-steps", type=int, default=500)
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the FP32-vs-FP64 error measurement")
     ap.add_argument("--sweep-cols", type=int, choices=(0, 2, 4), default=0,

@@ -197,6 +197,23 @@ int rkb_adjoint_gradient(void *adj, const double *b, const double *n_field, doub
 int rkb_adjoint_checkpoint_interval(void *adj);
 /* Device milliseconds of the last forward / gradient call (CUDA events). */
 double rkb_adjoint_last_ms(void *adj);
+/* A batch of n_members equally sized problems advanced together (every
+ * kernel launch covers all members), in FP64 (precision 64) or FP32 (32;
+ * misfit and mass sums stay FP64).  Per-member arrays are stacked member by
+ * member: h0/hu0/hv0/b/n_field/grad_* are (n_members, nx*ny) with each
+ * member Fortran-ordered, gauge_i/j are (n_members, n_gauges), obs and
+ * eta_gauges are (n_steps, n_members, n_gauges), dts (n_members, n_steps),
+ * J (n_members).  hu0, hv0 may be NULL (zero).  rkb_adjoint_create is this
+ * call with precision 64 and one member; the functions above take either. */
+int rkb_adjoint_batch_create(int precision, int n_members, int nx, int ny, int nghost, double dx,
+                             double dy, double cfl, int use_hllc, int n_steps, const double *h0,
+                             const double *hu0, const double *hv0, const int *gauge_i,
+                             const int *gauge_j, int n_gauges, void **adj);
+int rkb_adjoint_members(void *adj);
+int rkb_adjoint_precision(void *adj);
+/* FP64 interior mass sum(h) per member before (out[m]) and after
+ * (out[n_members + m]) the last forward run. */
+int rkb_adjoint_mass(void *adj, double *out);
 /* Host builds of the face flux / cell update and their adjoints (for
  * finite-difference checks without a GPU). */
 void rkb_test_face_flux(int dir, int hllc, const double *in8, double *out6);

@@ -120,6 +120,11 @@ def load(path: str | None = None):
     _sig(lib, "rkb_adjoint_gradient", [H, DP, DP, D, DP, DP, DP], I)
     _sig(lib, "rkb_adjoint_checkpoint_interval", [H], I)
     _sig(lib, "rkb_adjoint_last_ms", [H], D)
+    _sig(lib, "rkb_adjoint_batch_create",
+         [I, I, I, I, I, D, D, D, I, I, DP, DP, DP, IP, IP, I, HP], I)
+    _sig(lib, "rkb_adjoint_members", [H], I)
+    _sig(lib, "rkb_adjoint_precision", [H], I)
+    _sig(lib, "rkb_adjoint_mass", [H, DP], I)
     _sig(lib, "rkb_test_face_flux", [I, I, DP, DP], None)
     _sig(lib, "rkb_test_face_adj", [I, I, DP, DP, DP], None)
     _sig(lib, "rkb_test_cell", [DP, D, DP], None)

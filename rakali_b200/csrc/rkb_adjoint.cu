@@ -1,847 +1,19 @@
-// Adjoint of the FP64 structured step for gauge-misfit gradients.
-//
-// J(b, n) = sum over steps k = 1..N and gauge cells g of (eta_g^k - obs_g^k)^2
-// for the SSP-RK2 step of rki_solver.F90:659-815 with wall boundaries, HLL or
-// HLLC fluxes and Manning friction with a per-cell n field, on a fixed dt
-// sequence (recorded once from CFL steps and replayed, so J is a
-// piecewise-smooth function of b and n).  Gradients dJ/db and dJ/dn come from
-// hand-written reverse kernels:
-//
-//   forward, per stage:  slopes -> faces -> cells          (taped: slopes, face outputs)
-//   reverse, per stage:  cells -> faces -> reconstruction -> slope gather -> walls
-//
-// Every reverse kernel gathers (each output element is written by one thread),
-// so there are no atomics and the gradient is deterministic.  States are
-// checkpointed every K ~ sqrt(N) steps and recomputed segment by segment.
-//
-// The forward kernels evaluate the reference's expressions in its order with
-// --fmad=false, like rkb_step_f64.cu: with a uniform n field equal to the
-// scalar manning_n the trajectory is bit-identical to the production step.
-#include <algorithm>
-#include <cmath>
-#include <cstring>
-#include <string>
-#include <vector>
-
-#include "rkb_adjoint.cuh"
-#include "rkb_kernels.h"
+// FP64 instance of the gauge-misfit adjoint (rkb_adjoint_impl.cuh), compiled
+// with --fmad=false so its forward is bit-identical to the production step,
+// and the C ABI of both precisions (the FP32 instance is rkb_adjoint32.cu).
+#include "rkb_adjoint_impl.cuh"
 
 namespace rkb {
-namespace {
 
-constexpr int kBX = 32, kBY = 8;
-
-struct Tape {
-  double* s[6];   // x-slopes (eta, hu, hv), y-slopes (eta, hu, hv)
-  double* fx[6];  // x-face i-1/2 at (i, j): fh, fqx, fqy, wbR, hL2, pL2
-  double* fy[6];  // y-face j-1/2 at (i, j)
-};
-
-struct Rev {
-  double* go[3];   // adjoint of the cell's flux divergence (o_fh, o_fhu, o_fhv)
-  double* ga[3];   // direct adjoint of the stage input at interior cells (a = h + dt o)
-  double* gfx[8];  // x-face input adjoints (eL, qxL, qyL, bL, eR, qxR, qyR, bR)
-  double* gfy[8];
-  double* gs[6];   // slope adjoints
-  int* ch;         // minmod branches, 2 bits per slope (6 slopes)
-  double* gd[4];   // reconstruction adjoints of eta, hu, hv, b at the cell
-};
-
-__device__ __forceinline__ bool in_box(int i, int j, int i0, int i1, int j0, int j1) {
-  return i >= i0 && i <= i1 && j >= j0 && j <= j1;
+AdjointBase* make_adjoint64(int nm, int nx, int ny, int ng, double dx, double dy, double cfl,
+                            int hllc, int nsteps, const double* h0, const double* hu0,
+                            const double* hv0, const int* gi, const int* gj, int ngauge,
+                            std::string& err, int& rc) {
+  return adj::make_adjoint<double>(nm, nx, ny, ng, dx, dy, cfl, hllc, nsteps, h0, hu0, hv0, gi, gj,
+                                   ngauge, err, rc);
 }
 
-// ---- forward ------------------------------------------------------------------
-
-// Wall ghosts (rki_boundary.F90:220-291), W/E (pass 0) or S/N (pass 1).
-__global__ void k_walls(Grid g, FieldSet V, double* __restrict__ b, int pass) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int side = blockIdx.y;  // 0: west / south, 1: east / north
-  const int n_tan = pass == 0 ? g.nyt : g.nxt;
-  if (t >= n_tan) return;
-  for (int k = 1; k <= g.ng; ++k) {
-    int ig, jg, im, jm;
-    if (pass == 0) {
-      jg = jm = t;
-      ig = side == 0 ? g.ng - k : g.nxt - g.ng + k - 1;
-      im = side == 0 ? g.ng + k - 1 : g.nxt - g.ng - k;
-    } else {
-      ig = im = t;
-      jg = side == 0 ? g.ng - k : g.nyt - g.ng + k - 1;
-      jm = side == 0 ? g.ng + k - 1 : g.nyt - g.ng - k;
-    }
-    const size_t q = g.at(ig, jg), m = g.at(im, jm);
-    const double bm = b[m];
-    b[q] = bm;
-    V.h[q] = pos(V.h[m] + bm - bm);
-    if (pass == 0) { V.hu[q] = -V.hu[m]; V.hv[q] = V.hv[m]; }
-    else { V.hv[q] = -V.hv[m]; V.hu[q] = V.hu[m]; }
-  }
-}
-
-__global__ void k_slopes(Grid g, FieldSet V, const double* __restrict__ b, Tape T) {
-  const int i = g.ng - 1 + blockIdx.x * kBX + threadIdx.x % kBX;
-  const int j = g.ng - 1 + blockIdx.y * kBY + threadIdx.x / kBX;
-  const int ie = g.nxt - g.ng, je = g.nyt - g.ng;
-  if (i > ie || j > je) return;
-  const size_t c = g.at(i, j);
-  auto eta = [&](size_t q) { return V.h[q] + b[q]; };
-  if (j >= g.ng && j < je) {  // x-slope
-    const size_t m = c - 1, p = c + 1;
-    cell_slope(V.h[m], V.h[c], V.h[p], eta(m), eta(c), eta(p), V.hu[m], V.hu[c], V.hu[p], V.hv[m],
-               V.hv[c], V.hv[p], T.s[0][c], T.s[1][c], T.s[2][c]);
-  }
-  if (i >= g.ng && i < ie) {  // y-slope
-    const size_t m = c - g.pitch, p = c + g.pitch;
-    cell_slope(V.h[m], V.h[c], V.h[p], eta(m), eta(c), eta(p), V.hu[m], V.hu[c], V.hu[p], V.hv[m],
-               V.hv[c], V.hv[p], T.s[3][c], T.s[4][c], T.s[5][c]);
-  }
-}
-
-// Reconstructed left / right states of x-face (i-1/2, j) or y-face (i, j-1/2).
-struct FaceIn {
-  double eL, qxL, qyL, bL, eR, qxR, qyR, bR;
-};
-
-__device__ __forceinline__ FaceIn face_in(const Grid& g, const FieldSet& V,
-                                          const double* __restrict__ b, const Tape& T, size_t qL,
-                                          size_t qR, int dir) {
-  const int o = dir == 0 ? 0 : 3;
-  FaceIn f;
-  f.eL = (V.h[qL] + b[qL]) + 0.5 * T.s[o][qL];
-  f.qxL = V.hu[qL] + 0.5 * T.s[o + 1][qL];
-  f.qyL = V.hv[qL] + 0.5 * T.s[o + 2][qL];
-  f.bL = b[qL];
-  f.eR = (V.h[qR] + b[qR]) - 0.5 * T.s[o][qR];
-  f.qxR = V.hu[qR] - 0.5 * T.s[o + 1][qR];
-  f.qyR = V.hv[qR] - 0.5 * T.s[o + 2][qR];
-  f.bR = b[qR];
-  return f;
-}
-
-template <bool HLLC>
-__global__ void k_faces(Grid g, FieldSet V, const double* __restrict__ b, Tape T) {
-  const int i = g.ng + blockIdx.x * kBX + threadIdx.x % kBX;
-  const int j = g.ng + blockIdx.y * kBY + threadIdx.x / kBX;
-  const int ie = g.nxt - g.ng, je = g.nyt - g.ng;
-  if (i > ie || j > je) return;
-  const size_t c = g.at(i, j);
-  if (j < je) {  // x-face between (i-1, j) and (i, j)
-    const FaceIn f = face_in(g, V, b, T, c - 1, c, 0);
-    FaceOut o;
-    face_flux<0, HLLC>(f.eL, f.qxL, f.qyL, f.bL, f.eR, f.qxR, f.qyR, f.bR, o);
-    T.fx[0][c] = o.fh; T.fx[1][c] = o.fqx; T.fx[2][c] = o.fqy;
-    T.fx[3][c] = o.wbR; T.fx[4][c] = o.hL2; T.fx[5][c] = o.pL2;
-  }
-  if (i < ie) {  // y-face between (i, j-1) and (i, j)
-    const FaceIn f = face_in(g, V, b, T, c - g.pitch, c, 1);
-    FaceOut o;
-    face_flux<1, HLLC>(f.eL, f.qxL, f.qyL, f.bL, f.eR, f.qxR, f.qyR, f.bR, o);
-    T.fy[0][c] = o.fh; T.fy[1][c] = o.fqx; T.fy[2][c] = o.fqy;
-    T.fy[3][c] = o.wbR; T.fy[4][c] = o.hL2; T.fy[5][c] = o.pL2;
-  }
-}
-
-// Flux divergence of interior cell c in k_stage's expression order.
-__device__ __forceinline__ void divergence(const Grid& g, const Tape& T, size_t c, double& ofh,
-                                           double& ofhu, double& ofhv) {
-  const size_t r = c + 1, t = c + g.pitch;
-  const double dx = g.dx, dy = g.dy;
-  ofh = -((T.fx[0][r] - T.fx[0][c]) / dx) - (T.fy[0][t] - T.fy[0][c]) / dy;
-  ofhu = -((T.fx[1][r] - T.fx[1][c]) / dx) - (T.fy[1][t] - T.fy[1][c]) / dy -
-         kHalfG * (T.fx[3][c] - T.fx[4][r] + T.fx[5][r]) / dx;
-  ofhv = -((T.fx[2][r] - T.fx[2][c]) / dx) - (T.fy[2][t] - T.fy[2][c]) / dy -
-         kHalfG * (T.fy[3][c] - T.fy[4][t] + T.fy[5][t]) / dy;
-}
-
-// Cell update of stage 1 (out = protect(sources(V + dt L))) or stage 2 (RK2
-// average with the base state and the second clamp).
-__global__ void k_cells(Grid g, FieldSet V, FieldSet base, const double* __restrict__ nf, Tape T,
-                        double dt, int stage, FieldSet out) {
-  const int i = g.ng + blockIdx.x * kBX + threadIdx.x % kBX;
-  const int j = g.ng + blockIdx.y * kBY + threadIdx.x / kBX;
-  if (i >= g.nxt - g.ng || j >= g.nyt - g.ng) return;
-  const size_t c = g.at(i, j);
-  double ofh, ofhu, ofhv;
-  divergence(g, T, c, ofh, ofhu, ofhv);
-  double a = V.h[c], u = V.hu[c], v = V.hv[c];
-  a = a + dt * ofh;
-  u = u + dt * ofhu;
-  v = v + dt * ofhv;
-  protect(a, u, v);
-  friction(a, u, v, nf[c], dt);
-  if (stage == 2) {
-    a = 0.5 * (base.h[c] + a);
-    u = 0.5 * (base.hu[c] + u);
-    v = 0.5 * (base.hv[c] + v);
-    protect(a, u, v);
-  }
-  out.h[c] = a;
-  out.hu[c] = u;
-  out.hv[c] = v;
-}
-
-// CFL maxima of a state (same wave speed and reduction as the step).
-__global__ void k_speeds(Grid g, FieldSet V, unsigned long long* mx) {
-  const int i = g.ng + blockIdx.x * kBX + threadIdx.x % kBX;
-  const int j = g.ng + blockIdx.y * kBY + threadIdx.x / kBX;
-  double sx = 0.0, sy = 0.0;
-  if (i < g.nxt - g.ng && j < g.nyt - g.ng) {
-    const size_t c = g.at(i, j);
-    wave_speed(V.h[c], V.hu[c], V.hv[c], sx, sy);
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    sx = fmax(sx, __shfl_xor_sync(0xffffffffu, sx, o));
-    sy = fmax(sy, __shfl_xor_sync(0xffffffffu, sy, o));
-  }
-  if ((threadIdx.x & 31) == 0) {
-    atomic_max_pos(&mx[0], sx);
-    atomic_max_pos(&mx[1], sy);
-  }
-}
-
-// Gauge residuals eta - obs of one step; r[k] for gauge k.
-__global__ void k_gauges(Grid g, FieldSet V, const double* __restrict__ b, const int* __restrict__ gq,
-                         const double* __restrict__ obs, int ng, double* r) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= ng) return;
-  const size_t q = (size_t)gq[k];
-  r[k] = (V.h[q] + b[q]) - obs[k];
-}
-
-// ---- reverse ------------------------------------------------------------------
-
-// Cells: output adjoint gout -> divergence adjoint go, direct input adjoint
-// ga (a = h + dt o), base adjoint (stage 2), n adjoint.
-__global__ void k_cells_adj(Grid g, FieldSet V, FieldSet base, const double* __restrict__ nf,
-                            Tape T, double dt, int stage, FieldSet gout, Rev R, FieldSet gbase,
-                            double* __restrict__ gn) {
-  const int i = g.ng + blockIdx.x * kBX + threadIdx.x % kBX;
-  const int j = g.ng + blockIdx.y * kBY + threadIdx.x / kBX;
-  if (i >= g.nxt - g.ng || j >= g.nyt - g.ng) return;
-  const size_t c = g.at(i, j);
-  double ofh, ofhu, ofhv;
-  divergence(g, T, c, ofh, ofhu, ofhv);
-  // forward with intermediates
-  const double a0 = V.h[c] + dt * ofh, u0 = V.hu[c] + dt * ofhu, v0 = V.hv[c] + dt * ofhv;
-  double a1 = a0, u1 = u0, v1 = v0;
-  protect(a1, u1, v1);
-  double a2 = a1, u2 = u1, v2 = v1;
-  friction(a2, u2, v2, nf[c], dt);
-  double ga = gout.h[c], gu = gout.hu[c], gv = gout.hv[c];
-  if (stage == 2) {
-    const double ap = 0.5 * (base.h[c] + a2), up = 0.5 * (base.hu[c] + u2),
-                 vp = 0.5 * (base.hv[c] + v2);
-    protect_adj(ap, up, vp, ga, gu, gv);
-    gbase.h[c] = 0.5 * ga;
-    gbase.hu[c] = 0.5 * gu;
-    gbase.hv[c] = 0.5 * gv;
-    ga *= 0.5;
-    gu *= 0.5;
-    gv *= 0.5;
-  }
-  double gnc = 0.0;
-  friction_adj(a1, u1, v1, nf[c], dt, ga, gu, gv, gnc);
-  gn[c] += gnc;
-  protect_adj(a0, u0, v0, ga, gu, gv);
-  R.ga[0][c] = ga;
-  R.ga[1][c] = gu;
-  R.ga[2][c] = gv;
-  R.go[0][c] = dt * ga;
-  R.go[1][c] = dt * gu;
-  R.go[2][c] = dt * gv;
-}
-
-// Faces: divergence adjoints of the two adjacent cells -> face output
-// adjoints -> adjoints of the reconstructed inputs.
-template <bool HLLC>
-__global__ void k_faces_adj(Grid g, FieldSet V, const double* __restrict__ b, Tape T, Rev R) {
-  const int i = g.ng + blockIdx.x * kBX + threadIdx.x % kBX;
-  const int j = g.ng + blockIdx.y * kBY + threadIdx.x / kBX;
-  const int ie = g.nxt - g.ng, je = g.nyt - g.ng;
-  if (i > ie || j > je) return;
-  const size_t c = g.at(i, j);
-  auto go = [&](int k, int ii, int jj) {  // zero outside the interior
-    return (ii >= g.ng && ii < ie && jj >= g.ng && jj < je) ? R.go[k][g.at(ii, jj)] : 0.0;
-  };
-  if (j < je) {
-    const double dx = g.dx;
-    const double lh = go(0, i - 1, j), lu = go(1, i - 1, j), lv = go(2, i - 1, j);
-    const double rh = go(0, i, j), ru = go(1, i, j), rv = go(2, i, j);
-    const double gout[6] = {(-lh + rh) / dx, (-lu + ru) / dx, (-lv + rv) / dx,
-                            -kHalfG * ru / dx, kHalfG * lu / dx, -kHalfG * lu / dx};
-    const FaceIn f = face_in(g, V, b, T, c - 1, c, 0);
-    double gin[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    face_adj<0, HLLC>(f.eL, f.qxL, f.qyL, f.bL, f.eR, f.qxR, f.qyR, f.bR, gout, gin);
-    for (int k = 0; k < 8; ++k) R.gfx[k][c] = gin[k];
-  }
-  if (i < ie) {
-    const double dy = g.dy;
-    const double bh = go(0, i, j - 1), bu = go(1, i, j - 1), bv = go(2, i, j - 1);
-    const double th = go(0, i, j), tu = go(1, i, j), tv = go(2, i, j);
-    const double gout[6] = {(-bh + th) / dy, (-bu + tu) / dy, (-bv + tv) / dy,
-                            -kHalfG * tv / dy, kHalfG * bv / dy, -kHalfG * bv / dy};
-    const FaceIn f = face_in(g, V, b, T, c - g.pitch, c, 1);
-    double gin[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    face_adj<1, HLLC>(f.eL, f.qxL, f.qyL, f.bL, f.eR, f.qxR, f.qyR, f.bR, gout, gin);
-    for (int k = 0; k < 8; ++k) R.gfy[k][c] = gin[k];
-  }
-}
-
-// Reconstruction: face input adjoints -> adjoints of the cell's eta, hu, hv,
-// b (direct) and of its six slopes, with the minmod branch of each slope.
-__global__ void k_recon_adj(Grid g, FieldSet V, const double* __restrict__ b, Rev R) {
-  const int i = g.ng - 1 + blockIdx.x * kBX + threadIdx.x % kBX;
-  const int j = g.ng - 1 + blockIdx.y * kBY + threadIdx.x / kBX;
-  const int ie = g.nxt - g.ng, je = g.nyt - g.ng;
-  if (i > ie || j > je) return;
-  const size_t c = g.at(i, j);
-  double de = 0.0, du = 0.0, dv = 0.0, db = 0.0;
-  int ch = 0;
-  auto eta = [&](size_t q) { return V.h[q] + b[q]; };
-  for (int dir = 0; dir < 2; ++dir) {
-    const bool in_range = dir == 0 ? (j >= g.ng && j < je) : (i >= g.ng && i < ie);
-    if (!in_range) continue;
-    const int lo = dir == 0 ? i : j, hi = dir == 0 ? ie : je;
-    const size_t step = dir == 0 ? 1 : (size_t)g.pitch;
-    double* const* gf = dir == 0 ? R.gfx : R.gfy;
-    // right/top face of c is stored at c + step (exists if lo + 1 <= hi),
-    // left/bottom face at c (exists if lo >= ng)
-    double gr[8] = {0, 0, 0, 0, 0, 0, 0, 0}, gl[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    if (lo + 1 <= hi)
-      for (int k = 0; k < 8; ++k) gr[k] = gf[k][c + step];
-    if (lo >= g.ng)
-      for (int k = 0; k < 8; ++k) gl[k] = gf[k][c];
-    // eL = eta + s/2 on the right face, eR = eta - s/2 on the left face
-    de += gr[0] + gl[4];
-    du += gr[1] + gl[5];
-    dv += gr[2] + gl[6];
-    db += gr[3] + gl[7];
-    const int o = dir == 0 ? 0 : 3;
-    R.gs[o][c] = 0.5 * (gr[0] - gl[4]);
-    R.gs[o + 1][c] = 0.5 * (gr[1] - gl[5]);
-    R.gs[o + 2][c] = 0.5 * (gr[2] - gl[6]);
-    // minmod branches (cell_slope: zero near dry cells)
-    const size_t m = c - step, p = c + step;
-    if (!(V.h[c] < kThin || V.h[m] < kDry || V.h[p] < kDry)) {
-      const int c0 = minmod_choice(eta(c) - eta(m), eta(p) - eta(c));
-      const int c1 = minmod_choice(V.hu[c] - V.hu[m], V.hu[p] - V.hu[c]);
-      const int c2 = minmod_choice(V.hv[c] - V.hv[m], V.hv[p] - V.hv[c]);
-      ch |= (c0 | (c1 << 2) | (c2 << 4)) << (dir * 6);
-    }
-  }
-  R.gd[0][c] = de;
-  R.gd[1][c] = du;
-  R.gd[2][c] = dv;
-  R.gd[3][c] = db;
-  R.ch[c] = ch;
-}
-
-// Slope gather: every cell collects the slope adjoints of itself and its
-// neighbours (minmod branch a = q_c - q_{c-1}, b = q_{c+1} - q_c), plus the
-// direct reconstruction and cell-update adjoints.  gV receives the adjoint of
-// the stage input (all cells, ghosts included); gb accumulates the bed's.
-__global__ void k_gather_adj(Grid g, Rev R, FieldSet gV, double* __restrict__ gb) {
-  const int i = g.ng - 2 + blockIdx.x * kBX + threadIdx.x % kBX;
-  const int j = g.ng - 2 + blockIdx.y * kBY + threadIdx.x / kBX;
-  if (i > g.nxt - g.ng + 1 || j > g.nyt - g.ng + 1) return;
-  const int ie = g.nxt - g.ng, je = g.nyt - g.ng;
-  const size_t c = g.at(i, j);
-  // slope ranges: x-slopes on [ng-1, ie] x [ng, je-1], y-slopes on [ng, ie-1] x [ng-1, je]
-  auto xs = [&](int ii, int jj) { return in_box(ii, jj, g.ng - 1, ie, g.ng, je - 1); };
-  auto ys = [&](int ii, int jj) { return in_box(ii, jj, g.ng, ie - 1, g.ng - 1, je); };
-  auto rc = [&](int ii, int jj) { return in_box(ii, jj, g.ng - 1, ie, g.ng - 1, je); };
-  double acc[3] = {0.0, 0.0, 0.0};
-  for (int dir = 0; dir < 2; ++dir) {
-    const int di = dir == 0 ? 1 : 0, dj = dir == 0 ? 0 : 1;
-    auto has = [&](int ii, int jj) { return dir == 0 ? xs(ii, jj) : ys(ii, jj); };
-    for (int v = 0; v < 3; ++v) {
-      const int o = dir * 3 + v;
-      const int sh = dir * 6 + 2 * v;
-      double s = 0.0;
-      if (has(i, j)) {
-        const int chc = (R.ch[c] >> sh) & 3;
-        if (chc == 1) s += R.gs[o][c];
-        else if (chc == 2) s -= R.gs[o][c];
-      }
-      if (has(i + di, j + dj)) {  // neighbour above chose a = q_{c+1} - q_c
-        const size_t p = g.at(i + di, j + dj);
-        if (((R.ch[p] >> sh) & 3) == 1) s -= R.gs[o][p];
-      }
-      if (has(i - di, j - dj)) {  // neighbour below chose b = q_c - q_{c-1}
-        const size_t m = g.at(i - di, j - dj);
-        if (((R.ch[m] >> sh) & 3) == 2) s += R.gs[o][m];
-      }
-      acc[v] += s;
-    }
-  }
-  double ge = acc[0], gu = acc[1], gv = acc[2], gbb = 0.0;
-  if (rc(i, j)) {
-    ge += R.gd[0][c];
-    gu += R.gd[1][c];
-    gv += R.gd[2][c];
-    gbb += R.gd[3][c];
-  }
-  double gh = ge;  // eta = h + b
-  gbb += ge;
-  if (i >= g.ng && i < ie && j >= g.ng && j < je) {
-    gh += R.ga[0][c];
-    gu += R.ga[1][c];
-    gv += R.ga[2][c];
-  }
-  gV.h[c] = gh;
-  gV.hu[c] = gu;
-  gV.hv[c] = gv;
-  gb[c] += gbb;
-}
-
-// Wall ghosts, reversed: a ghost's adjoint moves to the cell it mirrors
-// (normal momentum with a sign change); run S/N (pass 1) before W/E (pass 0).
-// With `bed`, fold the bed adjoint instead of the state's.
-__global__ void k_walls_adj(Grid g, FieldSet V, FieldSet gV, double* __restrict__ gb, int pass,
-                            int bed) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int side = blockIdx.y;
-  const int n_tan = pass == 0 ? g.nyt : g.nxt;
-  if (t >= n_tan) return;
-  // forward order k = 1..ng; mirrors are interior or earlier-filled cells, so
-  // reverse k = ng..1
-  for (int k = g.ng; k >= 1; --k) {
-    int ig, jg, im, jm;
-    if (pass == 0) {
-      jg = jm = t;
-      ig = side == 0 ? g.ng - k : g.nxt - g.ng + k - 1;
-      im = side == 0 ? g.ng + k - 1 : g.nxt - g.ng - k;
-    } else {
-      ig = im = t;
-      jg = side == 0 ? g.ng - k : g.nyt - g.ng + k - 1;
-      jm = side == 0 ? g.ng + k - 1 : g.nyt - g.ng - k;
-    }
-    const size_t q = g.at(ig, jg), m = g.at(im, jm);
-    if (bed) {
-      gb[m] += gb[q];
-      gb[q] = 0.0;
-      continue;
-    }
-    if (V.h[m] > 0.0) gV.h[m] += gV.h[q];  // h_g = max(0, h_m)
-    gV.h[q] = 0.0;
-    if (pass == 0) {
-      gV.hu[m] -= gV.hu[q];
-      gV.hv[m] += gV.hv[q];
-    } else {
-      gV.hv[m] -= gV.hv[q];
-      gV.hu[m] += gV.hu[q];
-    }
-    gV.hu[q] = 0.0;
-    gV.hv[q] = 0.0;
-  }
-}
-
-__global__ void k_gauges_adj(const int* __restrict__ gq, const double* __restrict__ r, int ng,
-                             FieldSet lam, double* __restrict__ gb) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= ng) return;
-  const size_t q = (size_t)gq[k];
-  lam.h[q] += 2.0 * r[k];  // gauges are distinct cells: no two threads share q
-  gb[q] += 2.0 * r[k];
-}
-
-__global__ void k_add(Grid g, FieldSet a, FieldSet b) {  // interior a += b
-  const int i = g.ng + blockIdx.x * kBX + threadIdx.x % kBX;
-  const int j = g.ng + blockIdx.y * kBY + threadIdx.x / kBX;
-  if (i >= g.nxt - g.ng || j >= g.nyt - g.ng) return;
-  const size_t c = g.at(i, j);
-  a.h[c] += b.h[c];
-  a.hu[c] += b.hu[c];
-  a.hv[c] += b.hv[c];
-}
-
-}  // namespace
-
-// ---------------------------------------------------------------------------
-// Host driver
-// ---------------------------------------------------------------------------
-
-#define ADJ_TRY(expr)                      \
-  do {                                     \
-    cudaError_t e_ = (expr);               \
-    if (e_ != cudaSuccess) return -1;      \
-  } while (0)
-
-class Adjoint {
- public:
-  ~Adjoint() {
-    for (auto& e : ev_)
-      if (e) cudaEventDestroy(e);
-    if (mem_) cudaFree(mem_);
-    if (obs_d_) cudaFree(obs_d_);
-    if (stream_) cudaStreamDestroy(stream_);
-  }
-
-  int create(int nx, int ny, int ng, double dx, double dy, double cfl, int hllc, int nsteps,
-             const double* h0, const double* hu0, const double* hv0, const int* gi, const int* gj,
-             int ngauge, std::string& err) {
-    if (nx < 2 || ny < 2 || ng < 2 || nsteps < 1 || ngauge < 0) {
-      err = "invalid sizes";
-      return -2;
-    }
-    g_.ng = ng;
-    g_.nxt = nx + 2 * ng;
-    g_.nyt = ny + 2 * ng;
-    g_.pitch = (g_.nxt + 31) / 32 * 32;
-    g_.dx = dx;
-    g_.dy = dy;
-    cfl_ = cfl;
-    hllc_ = hllc;
-    nsteps_ = nsteps;
-    ngauge_ = ngauge;
-    std::vector<int> gq(ngauge);
-    for (int k = 0; k < ngauge; ++k) {
-      if (gi[k] < 0 || gi[k] >= nx || gj[k] < 0 || gj[k] >= ny) {
-        err = "gauge outside the interior";
-        return -2;
-      }
-      gq[k] = (int)g_.at(gi[k] + ng, gj[k] + ng);
-      for (int m = 0; m < k; ++m)
-        if (gq[m] == gq[k]) {
-          err = "gauges must be distinct cells";
-          return -2;
-        }
-    }
-    K_ = std::max(1, (int)std::ceil(std::sqrt((double)nsteps)));
-    nck_ = (nsteps + K_ - 1) / K_ + 1;
-    if (cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking) != cudaSuccess) return -1;
-    const size_t f = (size_t)g_.pitch * g_.nyt;
-    // fields: b, n; U, Us, lam, lam*, gbase, gV (3 each); gb, gn; tapes
-    // (2 x 18); reverse scratch (3+3+8+8+6+4) + branch bits; checkpoints;
-    // segment states
-    nfields_ = 2 + 6 * 3 + 2 + 2 * 18 + (3 + 3 + 8 + 8 + 6 + 4) + 1 + 3 * (size_t)nck_ +
-               3 * (size_t)(K_ + 1);
-    const size_t bytes = nfields_ * f * sizeof(double) + 8 * (size_t)nsteps * ngauge + 64 +
-                         sizeof(int) * (size_t)ngauge + 1024;
-    if (cudaMalloc(&mem_, bytes) != cudaSuccess) {
-      mem_ = nullptr;
-      err = "device allocation failed";
-      return -1;
-    }
-    cudaMemsetAsync(mem_, 0, bytes, stream_);
-    double* p = (double*)mem_;
-    auto take = [&]() { double* q = p; p += f; return q; };
-    auto takeset = [&]() { FieldSet s{take(), take(), take()}; return s; };
-    b_ = take();
-    nf_ = take();
-    U_ = takeset();
-    Us_ = takeset();
-    lam_ = takeset();
-    lams_ = takeset();
-    gbase_ = takeset();
-    gV_ = takeset();
-    gb_ = take();
-    gn_ = take();
-    for (Tape* t : {&t1_, &t2_}) {
-      for (auto& x : t->s) x = take();
-      for (auto& x : t->fx) x = take();
-      for (auto& x : t->fy) x = take();
-    }
-    for (auto& x : R_.go) x = take();
-    for (auto& x : R_.ga) x = take();
-    for (auto& x : R_.gfx) x = take();
-    for (auto& x : R_.gfy) x = take();
-    for (auto& x : R_.gs) x = take();
-    for (auto& x : R_.gd) x = take();
-    R_.ch = (int*)take();
-    ck_.resize(nck_);
-    for (auto& c : ck_) c = takeset();
-    seg_.resize(K_ + 1);
-    for (auto& c : seg_) c = takeset();
-    r_ = p;
-    p += (size_t)nsteps * ngauge;
-    mx_ = (unsigned long long*)p;
-    p += 8;
-    gq_ = (int*)p;
-    ADJ_TRY(cudaMemcpyAsync(gq_, gq.data(), sizeof(int) * ngauge, cudaMemcpyHostToDevice, stream_));
-    // initial state: interior from the caller, F-order (nx, ny)
-    std::vector<double> tmp(f, 0.0);
-    const double* src[3] = {h0, hu0, hv0};
-    for (int k = 0; k < 3; ++k) {
-      std::fill(tmp.begin(), tmp.end(), 0.0);
-      for (int j = 0; j < ny; ++j)
-        for (int i = 0; i < nx; ++i) tmp[g_.at(i + ng, j + ng)] = src[k][(size_t)i + (size_t)j * nx];
-      double* d = k == 0 ? ck_[0].h : k == 1 ? ck_[0].hu : ck_[0].hv;
-      ADJ_TRY(cudaMemcpyAsync(d, tmp.data(), f * sizeof(double), cudaMemcpyHostToDevice, stream_));
-    }
-    ADJ_TRY(cudaStreamSynchronize(stream_));
-    dts_.assign(nsteps, 0.0);
-    obs_.assign((size_t)nsteps * ngauge, 0.0);
-    return 0;
-  }
-
-  int set_obs(const double* obs) {
-    std::memcpy(obs_.data(), obs, obs_.size() * sizeof(double));
-    obs_dev_dirty_ = true;
-    return 0;
-  }
-  int set_dt(const double* dts) {
-    std::memcpy(dts_.data(), dts, dts_.size() * sizeof(double));
-    have_dt_ = true;
-    return 0;
-  }
-  void get_dt(double* dts) const { std::memcpy(dts, dts_.data(), dts_.size() * sizeof(double)); }
-
-  // Forward run.  record: dt from the CFL condition of each state (stored);
-  // else the stored dt sequence.  J and, optionally, the gauge surfaces
-  // (nsteps x ngauge) are returned.
-  int forward(const double* b, const double* n, double n_scalar, bool record, double* J,
-              double* eta_out) {
-    if (!record && !have_dt_) return -2;
-    if (upload_params(b, n, n_scalar) != 0) return -1;
-    if (mark(0) != 0) return -1;
-    if (copy(U_, ck_[0]) != 0) return -1;
-    std::vector<double> r((size_t)nsteps_ * ngauge_);
-    for (int k = 0; k < nsteps_; ++k) {
-      if (record) {
-        double dt;
-        if (cfl_step(U_, dt) != 0) return -1;
-        dts_[k] = dt;
-      }
-      if (step(U_, U_, dts_[k]) != 0) return -1;
-      if (ngauge_ > 0) {
-        k_gauges<<<(ngauge_ + 127) / 128, 128, 0, stream_>>>(g_, U_, b_, gq_, obs_dev() + (size_t)k * ngauge_,
-                                                              ngauge_, r_ + (size_t)k * ngauge_);
-      }
-    }
-    if (record) have_dt_ = true;
-    if (mark(1) != 0) return -1;
-    ADJ_TRY(cudaMemcpyAsync(r.data(), r_, r.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_));
-    ADJ_TRY(cudaStreamSynchronize(stream_));
-    double acc = 0.0;
-    for (double x : r) acc += x * x;
-    *J = acc;
-    if (eta_out)
-      for (int k = 0; k < nsteps_; ++k)
-        for (int m = 0; m < ngauge_; ++m)
-          eta_out[(size_t)k * ngauge_ + m] = r[(size_t)k * ngauge_ + m] + obs_[(size_t)k * ngauge_ + m];
-    return 0;
-  }
-
-  // J and its gradient with respect to the interior bed and n field.
-  int gradient(const double* b, const double* n, double n_scalar, double* J, double* gb_out,
-               double* gn_out) {
-    if (!have_dt_) return -2;
-    if (upload_params(b, n, n_scalar) != 0) return -1;
-    const size_t f = (size_t)g_.pitch * g_.nyt;
-    if (mark(0) != 0) return -1;
-    // forward with checkpoints
-    if (copy(U_, ck_[0]) != 0) return -1;
-    for (int k = 0; k < nsteps_; ++k) {
-      if (step(U_, U_, dts_[k]) != 0) return -1;
-      if (ngauge_ > 0)
-        k_gauges<<<(ngauge_ + 127) / 128, 128, 0, stream_>>>(g_, U_, b_, gq_, obs_dev() + (size_t)k * ngauge_,
-                                                              ngauge_, r_ + (size_t)k * ngauge_);
-      if ((k + 1) % K_ == 0 && (k + 1) / K_ < nck_)
-        if (copy(ck_[(k + 1) / K_], U_) != 0) return -1;
-    }
-    std::vector<double> r((size_t)nsteps_ * ngauge_);
-    ADJ_TRY(cudaMemcpyAsync(r.data(), r_, r.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_));
-    // reverse
-    for (FieldSet* s : {&lam_}) {
-      ADJ_TRY(cudaMemsetAsync(s->h, 0, f * sizeof(double), stream_));
-      ADJ_TRY(cudaMemsetAsync(s->hu, 0, f * sizeof(double), stream_));
-      ADJ_TRY(cudaMemsetAsync(s->hv, 0, f * sizeof(double), stream_));
-    }
-    ADJ_TRY(cudaMemsetAsync(gb_, 0, f * sizeof(double), stream_));
-    ADJ_TRY(cudaMemsetAsync(gn_, 0, f * sizeof(double), stream_));
-    const int nseg = (nsteps_ + K_ - 1) / K_;
-    for (int s = nseg - 1; s >= 0; --s) {
-      const int k0 = s * K_, k1 = std::min(nsteps_, k0 + K_);
-      if (copy(seg_[0], ck_[s]) != 0) return -1;
-      for (int k = k0; k < k1 - 1; ++k)
-        if (step(seg_[k - k0], seg_[k - k0 + 1], dts_[k]) != 0) return -1;
-      for (int k = k1 - 1; k >= k0; --k) {
-        // misfit at U^{k+1}
-        if (ngauge_ > 0)
-          k_gauges_adj<<<(ngauge_ + 127) / 128, 128, 0, stream_>>>(gq_, r_ + (size_t)k * ngauge_, ngauge_,
-                                                                  lam_, gb_);
-        if (step_adj(seg_[k - k0], dts_[k]) != 0) return -1;
-      }
-    }
-    // bed ghosts mirror interior cells: fold their adjoints in (S/N then W/E)
-    walls_adj(gV_, true);
-    if (mark(1) != 0) return -1;
-    ADJ_TRY(cudaStreamSynchronize(stream_));
-    double acc = 0.0;
-    for (double x : r) acc += x * x;
-    *J = acc;
-    const int nx = g_.nx_phys(), ny = g_.ny_phys();
-    std::vector<double> tmp(f);
-    ADJ_TRY(cudaMemcpy(tmp.data(), gb_, f * sizeof(double), cudaMemcpyDeviceToHost));
-    for (int j = 0; j < ny; ++j)
-      for (int i = 0; i < nx; ++i)
-        gb_out[(size_t)i + (size_t)j * nx] = tmp[g_.at(i + g_.ng, j + g_.ng)];
-    ADJ_TRY(cudaMemcpy(tmp.data(), gn_, f * sizeof(double), cudaMemcpyDeviceToHost));
-    for (int j = 0; j < ny; ++j)
-      for (int i = 0; i < nx; ++i)
-        gn_out[(size_t)i + (size_t)j * nx] = tmp[g_.at(i + g_.ng, j + g_.ng)];
-    return 0;
-  }
-
-  int checkpoint_interval() const { return K_; }
-  // Device milliseconds of the last forward / gradient run (CUDA events on
-  // the adjoint's stream, from the initial state to the last kernel).
-  double last_ms() {
-    float f = 0.0f;
-    if (!ev_[0] || cudaEventSynchronize(ev_[1]) != cudaSuccess ||
-        cudaEventElapsedTime(&f, ev_[0], ev_[1]) != cudaSuccess)
-      return -1.0;
-    return f;
-  }
-
- private:
-  int mark(int k) {
-    if (!ev_[k] && cudaEventCreate(&ev_[k]) != cudaSuccess) return -1;
-    return cudaEventRecord(ev_[k], stream_) == cudaSuccess ? 0 : -1;
-  }
-  cudaEvent_t ev_[2] = {nullptr, nullptr};
-
-  dim3 blocks(int x0, int x1, int y0, int y1) const {  // cover [x0, x1] x [y0, y1]
-    return dim3((unsigned)((x1 - x0 + kBX) / kBX), (unsigned)((y1 - y0 + kBY) / kBY));
-  }
-  const double* obs_dev() {
-    if (obs_dev_dirty_) {
-      if (!obs_d_) cudaMalloc(&obs_d_, obs_.size() * sizeof(double) + 8);
-      cudaMemcpyAsync(obs_d_, obs_.data(), obs_.size() * sizeof(double), cudaMemcpyHostToDevice, stream_);
-      obs_dev_dirty_ = false;
-    }
-    return obs_d_;
-  }
-
-  int upload_params(const double* b, const double* n, double n_scalar) {
-    const int nx = g_.nx_phys(), ny = g_.ny_phys();
-    const size_t f = (size_t)g_.pitch * g_.nyt;
-    std::vector<double> tb(f, 0.0), tn(f, 0.0);
-    for (int j = 0; j < ny; ++j)
-      for (int i = 0; i < nx; ++i) {
-        const size_t q = g_.at(i + g_.ng, j + g_.ng), s = (size_t)i + (size_t)j * nx;
-        tb[q] = b[s];
-        tn[q] = n ? n[s] : n_scalar;
-      }
-    ADJ_TRY(cudaMemcpyAsync(b_, tb.data(), f * sizeof(double), cudaMemcpyHostToDevice, stream_));
-    ADJ_TRY(cudaMemcpyAsync(nf_, tn.data(), f * sizeof(double), cudaMemcpyHostToDevice, stream_));
-    return cudaStreamSynchronize(stream_) == cudaSuccess ? 0 : -1;
-  }
-
-  int copy(FieldSet& dst, const FieldSet& src) {
-    const size_t bytes = (size_t)g_.pitch * g_.nyt * sizeof(double);
-    ADJ_TRY(cudaMemcpyAsync(dst.h, src.h, bytes, cudaMemcpyDeviceToDevice, stream_));
-    ADJ_TRY(cudaMemcpyAsync(dst.hu, src.hu, bytes, cudaMemcpyDeviceToDevice, stream_));
-    ADJ_TRY(cudaMemcpyAsync(dst.hv, src.hv, bytes, cudaMemcpyDeviceToDevice, stream_));
-    return 0;
-  }
-
-  void walls(FieldSet V) {
-    const int tpb = 128;
-    k_walls<<<dim3((unsigned)((g_.nyt + tpb - 1) / tpb), 2), tpb, 0, stream_>>>(g_, V, b_, 0);
-    k_walls<<<dim3((unsigned)((g_.nxt + tpb - 1) / tpb), 2), tpb, 0, stream_>>>(g_, V, b_, 1);
-  }
-
-  void walls_adj(FieldSet V, bool bed) {
-    const int tpb = 128;
-    k_walls_adj<<<dim3((unsigned)((g_.nxt + tpb - 1) / tpb), 2), tpb, 0, stream_>>>(g_, V, gV_, gb_, 1,
-                                                                                      bed ? 1 : 0);
-    k_walls_adj<<<dim3((unsigned)((g_.nyt + tpb - 1) / tpb), 2), tpb, 0, stream_>>>(g_, V, gV_, gb_, 0,
-                                                                                      bed ? 1 : 0);
-  }
-
-  void tape(FieldSet V, Tape& T) {
-    const int ie = g_.nxt - g_.ng, je = g_.nyt - g_.ng;
-    k_slopes<<<blocks(g_.ng - 1, ie, g_.ng - 1, je), kBX * kBY, 0, stream_>>>(g_, V, b_, T);
-    if (hllc_)
-      k_faces<true><<<blocks(g_.ng, ie, g_.ng, je), kBX * kBY, 0, stream_>>>(g_, V, b_, T);
-    else
-      k_faces<false><<<blocks(g_.ng, ie, g_.ng, je), kBX * kBY, 0, stream_>>>(g_, V, b_, T);
-  }
-
-  dim3 interior() const {
-    return blocks(g_.ng, g_.nxt - g_.ng - 1, g_.ng, g_.nyt - g_.ng - 1);
-  }
-
-  // One step U -> out.  out may alias U: stage 2 reads the RK2 base only at
-  // the cell it writes, and its neighbours come from the stage-1 result.
-  int step(FieldSet U, FieldSet out, double dt) {
-    walls(U);
-    tape(U, t1_);
-    k_cells<<<interior(), kBX * kBY, 0, stream_>>>(g_, U, U, nf_, t1_, dt, 1, Us_);
-    walls(Us_);
-    tape(Us_, t2_);
-    k_cells<<<interior(), kBX * kBY, 0, stream_>>>(g_, Us_, U, nf_, t2_, dt, 2, out);
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
-  }
-
-  int cfl_step(FieldSet U, double& dt) {
-    unsigned long long h[2] = {0, 0};
-    ADJ_TRY(cudaMemsetAsync(mx_, 0, 2 * sizeof(unsigned long long), stream_));
-    k_speeds<<<interior(), kBX * kBY, 0, stream_>>>(g_, U, mx_);
-    ADJ_TRY(cudaMemcpyAsync(h, mx_, sizeof(h), cudaMemcpyDeviceToHost, stream_));
-    ADJ_TRY(cudaStreamSynchronize(stream_));
-    double sx, sy;
-    std::memcpy(&sx, &h[0], 8);
-    std::memcpy(&sy, &h[1], 8);
-    dt = cfl_dt(sx, sy, g_, cfl_);
-    return 0;
-  }
-
-  // Reverse of one stage: gout (adjoint of the stage output, interior) ->
-  // gV_ (adjoint of the stage input after the wall fold), gbase_ (stage 2).
-  int stage_adj(FieldSet V, FieldSet base, Tape& T, double dt, int stage, FieldSet gout) {
-    const int ie = g_.nxt - g_.ng, je = g_.nyt - g_.ng;
-    const size_t fb = (size_t)g_.pitch * g_.nyt * sizeof(double);
-    ADJ_TRY(cudaMemsetAsync(gV_.h, 0, fb, stream_));  // the outer ghost layers are not gathered
-    ADJ_TRY(cudaMemsetAsync(gV_.hu, 0, fb, stream_));
-    ADJ_TRY(cudaMemsetAsync(gV_.hv, 0, fb, stream_));
-    k_cells_adj<<<interior(), kBX * kBY, 0, stream_>>>(g_, V, base, nf_, T, dt, stage, gout, R_,
-                                                         gbase_, gn_);
-    if (hllc_)
-      k_faces_adj<true><<<blocks(g_.ng, ie, g_.ng, je), kBX * kBY, 0, stream_>>>(g_, V, b_, T, R_);
-    else
-      k_faces_adj<false><<<blocks(g_.ng, ie, g_.ng, je), kBX * kBY, 0, stream_>>>(g_, V, b_, T, R_);
-    k_recon_adj<<<blocks(g_.ng - 1, ie, g_.ng - 1, je), kBX * kBY, 0, stream_>>>(g_, V, b_, R_);
-    k_gather_adj<<<blocks(g_.ng - 2, ie + 1, g_.ng - 2, je + 1), kBX * kBY, 0, stream_>>>(g_, R_, gV_, gb_);
-    walls_adj(V, false);
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
-  }
-
-  // Reverse of the step from U (= U^k): lam_ (adjoint of U^{k+1}) -> lam_
-  // (adjoint of U^k).  Recomputes U* and both tapes.
-  int step_adj(FieldSet U, double dt) {
-    walls(U);
-    tape(U, t1_);
-    k_cells<<<interior(), kBX * kBY, 0, stream_>>>(g_, U, U, nf_, t1_, dt, 1, Us_);
-    walls(Us_);
-    tape(Us_, t2_);
-    if (stage_adj(Us_, U, t2_, dt, 2, lam_) != 0) return -1;  // gV_ = adjoint of U*
-    if (copy(lams_, gV_) != 0) return -1;
-    if (stage_adj(U, U, t1_, dt, 1, lams_) != 0) return -1;  // gV_ = adjoint of U^k (stage 1)
-    k_add<<<interior(), kBX * kBY, 0, stream_>>>(g_, gV_, gbase_);
-    return copy(lam_, gV_);
-  }
-
-  Grid g_{};
-  double cfl_ = 0.45;
-  int hllc_ = 0, nsteps_ = 0, ngauge_ = 0, K_ = 1, nck_ = 1;
-  size_t nfields_ = 0;
-  cudaStream_t stream_ = nullptr;
-  void* mem_ = nullptr;
-  double *b_ = nullptr, *nf_ = nullptr, *gb_ = nullptr, *gn_ = nullptr, *r_ = nullptr;
-  double* obs_d_ = nullptr;
-  unsigned long long* mx_ = nullptr;
-  int* gq_ = nullptr;
-  FieldSet U_{}, Us_{}, lam_{}, lams_{}, gbase_{}, gV_{};
-  Tape t1_{}, t2_{};
-  Rev R_{};
-  std::vector<FieldSet> ck_, seg_;
-  std::vector<double> dts_, obs_;
-  bool have_dt_ = false, obs_dev_dirty_ = true;
-};
+void set_last_error(const std::string& msg);
 
 }  // namespace rkb
 
@@ -849,76 +21,98 @@ class Adjoint {
 // C ABI (declared in include/rakali.h)
 // ---------------------------------------------------------------------------
 
-namespace rkb {
-void set_last_error(const std::string& msg);
-}
+namespace {
+rkb::AdjointBase* as_adj(void* a) { return static_cast<rkb::AdjointBase*>(a); }
+}  // namespace
 
 extern "C" {
 
-int rkb_adjoint_create(int nx, int ny, int nghost, double dx, double dy, double cfl, int use_hllc,
-                       int n_steps, const double* h0, const double* hu0, const double* hv0,
-                       const int* gauge_i, const int* gauge_j, int n_gauges, void** adj) {
+int rkb_adjoint_batch_create(int precision, int n_members, int nx, int ny, int nghost, double dx,
+                             double dy, double cfl, int use_hllc, int n_steps, const double* h0,
+                             const double* hu0, const double* hv0, const int* gauge_i,
+                             const int* gauge_j, int n_gauges, void** adj) {
   if (!adj) return -2;
   *adj = nullptr;
+  if (precision != 32 && precision != 64) {
+    rkb::set_last_error("precision must be 32 or 64");
+    return -2;
+  }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) {
     rkb::set_last_error("no CUDA device available");
     return -1;
   }
-  auto* a = new rkb::Adjoint();
   std::string err;
-  const int rc = a->create(nx, ny, nghost, dx, dy, cfl, use_hllc, n_steps, h0, hu0, hv0, gauge_i,
-                           gauge_j, n_gauges, err);
-  if (rc != 0) {
-    delete a;
+  int rc = 0;
+  rkb::AdjointBase* a =
+      precision == 64
+          ? rkb::make_adjoint64(n_members, nx, ny, nghost, dx, dy, cfl, use_hllc, n_steps, h0, hu0,
+                                hv0, gauge_i, gauge_j, n_gauges, err, rc)
+          : rkb::make_adjoint32(n_members, nx, ny, nghost, dx, dy, cfl, use_hllc, n_steps, h0, hu0,
+                                hv0, gauge_i, gauge_j, n_gauges, err, rc);
+  if (!a) {
     rkb::set_last_error(err.empty() ? "adjoint setup failed" : err);
-    return rc;
+    return rc != 0 ? rc : -1;
   }
   *adj = a;
   return 0;
 }
 
+int rkb_adjoint_create(int nx, int ny, int nghost, double dx, double dy, double cfl, int use_hllc,
+                       int n_steps, const double* h0, const double* hu0, const double* hv0,
+                       const int* gauge_i, const int* gauge_j, int n_gauges, void** adj) {
+  return rkb_adjoint_batch_create(64, 1, nx, ny, nghost, dx, dy, cfl, use_hllc, n_steps, h0, hu0,
+                                  hv0, gauge_i, gauge_j, n_gauges, adj);
+}
+
 void rkb_adjoint_destroy(void** adj) {
   if (!adj || !*adj) return;
-  delete static_cast<rkb::Adjoint*>(*adj);
+  delete as_adj(*adj);
   *adj = nullptr;
 }
 
 int rkb_adjoint_set_obs(void* adj, const double* obs) {
   if (!adj || !obs) return -2;
-  return static_cast<rkb::Adjoint*>(adj)->set_obs(obs);
+  return as_adj(adj)->set_obs(obs);
 }
 
 int rkb_adjoint_set_dt(void* adj, const double* dts) {
   if (!adj || !dts) return -2;
-  return static_cast<rkb::Adjoint*>(adj)->set_dt(dts);
+  return as_adj(adj)->set_dt(dts);
 }
 
 int rkb_adjoint_get_dt(void* adj, double* dts) {
   if (!adj || !dts) return -2;
-  static_cast<rkb::Adjoint*>(adj)->get_dt(dts);
+  as_adj(adj)->get_dt(dts);
   return 0;
 }
 
 int rkb_adjoint_forward(void* adj, const double* b, const double* n_field, double n_scalar,
                         int record_dt, double* J, double* eta_gauges) {
   if (!adj || !b || !J) return -2;
-  return static_cast<rkb::Adjoint*>(adj)->forward(b, n_field, n_scalar, record_dt != 0, J,
-                                                  eta_gauges);
+  return as_adj(adj)->forward(b, n_field, n_scalar, record_dt != 0, J, eta_gauges);
 }
 
 int rkb_adjoint_gradient(void* adj, const double* b, const double* n_field, double n_scalar,
                          double* J, double* grad_b, double* grad_n) {
   if (!adj || !b || !J || !grad_b || !grad_n) return -2;
-  return static_cast<rkb::Adjoint*>(adj)->gradient(b, n_field, n_scalar, J, grad_b, grad_n);
+  return as_adj(adj)->gradient(b, n_field, n_scalar, J, grad_b, grad_n);
 }
 
 int rkb_adjoint_checkpoint_interval(void* adj) {
-  return adj ? static_cast<rkb::Adjoint*>(adj)->checkpoint_interval() : -2;
+  return adj ? as_adj(adj)->checkpoint_interval() : -2;
 }
 
-double rkb_adjoint_last_ms(void* adj) {
-  return adj ? static_cast<rkb::Adjoint*>(adj)->last_ms() : -1.0;
+double rkb_adjoint_last_ms(void* adj) { return adj ? as_adj(adj)->last_ms() : -1.0; }
+
+int rkb_adjoint_members(void* adj) { return adj ? as_adj(adj)->members() : -2; }
+
+int rkb_adjoint_precision(void* adj) { return adj ? as_adj(adj)->precision() : -2; }
+
+int rkb_adjoint_mass(void* adj, double* out) {
+  if (!adj || !out) return -2;
+  as_adj(adj)->mass(out);
+  return 0;
 }
 
 // Host builds of the face and cell derivatives, for finite-difference checks.

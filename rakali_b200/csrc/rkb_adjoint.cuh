@@ -1,4 +1,4 @@
-// Reverse-mode derivatives of the structured step's pointwise pieces (FP64).
+// Reverse-mode derivatives of the structured step's pointwise pieces.
 //
 // Each *_adj function recomputes the forward values it needs from the same
 // inputs as the forward function (rkb_face.cuh, rkb_common.cuh) and
@@ -15,11 +15,17 @@
 
 namespace rkb {
 
+// h^(1/3): correctly rounded in FP64 (the production step's friction term),
+// the CUDA / libm cube root in FP32.
+RKB_HD double pow_third(double h) { return cr_pow_third(h); }
+RKB_HD float pow_third(float h) { return cbrtf(h); }
+
 // Derivative of velocity(): u = q/h when h > DRY_THRESHOLD, else 0.
-RKB_HD void velocity_adj(double h, double qx, double qy, double gu, double gv, double& gh,
-                         double& gqx, double& gqy) {
-  if (h > kDry) {
-    const double u = qx / h, v = qy / h;
+template <typename T>
+RKB_HD void velocity_adj(T h, T qx, T qy, T gu, T gv, T& gh,
+                         T& gqx, T& gqy) {
+  if (h > T(kDry)) {
+    const T u = qx / h, v = qy / h;
     gqx += gu / h;
     gqy += gv / h;
     gh += -(gu * u + gv * v) / h;
@@ -28,82 +34,82 @@ RKB_HD void velocity_adj(double h, double qx, double qy, double gu, double gv, d
 
 // Adjoint of riemann<DIR, HLLC>(hl, qxl, qyl, hr, qxr, qyr) given the output
 // adjoints (gfh, gfqx, gfqy); accumulates into g[6] = (hl, qxl, qyl, hr, qxr, qyr).
-template <int DIR, bool HLLC>
-RKB_HD void riemann_adj(double hl, double qxl, double qyl, double hr, double qxr, double qyr,
-                        double gfh, double gfqx, double gfqy, double g[6]) {
-  double ul, vl, ur, vr;
+template <int DIR, bool HLLC, typename T>
+RKB_HD void riemann_adj(T hl, T qxl, T qyl, T hr, T qxr, T qyr,
+                        T gfh, T gfqx, T gfqy, T g[6]) {
+  T ul, vl, ur, vr;
   velocity(hl, qxl, qyl, ul, vl);
   velocity(hr, qxr, qyr, ur, vr);
-  const double al = sqrt(kG * pos(hl));
-  const double ar = sqrt(kG * pos(hr));
-  const double nl = DIR == 0 ? ul : vl;
-  const double nr = DIR == 0 ? ur : vr;
+  const T al = sqrt(T(kG) * pos(hl));
+  const T ar = sqrt(T(kG) * pos(hr));
+  const T nl = DIR == 0 ? ul : vl;
+  const T nr = DIR == 0 ? ur : vr;
   int branch;
-  double sl, sr;
+  T sl, sr;
   bool sl_first = true, sr_first = true;  // which argument of min / max was taken
-  if (hr <= kDry) {
+  if (hr <= T(kDry)) {
     branch = 0;
     sl = nl - al;
-    sr = nl + 2.0 * al;
-  } else if (hl <= kDry) {
+    sr = nl + T(2) * al;
+  } else if (hl <= T(kDry)) {
     branch = 1;
-    sl = nr - 2.0 * ar;
+    sl = nr - T(2) * ar;
     sr = nr + ar;
   } else {
     branch = 2;
-    const double a1 = nl - al, a2 = nr - ar, b1 = nl + al, b2 = nr + ar;
+    const T a1 = nl - al, a2 = nr - ar, b1 = nl + al, b2 = nr + ar;
     sl_first = a1 < a2;  // dmin(a, b) = a < b ? a : b
     sl = sl_first ? a1 : a2;
     sr_first = b1 > b2;  // dmax(a, b) = a > b ? a : b
     sr = sr_first ? b1 : b2;
   }
   // side fluxes L, R (h, x, y components) and states U
-  double L[3], R[3];
+  T L[3], R[3];
   if (DIR == 0) {
-    L[0] = qxl; L[1] = qxl * ul + kHalfG * hl * hl; L[2] = qxl * vl;
-    R[0] = qxr; R[1] = qxr * ur + kHalfG * hr * hr; R[2] = qxr * vr;
+    L[0] = qxl; L[1] = qxl * ul + T(kHalfG) * hl * hl; L[2] = qxl * vl;
+    R[0] = qxr; R[1] = qxr * ur + T(kHalfG) * hr * hr; R[2] = qxr * vr;
   } else {
-    L[0] = qyl; L[1] = qxl * vl; L[2] = qyl * vl + kHalfG * hl * hl;
-    R[0] = qyr; R[1] = qxr * vr; R[2] = qyr * vr + kHalfG * hr * hr;
+    L[0] = qyl; L[1] = qxl * vl; L[2] = qyl * vl + T(kHalfG) * hl * hl;
+    R[0] = qyr; R[1] = qxr * vr; R[2] = qyr * vr + T(kHalfG) * hr * hr;
   }
-  const double UL[3] = {hl, qxl, qyl}, UR[3] = {hr, qxr, qyr};
-  double gF[3] = {gfh, gfqx, gfqy};
-  double gL[3] = {0, 0, 0}, gR[3] = {0, 0, 0}, gUL[3] = {0, 0, 0}, gUR[3] = {0, 0, 0};
-  double gsl = 0.0, gsr = 0.0;
-  double gul = 0.0, gvl = 0.0, gur = 0.0, gvr = 0.0;
-  if (sl >= 0.0) {
+  const T UL[3] = {hl, qxl, qyl}, UR[3] = {hr, qxr, qyr};
+  T gF[3] = {gfh, gfqx, gfqy};
+  T gL[3] = {0, 0, 0}, gR[3] = {0, 0, 0}, gUL[3] = {0, 0, 0}, gUR[3] = {0, 0, 0};
+  T gsl = T(0), gsr = T(0);
+  T gul = T(0), gvl = T(0), gur = T(0), gvr = T(0);
+  if (sl >= T(0)) {
     for (int k = 0; k < 3; ++k) gL[k] += gF[k];
-  } else if (sr <= 0.0) {
+  } else if (sr <= T(0)) {
     for (int k = 0; k < 3; ++k) gR[k] += gF[k];
   } else {
-    const double inv = 1.0 / (sr - sl);
-    const double slsr = sl * sr;
+    const T inv = T(1) / (sr - sl);
+    const T slsr = sl * sr;
     const int t = DIR == 0 ? 2 : 1;  // tangential component
     if (HLLC) {
       // tangential flux = fh * (upwind tangential velocity) (rki_kernel_flux.F90:584-783)
-      const double un_l = DIR == 0 ? ul : vl, un_r = DIR == 0 ? ur : vr;
-      const double ut_l = DIR == 0 ? vl : ul, ut_r = DIR == 0 ? vr : ur;
-      const double hrr = hr, hll = hl;
-      const double den = hrr * (un_r - sr) - hll * (un_l - sl);
-      double ss;
-      if (fabs(den) > kDry)
+      const T un_l = DIR == 0 ? ul : vl, un_r = DIR == 0 ? ur : vr;
+      const T ut_l = DIR == 0 ? vl : ul, ut_r = DIR == 0 ? vr : ur;
+      const T hrr = hr, hll = hl;
+      const T den = hrr * (un_r - sr) - hll * (un_l - sl);
+      T ss;
+      if (fabs(den) > T(kDry))
         ss = (sl * hrr * (un_r - sr) - sr * hll * (un_l - sl)) / den;
       else
-        ss = 0.5 * (un_l + un_r);
-      const double fh = (sr * L[0] - sl * R[0] + slsr * (UR[0] - UL[0])) * inv;
-      const double gt = gF[t];
-      gF[0] += gt * (ss >= 0.0 ? ut_l : ut_r);
-      if (ss >= 0.0) {
+        ss = T(0.5) * (un_l + un_r);
+      const T fh = (sr * L[0] - sl * R[0] + slsr * (UR[0] - UL[0])) * inv;
+      const T gt = gF[t];
+      gF[0] += gt * (ss >= T(0) ? ut_l : ut_r);
+      if (ss >= T(0)) {
         if (DIR == 0) gvl += gt * fh; else gul += gt * fh;
       } else {
         if (DIR == 0) gvr += gt * fh; else gur += gt * fh;
       }
-      gF[t] = 0.0;
+      gF[t] = T(0);
     }
     for (int k = 0; k < 3; ++k) {
       if (HLLC && k == t) continue;
-      const double d = UR[k] - UL[k];
-      const double F = (sr * L[k] - sl * R[k] + slsr * d) * inv;
+      const T d = UR[k] - UL[k];
+      const T F = (sr * L[k] - sl * R[k] + slsr * d) * inv;
       gL[k] += gF[k] * sr * inv;
       gR[k] += -gF[k] * sl * inv;
       gUR[k] += gF[k] * slsr * inv;
@@ -113,41 +119,41 @@ RKB_HD void riemann_adj(double hl, double qxl, double qyl, double hr, double qxr
     }
   }
   // wave speeds
-  double gnl = 0.0, gnr = 0.0, gal = 0.0, gar = 0.0;
+  T gnl = T(0), gnr = T(0), gal = T(0), gar = T(0);
   if (branch == 0) {
     gnl += gsl + gsr;
-    gal += -gsl + 2.0 * gsr;
+    gal += -gsl + T(2) * gsr;
   } else if (branch == 1) {
     gnr += gsl + gsr;
-    gar += -2.0 * gsl + gsr;
+    gar += -T(2) * gsl + gsr;
   } else {
     if (sl_first) { gnl += gsl; gal -= gsl; } else { gnr += gsl; gar -= gsl; }
     if (sr_first) { gnl += gsr; gal += gsr; } else { gnr += gsr; gar += gsr; }
   }
   if (DIR == 0) { gul += gnl; gur += gnr; } else { gvl += gnl; gvr += gnr; }
-  double ghl = 0.0, ghr = 0.0;
-  if (al > 0.0) ghl += gal * kG / (2.0 * al);
-  if (ar > 0.0) ghr += gar * kG / (2.0 * ar);
+  T ghl = T(0), ghr = T(0);
+  if (al > T(0)) ghl += gal * T(kG) / (T(2) * al);
+  if (ar > T(0)) ghr += gar * T(kG) / (T(2) * ar);
   // side fluxes -> (q, u, v, h)
-  double gqxl = 0.0, gqyl = 0.0, gqxr = 0.0, gqyr = 0.0;
+  T gqxl = T(0), gqyl = T(0), gqxr = T(0), gqyr = T(0);
   if (DIR == 0) {
     gqxl += gL[0] + gL[1] * ul + gL[2] * vl;
     gul += gL[1] * qxl;
     gvl += gL[2] * qxl;
-    ghl += gL[1] * 2.0 * kHalfG * hl;
+    ghl += gL[1] * T(2) * T(kHalfG) * hl;
     gqxr += gR[0] + gR[1] * ur + gR[2] * vr;
     gur += gR[1] * qxr;
     gvr += gR[2] * qxr;
-    ghr += gR[1] * 2.0 * kHalfG * hr;
+    ghr += gR[1] * T(2) * T(kHalfG) * hr;
   } else {
     gqyl += gL[0] + gL[2] * vl;
     gqxl += gL[1] * vl;
     gvl += gL[1] * qxl + gL[2] * qyl;
-    ghl += gL[2] * 2.0 * kHalfG * hl;
+    ghl += gL[2] * T(2) * T(kHalfG) * hl;
     gqyr += gR[0] + gR[2] * vr;
     gqxr += gR[1] * vr;
     gvr += gR[1] * qxr + gR[2] * qyr;
-    ghr += gR[2] * 2.0 * kHalfG * hr;
+    ghr += gR[2] * T(2) * T(kHalfG) * hr;
   }
   ghl += gUL[0]; gqxl += gUL[1]; gqyl += gUL[2];
   ghr += gUR[0]; gqxr += gUR[1]; gqyr += gUR[2];
@@ -160,89 +166,90 @@ RKB_HD void riemann_adj(double hl, double qxl, double qyl, double hr, double qxr
 // Adjoint of face_flux<DIR, HLLC>(eL, qxL, qyL, bL, eR, qxR, qyR, bR) given
 // gout = adjoints of (fh, fqx, fqy, wbR, hL2, pL2); accumulates into
 // gin[8] = (eL, qxL, qyL, bL, eR, qxR, qyR, bR).
-template <int DIR, bool HLLC>
-RKB_HD void face_adj(double eL, double qxL, double qyL, double bL, double eR, double qxR,
-                     double qyR, double bR, const double gout[6], double gin[8]) {
-  const double hL = pos(eL - bL);
-  const double hR = pos(eR - bR);
+template <int DIR, bool HLLC, typename T>
+RKB_HD void face_adj(T eL, T qxL, T qyL, T bL, T eR, T qxR,
+                     T qyR, T bR, const T gout[6], T gin[8]) {
+  const T hL = pos(eL - bL);
+  const T hR = pos(eR - bR);
   const bool bl_max = bL > bR;  // dmax(bL, bR) = bL > bR ? bL : bR
-  const double bmax = bl_max ? bL : bR;
-  const double xl = hL + bL - bmax, xr = hR + bR - bmax;
-  const double hyl = pos(xl);
-  const double hyr = pos(xr);
-  double ul, vl, ur, vr;
+  const T bmax = bl_max ? bL : bR;
+  const T xl = hL + bL - bmax, xr = hR + bR - bmax;
+  const T hyl = pos(xl);
+  const T hyr = pos(xr);
+  T ul, vl, ur, vr;
   velocity(hL, qxL, qyL, ul, vl);
   velocity(hR, qxR, qyR, ur, vr);
-  double gr[6] = {0, 0, 0, 0, 0, 0};
+  T gr[6] = {0, 0, 0, 0, 0, 0};
   riemann_adj<DIR, HLLC>(hyl, hyl * ul, hyl * vl, hyr, hyr * ur, hyr * vr, gout[0], gout[1],
                          gout[2], gr);
-  double ghyl = gr[0], ghyr = gr[3];
-  double gul = 0.0, gvl = 0.0, gur = 0.0, gvr = 0.0;
+  T ghyl = gr[0], ghyr = gr[3];
+  T gul = T(0), gvl = T(0), gur = T(0), gvr = T(0);
   ghyl += gr[1] * ul + gr[2] * vl;
   gul += gr[1] * hyl;
   gvl += gr[2] * hyl;
   ghyr += gr[4] * ur + gr[5] * vr;
   gur += gr[4] * hyr;
   gvr += gr[5] * hyr;
-  double ghL = 0.0, ghR = 0.0;
-  ghyr += 2.0 * hyr * gout[3];
-  ghR += -2.0 * hR * gout[3];
-  ghyl += 2.0 * hyl * gout[4];
-  ghL += 2.0 * hL * gout[5];
-  double gqxL = 0.0, gqyL = 0.0, gqxR = 0.0, gqyR = 0.0;
+  T ghL = T(0), ghR = T(0);
+  ghyr += T(2) * hyr * gout[3];
+  ghR += -T(2) * hR * gout[3];
+  ghyl += T(2) * hyl * gout[4];
+  ghL += T(2) * hL * gout[5];
+  T gqxL = T(0), gqyL = T(0), gqxR = T(0), gqyR = T(0);
   velocity_adj(hL, qxL, qyL, gul, gvl, ghL, gqxL, gqyL);
   velocity_adj(hR, qxR, qyR, gur, gvr, ghR, gqxR, gqyR);
-  double gbL = 0.0, gbR = 0.0, gbmax = 0.0;
-  if (xl > 0.0) { ghL += ghyl; gbL += ghyl; gbmax -= ghyl; }
-  if (xr > 0.0) { ghR += ghyr; gbR += ghyr; gbmax -= ghyr; }
+  T gbL = T(0), gbR = T(0), gbmax = T(0);
+  if (xl > T(0)) { ghL += ghyl; gbL += ghyl; gbmax -= ghyl; }
+  if (xr > T(0)) { ghR += ghyr; gbR += ghyr; gbmax -= ghyr; }
   if (bl_max) gbL += gbmax; else gbR += gbmax;
-  double geL = 0.0, geR = 0.0;
-  if (eL - bL > 0.0) { geL += ghL; gbL -= ghL; }
-  if (eR - bR > 0.0) { geR += ghR; gbR -= ghR; }
+  T geL = T(0), geR = T(0);
+  if (eL - bL > T(0)) { geL += ghL; gbL -= ghL; }
+  if (eR - bR > T(0)) { geR += ghR; gbR -= ghR; }
   gin[0] += geL; gin[1] += gqxL; gin[2] += gqyL; gin[3] += gbL;
   gin[4] += geR; gin[5] += gqxR; gin[6] += gqyR; gin[7] += gbR;
 }
 
 // Adjoint of protect(h, u, v) at input (h, u, v): (gh, gu, gv) are the output
 // adjoints on entry and the input adjoints on return.
-RKB_HD void protect_adj(double h, double u, double v, double& gh, double& gu, double& gv) {
-  if (h < 0.0) {
-    gh = 0.0; gu = 0.0; gv = 0.0;
+template <typename T>
+RKB_HD void protect_adj(T h, T u, T v, T& gh, T& gu, T& gv) {
+  if (h < T(0)) {
+    gh = T(0); gu = T(0); gv = T(0);
     return;
   }
-  if (h < kDry) {
-    gu = 0.0; gv = 0.0;
+  if (h < T(kDry)) {
+    gu = T(0); gv = T(0);
     return;
   }
   // forward with intermediates
-  const double h2 = h * h;
-  const double h4 = h2 * h2;
-  const bool kp = h4 < kEps4;
-  double u1 = u, v1 = v, r = 0.0;
+  const T h2 = h * h;
+  const T h4 = h2 * h2;
+  const bool kp = h4 < T(kEps4);
+  T u1 = u, v1 = v, r = T(0);
   if (kp) {
-    r = sqrt(h4 + kEps4);
-    u1 = h * (kSqrt2 * h * u / r);
-    v1 = h * (kSqrt2 * h * v / r);
+    r = sqrt(h4 + T(kEps4));
+    u1 = h * (T(kSqrt2) * h * u / r);
+    v1 = h * (T(kSqrt2) * h * v / r);
   }
-  const double sp2 = (u1 * u1 + v1 * v1) / (h * h);
-  const double fr2 = kFroude * kFroude * kG * h;
-  double ghh = gh, gu1 = gu, gv1 = gv;
+  const T sp2 = (u1 * u1 + v1 * v1) / (h * h);
+  const T fr2 = T(kFroude) * T(kFroude) * T(kG) * h;
+  T ghh = gh, gu1 = gu, gv1 = gv;
   if (sp2 > fr2) {
     // u2 = u1 sqrt(fr2 / sp2) = u1 sqrt(F^2 g h^3 / (u1^2 + v1^2))
-    const double sc = sqrt(fr2 / sp2);
-    const double q2 = u1 * u1 + v1 * v1;
+    const T sc = sqrt(fr2 / sp2);
+    const T q2 = u1 * u1 + v1 * v1;
     // d sc / d u1 = -sc u1 / q2, d sc / d h = 1.5 sc / h
-    const double gsc = gu * u1 + gv * v1;
+    const T gsc = gu * u1 + gv * v1;
     gu1 = gu * sc - gsc * sc * u1 / q2;
     gv1 = gv * sc - gsc * sc * v1 / q2;
-    ghh += gsc * 1.5 * sc / h;
+    ghh += gsc * T(1.5) * sc / h;
   }
-  double gu0 = gu1, gv0 = gv1;
+  T gu0 = gu1, gv0 = gv1;
   if (kp) {
     // u1 = sqrt2 h^2 u / r, r = sqrt(h^4 + eps4): d/du = sqrt2 h^2 / r,
     // d/dh = sqrt2 u (2 h / r - h^2 * 2 h^3 / r^3)
-    const double f = kSqrt2 * h2 / r;
-    const double df = kSqrt2 * (2.0 * h / r - h2 * 2.0 * h * h2 / (r * r * r));
+    const T f = T(kSqrt2) * h2 / r;
+    const T df = T(kSqrt2) * (T(2) * h / r - h2 * T(2) * h * h2 / (r * r * r));
     gu0 = gu1 * f;
     gv0 = gv1 * f;
     ghh += (gu1 * u + gv1 * v) * df;
@@ -253,14 +260,15 @@ RKB_HD void protect_adj(double h, double u, double v, double& gh, double& gu, do
 }
 
 // Manning friction of sources() with a per-cell n (rki_kernel_fused.F90:121-130).
-RKB_HD void friction(double h, double& u, double& v, double n, double dt) {
-  if (h > kDry && n > 0.0) {
-    const double n_sq = n * n;
-    const double uu = u / h;
-    const double vv = v / h;
-    const double speed = sqrt(uu * uu + vv * vv);
-    const double cf = kG * n_sq / cr_pow_third(h);
-    const double den = 1.0 + dt * cf * speed / h;
+template <typename T>
+RKB_HD void friction(T h, T& u, T& v, T n, T dt) {
+  if (h > T(kDry) && n > T(0)) {
+    const T n_sq = n * n;
+    const T uu = u / h;
+    const T vv = v / h;
+    const T speed = sqrt(uu * uu + vv * vv);
+    const T cf = T(kG) * n_sq / pow_third(h);
+    const T den = T(1) + dt * cf * speed / h;
     u = u / den;
     v = v / den;
   }
@@ -268,24 +276,25 @@ RKB_HD void friction(double h, double& u, double& v, double n, double dt) {
 
 // Adjoint of friction at input (h, u, v, n): (gu, gv) output adjoints in,
 // input adjoints out; gh, gn accumulated.
-RKB_HD void friction_adj(double h, double u, double v, double n, double dt, double& gh,
-                         double& gu, double& gv, double& gn) {
-  if (!(h > kDry && n > 0.0)) return;
-  const double uu = u / h, vv = v / h;
-  const double sp = sqrt(uu * uu + vv * vv);
-  const double c3 = cr_pow_third(h);
-  const double cf = kG * n * n / c3;
-  const double den = 1.0 + dt * cf * sp / h;
-  const double gden = -(gu * u + gv * v) / (den * den);
-  double gu0 = gu / den, gv0 = gv / den;
-  const double gcf = gden * dt * sp / h;
-  const double gsp = gden * dt * cf / h;
+template <typename T>
+RKB_HD void friction_adj(T h, T u, T v, T n, T dt, T& gh,
+                         T& gu, T& gv, T& gn) {
+  if (!(h > T(kDry) && n > T(0))) return;
+  const T uu = u / h, vv = v / h;
+  const T sp = sqrt(uu * uu + vv * vv);
+  const T c3 = pow_third(h);
+  const T cf = T(kG) * n * n / c3;
+  const T den = T(1) + dt * cf * sp / h;
+  const T gden = -(gu * u + gv * v) / (den * den);
+  T gu0 = gu / den, gv0 = gv / den;
+  const T gcf = gden * dt * sp / h;
+  const T gsp = gden * dt * cf / h;
   gh += gden * (-dt * cf * sp / (h * h));
-  gn += gcf * 2.0 * kG * n / c3;
-  const double gc3 = -gcf * cf / c3;
-  gh += gc3 * c3 / (3.0 * h);
-  if (sp > 0.0) {
-    const double guu = gsp * uu / sp, gvv = gsp * vv / sp;
+  gn += gcf * T(2) * T(kG) * n / c3;
+  const T gc3 = -gcf * cf / c3;
+  gh += gc3 * c3 / (T(3) * h);
+  if (sp > T(0)) {
+    const T guu = gsp * uu / sp, gvv = gsp * vv / sp;
     gu0 += guu / h;
     gv0 += gvv / h;
     gh += -(guu * uu + gvv * vv) / h;
@@ -295,8 +304,9 @@ RKB_HD void friction_adj(double h, double u, double v, double n, double dt, doub
 }
 
 // minmod branch: 0 = zero, 1 = first argument, 2 = second (rki_kernel_flux.F90:380-393)
-RKB_HD int minmod_choice(double a, double b) {
-  if (a * b <= 0.0) return 0;
+template <typename T>
+RKB_HD int minmod_choice(T a, T b) {
+  if (a * b <= T(0)) return 0;
   return fabs(a) < fabs(b) ? 1 : 2;
 }
 

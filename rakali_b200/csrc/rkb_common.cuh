@@ -102,38 +102,47 @@ struct StepCtl {
 // Small FP64 helpers in the reference's evaluation order.
 // ---------------------------------------------------------------------------
 
-__host__ __device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
-__host__ __device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
+// The pointwise helpers are templates on the real type T: the production
+// FP64 kernels instantiate them with double; the FP32 adjoint with float.
+// Every constant enters as T(c), so the double instances evaluate exactly the
+// expressions written here.
+template <typename T>
+__host__ __device__ __forceinline__ T dmax(T a, T b) { return a > b ? a : b; }
+template <typename T>
+__host__ __device__ __forceinline__ T dmin(T a, T b) { return a < b ? a : b; }
 // Fortran max(0, x) for non-NaN x.
-__host__ __device__ __forceinline__ double pos(double x) { return x > 0.0 ? x : 0.0; }
+template <typename T>
+__host__ __device__ __forceinline__ T pos(T x) { return x > T(0) ? x : T(0); }
 
 // minmod, rki_kernel_flux.F90:380-393
-__host__ __device__ __forceinline__ double minmod(double a, double b) {
-  if (a * b <= 0.0) return 0.0;
+template <typename T>
+__host__ __device__ __forceinline__ T minmod(T a, T b) {
+  if (a * b <= T(0)) return T(0);
   return fabs(a) < fabs(b) ? a : b;
 }
 
 // Clamp + KP07 desingularisation + Froude backstop
 // (rki_kernel_fused.F90:93-119 and :441-463).
-__host__ __device__ __forceinline__ void protect(double& h, double& u, double& v) {
-  if (h < 0.0) {
-    h = 0.0; u = 0.0; v = 0.0;
-  } else if (h < kDry) {
-    u = 0.0; v = 0.0;
+template <typename T>
+__host__ __device__ __forceinline__ void protect(T& h, T& u, T& v) {
+  if (h < T(0)) {
+    h = T(0); u = T(0); v = T(0);
+  } else if (h < T(kDry)) {
+    u = T(0); v = T(0);
   } else {
-    double h2 = h * h;
-    double h4 = h2 * h2;
-    if (h4 < kEps4) {
-      double r = sqrt(h4 + kEps4);
-      double uu = kSqrt2 * h * u / r;
-      double vv = kSqrt2 * h * v / r;
+    T h2 = h * h;
+    T h4 = h2 * h2;
+    if (h4 < T(kEps4)) {
+      T r = sqrt(h4 + T(kEps4));
+      T uu = T(kSqrt2) * h * u / r;
+      T vv = T(kSqrt2) * h * v / r;
       u = h * uu;
       v = h * vv;
     }
-    double sp2 = (u * u + v * v) / (h * h);
-    double fr2 = kFroude * kFroude * kG * h;
+    T sp2 = (u * u + v * v) / (h * h);
+    T fr2 = T(kFroude) * T(kFroude) * T(kG) * h;
     if (sp2 > fr2) {
-      double sc = sqrt(fr2 / sp2);
+      T sc = sqrt(fr2 / sp2);
       u = u * sc;
       v = v * sc;
     }
@@ -142,15 +151,16 @@ __host__ __device__ __forceinline__ void protect(double& h, double& u, double& v
 
 // Wave speed terms of compute_timestep (rki_kernel_timestep.F90:52-66):
 // returns (|u|_KP07 + sqrt(g h)) along x and y, before the division by dx/dy.
-__host__ __device__ __forceinline__ void wave_speed(double h, double hu, double hv, double& sx, double& sy) {
-  sx = 0.0;
-  sy = 0.0;
-  if (h > kDry) {
-    double c = sqrt(kG * h);
-    double h2 = h * h;
-    double den = sqrt(h2 * h2 + kEps4);
-    double ua = fabs(hu) * kSqrt2 * h / den;
-    double va = fabs(hv) * kSqrt2 * h / den;
+template <typename T>
+__host__ __device__ __forceinline__ void wave_speed(T h, T hu, T hv, T& sx, T& sy) {
+  sx = T(0);
+  sy = T(0);
+  if (h > T(kDry)) {
+    T c = sqrt(T(kG) * h);
+    T h2 = h * h;
+    T den = sqrt(h2 * h2 + T(kEps4));
+    T ua = fabs(hu) * T(kSqrt2) * h / den;
+    T va = fabs(hv) * T(kSqrt2) * h / den;
     sx = ua + c;
     sy = va + c;
   }

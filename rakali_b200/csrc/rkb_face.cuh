@@ -1,4 +1,7 @@
-// Face-level numerics of the structured barotropic flux (FP64).
+// Face-level numerics of the structured barotropic flux.
+//
+// Templates on the real type T (double in the production step and the FP64
+// adjoint, float in the FP32 adjoint); constants enter as T(c).
 //
 // One call evaluates one cell face: Audusse hydrostatic reconstruction of the
 // two side states, then the HLL or HLLC Riemann flux.  The reference
@@ -15,111 +18,114 @@ namespace rkb {
 // h_hyd^2 - h_pre^2 (the neighbour to the right adds it first); hL2 and pL2
 // are the left side's h_hyd^2 and h_pre^2, subtracted and added in that order
 // by the neighbour to the left (rki_kernel_flux.F90:361-369).
-struct FaceOut {
-  double fh, fqx, fqy;
-  double wbR, hL2, pL2;
+template <typename T>
+struct FaceOutT {
+  T fh, fqx, fqy;
+  T wbR, hL2, pL2;
 };
+using FaceOut = FaceOutT<double>;
 
-__host__ __device__ __forceinline__ void velocity(double h, double qx, double qy, double& u, double& v) {
-  if (h > kDry) {
+template <typename T>
+__host__ __device__ __forceinline__ void velocity(T h, T qx, T qy, T& u, T& v) {
+  if (h > T(kDry)) {
     u = qx / h;
     v = qy / h;
   } else {
-    u = 0.0;
-    v = 0.0;
+    u = T(0);
+    v = T(0);
   }
 }
 
 // HLL / HLLC in direction DIR (0: x, normal momentum qx; 1: y, normal qy).
 // hll_flux_x/y rki_kernel_flux.F90:410-582, hllc_flux_x/y :584-783.
-template <int DIR, bool HLLC>
-__host__ __device__ __forceinline__ void riemann(double hl, double qxl, double qyl, double hr, double qxr,
-                                        double qyr, double& fh, double& fqx, double& fqy) {
-  double ul, vl, ur, vr;
+template <int DIR, bool HLLC, typename T>
+__host__ __device__ __forceinline__ void riemann(T hl, T qxl, T qyl, T hr, T qxr, T qyr, T& fh,
+                                                 T& fqx, T& fqy) {
+  T ul, vl, ur, vr;
   velocity(hl, qxl, qyl, ul, vl);
   velocity(hr, qxr, qyr, ur, vr);
-  const double al = sqrt(kG * pos(hl));
-  const double ar = sqrt(kG * pos(hr));
-  const double nl = DIR == 0 ? ul : vl;
-  const double nr = DIR == 0 ? ur : vr;
-  double sl, sr;
-  if (hr <= kDry) {
+  const T al = sqrt(T(kG) * pos(hl));
+  const T ar = sqrt(T(kG) * pos(hr));
+  const T nl = DIR == 0 ? ul : vl;
+  const T nr = DIR == 0 ? ur : vr;
+  T sl, sr;
+  if (hr <= T(kDry)) {
     sl = nl - al;
-    sr = nl + 2.0 * al;
-  } else if (hl <= kDry) {
-    sl = nr - 2.0 * ar;
+    sr = nl + T(2) * al;
+  } else if (hl <= T(kDry)) {
+    sl = nr - T(2) * ar;
     sr = nr + ar;
   } else {
     sl = dmin(nl - al, nr - ar);
     sr = dmax(nl + al, nr + ar);
   }
-  double lh, lx, ly, rh, rx, ry;
+  T lh, lx, ly, rh, rx, ry;
   if (DIR == 0) {
     lh = qxl;
-    lx = qxl * ul + kHalfG * hl * hl;
+    lx = qxl * ul + T(kHalfG) * hl * hl;
     ly = qxl * vl;
     rh = qxr;
-    rx = qxr * ur + kHalfG * hr * hr;
+    rx = qxr * ur + T(kHalfG) * hr * hr;
     ry = qxr * vr;
   } else {
     lh = qyl;
     lx = qxl * vl;
-    ly = qyl * vl + kHalfG * hl * hl;
+    ly = qyl * vl + T(kHalfG) * hl * hl;
     rh = qyr;
     rx = qxr * vr;
-    ry = qyr * vr + kHalfG * hr * hr;
+    ry = qyr * vr + T(kHalfG) * hr * hr;
   }
-  if (sl >= 0.0) {
+  if (sl >= T(0)) {
     fh = lh; fqx = lx; fqy = ly;
     return;
   }
-  if (sr <= 0.0) {
+  if (sr <= T(0)) {
     fh = rh; fqx = rx; fqy = ry;
     return;
   }
-  const double inv = 1.0 / (sr - sl);
-  const double slsr = sl * sr;
+  const T inv = T(1) / (sr - sl);
+  const T slsr = sl * sr;
   fh = (sr * lh - sl * rh + slsr * (hr - hl)) * inv;
   if (DIR == 0) {
     fqx = (sr * lx - sl * rx + slsr * (qxr - qxl)) * inv;
     if (!HLLC) {
       fqy = (sr * ly - sl * ry + slsr * (qyr - qyl)) * inv;
     } else {
-      const double den = hr * (ur - sr) - hl * (ul - sl);
-      double ss;
-      if (fabs(den) > kDry)
+      const T den = hr * (ur - sr) - hl * (ul - sl);
+      T ss;
+      if (fabs(den) > T(kDry))
         ss = (sl * hr * (ur - sr) - sr * hl * (ul - sl)) / den;
       else
-        ss = 0.5 * (ul + ur);
-      fqy = ss >= 0.0 ? fh * vl : fh * vr;
+        ss = T(0.5) * (ul + ur);
+      fqy = ss >= T(0) ? fh * vl : fh * vr;
     }
   } else {
     fqy = (sr * ly - sl * ry + slsr * (qyr - qyl)) * inv;
     if (!HLLC) {
       fqx = (sr * lx - sl * rx + slsr * (qxr - qxl)) * inv;
     } else {
-      const double den = hr * (vr - sr) - hl * (vl - sl);
-      double ss;
-      if (fabs(den) > kDry)
+      const T den = hr * (vr - sr) - hl * (vl - sl);
+      T ss;
+      if (fabs(den) > T(kDry))
         ss = (sl * hr * (vr - sr) - sr * hl * (vl - sl)) / den;
       else
-        ss = 0.5 * (vl + vr);
-      fqx = ss >= 0.0 ? fh * ul : fh * ur;
+        ss = T(0.5) * (vl + vr);
+      fqx = ss >= T(0) ? fh * ul : fh * ur;
     }
   }
 }
 
 // One face from the reconstructed side values (eta, hu, hv) and the beds.
 // The Audusse step follows rki_kernel_flux.F90:186-224.
-template <int DIR, bool HLLC>
-__host__ __device__ __forceinline__ void face_flux(double eL, double qxL, double qyL, double bL, double eR,
-                                          double qxR, double qyR, double bR, FaceOut& o) {
-  const double hL = pos(eL - bL);
-  const double hR = pos(eR - bR);
-  const double bmax = dmax(bL, bR);
-  const double hyl = pos(hL + bL - bmax);
-  const double hyr = pos(hR + bR - bmax);
-  double ul, vl, ur, vr;
+template <int DIR, bool HLLC, typename T>
+__host__ __device__ __forceinline__ void face_flux(T eL, T qxL, T qyL, T bL, T eR, T qxR, T qyR,
+                                                   T bR, FaceOutT<T>& o) {
+  const T hL = pos(eL - bL);
+  const T hR = pos(eR - bR);
+  const T bmax = dmax(bL, bR);
+  const T hyl = pos(hL + bL - bmax);
+  const T hyr = pos(hR + bR - bmax);
+  T ul, vl, ur, vr;
   velocity(hL, qxL, qyL, ul, vl);
   velocity(hR, qxR, qyR, ur, vr);
   riemann<DIR, HLLC>(hyl, hyl * ul, hyl * vl, hyr, hyr * ur, hyr * vr, o.fh, o.fqx, o.fqy);
@@ -130,12 +136,11 @@ __host__ __device__ __forceinline__ void face_flux(double eL, double qxL, double
 
 // Limited slope of one cell along one direction (rki_kernel_flux.F90:159-181):
 // zero near wet/dry fronts, else minmod of the one-sided differences.
-__host__ __device__ __forceinline__ void cell_slope(double hm, double hc, double hp, double em, double ec,
-                                           double ep, double um, double uc, double up, double vm,
-                                           double vc, double vp, double& se, double& su,
-                                           double& sv) {
-  if (hc < kThin || hm < kDry || hp < kDry) {
-    se = 0.0; su = 0.0; sv = 0.0;
+template <typename T>
+__host__ __device__ __forceinline__ void cell_slope(T hm, T hc, T hp, T em, T ec, T ep, T um, T uc,
+                                                    T up, T vm, T vc, T vp, T& se, T& su, T& sv) {
+  if (hc < T(kThin) || hm < T(kDry) || hp < T(kDry)) {
+    se = T(0); su = T(0); sv = T(0);
   } else {
     se = minmod(ec - em, ep - ec);
     su = minmod(uc - um, up - uc);
