@@ -112,7 +112,10 @@ int rki_set_tidal_constituents(void *handle, const double *amp, const double *ph
 void rki_sync_host(void *handle);
 void rki_sync_from_device(void *handle);
 
-/* rki_api.F90:1409-1471: restart files (see DESIGN; returns -3) */
+/* rki_api.F90:1409-1471: restart files.  save (finalised handle) writes
+ * interior h, hu, hv, b and the time as NetCDF classic (64-bit offset);
+ * load (before finalize) restores them and the clock; -3 on a grid
+ * mismatch or an unreadable file (NetCDF-4/HDF5 containers included). */
 int rki_save_restart(void *handle, const char *filename, int len);
 int rki_load_restart(void *handle, const char *filename, int len);
 
@@ -220,6 +223,18 @@ void rkb_test_face_flux(int dir, int hllc, const double *in8, double *out6);
 void rkb_test_face_adj(int dir, int hllc, const double *in8, const double *gout6, double *gin8);
 void rkb_test_cell(const double *in4, double dt, double *out3);
 void rkb_test_cell_adj(const double *in4, double dt, const double *gout3, double *gin4);
+
+/* NetCDF classic (64-bit offset) restart codec without a simulation: the
+ * variables of rki_save_restart (h, hu, hv, b as (y, x) FP64 with units,
+ * scalar time; dimensions x, y; global Conventions, title, source, dx, dy,
+ * nghost).  Arrays are interior (nx, ny) Fortran order.  read returns 0,
+ * 1 when the file's grid is not nx x ny, -1 when unreadable (NetCDF-4/HDF5
+ * containers included), -2 on bad arguments. */
+int rkb_restart_write(const char *path, int nx, int ny, const double *h, const double *hu,
+                      const double *hv, const double *b, double time, double dx, double dy,
+                      int nghost);
+int rkb_restart_read(const char *path, int nx, int ny, double *h, double *hu, double *hv,
+                     double *b, double *time);
 
 /* Run n steps bracketed by CUDA events on the simulation's own stream;
  * *ms = device time of the n steps (state already resident). */

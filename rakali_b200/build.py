@@ -41,6 +41,7 @@ UNITS = {
     "rkb_batch.cu": [],
     "rkb_api.cu": [],
     "rkb_config.cpp": [],
+    "rkb_netcdf.cpp": [],
 }
 
 

@@ -474,9 +474,40 @@ class Rakali:
             int(a.size)), "set_tidal_constituents")
 
     def save_restart(self, filename):
-        self._check_alive()
+        """Write h, hu, hv, b and the time to a NetCDF (classic) restart file.
+
+        The variables, dimensions and attributes are those of the reference's
+        restart_write (src/io/structured/rki_output.F90:740-853); step count
+        and configuration are not saved.
+        """
+        self._check_ready()
+        parent = Path(str(filename)).resolve().parent
+        if not parent.is_dir():
+            raise FileNotFoundError(f"directory {parent} does not exist")
         raw = str(filename).encode()
         self._rc(self._lib.rki_save_restart(self._handle, raw, len(raw)), "save_restart")
+
+    @classmethod
+    def from_restart(cls, restart_file, namelist=None, **kwargs):
+        """Create a simulation whose state (h, hu, hv, b, time) comes from a
+        restart file; the namelist or keyword arguments give the configuration,
+        whose grid must match the file's (python/rakali/_core.py:1506-1556)."""
+        path = Path(str(restart_file))
+        if not path.is_file():
+            raise FileNotFoundError(f"Restart file not found: {path}")
+        raw = str(path.resolve()).encode()
+        kwargs.pop("defer_init", None)
+        sim = cls(namelist=namelist, defer_init=True, **kwargs)
+        try:
+            rc = sim._lib.rki_load_restart(sim._handle, raw, len(raw))
+            if rc != 0:
+                raise RuntimeError(f"rki_load_restart('{path}') failed (rc={rc}): "
+                                   f"{_lib.last_error(sim._lib)}")
+            sim.finalize()
+        except Exception:
+            sim.close()
+            raise
+        return sim
 
     # --- additions --------------------------------------------------------
     def mass_budget(self):

@@ -14,6 +14,7 @@
 
 #include "../../include/rakali.h"
 #include "rkb_batch.hpp"
+#include "rkb_netcdf.hpp"
 #include "rkb_sim.hpp"
 
 namespace {
@@ -327,21 +328,46 @@ void rki_sync_from_device(void* handle) {
 }
 
 int rki_save_restart(void* handle, const char* filename, int len) {
-  (void)filename; (void)len;
   rkb::Sim* s = sim_of(handle);
   if (!s) return kBadHandle;
   if (!s->is_initialised) return -1;
   if (!s->is_finalised) return -2;
-  return fail(-3, "NetCDF restart files are not provided by this library");
+  if (!filename || len <= 0) return fail(-3, "empty restart file name");
+  std::string err;
+  const int rc = s->save_restart(std::string(filename, (size_t)len), err);
+  return rc == 0 ? 0 : fail(-3, err);
 }
 
 int rki_load_restart(void* handle, const char* filename, int len) {
-  (void)filename; (void)len;
   rkb::Sim* s = sim_of(handle);
   if (!s) return kBadHandle;
   if (!s->is_initialised) return -1;
   if (s->is_finalised) return -2;
-  return fail(-3, "NetCDF restart files are not provided by this library");
+  if (!filename || len <= 0) return fail(-3, "empty restart file name");
+  std::string err;
+  const int rc = s->load_restart(std::string(filename, (size_t)len), err);
+  return rc == 0 ? 0 : fail(-3, err);
+}
+
+// Host-only codec entry points (no simulation, no GPU): interior (nx, ny)
+// Fortran-order arrays; read returns 0, 1 (grid mismatch) or -1.
+int rkb_restart_write(const char* path, int nx, int ny, const double* h, const double* hu,
+                      const double* hv, const double* b, double time, double dx, double dy,
+                      int nghost) {
+  if (!path || !h || !hu || !hv || !b || nx < 1 || ny < 1) return fail(-2, "invalid arguments");
+  std::string err;
+  if (!rkb::nc::write_restart(path, nx, ny, h, hu, hv, b, time, dx, dy, nghost, err))
+    return fail(-1, err);
+  return 0;
+}
+
+int rkb_restart_read(const char* path, int nx, int ny, double* h, double* hu, double* hv,
+                     double* b, double* time) {
+  if (!path || !h || !hu || !hv || !b || !time || nx < 1 || ny < 1)
+    return fail(-2, "invalid arguments");
+  std::string err;
+  const int rc = rkb::nc::read_restart(path, nx, ny, h, hu, hv, b, *time, err);
+  return rc == 0 ? 0 : fail(rc, err);
 }
 
 int rki_set_use_ppm_tracer(void* handle, int flag) {

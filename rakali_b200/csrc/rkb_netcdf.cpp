@@ -1,0 +1,303 @@
+// NetCDF classic restart files (see rkb_netcdf.hpp).  The encoding follows
+// the published NetCDF classic format specification: big-endian header of
+// dimensions, global attributes and variables (name, dimension ids,
+// attributes, type, size, data offset), then each fixed-size variable's
+// values contiguous at its offset, padded to 4 bytes.
+#include "rkb_netcdf.hpp"
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+namespace rkb {
+namespace nc {
+namespace {
+
+constexpr uint32_t kDimTag = 0x0A, kVarTag = 0x0B, kAttTag = 0x0C;
+constexpr uint32_t kChar = 2, kShort = 3, kInt = 4, kFloat = 5, kDouble = 6, kByte = 1;
+
+uint32_t pad4(uint32_t n) { return (n + 3u) & ~3u; }
+
+// ---- writer -----------------------------------------------------------------
+
+struct Out {
+  std::vector<unsigned char> b;
+  void u32(uint32_t v) {
+    for (int s = 24; s >= 0; s -= 8) b.push_back((unsigned char)(v >> s));
+  }
+  void u64(uint64_t v) {
+    for (int s = 56; s >= 0; s -= 8) b.push_back((unsigned char)(v >> s));
+  }
+  void name(const std::string& s) {
+    u32((uint32_t)s.size());
+    b.insert(b.end(), s.begin(), s.end());
+    while (b.size() % 4) b.push_back(0);
+  }
+  void text_att(const std::string& n, const std::string& v) {
+    name(n);
+    u32(kChar);
+    u32((uint32_t)v.size());
+    b.insert(b.end(), v.begin(), v.end());
+    while (b.size() % 4) b.push_back(0);
+  }
+};
+
+void put_be_doubles(std::vector<unsigned char>& dst, const double* v, size_t n) {
+  const size_t o = dst.size();
+  dst.resize(o + 8 * n);
+  for (size_t k = 0; k < n; ++k) {
+    uint64_t u;
+    std::memcpy(&u, &v[k], 8);
+    for (int s = 0; s < 8; ++s) dst[o + 8 * k + s] = (unsigned char)(u >> (56 - 8 * s));
+  }
+}
+
+std::string num(double x) {
+  char buf[64];
+  std::snprintf(buf, sizeof(buf), "%.17g", x);
+  return buf;
+}
+
+// ---- reader -----------------------------------------------------------------
+
+struct In {
+  const unsigned char* p;
+  size_t n, o = 0;
+  bool ok = true;
+  uint32_t u32() {
+    if (o + 4 > n) { ok = false; return 0; }
+    const uint32_t v = (uint32_t)p[o] << 24 | (uint32_t)p[o + 1] << 16 | (uint32_t)p[o + 2] << 8 |
+                       (uint32_t)p[o + 3];
+    o += 4;
+    return v;
+  }
+  uint64_t u64() {
+    const uint64_t hi = u32();
+    return hi << 32 | u32();
+  }
+  std::string name() {
+    const uint32_t len = u32();
+    if (!ok || o + pad4(len) > n) { ok = false; return {}; }
+    std::string s((const char*)p + o, len);
+    o += pad4(len);
+    return s;
+  }
+  void skip_atts() {
+    const uint32_t tag = u32(), cnt = u32();
+    if (tag == 0 && cnt == 0) return;
+    if (tag != kAttTag) { ok = false; return; }
+    for (uint32_t a = 0; a < cnt && ok; ++a) {
+      name();
+      const uint32_t type = u32(), nel = u32();
+      const uint32_t sz = type == kByte || type == kChar ? 1 : type == kShort ? 2 :
+                          type == kDouble ? 8 : 4;
+      const uint64_t bytes = pad4(nel * sz);
+      if (o + bytes > n) { ok = false; return; }
+      o += bytes;
+    }
+  }
+};
+
+struct Var {
+  std::string name;
+  std::vector<uint32_t> dims;
+  uint32_t type = 0;
+  uint64_t begin = 0;
+};
+
+}  // namespace
+
+bool write_restart(const std::string& path, int nx, int ny, const double* h, const double* hu,
+                   const double* hv, const double* b, double time, double dx, double dy, int ng,
+                   std::string& err) {
+  const uint64_t n2 = (uint64_t)nx * (uint64_t)ny;
+  if (8 * n2 >= 0xFFFFFFFCull) {
+    err = "grid too large for a 64-bit-offset NetCDF variable (4 GiB each)";
+    return false;
+  }
+  // header with placeholder offsets, patched once its size is known
+  Out hd;
+  hd.b = {'C', 'D', 'F', 2};
+  hd.u32(0);  // numrecs
+  hd.u32(kDimTag);
+  hd.u32(2);
+  hd.name("x");
+  hd.u32((uint32_t)nx);
+  hd.name("y");
+  hd.u32((uint32_t)ny);
+  hd.u32(kAttTag);
+  hd.u32(6);
+  hd.text_att("Conventions", "CF-1.11");
+  hd.text_att("title", "Tidal restart file");
+  hd.text_att("source", "rakali_b200");
+  hd.text_att("dx", num(dx));
+  hd.text_att("dy", num(dy));
+  hd.text_att("nghost", std::to_string(ng));
+  hd.u32(kVarTag);
+  hd.u32(5);
+  const char* names[5] = {"h", "hu", "hv", "b", "time"};
+  const char* units[5] = {"m", "m2 s-1", "m2 s-1", "m", "seconds since simulation start"};
+  size_t begin_at[5];
+  for (int v = 0; v < 5; ++v) {
+    hd.name(names[v]);
+    if (v < 4) {
+      hd.u32(2);
+      hd.u32(1);  // y (slowest)
+      hd.u32(0);  // x
+    } else {
+      hd.u32(0);
+    }
+    hd.u32(kAttTag);
+    hd.u32(1);
+    hd.text_att("units", units[v]);
+    hd.u32(kDouble);
+    hd.u32(v < 4 ? (uint32_t)(8 * n2) : 8u);
+    begin_at[v] = hd.b.size();
+    hd.u64(0);
+  }
+  uint64_t off = hd.b.size();
+  for (int v = 0; v < 5; ++v) {
+    for (int s = 0; s < 8; ++s) hd.b[begin_at[v] + s] = (unsigned char)(off >> (56 - 8 * s));
+    off += v < 4 ? 8 * n2 : 8;
+  }
+  FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f) {
+    err = "cannot open " + path + " for writing";
+    return false;
+  }
+  bool ok = std::fwrite(hd.b.data(), 1, hd.b.size(), f) == hd.b.size();
+  std::vector<unsigned char> buf;
+  const double* fields[4] = {h, hu, hv, b};
+  for (int v = 0; v < 4 && ok; ++v) {
+    buf.clear();
+    put_be_doubles(buf, fields[v], n2);
+    ok = std::fwrite(buf.data(), 1, buf.size(), f) == buf.size();
+  }
+  if (ok) {
+    buf.clear();
+    put_be_doubles(buf, &time, 1);
+    ok = std::fwrite(buf.data(), 1, buf.size(), f) == buf.size();
+  }
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) err = "write to " + path + " failed";
+  return ok;
+}
+
+int read_restart(const std::string& path, int nx, int ny, double* h, double* hu, double* hv,
+                 double* b, double& time, std::string& err) {
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) {
+    err = "cannot open " + path;
+    return -1;
+  }
+  std::vector<unsigned char> data;
+  unsigned char chunk[1 << 16];
+  size_t got;
+  while ((got = std::fread(chunk, 1, sizeof(chunk), f)) > 0) data.insert(data.end(), chunk, chunk + got);
+  std::fclose(f);
+  if (data.size() >= 8 && std::memcmp(data.data(), "\x89HDF\r\n\x1a\n", 8) == 0) {
+    err = path + " is a NetCDF-4 (HDF5) file; this library reads NetCDF classic and "
+                 "64-bit-offset restart files";
+    return -1;
+  }
+  if (data.size() < 4 || std::memcmp(data.data(), "CDF", 3) != 0 || (data[3] != 1 && data[3] != 2)) {
+    err = path + " is not a NetCDF classic file";
+    return -1;
+  }
+  const bool off64 = data[3] == 2;
+  In in{data.data(), data.size()};
+  in.o = 4;
+  in.u32();  // numrecs
+  std::vector<std::pair<std::string, uint32_t>> dims;
+  {
+    const uint32_t tag = in.u32(), cnt = in.u32();
+    if (!(tag == 0 && cnt == 0)) {
+      if (tag != kDimTag) in.ok = false;
+      for (uint32_t d = 0; d < cnt && in.ok; ++d) {
+        std::string nm = in.name();
+        dims.emplace_back(nm, in.u32());
+      }
+    }
+  }
+  in.skip_atts();
+  std::vector<Var> vars;
+  {
+    const uint32_t tag = in.u32(), cnt = in.u32();
+    if (!(tag == 0 && cnt == 0)) {
+      if (tag != kVarTag) in.ok = false;
+      for (uint32_t v = 0; v < cnt && in.ok; ++v) {
+        Var var;
+        var.name = in.name();
+        const uint32_t nd = in.u32();
+        for (uint32_t d = 0; d < nd && in.ok; ++d) var.dims.push_back(in.u32());
+        in.skip_atts();
+        var.type = in.u32();
+        in.u32();  // vsize
+        var.begin = off64 ? in.u64() : in.u32();
+        vars.push_back(var);
+      }
+    }
+  }
+  if (!in.ok) {
+    err = path + ": malformed NetCDF header";
+    return -1;
+  }
+  int fx = -1, fy = -1;
+  for (size_t d = 0; d < dims.size(); ++d) {
+    if (dims[d].first == "x") fx = (int)d;
+    if (dims[d].first == "y") fy = (int)d;
+  }
+  if (fx < 0 || fy < 0) {
+    err = path + ": dimensions x and y not found";
+    return -1;
+  }
+  if ((int)dims[fx].second != nx || (int)dims[fy].second != ny) {
+    err = "restart grid mismatch: file has " + std::to_string(dims[fx].second) + " x " +
+          std::to_string(dims[fy].second) + " but the simulation expects " + std::to_string(nx) +
+          " x " + std::to_string(ny);
+    return 1;
+  }
+  const uint64_t n2 = (uint64_t)nx * (uint64_t)ny;
+  auto read_var = [&](const char* nm, double* dst, uint64_t count) -> bool {
+    for (const Var& v : vars) {
+      if (v.name != nm) continue;
+      const bool shape_ok = count == 1 ? v.dims.empty()
+                                       : (v.dims.size() == 2 && v.dims[0] == (uint32_t)fy &&
+                                          v.dims[1] == (uint32_t)fx);
+      if (!shape_ok || (v.type != kDouble && v.type != kFloat)) {
+        err = path + ": variable " + nm + " has an unexpected shape or type";
+        return false;
+      }
+      const uint64_t sz = v.type == kDouble ? 8 : 4;
+      if (v.begin + sz * count > data.size()) {
+        err = path + ": variable " + nm + " is truncated";
+        return false;
+      }
+      const unsigned char* q = data.data() + v.begin;
+      for (uint64_t k = 0; k < count; ++k, q += sz) {
+        if (sz == 8) {
+          uint64_t u = 0;
+          for (int s = 0; s < 8; ++s) u = u << 8 | q[s];
+          std::memcpy(&dst[k], &u, 8);
+        } else {
+          uint32_t u = 0;
+          for (int s = 0; s < 4; ++s) u = u << 8 | q[s];
+          float x;
+          std::memcpy(&x, &u, 4);
+          dst[k] = x;
+        }
+      }
+      return true;
+    }
+    err = path + ": variable " + nm + " not found";
+    return false;
+  };
+  if (!read_var("h", h, n2) || !read_var("hu", hu, n2) || !read_var("hv", hv, n2) ||
+      !read_var("b", b, n2) || !read_var("time", &time, 1))
+    return -1;
+  return 0;
+}
+
+}  // namespace nc
+}  // namespace rkb

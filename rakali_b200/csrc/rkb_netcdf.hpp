@@ -1,0 +1,29 @@
+// Restart files in the NetCDF classic format (64-bit offset variant), the
+// layout of the reference's restart_write / restart_read
+// (src/io/structured/rki_output.F90:740-988): dimensions x = nx_phys and
+// y = ny_phys, variables h, hu, hv, b (y, x) in FP64 with "units"
+// attributes, a scalar "time", and global attributes Conventions, title,
+// source, dx, dy, nghost.  The reference writes NetCDF-4 (an HDF5 container)
+// through libnetcdf; classic files hold the same variables and every NetCDF
+// library (netcdf-fortran's nf90_open included) reads them.  The reader
+// accepts classic and 64-bit-offset files and refuses HDF5 containers with a
+// message.
+#pragma once
+
+#include <string>
+
+namespace rkb {
+namespace nc {
+
+// Interior arrays are (nx, ny) Fortran order (x fastest), which is the
+// file's (y, x) row-major order.
+bool write_restart(const std::string& path, int nx, int ny, const double* h, const double* hu,
+                   const double* hv, const double* b, double time, double dx, double dy, int ng,
+                   std::string& err);
+
+// 0: read; 1: the file's grid is not nx x ny; -1: not readable (err says why).
+int read_restart(const std::string& path, int nx, int ny, double* h, double* hu, double* hv,
+                 double* b, double& time, std::string& err);
+
+}  // namespace nc
+}  // namespace rkb

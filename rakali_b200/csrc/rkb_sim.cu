@@ -1,6 +1,8 @@
 // Host driver of one structured simulation (see rkb_sim.hpp).
 #include "rkb_sim.hpp"
 
+#include "rkb_netcdf.hpp"
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -302,6 +304,51 @@ int Sim::alloc_device(std::string& err) {
   args_.scheme = phys.scheme;
   args_.n_stages = phys.n_stages;
   cur_ = 0;
+  // the clock starts at the restart time when a restart file was loaded
+  hctl_->t = t_current_;
+  if (cudaMemcpyAsync(&args_.ctl->t, &hctl_->t, sizeof(double), cudaMemcpyHostToDevice,
+                      stream_) != cudaSuccess ||
+      cudaStreamSynchronize(stream_) != cudaSuccess)
+    return -1;
+  return 0;
+}
+
+// restart_write (src/io/structured/rki_output.F90:740-853): interior h, hu,
+// hv, b and the clock, after refresh_host.
+int Sim::save_restart(const std::string& path, std::string& err) {
+  if (on_device_ && !host_is_current_) sync_host();
+  const int nx = cfg.nx, ny = cfg.ny;
+  std::vector<double> f[4];
+  for (int k = 0; k < 4; ++k) {
+    f[k].resize((size_t)nx * ny);
+    for (int j = 0; j < ny; ++j)
+      std::memcpy(f[k].data() + (size_t)j * nx, hf_[k] + (size_t)g.ng + (size_t)(g.ng + j) * g.nxt,
+                  (size_t)nx * sizeof(double));
+  }
+  return nc::write_restart(path, nx, ny, f[0].data(), f[1].data(), f[2].data(), f[3].data(),
+                           t_current_, g.dx, g.dy, g.ng, err)
+             ? 0
+             : -3;
+}
+
+// restart_read (rki_output.F90:855-988) before finalize: the interior state
+// and bed come from the file (the initial condition is then not applied) and
+// the clock starts at the file's time.  1: grid mismatch.
+int Sim::load_restart(const std::string& path, std::string& err) {
+  const int nx = cfg.nx, ny = cfg.ny;
+  std::vector<double> f[4];
+  for (auto& v : f) v.resize((size_t)nx * ny);
+  double t = 0.0;
+  const int rc = nc::read_restart(path, nx, ny, f[0].data(), f[1].data(), f[2].data(), f[3].data(),
+                                  t, err);
+  if (rc != 0) return rc;
+  for (int k = 0; k < 4; ++k)
+    for (int j = 0; j < ny; ++j)
+      std::memcpy(hf_[k] + (size_t)g.ng + (size_t)(g.ng + j) * g.nxt, f[k].data() + (size_t)j * nx,
+                  (size_t)nx * sizeof(double));
+  user_set_h = true;
+  user_set_bathymetry = true;
+  t_current_ = t;
   return 0;
 }
 

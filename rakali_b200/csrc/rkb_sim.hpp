@@ -33,6 +33,8 @@ class Sim {
   // out[k] = mean ms of launch k of a step (bc1, stage1, bc2, stage2 in order,
   // the boundary launches summed), out[4] = launches per step.
   int profile_steps(int n, double out[5]);
+  int save_restart(const std::string& path, std::string& err);  // NetCDF classic
+  int load_restart(const std::string& path, std::string& err);  // before finalize; 1 = grid mismatch
   int advance(double target_time);  // rki_advance
 
   // Field access (F-order host arrays with ghosts).  `which`: 0 h, 1 hu,
