@@ -22,14 +22,15 @@
 // exactly zero.  Dry cells store the bed rounded down (eta <= b), so they
 // read back as h <= 0.
 //
-// Data movement: one warp sweeps a strip of 124 columns up a range of rows.
-// Lane l (0..30) owns columns x0 + 4l .. x0 + 4l + 3; lane 31 owns the right
-// halo and the left halo (x0 - 2, x0 - 1) and computes the strip's right
-// edge face.  Rows arrive through a per-warp ring of shared-memory slots
-// filled by 1D bulk asynchronous copies (cp.async.bulk, completion on an
-// mbarrier); x-neighbours are exchanged with warp shuffles, y-neighbours
-// stay in registers.  No block barrier on the data path.  Every wait is
-// bounded in time; a wait that gives up sets StepCtl::error.
+// Data movement: one warp sweeps a strip of 30 C columns (C = 2 or 4 columns
+// per lane) up a range of rows; lanes 0..29 own the output columns, lane 30
+// the C columns right of the strip and lane 31 those left of it, so the lanes
+// form a ring and x-neighbours are plain shuffles.  Rows arrive through a
+// per-warp ring of shared-memory slots filled by 1D bulk asynchronous copies
+// (cp.async.bulk, completion on an mbarrier); y-neighbours stay in
+// registers.  No block barrier on the data path.  Every wait is bounded in
+// time; a wait that gives up sets StepCtl::error.  A lane's columns are
+// processed in pairs on packed FP32 arithmetic.
 #include <cstdint>
 
 #include "rkb_crmath.cuh"
@@ -155,12 +156,6 @@ __device__ __forceinline__ float surface_of(double h, double b) {
   return h > 0.0 ? __double2float_rn(h + b) : __double2float_rd(b);
 }
 
-// Cell flags: bit 0 h >= DRY_THRESHOLD, bit 1 h >= THIN_THRESHOLD (FP64 test).
-__device__ __forceinline__ unsigned cell_flags(float e, double b) {
-  const double h = (double)e - b;
-  return (h >= kDry ? 1u : 0u) | (h >= kThin ? 2u : 0u);
-}
-
 __device__ __forceinline__ float minmodf(float a, float b) {
   if (a * b <= 0.0f) return 0.0f;
   return fabsf(a) < fabsf(b) ? a : b;
@@ -184,11 +179,7 @@ __device__ __forceinline__ Slope slope(unsigned fm, unsigned fc, unsigned fp, fl
   return s;
 }
 
-// One face.  n = normal momentum, t = tangential momentum; hL, hR are the
-// reconstructed depths max(0, h_cell +- s/2) of the two sides and bL, bR the
-// cell beds.
-//
-// The Audusse hydrostatic depths max(0, eta - max(b_L, b_R))
+// Faces.  The Audusse hydrostatic depths max(0, eta - max(b_L, b_R))
 // (rki_kernel_flux.F90:186-224) are FP64 differences: they are what keeps a
 // lake at rest at rest, and in FP64 a dry island whose top lies a hair above
 // the lake surface gets exactly zero depth on both sides of its shore faces.
@@ -211,46 +202,82 @@ struct FaceF {
   float fh, en, dq, ft;
 };
 
+// Packed FP32 pairs (add / mul / fma on two lanes of a 64-bit register).
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, neg2(b)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 splat(float x) { return make_float2(x, x); }
+
+struct FaceF2 {
+  float2 fh, en, dq, ft;
+};
+
+// Two independent faces at once (two columns of a lane, or two neighbouring
+// x-faces), each as described above: the FP64 depths and tests and the
+// reciprocal / square-root approximations per face, the FP32 arithmetic on
+// packed pairs (FADD2 / FMUL2 / FFMA2).  Per face: n = normal momentum, t =
+// tangential momentum, hL / hR the reconstructed depths max(0, h_cell +- s/2),
+// bL / bR the cell beds.
 template <bool HLLC>
-__device__ __forceinline__ FaceF face(float eL, float nL, float tL, float hL, double bL, float eR,
-                                      float nR, float tR, float hR, double bR) {
-  const double bmax = bL > bR ? bL : bR;
-  const double yLd = pos((double)eL - bmax), yRd = pos((double)eR - bmax);
-  const float yl = __double2float_rn(yLd), yr = __double2float_rn(yRd);
-  const float dy = (yl > 0.0f && yr > 0.0f) ? eR - eL : yr - yl;
-  const bool wyl = yLd > kDry, wyr = yRd > kDry;
-  const float rl = rcp_approx(fmaxf(hL, kDryF)), rr = rcp_approx(fmaxf(hR, kDryF));
-  const float ul = hL > kDryF ? nL * rl : 0.0f, vl = hL > kDryF ? tL * rl : 0.0f;
-  const float ur = hR > kDryF ? nR * rr : 0.0f, vr = hR > kDryF ? tR * rr : 0.0f;
-  // HLL / HLLC on the hydrostatic states (rki_kernel_flux.F90:410-783)
-  const float qnl = yl * ul, qtl = yl * vl, qnr = yr * ur, qtr = yr * vr;
-  const float unl = wyl ? ul : 0.0f, utl = wyl ? vl : 0.0f;
-  const float unr = wyr ? ur : 0.0f, utr = wyr ? vr : 0.0f;
-  const float al = sqrt_approx(kGf * yl), ar = sqrt_approx(kGf * yr);
-  const float sl = !wyr ? unl - al : (!wyl ? unr - 2.0f * ar : fminf(unl - al, unr - ar));
-  const float sr = !wyr ? unl + 2.0f * al : (!wyl ? unr + ar : fmaxf(unl + al, unr + ar));
-  FaceF o;
-  o.dq = kHalfGf * dy * (yl + yr);
-  const float ln = qnl * unl, rn = qnr * unr;  // advective parts of the normal fluxes
-  const float lt = qnl * utl, rt = qnr * utr;
-  // F = F_L - s_L (F_R - F_L - s_R (U_R - U_L)) / (s_R - s_L) when s_L < 0 < s_R
-  const float inv = rcp_approx(sr - sl);
-  const float mfh = qnl - sl * ((qnr - qnl) - sr * dy) * inv;
-  const float men = ln - sl * (((rn - ln) + o.dq) - sr * (qnr - qnl)) * inv;
-  float mft;
+__device__ __forceinline__ FaceF2 face2(float2 eL, float2 nL, float2 tL, float2 hL, double bL0,
+                                        double bL1, float2 eR, float2 nR, float2 tR, float2 hR,
+                                        double bR0, double bR1) {
+  const double bm0 = bL0 > bR0 ? bL0 : bR0, bm1 = bL1 > bR1 ? bL1 : bR1;
+  const double yl0 = pos((double)eL.x - bm0), yl1 = pos((double)eL.y - bm1);
+  const double yr0 = pos((double)eR.x - bm0), yr1 = pos((double)eR.y - bm1);
+  const float2 yl = make_float2(__double2float_rn(yl0), __double2float_rn(yl1));
+  const float2 yr = make_float2(__double2float_rn(yr0), __double2float_rn(yr1));
+  const float2 de = sub2(eR, eL), dyy = sub2(yr, yl);
+  const float2 dy = make_float2((yl.x > 0.0f && yr.x > 0.0f) ? de.x : dyy.x,
+                                (yl.y > 0.0f && yr.y > 0.0f) ? de.y : dyy.y);
+  const bool wl0 = yl0 > kDry, wl1 = yl1 > kDry, wr0 = yr0 > kDry, wr1 = yr1 > kDry;
+  const float2 rl = make_float2(hL.x > kDryF ? rcp_approx(hL.x) : 0.0f,
+                                hL.y > kDryF ? rcp_approx(hL.y) : 0.0f);
+  const float2 rr = make_float2(hR.x > kDryF ? rcp_approx(hR.x) : 0.0f,
+                                hR.y > kDryF ? rcp_approx(hR.y) : 0.0f);
+  const float2 ul = mul2(nL, rl), vl = mul2(tL, rl), ur = mul2(nR, rr), vr = mul2(tR, rr);
+  const float2 qnl = mul2(yl, ul), qtl = mul2(yl, vl), qnr = mul2(yr, ur), qtr = mul2(yr, vr);
+  const float2 ml = make_float2(wl0 ? 1.0f : 0.0f, wl1 ? 1.0f : 0.0f);
+  const float2 mr = make_float2(wr0 ? 1.0f : 0.0f, wr1 ? 1.0f : 0.0f);
+  const float2 unl = mul2(ul, ml), utl = mul2(vl, ml), unr = mul2(ur, mr), utr = mul2(vr, mr);
+  const float2 gl = mul2(splat(kGf), yl), gr = mul2(splat(kGf), yr);
+  const float2 al = make_float2(sqrt_approx(gl.x), sqrt_approx(gl.y));
+  const float2 ar = make_float2(sqrt_approx(gr.x), sqrt_approx(gr.y));
+  const float2 a1 = sub2(unl, al), a2 = sub2(unr, ar), b1 = add2(unl, al), b2 = add2(unr, ar);
+  const float2 c1 = fma2(splat(-2.0f), ar, unr), c2 = fma2(splat(2.0f), al, unl);
+  const float2 sl = make_float2(!wr0 ? a1.x : (!wl0 ? c1.x : fminf(a1.x, a2.x)),
+                                !wr1 ? a1.y : (!wl1 ? c1.y : fminf(a1.y, a2.y)));
+  const float2 sr = make_float2(!wr0 ? c2.x : (!wl0 ? b2.x : fmaxf(b1.x, b2.x)),
+                                !wr1 ? c2.y : (!wl1 ? b2.y : fmaxf(b1.y, b2.y)));
+  FaceF2 o;
+  o.dq = mul2(mul2(splat(kHalfGf), dy), add2(yl, yr));
+  const float2 ln = mul2(qnl, unl), rn = mul2(qnr, unr);
+  const float2 lt = mul2(qnl, utl), rt = mul2(qnr, utr);
+  const float2 w = sub2(sr, sl);
+  const float2 inv = make_float2(rcp_approx(w.x), rcp_approx(w.y));
+  const float2 nsl = neg2(sl), nsr = neg2(sr);
+  const float2 dqn = sub2(qnr, qnl);
+  // F = F_L - s_L (F_R - F_L - s_R (U_R - U_L)) / (s_R - s_L)
+  const float2 mfh = fma2(mul2(nsl, fma2(nsr, dy, dqn)), inv, qnl);
+  const float2 men = fma2(mul2(nsl, fma2(nsr, dqn, add2(sub2(rn, ln), o.dq))), inv, ln);
+  float2 mft;
   if (!HLLC) {
-    mft = lt - sl * ((rt - lt) - sr * (qtr - qtl)) * inv;
+    mft = fma2(mul2(nsl, fma2(nsr, sub2(qtr, qtl), sub2(rt, lt))), inv, lt);
   } else {
-    const float den = yr * (unr - sr) - yl * (unl - sl);
-    const float ss = fabsf(den) > kDryF
-                         ? (sl * yr * (unr - sr) - sr * yl * (unl - sl)) * rcp_approx(den)
-                         : 0.5f * (unl + unr);
-    mft = ss >= 0.0f ? mfh * utl : mfh * utr;
+    const float2 den = sub2(mul2(yr, sub2(unr, sr)), mul2(yl, sub2(unl, sl)));
+    const float2 num = sub2(mul2(mul2(sl, yr), sub2(unr, sr)), mul2(mul2(sr, yl), sub2(unl, sl)));
+    const float2 avg = mul2(splat(0.5f), add2(unl, unr));
+    const float ss0 = fabsf(den.x) > kDryF ? num.x * rcp_approx(den.x) : avg.x;
+    const float ss1 = fabsf(den.y) > kDryF ? num.y * rcp_approx(den.y) : avg.y;
+    mft = mul2(mfh, make_float2(ss0 >= 0.0f ? utl.x : utr.x, ss1 >= 0.0f ? utl.y : utr.y));
   }
-  const bool up = sl >= 0.0f, down = sr <= 0.0f;  // supercritical to the right / left
-  o.fh = up ? qnl : (down ? qnr : mfh);
-  o.en = up ? ln : (down ? rn + o.dq : men);
-  o.ft = up ? lt : (down ? rt : mft);
+  const float2 rnq = add2(rn, o.dq);
+  const bool up0 = sl.x >= 0.0f, dn0 = sr.x <= 0.0f, up1 = sl.y >= 0.0f, dn1 = sr.y <= 0.0f;
+  o.fh = make_float2(up0 ? qnl.x : (dn0 ? qnr.x : mfh.x), up1 ? qnl.y : (dn1 ? qnr.y : mfh.y));
+  o.en = make_float2(up0 ? ln.x : (dn0 ? rnq.x : men.x), up1 ? ln.y : (dn1 ? rnq.y : men.y));
+  o.ft = make_float2(up0 ? lt.x : (dn0 ? rt.x : mft.x), up1 ? lt.y : (dn1 ? rt.y : mft.y));
   return o;
 }
 
@@ -268,34 +295,29 @@ __device__ __forceinline__ float cell_pressure(float hc, float s) {
 // threshold tests on the FP64 depth; returns that depth.
 __device__ __forceinline__ double protect(float& e, float& hu, float& hv, double b, float& h) {
   const double hd = (double)e - b;
-  if (hd < 0.0) {
-    e = __double2float_rd(b);
-    hu = 0.0f;
-    hv = 0.0f;
-    h = 0.0f;
-    return 0.0;
-  }
-  h = __double2float_rn(hd);
-  if (hd < kDry) {
-    hu = 0.0f;
-    hv = 0.0f;
-    return hd;
-  }
+  const bool neg = hd < 0.0, wet = hd >= kDry;
+  h = neg ? 0.0f : __double2float_rn(hd);
+  e = neg ? __double2float_rd(b) : e;
+  hu = wet ? hu : 0.0f;
+  hv = wet ? hv : 0.0f;
   const float h2 = h * h;
   const float h4 = h2 * h2;
-  if (h4 < kEps4F) {
-    const float f = kSqrt2F * h2 * rsqrt_approx(h4 + kEps4F);
-    hu = hu * f;
-    hv = hv * f;
-  }
   const float q2 = hu * hu + hv * hv;
   const float lim = kFroude2G * h * h2;  // (Fr_max^2 g h) h^2
-  if (q2 > lim) {
-    const float sc = sqrt_approx(lim) * rsqrt_approx(q2);
-    hu = hu * sc;
-    hv = hv * sc;
+  if (wet && (h4 < kEps4F || q2 > lim)) {  // rare: KP07 and / or the Froude backstop
+    if (h4 < kEps4F) {
+      const float f = kSqrt2F * h2 * rsqrt_approx(h4 + kEps4F);
+      hu = hu * f;
+      hv = hv * f;
+    }
+    const float q2b = hu * hu + hv * hv;
+    if (q2b > lim) {
+      const float sc = sqrt_approx(lim) * rsqrt_approx(q2b);
+      hu = hu * sc;
+      hv = hv * sc;
+    }
   }
-  return hd;
+  return neg ? 0.0 : hd;
 }
 
 // (|u| + c) along x and y with the KP07 velocity (rki_kernel_timestep.F90:52-66).
@@ -371,12 +393,24 @@ __device__ __forceinline__ void yslopes(const Row<C>& m, const Row<C>& c, const 
 template <bool HLLC, int C>
 __device__ __forceinline__ void yfaces(const Row<C>& lo, const Slope (&sl)[C], const Row<C>& hi,
                                        const Slope (&sh)[C], FaceF (&f)[C]) {
+  const float2 half = splat(0.5f), nhalf = splat(-0.5f);
 #pragma unroll
-  for (int k = 0; k < C; ++k)
-    f[k] = face<HLLC>(lo.e[k] + 0.5f * sl[k].e, lo.v[k] + 0.5f * sl[k].v, lo.u[k] + 0.5f * sl[k].u,
-                      fmaxf(lo.h[k] + 0.5f * sl[k].e, 0.0f), lo.b[k], hi.e[k] - 0.5f * sh[k].e,
-                      hi.v[k] - 0.5f * sh[k].v, hi.u[k] - 0.5f * sh[k].u,
-                      fmaxf(hi.h[k] - 0.5f * sh[k].e, 0.0f), hi.b[k]);
+  for (int k = 0; k < C; k += 2) {  // columns k, k + 1 as one pair
+    auto p = [&](float a, float b) { return make_float2(a, b); };
+    const float2 hlo = fma2(half, p(sl[k].e, sl[k + 1].e), p(lo.h[k], lo.h[k + 1]));
+    const float2 hhi = fma2(nhalf, p(sh[k].e, sh[k + 1].e), p(hi.h[k], hi.h[k + 1]));
+    const FaceF2 o = face2<HLLC>(
+        fma2(half, p(sl[k].e, sl[k + 1].e), p(lo.e[k], lo.e[k + 1])),
+        fma2(half, p(sl[k].v, sl[k + 1].v), p(lo.v[k], lo.v[k + 1])),
+        fma2(half, p(sl[k].u, sl[k + 1].u), p(lo.u[k], lo.u[k + 1])),
+        p(fmaxf(hlo.x, 0.0f), fmaxf(hlo.y, 0.0f)), lo.b[k], lo.b[k + 1],
+        fma2(nhalf, p(sh[k].e, sh[k + 1].e), p(hi.e[k], hi.e[k + 1])),
+        fma2(nhalf, p(sh[k].v, sh[k + 1].v), p(hi.v[k], hi.v[k + 1])),
+        fma2(nhalf, p(sh[k].u, sh[k + 1].u), p(hi.u[k], hi.u[k + 1])),
+        p(fmaxf(hhi.x, 0.0f), fmaxf(hhi.y, 0.0f)), hi.b[k], hi.b[k + 1]);
+    f[k] = FaceF{o.fh.x, o.en.x, o.dq.x, o.ft.x};
+    f[k + 1] = FaceF{o.fh.y, o.en.y, o.dq.y, o.ft.y};
+  }
 }
 
 // What a cell keeps of the face below it: mass flux, tangential (hu) flux,
@@ -566,16 +600,28 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
       const float lh = __shfl_sync(kFull, fmaxf(Cr.h[C - 1] + 0.5f * sx[C - 1].e, 0.0f), src_l);
       const double lb = __shfl_sync(kFull, Cr.b[C - 1], src_l);
       FaceF xf[C];
+      {
+        const float2 half = splat(0.5f), nhalf = splat(-0.5f);
+        auto p = [&](float a, float b) { return make_float2(a, b); };
 #pragma unroll
-      for (int k = 0; k < C; ++k) {
-        const float eL = k ? Cr.e[k - 1] + 0.5f * sx[k - 1].e : le;
-        const float uL = k ? Cr.u[k - 1] + 0.5f * sx[k - 1].u : lu;
-        const float vL = k ? Cr.v[k - 1] + 0.5f * sx[k - 1].v : lv;
-        const float hL = k ? fmaxf(Cr.h[k - 1] + 0.5f * sx[k - 1].e, 0.0f) : lh;
-        const double bL = k ? Cr.b[k - 1] : lb;
-        xf[k] = face<HLLC>(eL, uL, vL, hL, bL, Cr.e[k] - 0.5f * sx[k].e, Cr.u[k] - 0.5f * sx[k].u,
-                           Cr.v[k] - 0.5f * sx[k].v, fmaxf(Cr.h[k] - 0.5f * sx[k].e, 0.0f),
-                           Cr.b[k]);
+        for (int k = 0; k < C; k += 2) {
+          // left states: column k - 1 reconstructed right (the left lane's last for k = 0)
+          const float eL0 = k ? Cr.e[k - 1] + 0.5f * sx[k - 1].e : le;
+          const float uL0 = k ? Cr.u[k - 1] + 0.5f * sx[k - 1].u : lu;
+          const float vL0 = k ? Cr.v[k - 1] + 0.5f * sx[k - 1].v : lv;
+          const float hL0 = k ? fmaxf(Cr.h[k - 1] + 0.5f * sx[k - 1].e, 0.0f) : lh;
+          const double bL0 = k ? Cr.b[k - 1] : lb;
+          const FaceF2 o = face2<HLLC>(
+              p(eL0, Cr.e[k] + 0.5f * sx[k].e), p(uL0, Cr.u[k] + 0.5f * sx[k].u),
+              p(vL0, Cr.v[k] + 0.5f * sx[k].v), p(hL0, fmaxf(Cr.h[k] + 0.5f * sx[k].e, 0.0f)), bL0,
+              Cr.b[k], fma2(nhalf, p(sx[k].e, sx[k + 1].e), p(Cr.e[k], Cr.e[k + 1])),
+              fma2(nhalf, p(sx[k].u, sx[k + 1].u), p(Cr.u[k], Cr.u[k + 1])),
+              fma2(nhalf, p(sx[k].v, sx[k + 1].v), p(Cr.v[k], Cr.v[k + 1])),
+              p(fmaxf(Cr.h[k] - 0.5f * sx[k].e, 0.0f), fmaxf(Cr.h[k + 1] - 0.5f * sx[k + 1].e, 0.0f)),
+              Cr.b[k], Cr.b[k + 1]);
+          xf[k] = FaceF{o.fh.x, o.en.x, o.dq.x, o.ft.x};
+          xf[k + 1] = FaceF{o.fh.y, o.en.y, o.dq.y, o.ft.y};
+        }
       }
       // right face of the last column = the right lane's first face
       const float rfh = __shfl_sync(kFull, xf[0].fh, src_r);
@@ -624,14 +670,15 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
         const double hd = protect(e, hu, hv, bc, h);
         const int i = ib + k;
         const bool valid = out_lane && i < g.nxt - g.ng;  // forcing reads stay in bounds
-        if (hd > kDry) {
+        if (friction) {
           // Manning friction (rki_kernel_fused.F90:121-130): hu / (1 + dt g n^2 |q| h^-7/3)
-          if (friction) {
-            const float den = 1.0f + gn2dt * sqrt_approx(hu * hu + hv * hv) * __powf(h, -7.0f / 3.0f);
-            const float r = rcp_approx(den);
-            hu = hu * r;
-            hv = hv * r;
-          }
+          const float den = 1.0f + gn2dt * sqrt_approx(hu * hu + hv * hv) *
+                                       __powf(fmaxf(h, kDryF), -7.0f / 3.0f);
+          const float r = hd > kDry ? rcp_approx(den) : 1.0f;
+          hu = hu * r;
+          hv = hv * r;
+        }
+        if ((forcing || has_cor) && hd > kDry) {
           if (forcing && valid) {  // wind, pressure gradient (rki_kernel_fused.F90:131-146)
             const size_t q = (size_t)i + (size_t)j * (size_t)a.fpitch;
             hu = hu + dt * (float)(a.fo.wind_x[q] / kRho);
@@ -671,14 +718,14 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
         ne[k] = e;
         nu[k] = hu;
         nv[k] = hv;
-        if (valid) {
-          part += (double)dE;
-          if (STAGE == 2) {
-            float sx_, sy_;
-            wave_speed32(hfin, h, hu, hv, sx_, sy_);
-            wsx = fmaxf(wsx, sx_);
-            wsy = fmaxf(wsy, sy_);
-          }
+        part += valid ? (double)dE : 0.0;
+        if (STAGE == 2) {
+          const float c = sqrt_approx(kGf * h);
+          const float h2 = h * h;
+          const float f = kSqrt2F * h * rsqrt_approx(h2 * h2 + kEps4F);
+          const bool w = valid && hfin > kDry;
+          wsx = fmaxf(wsx, w ? fabsf(hu) * f + c : 0.0f);
+          wsy = fmaxf(wsy, w ? fabsf(hv) * f + c : 0.0f);
         }
       }
       if (out_lane) {
