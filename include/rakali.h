@@ -235,6 +235,12 @@ int rkb_restart_write(const char *path, int nx, int ny, const double *h, const d
                       int nghost);
 int rkb_restart_read(const char *path, int nx, int ny, double *h, double *hu, double *hv,
                      double *b, double *time);
+/* bathymetry_file input (src/io/rki_bathymetry.F90:21-163): variable b,
+ * elevation or depth over dimensions x, y (either order) of a NetCDF classic
+ * file into an interior (nx, ny) Fortran-order array; return codes as
+ * rkb_restart_read.  rki_finalize reads the namelist's bathymetry_file this
+ * way unless rki_set_bathymetry was called. */
+int rkb_bathymetry_read(const char *path, int nx, int ny, double *b);
 
 /* Run n steps bracketed by CUDA events on the simulation's own stream;
  * *ms = device time of the n steps (state already resident). */

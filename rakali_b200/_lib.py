@@ -131,6 +131,7 @@ def load(path: str | None = None):
     _sig(lib, "rkb_test_cell_adj", [DP, D, DP, DP], None)
     _sig(lib, "rkb_restart_write", [CP, I, I, DP, DP, DP, DP, D, D, D, I], I)
     _sig(lib, "rkb_restart_read", [CP, I, I, DP, DP, DP, DP, DP], I)
+    _sig(lib, "rkb_bathymetry_read", [CP, I, I, DP], I)
     _sig(lib, "rkb_time_steps", [H, I, DP], I)
     _sig(lib, "rkb_profile_steps", [H, I, DP], I)
     _sig(lib, "rkb_cr_pow_third", [D], D)

@@ -361,6 +361,13 @@ int rkb_restart_write(const char* path, int nx, int ny, const double* h, const d
   return 0;
 }
 
+int rkb_bathymetry_read(const char* path, int nx, int ny, double* b) {
+  if (!path || !b || nx < 1 || ny < 1) return fail(-2, "invalid arguments");
+  std::string err;
+  const int rc = rkb::nc::read_bathymetry(path, nx, ny, b, err);
+  return rc == 0 ? 0 : fail(rc, err);
+}
+
 int rkb_restart_read(const char* path, int nx, int ny, double* h, double* hu, double* hv,
                      double* b, double* time) {
   if (!path || !h || !hu || !hv || !b || !time || nx < 1 || ny < 1)

@@ -456,7 +456,6 @@ int validate(Config& c, std::string& err) {
   if (c.use_multilayer) { err = "use_multilayer is not provided (2D barotropic only)"; return -3; }
   if (c.use_nonhydrostatic) { err = "use_nonhydrostatic is not provided"; return -3; }
   if (c.time_scheme == "semi_implicit") { err = "time_scheme='semi_implicit' is unstructured-only"; return -3; }
-  if (!trim(c.bathymetry_file).empty()) { err = "bathymetry_file (NetCDF) is not read; use set_bathymetry"; return -3; }
   return 0;
 }
 

@@ -184,44 +184,89 @@ bool write_restart(const std::string& path, int nx, int ny, const double* h, con
   return ok;
 }
 
-int read_restart(const std::string& path, int nx, int ny, double* h, double* hu, double* hv,
-                 double* b, double& time, std::string& err) {
+namespace {
+
+// A whole classic file: its dimensions, its variables and the raw bytes.
+struct File {
+  std::vector<unsigned char> data;
+  std::vector<std::pair<std::string, uint32_t>> dims;
+  std::vector<Var> vars;
+
+  int dim(const char* nm) const {
+    for (size_t d = 0; d < dims.size(); ++d)
+      if (dims[d].first == nm) return (int)d;
+    return -1;
+  }
+  const Var* var(const char* nm) const {
+    for (const Var& v : vars)
+      if (v.name == nm) return &v;
+    return nullptr;
+  }
+  // count values of v (FP64 or FP32 in the file) into dst as doubles
+  bool values(const Var& v, uint64_t count, double* dst, std::string& err) const {
+    if (v.type != kDouble && v.type != kFloat) {
+      err = "variable " + v.name + " is neither double nor float";
+      return false;
+    }
+    const uint64_t sz = v.type == kDouble ? 8 : 4;
+    if (v.begin + sz * count > data.size()) {
+      err = "variable " + v.name + " is truncated";
+      return false;
+    }
+    const unsigned char* q = data.data() + v.begin;
+    for (uint64_t k = 0; k < count; ++k, q += sz) {
+      if (sz == 8) {
+        uint64_t u = 0;
+        for (int s = 0; s < 8; ++s) u = u << 8 | q[s];
+        std::memcpy(&dst[k], &u, 8);
+      } else {
+        uint32_t u = 0;
+        for (int s = 0; s < 4; ++s) u = u << 8 | q[s];
+        float x;
+        std::memcpy(&x, &u, 4);
+        dst[k] = x;
+      }
+    }
+    return true;
+  }
+};
+
+bool open_file(const std::string& path, File& F, std::string& err) {
   FILE* f = std::fopen(path.c_str(), "rb");
   if (!f) {
     err = "cannot open " + path;
-    return -1;
+    return false;
   }
-  std::vector<unsigned char> data;
   unsigned char chunk[1 << 16];
   size_t got;
-  while ((got = std::fread(chunk, 1, sizeof(chunk), f)) > 0) data.insert(data.end(), chunk, chunk + got);
+  while ((got = std::fread(chunk, 1, sizeof(chunk), f)) > 0)
+    F.data.insert(F.data.end(), chunk, chunk + got);
   std::fclose(f);
+  const std::vector<unsigned char>& data = F.data;
   if (data.size() >= 8 && std::memcmp(data.data(), "\x89HDF\r\n\x1a\n", 8) == 0) {
     err = path + " is a NetCDF-4 (HDF5) file; this library reads NetCDF classic and "
-                 "64-bit-offset restart files";
-    return -1;
+                 "64-bit-offset files";
+    return false;
   }
   if (data.size() < 4 || std::memcmp(data.data(), "CDF", 3) != 0 || (data[3] != 1 && data[3] != 2)) {
     err = path + " is not a NetCDF classic file";
-    return -1;
+    return false;
   }
   const bool off64 = data[3] == 2;
   In in{data.data(), data.size()};
   in.o = 4;
   in.u32();  // numrecs
-  std::vector<std::pair<std::string, uint32_t>> dims;
   {
     const uint32_t tag = in.u32(), cnt = in.u32();
     if (!(tag == 0 && cnt == 0)) {
       if (tag != kDimTag) in.ok = false;
       for (uint32_t d = 0; d < cnt && in.ok; ++d) {
         std::string nm = in.name();
-        dims.emplace_back(nm, in.u32());
+        F.dims.emplace_back(nm, in.u32());
       }
     }
   }
   in.skip_atts();
-  std::vector<Var> vars;
   {
     const uint32_t tag = in.u32(), cnt = in.u32();
     if (!(tag == 0 && cnt == 0)) {
@@ -235,67 +280,109 @@ int read_restart(const std::string& path, int nx, int ny, double* h, double* hu,
         var.type = in.u32();
         in.u32();  // vsize
         var.begin = off64 ? in.u64() : in.u32();
-        vars.push_back(var);
+        F.vars.push_back(var);
       }
     }
   }
   if (!in.ok) {
     err = path + ": malformed NetCDF header";
-    return -1;
+    return false;
   }
-  int fx = -1, fy = -1;
-  for (size_t d = 0; d < dims.size(); ++d) {
-    if (dims[d].first == "x") fx = (int)d;
-    if (dims[d].first == "y") fy = (int)d;
-  }
+  for (const Var& v : F.vars)
+    for (uint32_t d : v.dims)
+      if (d >= F.dims.size() || F.dims[d].second == 0) {
+        err = path + ": record (unlimited) or unknown dimensions are not supported";
+        return false;
+      }
+  return true;
+}
+
+std::string mismatch(uint32_t fnx, uint32_t fny, int nx, int ny) {
+  return "grid mismatch: file has " + std::to_string(fnx) + " x " + std::to_string(fny) +
+         " but the simulation expects " + std::to_string(nx) + " x " + std::to_string(ny);
+}
+
+}  // namespace
+
+int read_restart(const std::string& path, int nx, int ny, double* h, double* hu, double* hv,
+                 double* b, double& time, std::string& err) {
+  File F;
+  if (!open_file(path, F, err)) return -1;
+  const int fx = F.dim("x"), fy = F.dim("y");
   if (fx < 0 || fy < 0) {
     err = path + ": dimensions x and y not found";
     return -1;
   }
-  if ((int)dims[fx].second != nx || (int)dims[fy].second != ny) {
-    err = "restart grid mismatch: file has " + std::to_string(dims[fx].second) + " x " +
-          std::to_string(dims[fy].second) + " but the simulation expects " + std::to_string(nx) +
-          " x " + std::to_string(ny);
+  if ((int)F.dims[fx].second != nx || (int)F.dims[fy].second != ny) {
+    err = "restart " + mismatch(F.dims[fx].second, F.dims[fy].second, nx, ny);
     return 1;
   }
   const uint64_t n2 = (uint64_t)nx * (uint64_t)ny;
-  auto read_var = [&](const char* nm, double* dst, uint64_t count) -> bool {
-    for (const Var& v : vars) {
-      if (v.name != nm) continue;
-      const bool shape_ok = count == 1 ? v.dims.empty()
-                                       : (v.dims.size() == 2 && v.dims[0] == (uint32_t)fy &&
-                                          v.dims[1] == (uint32_t)fx);
-      if (!shape_ok || (v.type != kDouble && v.type != kFloat)) {
-        err = path + ": variable " + nm + " has an unexpected shape or type";
-        return false;
-      }
-      const uint64_t sz = v.type == kDouble ? 8 : 4;
-      if (v.begin + sz * count > data.size()) {
-        err = path + ": variable " + nm + " is truncated";
-        return false;
-      }
-      const unsigned char* q = data.data() + v.begin;
-      for (uint64_t k = 0; k < count; ++k, q += sz) {
-        if (sz == 8) {
-          uint64_t u = 0;
-          for (int s = 0; s < 8; ++s) u = u << 8 | q[s];
-          std::memcpy(&dst[k], &u, 8);
-        } else {
-          uint32_t u = 0;
-          for (int s = 0; s < 4; ++s) u = u << 8 | q[s];
-          float x;
-          std::memcpy(&x, &u, 4);
-          dst[k] = x;
-        }
-      }
-      return true;
+  auto field = [&](const char* nm, double* dst, uint64_t count) -> bool {
+    const Var* v = F.var(nm);
+    if (!v) {
+      err = path + ": variable " + nm + " not found";
+      return false;
     }
-    err = path + ": variable " + nm + " not found";
-    return false;
+    const bool shape_ok = count == 1 ? v->dims.empty()
+                                     : (v->dims.size() == 2 && v->dims[0] == (uint32_t)fy &&
+                                        v->dims[1] == (uint32_t)fx);
+    if (!shape_ok) {
+      err = path + ": variable " + nm + " has an unexpected shape";
+      return false;
+    }
+    if (!F.values(*v, count, dst, err)) {
+      err = path + ": " + err;
+      return false;
+    }
+    return true;
   };
-  if (!read_var("h", h, n2) || !read_var("hu", hu, n2) || !read_var("hv", hv, n2) ||
-      !read_var("b", b, n2) || !read_var("time", &time, 1))
+  if (!field("h", h, n2) || !field("hu", hu, n2) || !field("hv", hv, n2) || !field("b", b, n2) ||
+      !field("time", &time, 1))
     return -1;
+  return 0;
+}
+
+// load_bathymetry_into_array (src/io/rki_bathymetry.F90:21-138): variable b,
+// elevation or depth (first found) over dimensions x, y in either order.
+int read_bathymetry(const std::string& path, int nx, int ny, double* b, std::string& err) {
+  File F;
+  if (!open_file(path, F, err)) return -1;
+  const int fx = F.dim("x"), fy = F.dim("y");
+  if (fx < 0 || fy < 0) {
+    err = path + ": dimensions x and y not found";
+    return -1;
+  }
+  const Var* v = nullptr;
+  for (const char* nm : {"b", "elevation", "depth"})
+    if (!v) v = F.var(nm);
+  if (!v) {
+    err = path + ": no bathymetry variable (tried: b, elevation, depth)";
+    return -1;
+  }
+  if (v->dims.size() != 2) {
+    err = path + ": bathymetry variable " + v->name + " is not 2-D";
+    return -1;
+  }
+  // file (row-major) dims (y, x): x varies fastest, as in the Fortran array;
+  // (x, y): a C-order b[x][y], read transposed
+  const bool transposed = v->dims[1] == (uint32_t)fy;
+  const uint32_t fnx = F.dims[transposed ? v->dims[0] : v->dims[1]].second;
+  const uint32_t fny = F.dims[transposed ? v->dims[1] : v->dims[0]].second;
+  if ((int)fnx != nx || (int)fny != ny) {
+    err = "bathymetry " + mismatch(fnx, fny, nx, ny);
+    return 1;
+  }
+  const uint64_t n2 = (uint64_t)nx * (uint64_t)ny;
+  std::vector<double> tmp(n2);
+  if (!F.values(*v, n2, tmp.data(), err)) {
+    err = path + ": " + err;
+    return -1;
+  }
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i)
+      b[(size_t)i + (size_t)j * nx] =
+          transposed ? tmp[(size_t)j + (size_t)i * ny] : tmp[(size_t)i + (size_t)j * nx];
   return 0;
 }
 

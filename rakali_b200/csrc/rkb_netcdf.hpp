@@ -5,9 +5,9 @@
 // attributes, a scalar "time", and global attributes Conventions, title,
 // source, dx, dy, nghost.  The reference writes NetCDF-4 (an HDF5 container)
 // through libnetcdf; classic files hold the same variables and every NetCDF
-// library (netcdf-fortran's nf90_open included) reads them.  The reader
-// accepts classic and 64-bit-offset files and refuses HDF5 containers with a
-// message.
+// library (netcdf-fortran's nf90_open included) reads them.  The readers
+// accept classic and 64-bit-offset files with fixed-size variables and refuse
+// HDF5 containers with a message.
 #pragma once
 
 #include <string>
@@ -24,6 +24,11 @@ bool write_restart(const std::string& path, int nx, int ny, const double* h, con
 // 0: read; 1: the file's grid is not nx x ny; -1: not readable (err says why).
 int read_restart(const std::string& path, int nx, int ny, double* h, double* hu, double* hv,
                  double* b, double& time, std::string& err);
+
+// Bathymetry input (src/io/rki_bathymetry.F90:21-163): the first of the
+// variables b, elevation, depth, over dimensions x, y in either order, into
+// an interior (nx, ny) Fortran-order array.  Return codes as read_restart.
+int read_bathymetry(const std::string& path, int nx, int ny, double* b, std::string& err);
 
 }  // namespace nc
 }  // namespace rkb

@@ -13,6 +13,12 @@ namespace {
 
 size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
 
+std::string trim_copy(const std::string& s) {
+  const size_t a = s.find_first_not_of(" \t\r\n");
+  if (a == std::string::npos) return {};
+  return s.substr(a, s.find_last_not_of(" \t\r\n") - a + 1);
+}
+
 // Shu-Osher coefficients of the time schemes (rki_timestepper.F90:60-100):
 // stage k steps beta_k dt from X_k at time t + c_k dt, then mixes alpha_k U^n
 // + (1 - alpha_k) X_k+1 when alpha_k != 0.  ssp_coeff scales the CFL step.
@@ -188,6 +194,14 @@ int Sim::finalize(std::string& err) {
   const int nxt = g.nxt, nyt = g.nyt, ng = g.ng;
   double* b = hf_[3];
   auto at = [&](int i, int j) { return (size_t)i + (size_t)j * (size_t)nxt; };
+  // bathymetry_file unless the caller set the bed (rki_api.F90:238-240)
+  const std::string bfile = trim_copy(cfg.bathymetry_file);
+  if (!user_set_bathymetry && !bfile.empty()) {
+    std::vector<double> bi((size_t)cfg.nx * cfg.ny);
+    if (nc::read_bathymetry(bfile, cfg.nx, cfg.ny, bi.data(), err) != 0) return -3;
+    for (int j = 0; j < cfg.ny; ++j)
+      std::memcpy(b + at(ng, ng + j), bi.data() + (size_t)j * cfg.nx, (size_t)cfg.nx * sizeof(double));
+  }
   // fill_bathymetry_ghosts_array (src/io/rki_bathymetry.F90:165-196)
   for (int j = 0; j < nyt; ++j)
     for (int i = 0; i < ng; ++i) {

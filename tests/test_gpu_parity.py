@@ -446,3 +446,27 @@ def test_restart_refuses_grid_mismatch_and_finalised_handle(tmp_path):
         assert sim._lib.rki_load_restart(sim._handle, raw, len(raw)) == -2  # finalised
     with pytest.raises(RuntimeError, match="mismatch"):
         Rakali.from_restart(path, nx=17, ny=12, dx=1.0, dy=1.0, t_end=10.0)
+
+
+def test_bathymetry_file_equals_set_bathymetry(tmp_path):
+    """A namelist bathymetry_file (NetCDF classic) loads the same bed as
+    set_bathymetry: same ghosts, same initial condition, same steps."""
+    from scipy.io import netcdf_file
+
+    from rakali_b200 import Rakali
+    nx, ny, dx = 64, 48, 10.0
+    b = gaussian_bed(nx, ny, dx, dx, 8, seed=5, width=(30.0, 120.0))
+    path = tmp_path / "bed.nc"
+    with netcdf_file(str(path), "w", version=2) as f:
+        f.createDimension("x", nx)
+        f.createDimension("y", ny)
+        f.createVariable("elevation", "d", ("y", "x"))[:] = b.T
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, manning_n=0.02,
+               init_condition="still_water", eta_initial=0.2)
+    with Rakali(bathymetry_file=str(path), **cfg) as s1, Rakali(defer_init=True, **cfg) as s2:
+        s2.set_bathymetry(b)
+        s2.finalize()
+        assert np.array_equal(s1.b, s2.b) and np.array_equal(s1.h, s2.h)
+        s1.step(20)
+        s2.step(20)
+        assert np.array_equal(s1.h, s2.h) and np.array_equal(s1.hu, s2.hu)

@@ -100,3 +100,42 @@ def test_round_trip_and_refusals(lib, tmp_path):
     assert "HDF5" in _lib.last_error(lib)
     assert lib.rkb_restart_read(str(tmp_path / "none.nc").encode(), nx, ny, *map(_p, out),
                                 ctypes.byref(tm)) == -1
+
+
+def _scipy_bed(path, nx, ny, arr, name="b", order="yx", version=2):
+    from scipy.io import netcdf_file
+    with netcdf_file(str(path), "w", version=version) as f:
+        f.createDimension("x", nx)
+        f.createDimension("y", ny)
+        if order == "yx":  # row-major (y, x): x fastest, the Fortran (x, y) array
+            v = f.createVariable(name, "d", ("y", "x"))
+            v[:] = arr.T
+        else:  # a C-order b[x][y]
+            v = f.createVariable(name, "f", ("x", "y"))
+            v[:] = arr.astype(np.float32)
+
+
+@pytest.mark.parametrize("name,order", [("b", "yx"), ("elevation", "xy"), ("depth", "yx")])
+def test_bathymetry_file_reads_like_the_reference(lib, tmp_path, name, order):
+    """load_bathymetry_into_array (src/io/rki_bathymetry.F90:21-163): b, elevation or
+    depth over x, y in either order (a C-order (x, y) variable is read transposed)."""
+    nx, ny = 7, 5
+    arr = np.asfortranarray(np.random.default_rng(4).standard_normal((nx, ny)))
+    path = tmp_path / "bed.nc"
+    _scipy_bed(path, nx, ny, arr, name, order)
+    out = np.zeros((nx, ny), order="F")
+    assert lib.rkb_bathymetry_read(str(path).encode(), nx, ny, _p(out)) == 0
+    ref = arr if order == "yx" else arr.astype(np.float32).astype(np.float64)
+    assert np.array_equal(out, ref)
+    assert lib.rkb_bathymetry_read(str(path).encode(), nx, ny + 1,
+                                   _p(np.zeros((nx, ny + 1), order="F"))) == 1
+
+
+def test_bathymetry_file_without_known_variable(lib, tmp_path):
+    from rakali_b200 import _lib
+    nx, ny = 4, 3
+    path = tmp_path / "bed.nc"
+    _scipy_bed(path, nx, ny, np.zeros((nx, ny)), name="topo")
+    out = np.zeros((nx, ny), order="F")
+    assert lib.rkb_bathymetry_read(str(path).encode(), nx, ny, _p(out)) == -1
+    assert "b, elevation, depth" in _lib.last_error(lib)
