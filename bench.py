@@ -626,7 +626,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile", type=int, default=1,
                     help="stage-kernel variant (rkb_set_tile): 0-3 shared-memory tiles, "
-                         "4/5 marching strips of 64/32 rows")
+                         "4/5 marching strips of 64/32 rows, 6/7 tiles 32x8 / 32x12 with two "
+                         "extra warps")
     ap.add_argument("--precision", type=int, choices=(32, 64), default=64,
                     help="headline form: 64 = FP64 depth form (reference arithmetic), "
                          "32 = FP32 surface form")

@@ -534,7 +534,9 @@ class Rakali:
                      for p in ptrs)
 
     def set_tile(self, tile: int):
-        """Tile shape of the fused stage kernel (0: 32x8, 1: 32x16, 2: 64x4, 3: 16x16)."""
+        """Kernel shape of the FP64 stage (0: 32x8, 1: 32x16, 2: 64x4, 3: 16x16 tiles;
+        4 / 5: marching strips of 64 / 32 rows; 6 / 7: 32x8 / 32x12 tiles with two extra
+        warps)."""
         self._check_alive()
         self._rc(self._lib.rkb_set_tile(self._handle, int(tile)), "set_tile")
 

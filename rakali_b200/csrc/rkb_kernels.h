@@ -33,7 +33,8 @@ struct FluxOut {
 enum TileShape : int {
   kTile32x8 = 0, kTile32x16 = 1, kTile64x4 = 2, kTile16x16 = 3,  // shared-memory tiles
   kMarch64 = 4, kMarch32 = 5,  // warp-per-strip marching kernel, 64 / 32 rows per warp
-  kNumTiles = 6
+  kTile32x8w = 6, kTile32x12w = 7,  // shared-memory tiles with two extra warps
+  kNumTiles = 8
 };
 const char* tile_name(int tile);
 void tile_dims(int tile, int& tx, int& ty);

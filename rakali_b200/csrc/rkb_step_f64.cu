@@ -342,8 +342,10 @@ __device__ __forceinline__ void sponge(double& h, double& u, double& v, const Bc
 //          (rki_solver.F90:861-926): X_gk -> X_gk+1 with step beta_gk dt,
 //          then the SSP combination with U^n when alpha_gk != 0.  The last
 //          stage closes the step without the boundary mass budget.
-// Tile (bx, by) of a gx x gy tiling of one simulation.
-template <int TX, int TY, bool HLLC, int STAGE>
+// Tile (bx, by) of a gx x gy tiling of one simulation, with TX * TY + 32 XW
+// threads: XW extra warps share the slope and face loops (so that no warp
+// runs a third, mostly empty face round) and sit out the cell update.
+template <int TX, int TY, bool HLLC, int STAGE, int XW = 0>
 __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Physics* phys,
                                            const BcParams* bcp, const FieldSet& U0,
                                            const FieldSet& U1, const FieldSet& S,
@@ -353,7 +355,7 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
                                            int gk = 0) {
   using SM = StageSmem<TX, TY>;
   constexpr int TW = SM::TW;
-  constexpr int NTH = TX * TY;
+  constexpr int NTH = TX * TY + 32 * XW;
   extern __shared__ double smem[];
   double* th = smem;
   double* tu = th + SM::NT;
@@ -462,10 +464,12 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
   }
   __syncthreads();
 
-  // 4. cell update: one cell per thread
-  const int c = tid % TX, r = tid / TX;
+  // 4. cell update: one cell per thread (the extra warps repeat cell 0 and
+  // store nothing)
+  const int tc = tid < TX * TY ? tid : 0;
+  const int c = tc % TX, r = tc / TX;
   const int i = gx0 + c, j = gy0 + r;
-  const bool valid = i < g.nxt - g.ng && j < g.nyt - g.ng;
+  const bool valid = tid < TX * TY && i < g.nxt - g.ng && j < g.nyt - g.ng;
   const int fl_ = r * (TX + 1) + c, fr_ = fl_ + 1;
   const int fb_ = r * TX + c, ft_ = fb_ + TX;
   const double dx = g.dx, dy = g.dy;
@@ -587,19 +591,19 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
   finalize_step(g, ctl, phys, partials, nblocks, step_dt, cur, kBudget);
 }
 
-template <int TX, int TY, bool HLLC, int STAGE>
-__global__ void __launch_bounds__(TX * TY)
+template <int TX, int TY, bool HLLC, int STAGE, int XW = 0>
+__global__ void __launch_bounds__(TX * TY + 32 * XW)
     k_stage(Grid g, StepCtl* ctl, const Physics* phys, const BcParams* bcp, FieldSet U0,
             FieldSet U1, FieldSet S, const double* __restrict__ b, Forcing fo,
             double* __restrict__ partials, FluxOut fl, int gk) {
-  stage_body<TX, TY, HLLC, STAGE>(g, ctl, phys, bcp, U0, U1, S, b, fo, partials, fl, blockIdx.x,
-                                  blockIdx.y, gridDim.x, gridDim.y, gk);
+  stage_body<TX, TY, HLLC, STAGE, XW>(g, ctl, phys, bcp, U0, U1, S, b, fo, partials, fl,
+                                      blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, gk);
 }
 
 // Every simulation of a batch in one launch: map[blockIdx.x] = (simulation,
 // tile index within that simulation's tiling).
-template <int TX, int TY, bool HLLC, int STAGE>
-__global__ void __launch_bounds__(TX * TY)
+template <int TX, int TY, bool HLLC, int STAGE, int XW = 0>
+__global__ void __launch_bounds__(TX * TY + 32 * XW)
     k_stage_batch(const StepArgs* __restrict__ args, const int2* __restrict__ map) {
   __shared__ StepArgs sa;
   const int2 m = map[blockIdx.x];
@@ -608,9 +612,9 @@ __global__ void __launch_bounds__(TX * TY)
   const unsigned gx = (unsigned)((sa.g.nx_phys() + TX - 1) / TX);
   const unsigned gy = (unsigned)((sa.g.ny_phys() + TY - 1) / TY);
   const FluxOut none{};
-  stage_body<TX, TY, HLLC, STAGE>(sa.g, sa.ctl, sa.phys, sa.bc, sa.U0, sa.U1, sa.S, sa.b, sa.fo,
-                                  sa.partials, none, (unsigned)m.y % gx, (unsigned)m.y / gx, gx,
-                                  gy);
+  stage_body<TX, TY, HLLC, STAGE, XW>(sa.g, sa.ctl, sa.phys, sa.bc, sa.U0, sa.U1, sa.S, sa.b,
+                                      sa.fo, sa.partials, none, (unsigned)m.y % gx,
+                                      (unsigned)m.y / gx, gx, gy);
 }
 
 // ---------------------------------------------------------------------------
@@ -835,6 +839,8 @@ const char* tile_name(int tile) {
     case kTile32x16: return "32x16";
     case kTile64x4: return "64x4";
     case kTile16x16: return "16x16";
+    case kTile32x8w: return "32x8+2w";
+    case kTile32x12w: return "32x12+2w";
     case kMarch64: return "march28x64";
     default: return "march28x32";
   }
@@ -846,6 +852,8 @@ void tile_dims(int tile, int& tx, int& ty) {
     case kTile32x16: tx = 32; ty = 16; break;
     case kTile64x4: tx = 64; ty = 4; break;
     case kTile16x16: tx = 16; ty = 16; break;
+    case kTile32x8w: tx = 32; ty = 8; break;
+    case kTile32x12w: tx = 32; ty = 12; break;
     case kMarch64: tx = kMarchCols * kMarchWarps; ty = 64; break;
     default: tx = kMarchCols * kMarchWarps; ty = 32; break;
   }
@@ -865,12 +873,12 @@ size_t partials_doubles(const Grid& g, int tile) {
   return 4 * parts;
 }
 
-template <int TX, int TY, bool HLLC, int STAGE>
+template <int TX, int TY, bool HLLC, int STAGE, int XW = 0>
 static cudaError_t launch_stage_t(const StepArgs& a, FluxOut fl, cudaStream_t s, int gk) {
   using SM = StageSmem<TX, TY>;
-  auto kern = k_stage<TX, TY, HLLC, STAGE>;
+  auto kern = k_stage<TX, TY, HLLC, STAGE, XW>;
   dim3 grid = stage_grid(a.g, a.tile);
-  kern<<<grid, TX * TY, SM::BYTES, s>>>(a.g, a.ctl, a.phys, a.bc, a.U0, a.U1, a.S, a.b, a.fo,
+  kern<<<grid, TX * TY + 32 * XW, SM::BYTES, s>>>(a.g, a.ctl, a.phys, a.bc, a.U0, a.U1, a.S, a.b, a.fo,
                                         a.partials, fl, gk);
   return cudaGetLastError();
 }
@@ -883,17 +891,15 @@ static cudaError_t launch_march_t(const StepArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <int TX, int TY, bool HLLC>
+template <int TX, int TY, bool HLLC, int XW = 0>
 static cudaError_t configure_t() {
   cudaError_t e = cudaSuccess;
   const int bytes = (int)StageSmem<TX, TY>::BYTES;
-  e = cudaFuncSetAttribute(k_stage<TX, TY, HLLC, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_stage<TX, TY, HLLC, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_stage<TX, TY, HLLC, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_stage<TX, TY, HLLC, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  e = cudaFuncSetAttribute(k_stage<TX, TY, HLLC, 0, XW>, attr, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<TX, TY, HLLC, 1, XW>, attr, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<TX, TY, HLLC, 2, XW>, attr, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<TX, TY, HLLC, 3, XW>, attr, bytes);
   return e;
 }
 
@@ -904,6 +910,8 @@ cudaError_t configure_kernels(int tile, int hllc) {
     case kTile32x16: return h ? configure_t<32, 16, true>() : configure_t<32, 16, false>();
     case kTile64x4: return h ? configure_t<64, 4, true>() : configure_t<64, 4, false>();
     case kTile16x16: return h ? configure_t<16, 16, true>() : configure_t<16, 16, false>();
+    case kTile32x8w: return h ? configure_t<32, 8, true, 2>() : configure_t<32, 8, false, 2>();
+    case kTile32x12w: return h ? configure_t<32, 12, true, 2>() : configure_t<32, 12, false, 2>();
     // marching kernels use no dynamic shared memory; the generic stages run
     // on 32x16 tiles under them
     default: return h ? configure_t<32, 16, true>() : configure_t<32, 16, false>();
@@ -922,6 +930,10 @@ static cudaError_t launch_stage(const StepArgs& a, FluxOut fl, cudaStream_t s, i
       return h ? launch_stage_t<64, 4, true, STAGE>(a, fl, s, gk) : launch_stage_t<64, 4, false, STAGE>(a, fl, s, gk);
     case kTile16x16:
       return h ? launch_stage_t<16, 16, true, STAGE>(a, fl, s, gk) : launch_stage_t<16, 16, false, STAGE>(a, fl, s, gk);
+    case kTile32x8w:
+      return h ? launch_stage_t<32, 8, true, STAGE, 2>(a, fl, s, gk) : launch_stage_t<32, 8, false, STAGE, 2>(a, fl, s, gk);
+    case kTile32x12w:
+      return h ? launch_stage_t<32, 12, true, STAGE, 2>(a, fl, s, gk) : launch_stage_t<32, 12, false, STAGE, 2>(a, fl, s, gk);
     default:
       break;
   }
@@ -1017,13 +1029,13 @@ int batch_stage_blocks(const Grid& g, int tile) {
   return (int)(d.x * d.y);
 }
 
-template <int TX, int TY, bool HLLC>
+template <int TX, int TY, bool HLLC, int XW = 0>
 static cudaError_t configure_batch_t() {
   const int bytes = (int)StageSmem<TX, TY>::BYTES;
-  cudaError_t e = cudaFuncSetAttribute(k_stage_batch<TX, TY, HLLC, 1>,
+  cudaError_t e = cudaFuncSetAttribute(k_stage_batch<TX, TY, HLLC, 1, XW>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_stage_batch<TX, TY, HLLC, 2>,
+    e = cudaFuncSetAttribute(k_stage_batch<TX, TY, HLLC, 2, XW>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   return e;
 }
@@ -1035,13 +1047,16 @@ cudaError_t configure_batch(int tile, int hllc) {
     case kTile32x16: return h ? configure_batch_t<32, 16, true>() : configure_batch_t<32, 16, false>();
     case kTile64x4: return h ? configure_batch_t<64, 4, true>() : configure_batch_t<64, 4, false>();
     case kTile16x16: return h ? configure_batch_t<16, 16, true>() : configure_batch_t<16, 16, false>();
+    case kTile32x8w: return h ? configure_batch_t<32, 8, true, 2>() : configure_batch_t<32, 8, false, 2>();
+    case kTile32x12w: return h ? configure_batch_t<32, 12, true, 2>() : configure_batch_t<32, 12, false, 2>();
     default: return cudaErrorInvalidValue;  // batches use the shared-memory tiles
   }
 }
 
-template <int TX, int TY, bool HLLC, int STAGE>
+template <int TX, int TY, bool HLLC, int STAGE, int XW = 0>
 static cudaError_t launch_stage_batch_t(const BatchLaunch& bl, cudaStream_t s) {
-  k_stage_batch<TX, TY, HLLC, STAGE><<<(unsigned)bl.blocks, TX * TY, StageSmem<TX, TY>::BYTES, s>>>(
+  k_stage_batch<TX, TY, HLLC, STAGE, XW>
+      <<<(unsigned)bl.blocks, TX * TY + 32 * XW, StageSmem<TX, TY>::BYTES, s>>>(
       bl.args, bl.map);
   return cudaGetLastError();
 }
@@ -1058,6 +1073,10 @@ static cudaError_t launch_stage_batch(const BatchLaunch& bl, cudaStream_t s) {
       return h ? launch_stage_batch_t<64, 4, true, STAGE>(bl, s) : launch_stage_batch_t<64, 4, false, STAGE>(bl, s);
     case kTile16x16:
       return h ? launch_stage_batch_t<16, 16, true, STAGE>(bl, s) : launch_stage_batch_t<16, 16, false, STAGE>(bl, s);
+    case kTile32x8w:
+      return h ? launch_stage_batch_t<32, 8, true, STAGE, 2>(bl, s) : launch_stage_batch_t<32, 8, false, STAGE, 2>(bl, s);
+    case kTile32x12w:
+      return h ? launch_stage_batch_t<32, 12, true, STAGE, 2>(bl, s) : launch_stage_batch_t<32, 12, false, STAGE, 2>(bl, s);
     default:
       return cudaErrorInvalidValue;
   }

@@ -293,7 +293,7 @@ def test_tiles_agree():
     h = hump_depth(b, dx, dx, width=40.0)
     cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, use_hllc=True)
     ref = None
-    for tile in range(6):
+    for tile in range(8):
         sim, _ = pair(cfg, bathymetry=b, initial_h=h)
         with sim:
             sim.set_tile(tile)
