@@ -514,6 +514,42 @@ def run_config5(args):
         dfl = float(np.sum(gbf[0] * db) + np.sum(gnf[0] * dn))
         dd.append(abs(d32 - d64) / abs(d64))
         dd_floor.append(abs(dfl - d64) / abs(d64))
+    # The same comparison over the first steps only, where J is smooth at the
+    # scale of FP32 rounding (over all 500 steps the gradient of either
+    # precision moves by O(1) under the 1e-7 bed perturbation above).
+    ks = min(args.c5_cmp_steps, steps)
+    short = {}
+    for prec in (32, 64):
+        with GaugeMisfitBatch(1, n, n, dx, dx, ref["h"][None], [ref["gauges"]], ks,
+                              precision=prec) as ps:
+            ps.set_dt(ref["dt"][None, :ks])
+            ps.set_observations(ref["obs"][:ks, None, :])
+            Js, gbs, gns = ps.gradient(ref["b"][None], ref["n"][None])
+            short[prec] = (float(Js[0]), gbs[0], gns[0])
+            if prec == 64:
+                _, gbsf, gnsf = ps.gradient(ref["b"][None] + pert, ref["n"][None])
+    sd, sd_floor = [], []
+    for k in range(8):
+        db = wl.gaussian_bed(n, n, dx, dx, 3, 700 + k, base=0.0, amp=(-1.0, 1.0),
+                             width=(200.0, 1500.0))
+        dn = wl.gaussian_bed(n, n, dx, dx, 3, 800 + k, base=0.0, amp=(-0.01, 0.01),
+                             width=(200.0, 1500.0))
+        d64 = float(np.sum(short[64][1] * db) + np.sum(short[64][2] * dn))
+        d32 = float(np.sum(short[32][1] * db) + np.sum(short[32][2] * dn))
+        dfl = float(np.sum(gbsf[0] * db) + np.sum(gnsf[0] * dn))
+        sd.append(abs(d32 - d64) / abs(d64))
+        sd_floor.append(abs(dfl - d64) / abs(d64))
+    first_steps = {
+        "steps": ks,
+        "J_rel_err": abs(short[32][0] - short[64][0]) / abs(short[64][0]),
+        "grad_b_rel_l2": rel(short[32][1], short[64][1]),
+        "grad_n_rel_l2": rel(short[32][2], short[64][2]),
+        "directional_rel_err_median": float(np.median(sd)),
+        "directional_rel_err_max": float(np.max(sd)),
+        "fp64_floor": {"grad_b_rel_l2": rel(gbsf[0], short[64][1]),
+                       "grad_n_rel_l2": rel(gnsf[0], short[64][2]),
+                       "directional_rel_err_median": float(np.median(sd_floor)),
+                       "directional_rel_err_max": float(np.max(sd_floor))}}
     return {
         "workload": f"{nm} members x {n}x{n}, dx = {dx} m, 16-Gaussian bed per member "
                     f"(seeds 1000..{1000 + nm - 1}), 0.5 m hump on a smooth undulation, "
@@ -526,6 +562,7 @@ def run_config5(args):
         "forward_plus_adjoint_cell_updates_per_s": cells / (grad_ms * 1e-3),
         "cost_multiple_of_forward": grad_ms / fwd_ms,
         "mass_drift_rel_max": drift,
+        "vs_fp64_member0_first_steps": first_steps,
         "vs_fp64_member0": {
             "J_rel_err": abs(ref["J"] - float(J64[0])) / abs(float(J64[0])),
             "grad_b_rel_l2": rel(ref["gb"], gb64[0]), "grad_n_rel_l2": rel(ref["gn"], gn64[0]),
@@ -650,6 +687,8 @@ def main():
     ap.add_argument("--c5-members", type=int, default=64)
     ap.add_argument("--c5-side", type=int, default=2048)
     ap.add_argument("--c5-steps", type=int, default=500)
+    ap.add_argument("--c5-cmp-steps", type=int, default=50,
+                    help="steps of the FP32-vs-FP64 gradient comparison on member 0")
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the FP32-vs-FP64 error measurement")
     ap.add_argument("--sweep-cols", type=int, choices=(0, 2, 4), default=0,

@@ -242,6 +242,29 @@ int rkb_restart_read(const char *path, int nx, int ny, double *h, double *hu, do
  * way unless rki_set_bathymetry was called. */
 int rkb_bathymetry_read(const char *path, int nx, int ny, double *b);
 
+/* Gauge stations (src/io/structured/rki_gauges.F90) recorded on the device
+ * after every step, without host synchronisation: x, y in metres from the
+ * domain's lower-left corner; stations outside the domain are dropped;
+ * bilinear stencils and weights as compute_interp_weights (:245-336);
+ * interval = gauge_output_interval (s, <= 0: every step) with the driver's
+ * cadence (rki_driver.F90:469-473); capacity = records held on the device.
+ * Needs a finalised handle; returns the number of stations kept.  n = 0
+ * removes the stations. */
+int rkb_set_gauges(void *handle, int n, const double *x, const double *y, double interval,
+                   int capacity);
+/* For the kept stations: station[k] = index in the list given, station_b[k] =
+ * bilinear bed (either may be NULL); returns their number. */
+int rkb_gauge_stations(void *handle, int *station, double *station_b);
+/* Move up to max_records records to the host: times [count], values
+ * [count][stations][3] = eta, u, v (gauges_write, :490-575); returns count;
+ * *overflow = 1 if records were dropped because the buffer was full. */
+int rkb_read_gauges(void *handle, int max_records, double *times, double *values, int *overflow);
+/* Write a gauge file in the layout of create_gauge_netcdf (:338-488) as
+ * NetCDF classic: names are n fixed-width fields of name_len characters. */
+int rkb_write_gauges_netcdf(const char *path, int n, const char *names, int name_len,
+                            const double *x, const double *y, const double *b, int n_records,
+                            const double *times, const double *values);
+
 /* Run n steps bracketed by CUDA events on the simulation's own stream;
  * *ms = device time of the n steps (state already resident). */
 int rkb_time_steps(void *handle, int n, double *ms);

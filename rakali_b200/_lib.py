@@ -132,6 +132,10 @@ def load(path: str | None = None):
     _sig(lib, "rkb_restart_write", [CP, I, I, DP, DP, DP, DP, D, D, D, I], I)
     _sig(lib, "rkb_restart_read", [CP, I, I, DP, DP, DP, DP, DP], I)
     _sig(lib, "rkb_bathymetry_read", [CP, I, I, DP], I)
+    _sig(lib, "rkb_set_gauges", [H, I, DP, DP, D, I], I)
+    _sig(lib, "rkb_gauge_stations", [H, IP, DP], I)
+    _sig(lib, "rkb_read_gauges", [H, I, DP, DP, IP], I)
+    _sig(lib, "rkb_write_gauges_netcdf", [CP, I, CP, I, DP, DP, DP, I, DP, DP], I)
     _sig(lib, "rkb_time_steps", [H, I, DP], I)
     _sig(lib, "rkb_profile_steps", [H, I, DP], I)
     _sig(lib, "rkb_cr_pow_third", [D], D)

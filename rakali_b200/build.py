@@ -31,6 +31,7 @@ UNITS = {
     "rkb_step_f64.cu": ["--fmad=false"],
     "rkb_kernel_api.cu": ["--fmad=false"],
     "rkb_adjoint.cu": ["--fmad=false"],
+    "rkb_gauges.cu": ["--fmad=false"],
     # FP32 surface form: contracted multiply-adds, flush-to-zero, approximate
     # reciprocal and square root (the well-balanced products are written
     # with explicit round-to-nearest intrinsics and are never contracted)

@@ -487,6 +487,98 @@ class Rakali:
         raw = str(filename).encode()
         self._rc(self._lib.rki_save_restart(self._handle, raw, len(raw)), "save_restart")
 
+    # --- gauges (src/io/structured/rki_gauges.F90) --------------------------
+    def set_gauges(self, x, y, names=None, interval=0.0, capacity=65536):
+        """Record eta, u, v at stations (x, y in metres from the lower-left
+        corner) on the device after every step: bilinear stencils as the
+        reference's compute_interp_weights, cadence as its driver (every step
+        for interval <= 0, else every `interval` seconds).  Stations outside the
+        domain are dropped; returns the number kept.  Replaces earlier stations
+        and discards their records."""
+        self._check_ready()
+        x = np.ascontiguousarray(np.atleast_1d(x), dtype=np.float64)
+        y = np.ascontiguousarray(np.atleast_1d(y), dtype=np.float64)
+        if x.shape != y.shape or x.ndim != 1:
+            raise ValueError("x and y must be 1-D arrays of equal length")
+        names = [f"gauge_{k + 1}" for k in range(x.size)] if names is None else list(names)
+        if len(names) != x.size:
+            raise ValueError("one name per station")
+        dp = ctypes.POINTER(ctypes.c_double)
+        n = self._lib.rkb_set_gauges(self._handle, int(x.size), x.ctypes.data_as(dp),
+                                     y.ctypes.data_as(dp), float(interval), int(capacity))
+        if n < 0:
+            raise RuntimeError(f"set_gauges failed (rc={n}): {_lib.last_error(self._lib)}")
+        idx = np.zeros(n, dtype=np.int32)
+        bed = np.zeros(n)
+        self._lib.rkb_gauge_stations(self._handle, idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                     bed.ctypes.data_as(dp))
+        self._gauges = dict(names=[names[k] for k in idx], x=x[idx], y=y[idx], b=bed,
+                            time=[], values=[], overflow=False)
+        return int(n)
+
+    def set_gauges_file(self, path, interval=0.0, capacity=65536):
+        """Stations from a text file of ``name x y`` lines (``#`` comments and
+        blank lines skipped, malformed lines skipped, at most 100 stations;
+        read_gauge_file, rki_gauges.F90:129-206)."""
+        names, xs, ys = [], [], []
+        for line in Path(path).read_text().splitlines():
+            line = line.strip()
+            if not line or line.startswith("#"):
+                continue
+            if len(names) == 100:
+                break
+            parts = line.replace(",", " ").split()
+            try:
+                x, y = float(parts[1]), float(parts[2])
+            except (IndexError, ValueError):
+                continue
+            names.append(parts[0].strip("'\""))
+            xs.append(x)
+            ys.append(y)
+        return self.set_gauges(xs, ys, names, interval, capacity)
+
+    def gauge_records(self):
+        """All records since set_gauges: dict(time (K,), eta, u, v (K, stations),
+        names, x, y, b, overflow)."""
+        self._check_alive()
+        gs = getattr(self, "_gauges", None)
+        if gs is None:
+            raise RuntimeError("no gauges set")
+        n = len(gs["names"])
+        dp = ctypes.POINTER(ctypes.c_double)
+        while n > 0:
+            t = np.zeros(4096)
+            v = np.zeros((4096, n, 3))
+            ov = ctypes.c_int()
+            k = self._lib.rkb_read_gauges(self._handle, 4096, t.ctypes.data_as(dp),
+                                          v.ctypes.data_as(dp), ctypes.byref(ov))
+            if k < 0:
+                raise RuntimeError(f"read_gauges failed (rc={k})")
+            gs["overflow"] |= bool(ov.value)
+            if k == 0:
+                break
+            gs["time"].append(t[:k].copy())
+            gs["values"].append(v[:k].copy())
+        t = np.concatenate(gs["time"]) if gs["time"] else np.zeros(0)
+        v = np.concatenate(gs["values"]) if gs["values"] else np.zeros((0, n, 3))
+        return dict(time=t, eta=v[:, :, 0], u=v[:, :, 1], v=v[:, :, 2], names=list(gs["names"]),
+                    x=gs["x"].copy(), y=gs["y"].copy(), b=gs["b"].copy(), overflow=gs["overflow"])
+
+    def write_gauges(self, filename):
+        """Write the records so far as the reference's gauges.nc layout (NetCDF classic)."""
+        r = self.gauge_records()
+        n = len(r["names"])
+        width = 64
+        raw = b"".join(nm.encode()[:width].ljust(width, b"\0") for nm in r["names"])
+        vals = np.ascontiguousarray(np.stack([r["eta"], r["u"], r["v"]], axis=-1))
+        dp = ctypes.POINTER(ctypes.c_double)
+        t = np.ascontiguousarray(r["time"])
+        rc = self._lib.rkb_write_gauges_netcdf(
+            str(filename).encode(), n, raw, width, r["x"].ctypes.data_as(dp),
+            r["y"].ctypes.data_as(dp), r["b"].ctypes.data_as(dp), int(t.size),
+            t.ctypes.data_as(dp), vals.ctypes.data_as(dp))
+        self._rc(rc, "write_gauges")
+
     @classmethod
     def from_restart(cls, restart_file, namelist=None, **kwargs):
         """Create a simulation whose state (h, hu, hv, b, time) comes from a

@@ -349,6 +349,41 @@ int rki_load_restart(void* handle, const char* filename, int len) {
   return rc == 0 ? 0 : fail(-3, err);
 }
 
+int rkb_set_gauges(void* handle, int n, const double* x, const double* y, double interval,
+                   int capacity) {
+  rkb::Sim* s = sim_of(handle);
+  if (!s) return kBadHandle;
+  if (!s->is_initialised || !s->is_finalised) return -1;
+  std::string err;
+  const int rc = s->set_gauges(n, x, y, interval, capacity, err);
+  return rc >= 0 ? rc : fail(rc, err.empty() ? "gauge setup failed" : err);
+}
+
+int rkb_gauge_stations(void* handle, int* station, double* station_b) {
+  rkb::Sim* s = sim_of(handle);
+  if (!s) return kBadHandle;
+  return s->gauge_stations(station, station_b);
+}
+
+int rkb_read_gauges(void* handle, int max_records, double* times, double* values, int* overflow) {
+  rkb::Sim* s = sim_of(handle);
+  if (!s) return kBadHandle;
+  if (max_records < 0) return -2;
+  return s->read_gauges(max_records, times, values, overflow);
+}
+
+int rkb_write_gauges_netcdf(const char* path, int n, const char* names, int name_len,
+                            const double* x, const double* y, const double* b, int n_records,
+                            const double* times, const double* values) {
+  if (!path || n < 0 || n_records < 0 || (n > 0 && (!x || !y || !b)) ||
+      (n_records > 0 && (!times || (n > 0 && !values))))
+    return fail(-2, "invalid arguments");
+  std::string err;
+  if (!rkb::nc::write_gauges(path, n, names, name_len, x, y, b, n_records, times, values, err))
+    return fail(-1, err);
+  return 0;
+}
+
 // Host-only codec entry points (no simulation, no GPU): interior (nx, ny)
 // Fortran-order arrays; read returns 0, 1 (grid mismatch) or -1.
 int rkb_restart_write(const char* path, int nx, int ny, const double* h, const double* hu,

@@ -186,6 +186,138 @@ bool write_restart(const std::string& path, int nx, int ny, const double* h, con
 
 namespace {
 
+// A fixed-size variable to write: dimension ids (slowest first), text
+// attributes, and its values (FP64, or characters for NC_CHAR).
+struct OutVar {
+  std::string name;
+  std::vector<uint32_t> dims;
+  uint32_t type;
+  std::vector<std::pair<std::string, std::string>> atts;
+  const void* data;
+  uint64_t count;
+};
+
+bool write_classic(const std::string& path,
+                   const std::vector<std::pair<std::string, uint32_t>>& dims,
+                   const std::vector<std::pair<std::string, std::string>>& gatts,
+                   const std::vector<OutVar>& vars, std::string& err) {
+  Out hd;
+  hd.b = {'C', 'D', 'F', 2};
+  hd.u32(0);
+  hd.u32(kDimTag);
+  hd.u32((uint32_t)dims.size());
+  for (const auto& d : dims) {
+    hd.name(d.first);
+    hd.u32(d.second);
+  }
+  if (gatts.empty()) {
+    hd.u32(0);
+    hd.u32(0);
+  } else {
+    hd.u32(kAttTag);
+    hd.u32((uint32_t)gatts.size());
+    for (const auto& a : gatts) hd.text_att(a.first, a.second);
+  }
+  hd.u32(kVarTag);
+  hd.u32((uint32_t)vars.size());
+  std::vector<size_t> begin_at;
+  std::vector<uint64_t> sizes;
+  for (const OutVar& v : vars) {
+    hd.name(v.name);
+    hd.u32((uint32_t)v.dims.size());
+    for (uint32_t d : v.dims) hd.u32(d);
+    if (v.atts.empty()) {
+      hd.u32(0);
+      hd.u32(0);
+    } else {
+      hd.u32(kAttTag);
+      hd.u32((uint32_t)v.atts.size());
+      for (const auto& a : v.atts) hd.text_att(a.first, a.second);
+    }
+    hd.u32(v.type);
+    const uint64_t sz = pad4((uint32_t)(v.count * (v.type == kChar ? 1 : 8)));
+    if (sz >= 0xFFFFFFFCull) {
+      err = "variable " + v.name + " too large for a 64-bit-offset NetCDF file";
+      return false;
+    }
+    hd.u32((uint32_t)sz);
+    sizes.push_back(sz);
+    begin_at.push_back(hd.b.size());
+    hd.u64(0);
+  }
+  uint64_t off = hd.b.size();
+  for (size_t v = 0; v < vars.size(); ++v) {
+    for (int s = 0; s < 8; ++s) hd.b[begin_at[v] + s] = (unsigned char)(off >> (56 - 8 * s));
+    off += sizes[v];
+  }
+  FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f) {
+    err = "cannot open " + path + " for writing";
+    return false;
+  }
+  bool ok = std::fwrite(hd.b.data(), 1, hd.b.size(), f) == hd.b.size();
+  std::vector<unsigned char> buf;
+  for (size_t v = 0; v < vars.size() && ok; ++v) {
+    buf.clear();
+    if (vars[v].type == kChar) {
+      const unsigned char* c = (const unsigned char*)vars[v].data;
+      buf.assign(c, c + vars[v].count);
+    } else {
+      put_be_doubles(buf, (const double*)vars[v].data, vars[v].count);
+    }
+    buf.resize(sizes[v], 0);
+    ok = std::fwrite(buf.data(), 1, buf.size(), f) == buf.size();
+  }
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) err = "write to " + path + " failed";
+  return ok;
+}
+
+}  // namespace
+
+bool write_gauges(const std::string& path, int n, const char* names, int name_len,
+                  const double* x, const double* y, const double* b, int n_records,
+                  const double* times, const double* values, std::string& err) {
+  constexpr int kNameLen = 64;  // MAX_NAME_LEN, rki_gauges.F90:26
+  std::vector<char> nm((size_t)n * kNameLen, '\0');
+  for (int k = 0; k < n; ++k)
+    for (int c = 0; c < name_len && c < kNameLen; ++c) {
+      const char ch = names ? names[(size_t)k * name_len + c] : '\0';
+      if (ch == '\0') break;
+      nm[(size_t)k * kNameLen + c] = ch;
+    }
+  const uint64_t K = (uint64_t)n_records;
+  std::vector<double> eta(K * n), u(K * n), v(K * n);
+  for (uint64_t r = 0; r < K * n; ++r) {
+    eta[r] = values[3 * r];
+    u[r] = values[3 * r + 1];
+    v[r] = values[3 * r + 2];
+  }
+  // dimension ids: 0 station, 1 time, 2 name_strlen
+  const std::vector<std::pair<std::string, uint32_t>> dims = {
+      {"station", (uint32_t)n}, {"time", (uint32_t)n_records}, {"name_strlen", kNameLen}};
+  using A = std::vector<std::pair<std::string, std::string>>;
+  const std::vector<OutVar> vars = {
+      {"time", {1}, kDouble, A{{"units", "seconds"}, {"calendar", "proleptic_gregorian"}}, times, K},
+      {"station_name", {0, 2}, kChar, A{}, nm.data(), (uint64_t)n * kNameLen},
+      {"station_x", {0}, kDouble, A{{"units", "m"}, {"long_name", "gauge x-coordinate"}}, x,
+       (uint64_t)n},
+      {"station_y", {0}, kDouble, A{{"units", "m"}, {"long_name", "gauge y-coordinate"}}, y,
+       (uint64_t)n},
+      {"station_b", {0}, kDouble,
+       A{{"units", "m"}, {"long_name", "interpolated bottom elevation"}}, b, (uint64_t)n},
+      {"eta", {1, 0}, kDouble, A{{"units", "m"}, {"long_name", "water surface elevation"}},
+       eta.data(), K * n},
+      {"u", {1, 0}, kDouble, A{{"units", "m/s"}, {"long_name", "depth-averaged x-velocity"}},
+       u.data(), K * n},
+      {"v", {1, 0}, kDouble, A{{"units", "m/s"}, {"long_name", "depth-averaged y-velocity"}},
+       v.data(), K * n}};
+  return write_classic(path, dims, {{"title", "Rakali gauge time series"}, {"Conventions", "CF-1.8"}},
+                       vars, err);
+}
+
+namespace {
+
 // A whole classic file: its dimensions, its variables and the raw bytes.
 struct File {
   std::vector<unsigned char> data;

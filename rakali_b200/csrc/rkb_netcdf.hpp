@@ -30,5 +30,15 @@ int read_restart(const std::string& path, int nx, int ny, double* h, double* hu,
 // an interior (nx, ny) Fortran-order array.  Return codes as read_restart.
 int read_bathymetry(const std::string& path, int nx, int ny, double* b, std::string& err);
 
+// Gauge time series in the layout of create_gauge_netcdf / gauges_write
+// (src/io/structured/rki_gauges.F90:338-575): dimensions station, time,
+// name_strlen (64); station_name, station_x, station_y, station_b; eta, u, v
+// (time, station).  The time dimension has the record count (the reference's
+// is unlimited).  names: n fixed-width fields of name_len characters;
+// values: [n_records][n][3] (eta, u, v).
+bool write_gauges(const std::string& path, int n, const char* names, int name_len,
+                  const double* x, const double* y, const double* b, int n_records,
+                  const double* times, const double* values, std::string& err);
+
 }  // namespace nc
 }  // namespace rkb

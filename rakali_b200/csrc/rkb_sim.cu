@@ -67,11 +67,9 @@ void fill_scheme(Physics& p, int code) {
 }  // namespace
 
 Sim::~Sim() {
-  for (auto& ge : graphs_) {
-    if (ge.exec) cudaGraphExecDestroy(ge.exec);
-    if (ge.graph) cudaGraphDestroy(ge.graph);
-  }
-  graphs_.clear();
+  drop_graphs();
+  if (gauge_mem_) cudaFree(gauge_mem_);
+  gauge_mem_ = nullptr;
   free_device();
   for (auto& p : hf_) {
     if (p) cudaFreeHost(p);
@@ -327,6 +325,117 @@ int Sim::alloc_device(std::string& err) {
   return 0;
 }
 
+void Sim::drop_graphs() {
+  for (auto& ge : graphs_) {
+    if (ge.exec) cudaGraphExecDestroy(ge.exec);
+    if (ge.graph) cudaGraphDestroy(ge.graph);
+  }
+  graphs_.clear();
+}
+
+// gauges_init (src/io/structured/rki_gauges.F90:80-123) without the file
+// parsing: stations outside the domain are dropped; station_b is the
+// bilinear bed at each station (create_gauge_netcdf, :455-467).  The gauge
+// clock starts at the current time (rki_driver.F90:346-352).
+int Sim::set_gauges(int n, const double* x, const double* y, double interval, int capacity,
+                    std::string& err) {
+  if (n < 0 || capacity < 1 || (n > 0 && (!x || !y))) {
+    err = "invalid gauge arguments";
+    return -2;
+  }
+  if (cudaSetDevice(device_) != cudaSuccess) return -1;
+  if (on_device_ && cudaStreamSynchronize(stream_) != cudaSuccess) return -1;
+  drop_graphs();
+  if (gauge_mem_) cudaFree(gauge_mem_);
+  gauge_mem_ = nullptr;
+  gauge_dev_ = nullptr;
+  gauge_host_ = GaugeDev{};
+  gauge_station_.clear();
+  gauge_b_.clear();
+  GaugeStencils st;
+  gauge_stencils(g, x, y, n, st);
+  const int nl = (int)st.station.size();
+  if (nl == 0) return 0;
+  const size_t head = 256, ints = 2 * (size_t)nl * sizeof(int), dbl = 2 * (size_t)nl * 8;
+  const size_t recs = (size_t)capacity * (1 + 3 * (size_t)nl) * 8;
+  const size_t bytes = head + ((ints + 255) / 256) * 256 + dbl + recs;
+  if (cudaMalloc(&gauge_mem_, bytes) != cudaSuccess) {
+    gauge_mem_ = nullptr;
+    err = "device allocation of the gauge buffer failed";
+    return -1;
+  }
+  char* p = (char*)gauge_mem_;
+  gauge_dev_ = (GaugeDev*)p;
+  int* ix0 = (int*)(p + head);
+  int* iy0 = ix0 + nl;
+  double* wx = (double*)(p + head + ((ints + 255) / 256) * 256);
+  double* wy = wx + nl;
+  double* rec_t = wy + nl;
+  double* rec = rec_t + capacity;
+  GaugeDev h{};
+  h.n = nl;
+  h.cap = capacity;
+  h.interval = interval;
+  h.next = interval > 0.0 ? t_current_ + interval : t_current_;
+  h.ix0 = ix0;
+  h.iy0 = iy0;
+  h.wx = wx;
+  h.wy = wy;
+  h.rec_t = rec_t;
+  h.rec = rec;
+  RKB_TRY(cudaMemcpy(ix0, st.ix0.data(), nl * sizeof(int), cudaMemcpyHostToDevice));
+  RKB_TRY(cudaMemcpy(iy0, st.iy0.data(), nl * sizeof(int), cudaMemcpyHostToDevice));
+  RKB_TRY(cudaMemcpy(wx, st.wx.data(), nl * sizeof(double), cudaMemcpyHostToDevice));
+  RKB_TRY(cudaMemcpy(wy, st.wy.data(), nl * sizeof(double), cudaMemcpyHostToDevice));
+  RKB_TRY(cudaMemcpy(gauge_dev_, &h, sizeof(GaugeDev), cudaMemcpyHostToDevice));
+  gauge_host_ = h;
+  gauge_station_ = st.station;
+  // the bed at each station from the host bed (ghosts filled at finalize)
+  const double* b = hf_[3];
+  auto at = [&](int i, int j) { return (size_t)i + (size_t)j * (size_t)g.nxt; };
+  for (int k = 0; k < nl; ++k) {
+    const int i0 = st.ix0[k], j0 = st.iy0[k];
+    const double a = st.wx[k], c = st.wy[k];
+    gauge_b_.push_back((1.0 - a) * (1.0 - c) * b[at(i0, j0)] + a * (1.0 - c) * b[at(i0 + 1, j0)] +
+                       (1.0 - a) * c * b[at(i0, j0 + 1)] + a * c * b[at(i0 + 1, j0 + 1)]);
+  }
+  return nl;
+}
+
+int Sim::gauge_stations(int* station, double* station_b) const {
+  for (size_t k = 0; k < gauge_station_.size(); ++k) {
+    if (station) station[k] = gauge_station_[k];
+    if (station_b) station_b[k] = gauge_b_[k];
+  }
+  return (int)gauge_station_.size();
+}
+
+int Sim::read_gauges(int max_records, double* times, double* values, int* overflow) {
+  if (overflow) *overflow = 0;
+  if (!gauge_dev_) return 0;
+  if (cudaSetDevice(device_) != cudaSuccess) return -1;
+  if (on_device_ && cudaStreamSynchronize(stream_) != cudaSuccess) return -1;
+  GaugeDev h{};
+  RKB_TRY(cudaMemcpy(&h, gauge_dev_, sizeof(GaugeDev), cudaMemcpyDeviceToHost));
+  const int k = h.count < max_records ? h.count : max_records;
+  if (k > 0) {
+    if (times) RKB_TRY(cudaMemcpy(times, h.rec_t, (size_t)k * 8, cudaMemcpyDeviceToHost));
+    if (values)
+      RKB_TRY(cudaMemcpy(values, h.rec, (size_t)k * h.n * 3 * 8, cudaMemcpyDeviceToHost));
+  }
+  if (overflow) *overflow = h.overflow;
+  // the records read are consumed; later ones move to the front
+  const int rest = h.count - k;
+  if (rest > 0) {
+    RKB_TRY(cudaMemcpy(h.rec_t, h.rec_t + k, (size_t)rest * 8, cudaMemcpyDeviceToDevice));
+    RKB_TRY(cudaMemcpy(h.rec, h.rec + (size_t)k * h.n * 3, (size_t)rest * h.n * 3 * 8,
+                       cudaMemcpyDeviceToDevice));
+  }
+  const int counters[2] = {rest, 0};
+  RKB_TRY(cudaMemcpy(&gauge_dev_->count, counters, sizeof(counters), cudaMemcpyHostToDevice));
+  return k;
+}
+
 // restart_write (src/io/structured/rki_output.F90:740-853): interior h, hu,
 // hv, b and the clock, after refresh_host.
 int Sim::save_restart(const std::string& path, std::string& err) {
@@ -424,11 +533,7 @@ int Sim::upload_forcing() {
     for (int k = 0; k < 4; ++k)
       RKB_TRY(cudaMalloc((void**)&f[k], (size_t)g.pitch * g.nyt * sizeof(double)));
     args_.fo = Forcing{f[0], f[1], f[2], f[3]};
-    for (auto& ge : graphs_) {  // graphs hold the old (null) forcing pointers
-      if (ge.exec) cudaGraphExecDestroy(ge.exec);
-      if (ge.graph) cudaGraphDestroy(ge.graph);
-    }
-    graphs_.clear();
+    drop_graphs();  // graphs hold the old (null) forcing pointers
   }
   const double* dstf[4] = {args_.fo.wind_x, args_.fo.wind_y, args_.fo.atm, args_.fo.precip};
   for (int k = 0; k < 4; ++k)
@@ -640,11 +745,19 @@ cudaGraphExec_t Sim::graph_for(int steps) {
   if (cudaStreamSynchronize(stream_) != cudaSuccess) return nullptr;
   if (cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
     return nullptr;
+  const int ngauge = gauge_host_.n;
   for (int k = 0; k < steps; ++k) {
-    if (precision_ == 32)
+    if (precision_ == 32) {
       launch_step32(args32_, stream_);
-    else
+      if (ngauge > 0)
+        launch_gauge_record32(args32_.g, args_.ctl, gauge_dev_, ngauge, args32_.U0, args32_.U1,
+                              args32_.b, stream_);
+    } else {
       launch_step(args_, stream_);
+      if (ngauge > 0)
+        launch_gauge_record(g, args_.ctl, gauge_dev_, ngauge, args_.U0, args_.U1, args_.b,
+                            stream_);
+    }
   }
   if (cudaStreamEndCapture(stream_, &ge.graph) != cudaSuccess) return nullptr;
   if (cudaGraphInstantiate(&ge.exec, ge.graph, 0) != cudaSuccess) return nullptr;

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "rkb_config.hpp"
+#include "rkb_gauges.hpp"
 #include "rkb_kernels.h"
 
 namespace rkb {
@@ -34,6 +35,14 @@ class Sim {
   // the boundary launches summed), out[4] = launches per step.
   int profile_steps(int n, double out[5]);
   int save_restart(const std::string& path, std::string& err);  // NetCDF classic
+  // Gauge stations recorded on the device after every step (rkb_gauges.cu):
+  // returns the number of stations inside the domain, or < 0.
+  int set_gauges(int n, const double* x, const double* y, double interval, int capacity,
+                 std::string& err);
+  int gauge_stations(int* station, double* station_b) const;  // the stations inside
+  // Drain the recorded series: count returned, times [count], values
+  // [count][n][3] (eta, u, v), *overflow = records dropped since the last read.
+  int read_gauges(int max_records, double* times, double* values, int* overflow);
   int load_restart(const std::string& path, std::string& err);  // before finalize; 1 = grid mismatch
   int advance(double target_time);  // rki_advance
 
@@ -134,6 +143,14 @@ class Sim {
   int snap_cur_ = 0, snap_steps_ = 0;
   double snap_t_ = 0.0, snap_dt_ = 0.0;
   bool snap_stepped_ = false;
+
+  // gauges
+  void drop_graphs();
+  void* gauge_mem_ = nullptr;
+  GaugeDev* gauge_dev_ = nullptr;
+  GaugeDev gauge_host_{};
+  std::vector<int> gauge_station_;
+  std::vector<double> gauge_b_;
 
   struct GraphEntry {
     int steps, hllc, tile, prec, rows;

@@ -470,3 +470,109 @@ def test_bathymetry_file_equals_set_bathymetry(tmp_path):
         s1.step(20)
         s2.step(20)
         assert np.array_equal(s1.h, s2.h) and np.array_equal(s1.hu, s2.hu)
+
+
+# ---------------------------------------------------------------------------
+# gauges (src/io/structured/rki_gauges.F90), recorded on the device
+# ---------------------------------------------------------------------------
+
+def _gauge_weights(x, y, dx, dy, nx, ny, ng):
+    """compute_local_gauges + compute_interp_weights (rki_gauges.F90:208-336), 0-based."""
+    out = []
+    for k, (gx, gy) in enumerate(zip(x, y)):
+        ig, jg = math.floor(gx / dx) + 1, math.floor(gy / dy) + 1
+        if not (1 <= ig <= nx and 1 <= jg <= ny):
+            continue
+        ia, ja = ig + ng, jg + ng
+        xc, yc = (ig - 0.5) * dx, (jg - 0.5) * dy
+        if gx < xc:
+            i0, wx = (ia - 1, (gx - (xc - dx)) / dx) if ig > 1 else (ia, 0.0)
+        else:
+            i0, wx = (ia, (gx - xc) / dx) if ig < nx else (ia, 0.0)
+        if gy < yc:
+            j0, wy = (ja - 1, (gy - (yc - dy)) / dy) if jg > 1 else (ja, 0.0)
+        else:
+            j0, wy = (ja, (gy - yc) / dy) if jg < ny else (ja, 0.0)
+        out.append((k, i0 - 1, j0 - 1, max(0.0, min(1.0, wx)), max(0.0, min(1.0, wy))))
+    return out
+
+
+def _blend(a, i0, j0, wx, wy):
+    return ((1.0 - wx) * (1.0 - wy) * a[i0, j0] + wx * (1.0 - wy) * a[i0 + 1, j0]
+            + (1.0 - wx) * wy * a[i0, j0 + 1] + wx * wy * a[i0 + 1, j0 + 1])
+
+
+def test_gauges_match_the_reference_formula_on_the_oracle():
+    """Every-step records: bit-identical to gauges_write's formula applied to
+    the oracle's state after each step; edge stations clamp; outside dropped."""
+    nx, ny, dx = 80, 60, 10.0
+    b = gaussian_bed(nx, ny, dx, dx, 10, seed=31, width=(30.0, 120.0))
+    h = hump_depth(b, dx, dx, amp=0.4, width=60.0)
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, manning_n=0.02, use_hllc=True)
+    sim, orc = pair(cfg, bathymetry=b, initial_h=h)
+    xs = [3.0, 401.7, 795.0, 250.0, 555.5, 900.0, 10.0]
+    ys = [2.0, 300.2, 598.0, 5.0, 444.4, 30.0, -1.0]
+    w = _gauge_weights(xs, ys, dx, dx, nx, ny, orc.ng)
+    with sim:
+        kept = sim.set_gauges(xs, ys, names=[f"g{k}" for k in range(len(xs))])
+        assert kept == len(w) == 5
+        sim.step(12)
+        rec = sim.gauge_records()
+        assert rec["time"].size == 12 and not rec["overflow"]
+        for s in range(12):
+            orc.step(1)
+            assert rec["time"][s] == orc.time
+            A = orc.arrays
+            for m, (k, i0, j0, wx, wy) in enumerate(w):
+                hh = _blend(A["h"], i0, j0, wx, wy)
+                bb = _blend(A["b"], i0, j0, wx, wy)
+                hs = max(hh, 1.0e-6)
+                assert rec["eta"][s, m] == hh + bb
+                assert rec["u"][s, m] == _blend(A["hu"], i0, j0, wx, wy) / hs
+                assert rec["v"][s, m] == _blend(A["hv"], i0, j0, wx, wy) / hs
+        assert rec["names"] == [f"g{k}" for k, *_ in w]
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_gauge_interval_capacity_and_file(tmp_path, precision):
+    """interval > 0 follows the driver's next-time rule; a full buffer sets
+    overflow; the file round-trips through scipy."""
+    from scipy.io import netcdf_file
+
+    from rakali_b200 import Rakali
+    nx, ny, dx = 48, 40, 10.0
+    b = gaussian_bed(nx, ny, dx, dx, 6, seed=2, width=(30.0, 100.0))
+    h = hump_depth(b, dx, dx, amp=0.4, width=50.0)
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, manning_n=0.02)
+    with Rakali(defer_init=True, precision=precision, **cfg) as sim:
+        sim.set_bathymetry(b)
+        sim.set_initial_h(h)
+        sim.finalize()
+        sim.set_gauges([100.0, 250.0], [120.0, 200.0], names=["a", "b"], interval=3.0)
+        sim.step(40)
+        rec = sim.gauge_records()
+    # replay the cadence on the recorded clock: record when t >= next, next += 3
+    with Rakali(defer_init=True, precision=precision, **cfg) as ref:
+        ref.set_bathymetry(b)
+        ref.set_initial_h(h)
+        ref.finalize()
+        nxt, expect = 3.0, []
+        for _ in range(40):
+            ref.step(1)
+            if ref.time >= nxt:
+                expect.append(ref.time)
+                nxt += 3.0
+    assert np.array_equal(rec["time"], np.array(expect))
+    with Rakali(defer_init=True, precision=precision, **cfg) as sim:
+        sim.set_bathymetry(b)
+        sim.set_initial_h(h)
+        sim.finalize()
+        sim.set_gauges([100.0], [120.0], capacity=5)
+        sim.step(8)
+        rec = sim.gauge_records()
+        assert rec["time"].size == 5 and rec["overflow"]
+        path = tmp_path / "gauges.nc"
+        sim.write_gauges(path)
+        with netcdf_file(str(path), "r", mmap=False) as f:
+            assert np.array_equal(f.variables["eta"][:, 0], rec["eta"][:, 0])
+            assert np.array_equal(f.variables["time"][:], rec["time"])

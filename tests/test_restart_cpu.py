@@ -139,3 +139,32 @@ def test_bathymetry_file_without_known_variable(lib, tmp_path):
     out = np.zeros((nx, ny), order="F")
     assert lib.rkb_bathymetry_read(str(path).encode(), nx, ny, _p(out)) == -1
     assert "b, elevation, depth" in _lib.last_error(lib)
+
+
+def test_gauge_file_layout_reads_in_scipy(lib, tmp_path):
+    """rkb_write_gauges_netcdf writes create_gauge_netcdf's variables
+    (src/io/structured/rki_gauges.F90:338-488)."""
+    from scipy.io import netcdf_file
+    n, K = 3, 5
+    rng = np.random.default_rng(8)
+    x, y, b = rng.uniform(0, 100, n), rng.uniform(0, 50, n), rng.uniform(-5, 0, n)
+    t = np.arange(K, dtype=np.float64) * 2.5
+    vals = np.ascontiguousarray(rng.standard_normal((K, n, 3)))
+    names = [b"harbour", b"pier", b"x" * 70]
+    raw = b"".join(nm[:64].ljust(64, b"\0") for nm in names)
+    path = tmp_path / "gauges.nc"
+    assert lib.rkb_write_gauges_netcdf(str(path).encode(), n, raw, 64, _p(x), _p(y), _p(b), K,
+                                       _p(t), _p(vals)) == 0
+    with netcdf_file(str(path), "r", mmap=False) as f:
+        assert f.dimensions == {"station": n, "time": K, "name_strlen": 64}
+        assert np.array_equal(f.variables["time"][:], t)
+        assert f.variables["time"].units == b"seconds"
+        for k, nm in enumerate(names):
+            got = bytes(f.variables["station_name"][k]).rstrip(b"\0")
+            assert got == nm[:64]
+        for name, arr in (("station_x", x), ("station_y", y), ("station_b", b)):
+            assert np.array_equal(f.variables[name][:], arr)
+        for c, name in enumerate(("eta", "u", "v")):
+            assert f.variables[name].dimensions == ("time", "station")
+            assert np.array_equal(f.variables[name][:], vals[:, :, c])
+        assert f.title == b"Rakali gauge time series"
