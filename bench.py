@@ -41,6 +41,8 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+from rakali_b200 import replicas as rp  # noqa: E402  (after the path setup)
+
 N_CELLS_SIDE = 4096
 METRIC = "cell-updates/s on 1 B200: FP64 plain vs FP32, batched, fwd+adjoint, at stated err"
 # algorithmic bytes per cell-update of the two fused stage kernels (FP64):
@@ -124,15 +126,6 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def visible_gpu_index(local_rank: int) -> int:
-    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
-    if vis:
-        ids = [v.strip() for v in vis.split(",") if v.strip()]
-        if local_rank < len(ids) and ids[local_rank].isdigit():
-            return int(ids[local_rank])
-    return local_rank
-
-
 def traffic_per_launch(n_cells: int, precision: int = 64):
     """DRAM bytes per stage-2 launch from the committed ncu summary, scaled by cells."""
     p = ROOT / "profiles" / f"stage2_fp{precision}_ncu.json"
@@ -161,6 +154,18 @@ def cpu_baseline(threads: int, side: int = 1024, steps: int = 2, seed: int = 202
                       f"{used} OpenMP threads"}
 
 
+FORM_DESC = {64: "FP64 depth form (the reference's arithmetic, bit-identical to the oracle)",
+             32: "FP32 surface form (FP64 bed differences, wet/dry tests and mass sums)"}
+
+
+def arm_config(n: int, world: int, precision: int) -> dict:
+    """The `config` of the JSON line, shared by both arms."""
+    return {"workload": f"structured SSP-RK2 wet/dry step, {n}x{n} per GPU, dx=5 m, "
+                        "32-Gaussian bed, 0.5 m hump, Manning 0.025, walls, " + FORM_DESC[precision],
+            "cells_per_gpu": n * n, "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2 (every field >= 67 MB, 7+ fields per stage)"}
+
+
 def run_reference(args, rank, world):
     """CPU implementation of the path (the oracle port), all host threads."""
     if rank != 0:
@@ -185,9 +190,7 @@ def run_reference(args, rank, world):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"structured SSP-RK2 wet/dry step, {side}x{side} window of "
-                               "the 4096x4096 configuration (CPU oracle port)",
-                   "cells": side * side, "l2": "inputs larger than L2"},
+        "config": arm_config(N_CELLS_SIDE, world, 64),
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": used,
                          "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
@@ -214,18 +217,14 @@ def _form_numbers(sim, args, world, local_rank, dist, cells):
         return ms.value
 
     device_steps(max(args.warmup, 3))
-    if dist is not None:
-        dist.barrier()
+    rp.barrier(dist)
     torch.cuda.synchronize()
-    with ClockSampler(visible_gpu_index(local_rank)) as clk:
+    with ClockSampler(rp.visible_gpu_index(local_rank)) as clk:
         ms = device_steps(args.steps)
     torch.cuda.synchronize()
-    if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
-    value = world * cells * args.steps / (ms * 1e-3)
+    ms = rp.max_over_ranks(ms, dist)
+    rp.barrier(dist)
+    value = rp.weak_value(world, cells, args.steps, ms)
 
     # per-kernel device times (events between launches, same stream)
     prof = (ctypes.c_double * 5)()
@@ -244,11 +243,7 @@ def _form_numbers(sim, args, world, local_rank, dist, cells):
     sim.step(args.steps)
     h_back = sim.h_phys
     _ = float(h_back[0, 0])
-    e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = rp.max_over_ranks(time.perf_counter() - t0, dist)
     n = int(round(cells ** 0.5))
     nxt = n + 2 * sim.nghost
     e2e = {"value": world * cells * args.steps / e2e_s, "unit": "cell-updates/s",
@@ -320,7 +315,7 @@ def run_ensemble(args, world, local_rank, dist):
     torch.cuda.set_device(local_rank)
     rank = int(os.environ.get("RANK", "0"))
     t_setup = time.perf_counter()
-    members = wl.ensemble_members(n_inst=args.ensemble_members, seed=7 + rank)
+    members = wl.ensemble_members(n_inst=args.ensemble_members, seed=rp.replica_seed(7, rank))
     sims = [wl.build_member(m) for m in members]
     cells = sum(s.nx * s.ny for s in sims)
     setup_s = time.perf_counter() - t_setup
@@ -332,16 +327,12 @@ def run_ensemble(args, world, local_rank, dist):
         with Ensemble(sims, precision=prec) as ens:
             best = ens.autotune(trial_steps=3)
             ens.step(max(args.warmup, 3))
-            if dist is not None:
-                dist.barrier()
-            with ClockSampler(visible_gpu_index(local_rank)) as clk:
+            rp.barrier(dist)
+            with ClockSampler(rp.visible_gpu_index(local_rank)) as clk:
                 ms = ens.time_steps(args.ensemble_steps)
-            if dist is not None:
-                t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-                dist.all_reduce(t, op=dist.ReduceOp.MAX)
-                ms = float(t.item())
+            ms = rp.max_over_ranks(ms, dist)
             out["forms"][f"fp{prec}"] = {
-                "value": world * cells * args.ensemble_steps / (ms * 1e-3),
+                "value": rp.weak_value(world, cells, args.ensemble_steps, ms),
                 "unit": "cell-updates/s", "steps": args.ensemble_steps,
                 "ms_per_step": ms / args.ensemble_steps, "variant": list(ens.variant),
                 "autotune_best_ms_per_step": best, "clocks": clk.summary(),
@@ -615,17 +606,13 @@ def run_b200(args, rank, world, local_rank, dist):
         return 0
 
     f = forms[head]
-    desc = {64: "FP64 depth form (the reference's arithmetic, bit-identical to the oracle)",
-            32: "FP32 surface form (FP64 bed differences, wet/dry tests and mass sums)"}
+    desc = FORM_DESC
     line = {
         "metric": METRIC, "value": f["value"], "unit": "cell-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": f["ms"] / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if head == 32 else "f64", "data": "synthetic",
-        "config": {"workload": f"structured SSP-RK2 wet/dry step, {n}x{n} per GPU, dx=5 m, "
-                               "32-Gaussian bed, 0.5 m hump, Manning 0.025, walls, " + desc[head],
-                   "cells_per_gpu": cells, "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (every field >= 67 MB, 7+ fields per stage)"},
+        "config": arm_config(n, world, head),
         "e2e": f["e2e"],
         "gpu_launches": f["launches_per_step"] * args.steps,
         "roofline": f["roofline"],
