@@ -569,6 +569,10 @@ class Adjoint final : public AdjointBase {
       err = "invalid sizes";
       return -2;
     }
+    if (nx < ng || ny < ng) {  // one wall fill per stage: ghosts must mirror interior cells
+      err = "the adjoint needs an interior at least nghost cells wide in x and y";
+      return -2;
+    }
     nm_ = nm;
     g_.ng = ng;
     g_.nxt = nx + 2 * ng;

@@ -830,11 +830,17 @@ __device__ __forceinline__ void bc32_body(const StepArgs32& a, int stage, int w,
   if (type == kNested) return;
   const Edge e = make_edge(w, g);
   if (t >= e.n_tan) return;
-  const double time = stage == 1 ? ctl->t : ctl->t + dt;
+  // stage 9: the fill before dt of a narrow grid (see bc_body in the FP64
+  // step): time t, the previous dt; stage 1 of a narrow grid also writes the
+  // scratch buffer that stage 2 fills next
+  const double time = stage == 2 ? ctl->t + dt : ctl->t;
+  const double dtb = stage == 9 ? ctl->dt_prev : dt;
   const int cur = ctl->cur;
-  const FieldSet32 F = stage == 1 ? (cur ? a.U1 : a.U0) : a.S;
-  const FieldSet32 N = cur ? a.U0 : a.U1;
-  const bool both = stage == 2;
+  const int wide = g.ng > 2 ? g.ng : 2;
+  const bool narrow = g.nx_phys() < wide || g.ny_phys() < wide;
+  const FieldSet32 F = stage == 2 ? a.S : (cur ? a.U1 : a.U0);
+  const FieldSet32 N = stage == 2 ? (cur ? a.U0 : a.U1) : a.S;
+  const bool both = stage == 2 || (stage == 1 && narrow);
   double* b = a.b;
   auto depth = [&](size_t q) { return pos((double)F.eta[q] - b[q]); };
   auto put = [&](int ig, int jg, double vh, double vu, double vv) {
@@ -906,8 +912,8 @@ __device__ __forceinline__ void bc32_body(const StepArgs32& a, int stage, int w,
     const int i2 = ii - e.din;
     const int j2 = ji - e.djn;
     double eg;
-    if (dt > 0.0) {
-      const double detadt = (ei - eov) / dt;
+    if (dtb > 0.0) {
+      const double detadt = (ei - eov) / dtb;
       double detadx = 0.0;
       if (i2 >= 0 && i2 < g.nxt && j2 >= 0 && j2 < g.nyt) {
         const size_t q2 = g.at(i2, j2);
@@ -915,7 +921,7 @@ __device__ __forceinline__ void bc32_body(const StepArgs32& a, int stage, int w,
       }
       double cp = fabs(detadx) > 1.0e-10 ? -detadt / detadx : 0.0;
       cp = pos(dmin(cp, c));
-      eg = eov - cp * dt / dd * (eov - ei);
+      eg = eov - cp * dtb / dd * (eov - ei);
     } else {
       eg = ei;
     }
@@ -1113,12 +1119,13 @@ static cudaError_t launch_sweep(const StepArgs32& a, cudaStream_t s) {
   return a.cpl == 4 ? launch_sweep_t<4, STAGE>(a, s) : launch_sweep_t<2, STAGE>(a, s);
 }
 
-cudaError_t launch_bc32(const StepArgs32& a, int stage, cudaStream_t s) {
+static cudaError_t launch_bc32_pass(const StepArgs32& a, int stage, bool first_pass,
+                                    cudaStream_t s) {
   const Grid& g = a.g;
   const int tpb = 128;
   const bool pair_x = g.nx_phys() >= (g.ng > 2 ? g.ng : 2);
   const bool pair_y = g.ny_phys() >= (g.ng > 2 ? g.ng : 2);
-  int first = stage == 1 ? 1 : 0;
+  int first = first_pass ? 1 : 0;
   auto go = [&](int e0, int count, int n_tan) {
     dim3 grid((unsigned)((n_tan + tpb - 1) / tpb), (unsigned)count);
     k_bc32<<<grid, tpb, 0, s>>>(a, stage, e0, first);
@@ -1139,6 +1146,21 @@ cudaError_t launch_bc32(const StepArgs32& a, int stage, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+static bool narrow32(const Grid& g) {
+  const int wide = g.ng > 2 ? g.ng : 2;
+  return g.nx_phys() < wide || g.ny_phys() < wide;
+}
+
+// The fill of a stage; a narrow grid's step opens with the fill before dt.
+cudaError_t launch_bc32(const StepArgs32& a, int stage, cudaStream_t s) {
+  if (stage == 1 && narrow32(a.g)) {
+    const cudaError_t e = launch_bc32_pass(a, 9, true, s);
+    if (e != cudaSuccess) return e;
+    return launch_bc32_pass(a, 1, false, s);
+  }
+  return launch_bc32_pass(a, stage, stage == 1, s);
+}
+
 cudaError_t launch_step32(const StepArgs32& a, cudaStream_t s) {
   cudaError_t e = launch_bc32(a, 1, s);
   if (e == cudaSuccess) e = launch_sweep<1>(a, s);
@@ -1155,7 +1177,7 @@ int launches_per_step32(const StepArgs32& a) {
   const Grid& g = a.g;
   const int need = g.ng > 2 ? g.ng : 2;
   const int bc = (g.nx_phys() >= need ? 1 : 2) + (g.ny_phys() >= need ? 1 : 2);
-  return 2 * bc + 2;
+  return 2 * bc + 2 + (narrow32(g) ? bc : 0);
 }
 
 cudaError_t launch_max_speed32(const StepArgs32& a, cudaStream_t s) {

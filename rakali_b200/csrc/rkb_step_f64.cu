@@ -43,6 +43,14 @@ __device__ __forceinline__ FieldSet generic_in(const FieldSet& U0, const FieldSe
 // 1 or 2 (SSP-RK2) or 10 + k (generic stage k, time t + c_k dt).  `writer`
 // marks the one thread of the step's first boundary launch that publishes
 // this step's active flag and dt.
+//
+// Narrow grids (an interior thinner than max(nghost, 2) in x or y): a ghost
+// layer then mirrors a ghost of the opposite edge, so the values left by the
+// previous fill matter.  The reference fills its single array once before
+// computing dt (rki_solver.F90:719) and once per stage; for these grids the
+// step runs that extra fill (stage 9: time t, the previous step's dt) and
+// every stage's fill also writes the buffer the next stage reads, so each
+// fill sees the ghosts the reference's array holds at that point.
 __device__ __forceinline__ void bc_body(const StepArgs& a, int stage, int w, int t, bool writer) {
   const Grid& g = a.g;
   StepCtl* ctl = a.ctl;
@@ -66,26 +74,34 @@ __device__ __forceinline__ void bc_body(const StepArgs& a, int stage, int w, int
   double* eta_old_n = a.eta_old[3];
 
   const int cur = ctl->cur;
+  const int wide = g.ng > 2 ? g.ng : 2;
+  const bool narrow = g.nx_phys() < wide || g.ny_phys() < wide;
   double time;
+  double dtb = dt;  // the dt this fill uses (Chapman)
   FieldSet F;
   double* h2 = nullptr;
   double* hu2 = nullptr;
   double* hv2 = nullptr;
-  if (stage >= 10) {
+  auto also = [&](const FieldSet& N) { h2 = N.h; hu2 = N.hu; hv2 = N.hv; };
+  if (stage == 9) {  // the fill before dt (narrow grids only)
+    time = ctl->t;
+    dtb = ctl->dt_prev;
+    F = cur ? U1 : U0;
+  } else if (stage >= 10) {
     const int k = stage - 10, nst = a.phys->n_stages;
     time = ctl->t + a.phys->c[k] * dt;
     F = generic_in(U0, U1, S, k, nst, cur);
-    if (k == nst - 1) {
-      FieldSet N = cur ? U0 : U1;
-      h2 = N.h; hu2 = N.hu; hv2 = N.hv;
-    }
+    if (k == nst - 1)
+      also(cur ? U0 : U1);
+    else if (narrow)
+      also(generic_out(U0, U1, S, k, nst, cur));
   } else {
     time = stage == 1 ? ctl->t : ctl->t + dt;
     F = stage == 1 ? (cur ? U1 : U0) : S;
-    if (stage == 2) {
-      FieldSet N = cur ? U0 : U1;
-      h2 = N.h; hu2 = N.hu; hv2 = N.hv;
-    }
+    if (stage == 2)
+      also(cur ? U0 : U1);
+    else if (narrow)
+      also(S);
   }
   double* h = F.h;
   double* hu = F.hu;
@@ -184,8 +200,8 @@ __device__ __forceinline__ void bc_body(const StepArgs& a, int stage, int w, int
     const int i2 = ii - e.din;
     const int j2 = ji - e.djn;
     double eg;
-    if (dt > 0.0) {
-      const double detadt = (ei - eov) / dt;
+    if (dtb > 0.0) {
+      const double detadt = (ei - eov) / dtb;
       double detadx = 0.0;
       if (i2 >= 0 && i2 < g.nxt && j2 >= 0 && j2 < g.nyt) {
         const size_t q2 = g.at(i2, j2);
@@ -193,7 +209,7 @@ __device__ __forceinline__ void bc_body(const StepArgs& a, int stage, int w, int
       }
       double cp = fabs(detadx) > 1.0e-10 ? -detadt / detadx : 0.0;
       cp = pos(dmin(cp, c));
-      eg = eov - cp * dt / dd * (eov - ei);
+      eg = eov - cp * dtb / dd * (eov - ei);
     } else {
       eg = ei;
     }
@@ -944,14 +960,21 @@ static cudaError_t launch_stage(const StepArgs& a, FluxOut fl, cudaStream_t s, i
   return h ? launch_march_t<true, ST, 32>(a, s) : launch_march_t<false, ST, 32>(a, s);
 }
 
-cudaError_t launch_bc(const StepArgs& a, int stage, cudaStream_t s) {
+static bool narrow_grid(const Grid& g) {
+  const int wide = g.ng > 2 ? g.ng : 2;
+  return g.nx_phys() < wide || g.ny_phys() < wide;
+}
+
+// One boundary fill; `first`: this launch opens the step (publishes dt).
+static cudaError_t launch_bc_pass(const StepArgs& a, int stage, bool first_pass,
+                                  cudaStream_t s) {
   const Grid& g = a.g;
   const int tpb = 128;
   // Opposite edges may run in one launch only when neither reads cells the
   // other writes, i.e. when the interior is at least max(nghost, 2) wide.
   const bool pair_x = g.nx_phys() >= (g.ng > 2 ? g.ng : 2);
   const bool pair_y = g.ny_phys() >= (g.ng > 2 ? g.ng : 2);
-  int first = (stage == 1 || stage == 10) ? 1 : 0;
+  int first = first_pass ? 1 : 0;
   auto go = [&](int e0, int count, int n_tan) {
     dim3 grid((unsigned)((n_tan + tpb - 1) / tpb), (unsigned)count);
     k_bc<<<grid, tpb, 0, s>>>(a, stage, e0, first);
@@ -970,6 +993,17 @@ cudaError_t launch_bc(const StepArgs& a, int stage, cudaStream_t s) {
     go(3, 1, g.nxt);
   }
   return cudaGetLastError();
+}
+
+// The fill of a stage; a narrow grid's step opens with the fill before dt.
+cudaError_t launch_bc(const StepArgs& a, int stage, cudaStream_t s) {
+  const bool opens = stage == 1 || stage == 10;
+  if (opens && narrow_grid(a.g)) {
+    const cudaError_t e = launch_bc_pass(a, 9, true, s);
+    if (e != cudaSuccess) return e;
+    return launch_bc_pass(a, stage, false, s);
+  }
+  return launch_bc_pass(a, stage, opens, s);
 }
 
 // Generic Shu-Osher schemes (euler, rk3, rk43): per stage k a boundary fill
@@ -1009,8 +1043,9 @@ int launches_per_step(const StepArgs& a) {
   const Grid& g = a.g;
   const int need = g.ng > 2 ? g.ng : 2;
   const int bc = (g.nx_phys() >= need ? 1 : 2) + (g.ny_phys() >= need ? 1 : 2);
-  if (a.scheme != 2) return a.n_stages * (bc + 1);
-  return 2 * bc + 2;
+  const int pre = narrow_grid(g) ? bc : 0;
+  if (a.scheme != 2) return a.n_stages * (bc + 1) + pre;
+  return 2 * bc + 2 + pre;
 }
 
 cudaError_t launch_max_speed(const StepArgs& a, cudaStream_t s) {
