@@ -569,6 +569,10 @@ class Adjoint final : public AdjointBase {
       err = "invalid sizes";
       return -2;
     }
+    if ((ny + 2 * ng + kBY - 1) / kBY > 65535 || nm > 65535) {
+      err = "the adjoint supports at most 524000 rows and 65535 members";
+      return -2;
+    }
     if (nx < ng || ny < ng) {  // one wall fill per stage: ghosts must mirror interior cells
       err = "the adjoint needs an interior at least nghost cells wide in x and y";
       return -2;

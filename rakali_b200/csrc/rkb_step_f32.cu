@@ -996,14 +996,15 @@ __global__ void k_max_speed32(StepArgs32 a) {
 __global__ void k_to_surface(Grid g64, Grid g32, FieldSet src, const double* __restrict__ b64,
                              FieldSet32 dst, double* __restrict__ bed_out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y;
   if (i >= g64.nxt) return;
-  const size_t p = g64.at(i, j), q = g32.at(i, j);
-  const double b = b64[p];
-  dst.eta[q] = surface_of(src.h[p], b);
-  dst.hu[q] = (float)src.hu[p];
-  dst.hv[q] = (float)src.hv[p];
-  if (bed_out) bed_out[q] = b;
+  for (int j = blockIdx.y; j < g64.nyt; j += gridDim.y) {
+    const size_t p = g64.at(i, j), q = g32.at(i, j);
+    const double b = b64[p];
+    dst.eta[q] = surface_of(src.h[p], b);
+    dst.hu[q] = (float)src.hu[p];
+    dst.hv[q] = (float)src.hv[p];
+    if (bed_out) bed_out[q] = b;
+  }
 }
 
 // FP32 surface form -> FP64 depth form (h = max(0, eta - b)); with
@@ -1011,14 +1012,15 @@ __global__ void k_to_surface(Grid g64, Grid g32, FieldSet src, const double* __r
 __global__ void k_to_depth(Grid g32, Grid g64, FieldSet32 src, const double* __restrict__ b32,
                            FieldSet dst, double* __restrict__ bed_out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y;
   if (i >= g32.nxt) return;
-  const size_t q = g32.at(i, j), p = g64.at(i, j);
-  const double b = b32[q];
-  dst.h[p] = pos((double)src.eta[q] - b);
-  dst.hu[p] = (double)src.hu[q];
-  dst.hv[p] = (double)src.hv[q];
-  if (bed_out) bed_out[p] = b;
+  for (int j = blockIdx.y; j < g32.nyt; j += gridDim.y) {
+    const size_t q = g32.at(i, j), p = g64.at(i, j);
+    const double b = b32[q];
+    dst.h[p] = pos((double)src.eta[q] - b);
+    dst.hu[p] = (double)src.hu[q];
+    dst.hv[p] = (double)src.hv[q];
+    if (bed_out) bed_out[p] = b;
+  }
 }
 
 }  // namespace
@@ -1191,14 +1193,14 @@ cudaError_t launch_max_speed32(const StepArgs32& a, cudaStream_t s) {
 
 cudaError_t launch_to_surface(const Grid& g64, const Grid& g32, FieldSet src, const double* b64,
                               FieldSet32 dst, double* bed_out, cudaStream_t s) {
-  dim3 grid((unsigned)((g64.nxt + 127) / 128), (unsigned)g64.nyt);
+  dim3 grid((unsigned)((g64.nxt + 127) / 128), (unsigned)(g64.nyt < 65535 ? g64.nyt : 65535));
   k_to_surface<<<grid, 128, 0, s>>>(g64, g32, src, b64, dst, bed_out);
   return cudaGetLastError();
 }
 
 cudaError_t launch_to_depth(const Grid& g32, const Grid& g64, FieldSet32 src, const double* b32,
                             FieldSet dst, double* bed_out, cudaStream_t s) {
-  dim3 grid((unsigned)((g32.nxt + 127) / 128), (unsigned)g32.nyt);
+  dim3 grid((unsigned)((g32.nxt + 127) / 128), (unsigned)(g32.nyt < 65535 ? g32.nyt : 65535));
   k_to_depth<<<grid, 128, 0, s>>>(g32, g64, src, b32, dst, bed_out);
   return cudaGetLastError();
 }

@@ -612,8 +612,10 @@ __global__ void __launch_bounds__(TX * TY + 32 * XW)
     k_stage(Grid g, StepCtl* ctl, const Physics* phys, const BcParams* bcp, FieldSet U0,
             FieldSet U1, FieldSet S, const double* __restrict__ b, Forcing fo,
             double* __restrict__ partials, FluxOut fl, int gk) {
+  // one-dimensional grid over the gx x gy tiles (no limit on the row count)
+  const unsigned gx = (unsigned)((g.nx_phys() + TX - 1) / TX);
   stage_body<TX, TY, HLLC, STAGE, XW>(g, ctl, phys, bcp, U0, U1, S, b, fo, partials, fl,
-                                      blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, gk);
+                                      blockIdx.x % gx, blockIdx.x / gx, gx, gridDim.x / gx, gk);
 }
 
 // Every simulation of a batch in one launch: map[blockIdx.x] = (simulation,
@@ -893,8 +895,8 @@ template <int TX, int TY, bool HLLC, int STAGE, int XW = 0>
 static cudaError_t launch_stage_t(const StepArgs& a, FluxOut fl, cudaStream_t s, int gk) {
   using SM = StageSmem<TX, TY>;
   auto kern = k_stage<TX, TY, HLLC, STAGE, XW>;
-  dim3 grid = stage_grid(a.g, a.tile);
-  kern<<<grid, TX * TY + 32 * XW, SM::BYTES, s>>>(a.g, a.ctl, a.phys, a.bc, a.U0, a.U1, a.S, a.b, a.fo,
+  const dim3 d = stage_grid(a.g, a.tile);
+  kern<<<d.x * d.y, TX * TY + 32 * XW, SM::BYTES, s>>>(a.g, a.ctl, a.phys, a.bc, a.U0, a.U1, a.S, a.b, a.fo,
                                         a.partials, fl, gk);
   return cudaGetLastError();
 }

@@ -607,3 +607,29 @@ def test_narrow_grids_bit_exact_and_fp32_runs(nx, ny, nghost):
         s32.step(20)
         assert np.all(np.isfinite(s32.h_phys))
         assert np.abs((s32.h_phys + s32.b_phys) - (h64 + b)).max() <= 1e-4
+
+
+@pytest.mark.parametrize("nx,ny", [(3, 70000), (70000, 3)])
+def test_long_grids_beyond_65535_rows(nx, ny):
+    """Grids longer than a CUDA grid's y extent (65535) in either direction:
+    FP64 bit-identical to the oracle, the FP32 form (whose layout conversions
+    walk the rows) close to it."""
+    from rakali_b200 import Rakali
+    dx = 10.0
+    x = np.arange(nx)[:, None] * np.ones((1, ny))
+    y = np.ones((nx, 1)) * np.arange(ny)[None, :]
+    b = np.asfortranarray(-5.0 + 1.0e-4 * (x + y))
+    h = np.asfortranarray(np.maximum(0.2 * np.exp(-((x + y - 35000.0) / 40.0) ** 2) - b, 0.0))
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, manning_n=0.02)
+    sim, orc = pair(cfg, bathymetry=b, initial_h=h)
+    with sim:
+        sim.step(5)
+        orc.step(5)
+        compare_state(sim, orc, rtol=0.0)
+        e64 = sim.h_phys + sim.b_phys
+    with Rakali(defer_init=True, precision=32, **cfg) as s32:
+        s32.set_bathymetry(b)
+        s32.set_initial_h(h)
+        s32.finalize()
+        s32.step(5)
+        assert np.abs((s32.h_phys + s32.b_phys) - e64).max() <= 1e-4
