@@ -633,3 +633,28 @@ def test_long_grids_beyond_65535_rows(nx, ny):
         s32.finalize()
         s32.step(5)
         assert np.abs((s32.h_phys + s32.b_phys) - e64).max() <= 1e-4
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_all_dry_domain(precision):
+    """No water anywhere: the CFL step falls back to cfl min(dx, dy) / sqrt(g DRY)
+    (rki_kernel_timestep.F90:68-72) and nothing moves; FP64 equals the oracle."""
+    from rakali_b200 import Rakali
+    nx, ny, dx = 40, 30, 5.0
+    b = gaussian_bed(nx, ny, dx, dx, 5, seed=4, base=1.0, amp=(0.0, 2.0), width=(20.0, 60.0))
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, manning_n=0.02,
+               init_condition="still_water", eta_initial=0.0)
+    if precision == 64:
+        sim, orc = pair(cfg, bathymetry=b)
+        with sim:
+            sim.step(5)
+            orc.step(5)
+            assert sim.dt == orc.dt == 0.45 * dx / math.sqrt(G * 1.0e-6)
+            compare_state(sim, orc, rtol=0.0)
+            assert not sim.h_phys.any()
+    else:
+        with Rakali(defer_init=True, precision=32, **cfg) as sim:
+            sim.set_bathymetry(b)
+            sim.finalize()
+            sim.step(5)
+            assert not sim.h_phys.any() and not sim.hu_phys.any() and not sim.hv_phys.any()
