@@ -427,6 +427,18 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
     th[k] = vh; tu[k] = vu; tv[k] = vv; tb[k] = vb;
     te[k] = vh + vb;
   }
+  if (STAGE == 2 && tid < TX * TY) {
+    // the RK2 average reads U^n of this thread's cell after the face phase:
+    // start bringing those lines into L2 now
+    const int pi = gx0 + tid % TX, pj = gy0 + tid / TX;
+    if (pi < g.nxt - g.ng && pj < g.nyt - g.ng) {
+      const FieldSet old = cur ? U1 : U0;
+      const size_t q = g.at(pi, pj);
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(old.h + q));
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(old.hu + q));
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(old.hv + q));
+    }
+  }
   __syncthreads();
 
   // 2. limited slopes: x for cells c in [-1, TX], y for rows r in [-1, TY]
