@@ -144,7 +144,11 @@ int Batch::build() {
                            bl_.tile == tile_)
                         : (bl32_.blocks == nblocks && bl32_.max_nxt == max_nxt &&
                            bl32_.max_nyt == max_nyt && bl32_.cpl == cpl_);
-  if (realloc_ || !same) clear_graphs();  // graphs hold launch shapes and pointers
+  std::vector<int> gsig(n);
+  for (int i = 0; i < n; ++i) gsig[i] = sims_[i]->gauge_generation();
+  // graphs hold launch shapes and pointers, and the members' gauge recorders
+  if (realloc_ || !same || gsig != gauge_sig_) clear_graphs();
+  gauge_sig_ = gsig;
   bl_ = BatchLaunch{(const StepArgs*)dargs_, dmap_, n, nblocks, max_nxt, max_nyt, tile_, hllc_};
   bl32_ = BatchLaunch32{(const StepArgs32*)dargs_, dmap_, n, nblocks, max_nxt, max_nyt, cpl_, hllc_};
   return 0;
@@ -192,6 +196,7 @@ cudaGraphExec_t Batch::graph_for(int steps) {
       launch_step_batch(bl_, stream_);
     else
       launch_step32_batch(bl32_, stream_);
+    for (Sim* s : sims_) s->record_gauges(stream_);  // members with gauge stations
   }
   if (cudaStreamEndCapture(stream_, &ge.graph) != cudaSuccess) return nullptr;
   if (cudaGraphInstantiate(&ge.exec, ge.graph, 0) != cudaSuccess) return nullptr;

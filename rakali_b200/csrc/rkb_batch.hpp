@@ -43,6 +43,7 @@ class Batch {
   void clear_graphs();
 
   std::vector<Sim*> sims_;
+  std::vector<int> gauge_sig_;  // members' gauge generations the graphs were built with
   bool broken_ = false;
   int prec_ = 64;
   int tile_ = kTile32x16;

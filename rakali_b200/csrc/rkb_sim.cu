@@ -346,6 +346,7 @@ int Sim::set_gauges(int n, const double* x, const double* y, double interval, in
   if (cudaSetDevice(device_) != cudaSuccess) return -1;
   if (on_device_ && cudaStreamSynchronize(stream_) != cudaSuccess) return -1;
   drop_graphs();
+  ++gauge_gen_;
   if (gauge_mem_) cudaFree(gauge_mem_);
   gauge_mem_ = nullptr;
   gauge_dev_ = nullptr;
@@ -400,6 +401,15 @@ int Sim::set_gauges(int n, const double* x, const double* y, double interval, in
                        (1.0 - a) * c * b[at(i0, j0 + 1)] + a * c * b[at(i0 + 1, j0 + 1)]);
   }
   return nl;
+}
+
+cudaError_t Sim::record_gauges(cudaStream_t s) {
+  const int n = gauge_host_.n;
+  if (n <= 0) return cudaSuccess;
+  if (precision_ == 32)
+    return launch_gauge_record32(args32_.g, args_.ctl, gauge_dev_, n, args32_.U0, args32_.U1,
+                                 args32_.b, s);
+  return launch_gauge_record(g, args_.ctl, gauge_dev_, n, args_.U0, args_.U1, args_.b, s);
 }
 
 int Sim::gauge_stations(int* station, double* station_b) const {
@@ -1034,6 +1044,9 @@ int Sim::snapshot() {
     RKB_TRY(cudaMemcpyAsync(eta_old_[w].data(), args_.eta_old[w],
                             eta_old_[w].size() * sizeof(double), cudaMemcpyDeviceToHost,
                             stream_));
+  if (gauge_dev_)  // trial steps must leave no gauge records behind
+    RKB_TRY(cudaMemcpyAsync(&snap_gauge_, gauge_dev_, sizeof(GaugeDev), cudaMemcpyDeviceToHost,
+                            stream_));
   RKB_TRY(cudaStreamSynchronize(stream_));
   snap_cur_ = cur_;
   snap_t_ = t_current_;
@@ -1055,6 +1068,9 @@ int Sim::restore() {
   for (int w = 0; w < 4; ++w)
     RKB_TRY(cudaMemcpyAsync(args_.eta_old[w], eta_old_[w].data(),
                             eta_old_[w].size() * sizeof(double), cudaMemcpyHostToDevice,
+                            stream_));
+  if (gauge_dev_)
+    RKB_TRY(cudaMemcpyAsync(gauge_dev_, &snap_gauge_, sizeof(GaugeDev), cudaMemcpyHostToDevice,
                             stream_));
   RKB_TRY(cudaStreamSynchronize(stream_));
   cur_ = snap_cur_;

@@ -43,6 +43,10 @@ class Sim {
   // Drain the recorded series: count returned, times [count], values
   // [count][n][3] (eta, u, v), *overflow = records dropped since the last read.
   int read_gauges(int max_records, double* times, double* values, int* overflow);
+  // For batches: the recorder kernel of this simulation (nothing without
+  // stations), and a number that changes whenever the stations change.
+  cudaError_t record_gauges(cudaStream_t s);
+  int gauge_generation() const { return gauge_gen_; }
   int load_restart(const std::string& path, std::string& err);  // before finalize; 1 = grid mismatch
   int advance(double target_time);  // rki_advance
 
@@ -151,6 +155,8 @@ class Sim {
   GaugeDev gauge_host_{};
   std::vector<int> gauge_station_;
   std::vector<double> gauge_b_;
+  int gauge_gen_ = 0;
+  GaugeDev snap_gauge_{};  // recorder state at the last snapshot
 
   struct GraphEntry {
     int steps, hllc, tile, prec, rows;

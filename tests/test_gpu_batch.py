@@ -120,3 +120,27 @@ def test_batch_rejects_bad_members():
     ens.close()
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_batch_records_member_gauges(precision):
+    """A member's gauge stations record inside the batch's step graphs exactly as
+    when that member steps alone; autotuning trial steps leave no records."""
+    ms = _members(3, seed=4)
+    sims = [wl.build_member(m, precision) for m in ms]
+    alone = wl.build_member(ms[1], precision)
+    nx, ny, dx = ms[1]["kw"]["nx"], ms[1]["kw"]["ny"], ms[1]["kw"]["dx"]
+    xs, ys = [0.3 * nx * dx, 0.7 * nx * dx], [0.5 * ny * dx, 0.25 * ny * dx]
+    for s in (sims[1], alone):
+        s.set_gauges(xs, ys, names=["a", "b"])
+    with Ensemble(sims, precision=precision) as ens:
+        ens.autotune(trial_steps=2)
+        ens.step(7)
+    alone.step(7)
+    got, ref = sims[1].gauge_records(), alone.gauge_records()
+    assert got["time"].size == ref["time"].size == 7
+    assert np.array_equal(got["time"], ref["time"])
+    for key in ("eta", "u", "v"):
+        assert np.array_equal(got[key], ref[key])
+    for s in sims + [alone]:
+        s.close()
