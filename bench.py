@@ -555,6 +555,63 @@ def run_config5(args):
                        "grad_n_rel_l2": rel(gnsf[0], short[64][2]),
                        "directional_rel_err_median": float(np.median(sd_floor)),
                        "directional_rel_err_max": float(np.max(sd_floor))}}
+    # Frozen-slope gradients of member 0 over the whole window: the limited
+    # slopes held constant, which removes the limiter's branch sensitivity.
+    # Both gradients are also set against central-difference secants of the
+    # FP64 J along the same directions (step eps: 1 mm of bed at the
+    # directions' 1 m amplitude).
+    eps = 1e-3
+    frozen = {}
+    secant = []
+    for prec in (32, 64):
+        with GaugeMisfitBatch(1, n, n, dx, dx, ref["h"][None], [ref["gauges"]], steps,
+                              precision=prec) as pz:
+            pz.set_dt(ref["dt"][None])
+            pz.set_observations(ref["obs"][:, None, :])
+            pz.set_frozen_slopes(True)
+            _, gbz, gnz = pz.gradient(ref["b"][None], ref["n"][None])
+            frozen[prec] = (gbz[0], gnz[0])
+            if prec == 64:
+                _, gbzf, gnzf = pz.gradient(ref["b"][None] + pert, ref["n"][None])
+                for k in range(8):
+                    db = wl.gaussian_bed(n, n, dx, dx, 3, 700 + k, base=0.0, amp=(-1.0, 1.0),
+                                         width=(200.0, 1500.0))
+                    dn = wl.gaussian_bed(n, n, dx, dx, 3, 800 + k, base=0.0,
+                                         amp=(-0.01, 0.01), width=(200.0, 1500.0))
+                    Jp, _ = pz.forward(ref["b"][None] + eps * db[None],
+                                       ref["n"][None] + eps * dn[None])
+                    Jm, _ = pz.forward(ref["b"][None] - eps * db[None],
+                                       ref["n"][None] - eps * dn[None])
+                    secant.append(float(Jp[0] - Jm[0]) / (2.0 * eps))
+    fd, fd_floor, sec_frozen, sec_exact = [], [], [], []
+    for k in range(8):
+        db = wl.gaussian_bed(n, n, dx, dx, 3, 700 + k, base=0.0, amp=(-1.0, 1.0),
+                             width=(200.0, 1500.0))
+        dn = wl.gaussian_bed(n, n, dx, dx, 3, 800 + k, base=0.0, amp=(-0.01, 0.01),
+                             width=(200.0, 1500.0))
+        d64 = float(np.sum(frozen[64][0] * db) + np.sum(frozen[64][1] * dn))
+        d32 = float(np.sum(frozen[32][0] * db) + np.sum(frozen[32][1] * dn))
+        dfl = float(np.sum(gbzf[0] * db) + np.sum(gnzf[0] * dn))
+        dex = float(np.sum(gb64[0] * db) + np.sum(gn64[0] * dn))
+        fd.append(abs(d32 - d64) / abs(d64))
+        fd_floor.append(abs(dfl - d64) / abs(d64))
+        sec_frozen.append(abs(d64 - secant[k]) / abs(secant[k]))
+        sec_exact.append(abs(dex - secant[k]) / abs(secant[k]))
+    frozen_slopes = {
+        "steps": steps,
+        "grad_b_rel_l2": rel(frozen[32][0], frozen[64][0]),
+        "grad_n_rel_l2": rel(frozen[32][1], frozen[64][1]),
+        "directional_rel_err_median": float(np.median(fd)),
+        "directional_rel_err_max": float(np.max(fd)),
+        "fp64_floor": {"grad_b_rel_l2": rel(gbzf[0], frozen[64][0]),
+                       "grad_n_rel_l2": rel(gnzf[0], frozen[64][1]),
+                       "directional_rel_err_median": float(np.median(fd_floor)),
+                       "directional_rel_err_max": float(np.max(fd_floor))},
+        "vs_fp64_secants": {"eps": eps,
+                            "frozen_rel_err_median": float(np.median(sec_frozen)),
+                            "frozen_rel_err_max": float(np.max(sec_frozen)),
+                            "exact_rel_err_median": float(np.median(sec_exact)),
+                            "exact_rel_err_max": float(np.max(sec_exact))}}
     return {
         "workload": f"{nm} members x {n}x{n}, dx = {dx} m, 16-Gaussian bed per member "
                     f"(seeds 1000..{1000 + nm - 1}), 0.5 m hump on a smooth undulation, "
@@ -568,6 +625,7 @@ def run_config5(args):
         "cost_multiple_of_forward": grad_ms / fwd_ms,
         "mass_drift_rel_max": drift,
         "vs_fp64_member0_first_steps": first_steps,
+        "vs_fp64_member0_frozen_slopes": frozen_slopes,
         "vs_fp64_member0": {
             "J_rel_err": abs(ref["J"] - float(J64[0])) / abs(float(J64[0])),
             "grad_b_rel_l2": rel(ref["gb"], gb64[0]), "grad_n_rel_l2": rel(ref["gn"], gn64[0]),

@@ -217,6 +217,10 @@ int rkb_adjoint_precision(void *adj);
 /* FP64 interior mass sum(h) per member before (out[m]) and after
  * (out[n_members + m]) the last forward run. */
 int rkb_adjoint_mass(void *adj, double *out);
+/* on != 0: later gradients hold the limited slopes of each state fixed (their
+ * adjoints are dropped): not the exact derivative, but one that stays bounded
+ * over long windows, where the exact derivative of the minmod limiter grows. */
+int rkb_adjoint_set_frozen_slopes(void *adj, int on);
 /* Host builds of the face flux / cell update and their adjoints (for
  * finite-difference checks without a GPU). */
 void rkb_test_face_flux(int dir, int hllc, const double *in8, double *out6);

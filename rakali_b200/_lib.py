@@ -125,6 +125,7 @@ def load(path: str | None = None):
     _sig(lib, "rkb_adjoint_members", [H], I)
     _sig(lib, "rkb_adjoint_precision", [H], I)
     _sig(lib, "rkb_adjoint_mass", [H, DP], I)
+    _sig(lib, "rkb_adjoint_set_frozen_slopes", [H, I], I)
     _sig(lib, "rkb_test_face_flux", [I, I, DP, DP], None)
     _sig(lib, "rkb_test_face_adj", [I, I, DP, DP, DP], None)
     _sig(lib, "rkb_test_cell", [DP, D, DP], None)

@@ -115,6 +115,11 @@ class GaugeMisfit:
             ctypes.byref(J), gb.ctypes.data_as(_DP), gn.ctypes.data_as(_DP)), "gradient")
         return J.value, gb, gn
 
+    def set_frozen_slopes(self, on=True):
+        """Hold the limited slopes fixed in later gradients (bounded over long
+        windows; not the exact derivative of the limiter)."""
+        self._rc(self._lib.rkb_adjoint_set_frozen_slopes(self._a, int(bool(on))), "set_frozen_slopes")
+
     @property
     def checkpoint_interval(self):
         return int(self._lib.rkb_adjoint_checkpoint_interval(self._a))
@@ -258,6 +263,11 @@ class GaugeMisfitBatch:
         out = np.zeros((2, self.nm))
         self._rc(self._lib.rkb_adjoint_mass(self._a, out.ctypes.data_as(_DP)), "mass")
         return out
+
+    def set_frozen_slopes(self, on=True):
+        """Hold the limited slopes fixed in later gradients (bounded over long
+        windows; not the exact derivative of the limiter)."""
+        self._rc(self._lib.rkb_adjoint_set_frozen_slopes(self._a, int(bool(on))), "set_frozen_slopes")
 
     @property
     def checkpoint_interval(self):

@@ -109,6 +109,12 @@ int rkb_adjoint_members(void* adj) { return adj ? as_adj(adj)->members() : -2; }
 
 int rkb_adjoint_precision(void* adj) { return adj ? as_adj(adj)->precision() : -2; }
 
+int rkb_adjoint_set_frozen_slopes(void* adj, int on) {
+  if (!adj) return -2;
+  as_adj(adj)->set_frozen_slopes(on != 0);
+  return 0;
+}
+
 int rkb_adjoint_mass(void* adj, double* out) {
   if (!adj || !out) return -2;
   as_adj(adj)->mass(out);

@@ -52,6 +52,10 @@ class AdjointBase {
   virtual int members() const = 0;
   virtual int precision() const = 0;
   virtual void mass(double* out) const = 0;     // [2][member]: initial, after the last forward
+  // Frozen slopes: gradients of the step with its limited slopes held at
+  // their current values (an approximation that stays bounded over long
+  // windows where the exact derivative of the limiter does not).
+  virtual void set_frozen_slopes(bool on) = 0;
 };
 
 // Factories (one per precision, each in its own translation unit).
@@ -417,8 +421,11 @@ __global__ void k_recon_adj(Grid g, size_t ms, Fields<T> V, const T* __restrict_
 // neighbours (minmod branch a = q_c - q_{c-1}, b = q_{c+1} - q_c), plus the
 // direct reconstruction and cell-update adjoints.  gV receives the adjoint of
 // the stage input (all cells, ghosts included); gb accumulates the bed's.
+// frozen: the limited slopes are held constant (their adjoints are dropped),
+// the derivative of the step with the slopes of the current state frozen.
 template <typename T>
-__global__ void k_gather_adj(Grid g, size_t ms, Rev<T> R, Fields<T> gV, T* __restrict__ gb) {
+__global__ void k_gather_adj(Grid g, size_t ms, Rev<T> R, Fields<T> gV, T* __restrict__ gb,
+                             int frozen) {
   const int i = g.ng - 2 + blockIdx.x * kBX + threadIdx.x % kBX;
   const int j = g.ng - 2 + blockIdx.y * kBY + threadIdx.x / kBX;
   if (i > g.nxt - g.ng + 1 || j > g.nyt - g.ng + 1) return;
@@ -430,7 +437,7 @@ __global__ void k_gather_adj(Grid g, size_t ms, Rev<T> R, Fields<T> gV, T* __res
   auto ys = [&](int ii, int jj) { return in_box(ii, jj, g.ng, ie - 1, g.ng - 1, je); };
   auto rc = [&](int ii, int jj) { return in_box(ii, jj, g.ng - 1, ie, g.ng - 1, je); };
   T acc[3] = {T(0), T(0), T(0)};
-  for (int dir = 0; dir < 2; ++dir) {
+  for (int dir = 0; dir < 2 && !frozen; ++dir) {
     const int di = dir == 0 ? 1 : 0, dj = dir == 0 ? 0 : 1;
     auto has = [&](int ii, int jj) { return dir == 0 ? xs(ii, jj) : ys(ii, jj); };
     for (int v = 0; v < 3; ++v) {
@@ -695,6 +702,7 @@ class Adjoint final : public AdjointBase {
   int members() const override { return nm_; }
   int precision() const override { return sizeof(T) == 8 ? 64 : 32; }
   void mass(double* out) const override { std::memcpy(out, mass_.data(), mass_.size() * 8); }
+  void set_frozen_slopes(bool on) override { frozen_ = on; }
 
   // Forward run.  record: dt from the CFL condition of each state (stored);
   // else the stored dt sequence.  J[m] and, optionally, the gauge surfaces
@@ -961,7 +969,7 @@ class Adjoint final : public AdjointBase {
     k_recon_adj<T><<<blocks(g_.ng - 1, ie, g_.ng - 1, je), kBX * kBY, 0, stream_>>>(g_, ms_, V, b_,
                                                                                    R_);
     k_gather_adj<T><<<blocks(g_.ng - 2, ie + 1, g_.ng - 2, je + 1), kBX * kBY, 0, stream_>>>(
-        g_, ms_, R_, gV_, gb_);
+        g_, ms_, R_, gV_, gb_, frozen_ ? 1 : 0);
     walls_adj(V, false);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
   }
@@ -1002,6 +1010,7 @@ class Adjoint final : public AdjointBase {
   std::vector<Fields<T>> ck_, seg_;
   std::vector<double> dts_, obs_, mass_;  // dts_: [step][member]
   bool have_dt_ = false, obs_dev_dirty_ = true;
+  bool frozen_ = false;
 };
 
 #undef ADJ_TRY

@@ -273,3 +273,70 @@ def test_batch_fp32_against_fp64():
     assert gb_err.max() <= 4.0 * gb_floor.max() + 1e-3
     assert gn_err.max() <= 4.0 * gn_floor.max() + 1e-3
     assert max(dd) <= 1e-2
+
+
+
+@pytest.mark.parametrize("hllc", [False, True])
+def test_frozen_slope_gradient_matches_autograd_with_detached_slopes(hllc):
+    """set_frozen_slopes(True): the gradient with the limited slopes held constant
+    equals torch.autograd through the transcription with its slopes detached; J
+    is unchanged, and set_frozen_slopes(False) gives the exact gradient back bit
+    for bit."""
+    import torch
+
+    from tests import torch_step as ts
+    nx, ny, steps = 28, 22, 14
+    p, b, h, n, gauges, obs = _problem(nx, ny, steps, 6, seed=5, hllc=hllc, generic=True)
+    J0, gb0, gn0 = p.gradient(b, n)
+    p.set_frozen_slopes(True)
+    J, gb, gn = p.gradient(b, n)
+    assert J == J0
+    bt = torch.tensor(b, dtype=torch.float64, requires_grad=True)
+    nt = torch.tensor(n, dtype=torch.float64, requires_grad=True)
+    z = torch.zeros((nx, ny), dtype=torch.float64)
+    Jt = ts.misfit(bt, nt, torch.from_numpy(h), z, z, gauges, torch.from_numpy(obs), list(p.dt),
+                   2, 10.0, 10.0, hllc=hllc, frozen=True)
+    Jt.backward()
+    assert abs(float(Jt.detach()) - J) <= 1e-10 * abs(J)
+    for got, ref in ((gb, bt.grad.numpy()), (gn, nt.grad.numpy())):
+        scale = float(np.abs(ref).max())
+        assert scale > 0.0
+        assert float(np.abs(got - ref).max()) <= 1e-8 * scale
+    assert float(np.abs(gb - gb0).max()) > 0.0  # the slopes do carry sensitivity
+    p.set_frozen_slopes(False)
+    J1, gb1, gn1 = p.gradient(b, n)
+    assert J1 == J0 and np.array_equal(gb1, gb0) and np.array_equal(gn1, gn0)
+    p.close()
+
+
+def test_frozen_slope_gradient_fp32_against_fp64():
+    """Frozen-slope gradients of an FP32 batch against the FP64 batch on the same
+    dt sequence: relative L2 error (worst member) within 1e-2 and directional
+    derivatives along smooth directions within 2e-3 relative."""
+    from rakali_b200.adjoint import GaugeMisfitBatch
+    nm, nx, ny, steps = 3, 64, 48, 40
+    b, h, gauges, ob = _batch_inputs(nm, nx, ny, steps, 8, seed=43)
+    n = np.full((nm, nx, ny), 0.025)
+    with GaugeMisfitBatch(nm, nx, ny, 10.0, 10.0, h, gauges, steps, precision=64) as p64:
+        p64.record_dt(b, n)
+        dts = p64.dt
+        _, obs = p64.forward(ob, n)
+        p64.set_observations(obs)
+        p64.set_frozen_slopes(True)
+        _, gb64, gn64 = p64.gradient(b, n)
+    with GaugeMisfitBatch(nm, nx, ny, 10.0, 10.0, h, gauges, steps, precision=32) as p32:
+        p32.set_dt(dts)
+        p32.set_observations(obs)
+        p32.set_frozen_slopes(True)
+        _, gb32, gn32 = p32.gradient(b, n)
+    rel = max(float(np.linalg.norm(gb32[m] - gb64[m]) / np.linalg.norm(gb64[m])) for m in range(nm))
+    dd = []
+    for k in range(4):
+        db = np.array([gaussian_bed(nx, ny, 10.0, 10.0, 3, seed=500 + 10 * k + m, base=0.0,
+                                    amp=(-1.0, 1.0), width=(60.0, 200.0)) for m in range(nm)])
+        d64 = np.sum(gb64 * db, axis=(1, 2))
+        d32 = np.sum(gb32 * db, axis=(1, 2))
+        dd.extend(np.abs(d32 - d64) / np.abs(d64))
+    print(f"frozen fp32 vs fp64: grad b rel L2 {rel:.2e}, directional max {max(dd):.2e}")
+    assert rel <= 1e-2
+    assert max(dd) <= 2e-3

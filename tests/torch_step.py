@@ -146,20 +146,25 @@ def _slopes(h, e, hu, hv, dim, ng):
     return tuple(torch.where(gate, minmod(c(x) - m(x), p(x) - c(x)), z) for x in (e, hu, hv))
 
 
-def stage(h, hu, hv, b, n, dt, ng, dx, dy, hllc, base=None):
-    """One stage on states with ghosts; returns interior (h, hu, hv)."""
+def stage(h, hu, hv, b, n, dt, ng, dx, dy, hllc, base=None, frozen=False):
+    """One stage on states with ghosts; returns interior (h, hu, hv).  frozen:
+    the limited slopes enter as constants (detached from the graph)."""
     nxt, nyt = h.shape
     e = h + b
     inner_y = slice(ng, nyt - ng)
     inner_x = slice(ng, nxt - ng)
     # x direction: slopes of columns ng-1 .. nxt-ng over the interior rows
     sx = _slopes(h[:, inner_y], e[:, inner_y], hu[:, inner_y], hv[:, inner_y], 0, ng)
+    if frozen:
+        sx = tuple(t.detach() for t in sx)
     c = lambda x: x[ng - 1:nxt - ng + 1, inner_y]
     L = lambda x, s: (c(x) + 0.5 * s)[:-1]
     R = lambda x, s: (c(x) - 0.5 * s)[1:]
     fx = face_flux(0, hllc, L(e, sx[0]), L(hu, sx[1]), L(hv, sx[2]), c(b)[:-1],
                    R(e, sx[0]), R(hu, sx[1]), R(hv, sx[2]), c(b)[1:])
     sy = _slopes(h[inner_x, :], e[inner_x, :], hu[inner_x, :], hv[inner_x, :], 1, ng)
+    if frozen:
+        sy = tuple(t.detach() for t in sy)
     cy = lambda x: x[inner_x, ng - 1:nyt - ng + 1]
     B = lambda x, s: (cy(x) + 0.5 * s)[:, :-1]
     T = lambda x, s: (cy(x) - 0.5 * s)[:, 1:]
@@ -187,7 +192,7 @@ def embed(inner, ng):
     return out
 
 
-def misfit(b, n, h0, hu0, hv0, gauges, obs, dts, ng, dx, dy, hllc=False):
+def misfit(b, n, h0, hu0, hv0, gauges, obs, dts, ng, dx, dy, hllc=False, frozen=False):
     """J = sum over steps and gauges of (h + b - obs)^2; b, n, h0 interior tensors."""
     bf = embed(b, ng)
     h, hu, hv = embed(h0, ng), embed(hu0, ng), embed(hv0, ng)
@@ -197,10 +202,10 @@ def misfit(b, n, h0, hu0, hv0, gauges, obs, dts, ng, dx, dy, hllc=False):
     for k, dt in enumerate(dts):
         h, hu, hv, bf = walls(h, hu, hv, bf, ng)
         base = (h[ng:-ng, ng:-ng], hu[ng:-ng, ng:-ng], hv[ng:-ng, ng:-ng])
-        a, u, v = stage(h, hu, hv, bf, n, dt, ng, dx, dy, hllc)
+        a, u, v = stage(h, hu, hv, bf, n, dt, ng, dx, dy, hllc, frozen=frozen)
         hs, hus, hvs = embed(a, ng), embed(u, ng), embed(v, ng)
         hs, hus, hvs, bf = walls(hs, hus, hvs, bf, ng)
-        a, u, v = stage(hs, hus, hvs, bf, n, dt, ng, dx, dy, hllc, base=base)
+        a, u, v = stage(hs, hus, hvs, bf, n, dt, ng, dx, dy, hllc, base=base, frozen=frozen)
         h, hu, hv = embed(a, ng), embed(u, ng), embed(v, ng)
         eta = a[gi, gj] + b[gi, gj]
         J = J + ((eta - obs[k]) ** 2).sum()
