@@ -98,6 +98,7 @@ int Batch::build() {
   std::vector<StepArgs> a64;
   std::vector<StepArgs32> a32;
   int max_nxt = 0, max_nyt = 0;
+  int plain = 1;
   for (int i = 0; i < n; ++i) {
     Sim* s = sims_[i];
     max_nxt = std::max(max_nxt, s->g.nxt);
@@ -110,6 +111,7 @@ int Batch::build() {
       blocks[i] = batch_stage_blocks(s->g, tile_);
     } else {
       StepArgs32 a = s->device_args32();
+      plain = plain && a.plain;
       a32.push_back(a);
       blocks[i] = batch_sweep_blocks(a);
     }
@@ -143,14 +145,15 @@ int Batch::build() {
                         ? (bl_.blocks == nblocks && bl_.max_nxt == max_nxt && bl_.max_nyt == max_nyt &&
                            bl_.tile == tile_)
                         : (bl32_.blocks == nblocks && bl32_.max_nxt == max_nxt &&
-                           bl32_.max_nyt == max_nyt && bl32_.cpl == cpl_);
+                           bl32_.max_nyt == max_nyt && bl32_.cpl == cpl_ && bl32_.plain == plain);
   std::vector<int> gsig(n);
   for (int i = 0; i < n; ++i) gsig[i] = sims_[i]->gauge_generation();
   // graphs hold launch shapes and pointers, and the members' gauge recorders
   if (realloc_ || !same || gsig != gauge_sig_) clear_graphs();
   gauge_sig_ = gsig;
   bl_ = BatchLaunch{(const StepArgs*)dargs_, dmap_, n, nblocks, max_nxt, max_nyt, tile_, hllc_};
-  bl32_ = BatchLaunch32{(const StepArgs32*)dargs_, dmap_, n, nblocks, max_nxt, max_nyt, cpl_, hllc_};
+  bl32_ = BatchLaunch32{(const StepArgs32*)dargs_, dmap_, n, nblocks, max_nxt, max_nyt,
+                        cpl_, hllc_, plain};
   return 0;
 }
 

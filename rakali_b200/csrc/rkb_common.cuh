@@ -95,8 +95,12 @@ struct StepCtl {
   unsigned int done_blocks;  // last-block counter of the final stage kernel
   unsigned int ms_done_blocks;
   int steps_run;       // steps executed since the host last cleared it
-  int error;           // nonzero: a bounded device-side wait gave up (FP32 sweep)
+  int error;           // nonzero: kErrWait or kErrPhysics (FP32 sweep)
 };
+
+// StepCtl::error codes of the FP32 sweep.
+constexpr int kErrWait = 1;     // a bounded device-side wait for a bulk copy gave up
+constexpr int kErrPhysics = 2;  // a launch built without forcing / Coriolis / sponge met them
 
 // ---------------------------------------------------------------------------
 // Small FP64 helpers in the reference's evaluation order.

@@ -82,6 +82,7 @@ struct StepArgs32 {
   double* partials;
   double* eta_old[4];  // Chapman surfaces (FP64)
   int hllc;
+  int plain;           // no forcing, Coriolis or sponge: the sweep built without those terms
   int cpl;             // columns per lane of the sweep (2 or 4)
   int rows;            // rows per warp sweep
   int nstrips, nrowblk;
@@ -151,6 +152,7 @@ struct BatchLaunch32 {
   int blocks;
   int max_nxt, max_nyt;
   int cpl, hllc;
+  int plain;  // every member plain (StepArgs32::plain)
 };
 int batch_sweep_blocks(const StepArgs32& a);
 cudaError_t configure_batch32();

@@ -747,11 +747,12 @@ void Sim::pull_ctl() {
 
 cudaGraphExec_t Sim::graph_for(int steps) {
   const int rows = precision_ == 32 ? args32_.rows * 8 + args32_.cpl : 0;
+  const int plain = precision_ == 32 ? args32_.plain : 0;
   for (auto& ge : graphs_)
     if (ge.steps == steps && ge.hllc == args_.hllc && ge.tile == args_.tile &&
-        ge.prec == precision_ && ge.rows == rows)
+        ge.prec == precision_ && ge.rows == rows && ge.plain == plain)
       return ge.exec;
-  GraphEntry ge{steps, args_.hllc, args_.tile, precision_, rows, nullptr, nullptr};
+  GraphEntry ge{steps, args_.hllc, args_.tile, precision_, rows, plain, nullptr, nullptr};
   if (cudaStreamSynchronize(stream_) != cudaSuccess) return nullptr;
   if (cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
     return nullptr;
@@ -972,6 +973,8 @@ void Sim::sync_args32() {
   args32_.fpitch = g.pitch;
   for (int w = 0; w < 4; ++w) args32_.eta_old[w] = args_.eta_old[w];
   args32_.hllc = phys.use_hllc;
+  args32_.plain = !phys.forcing_active && !(std::fabs(phys.coriolis_f) > 1.0e-20) &&
+                  !(bc.sponge_width > 0 && bc.sponge_strength > 0.0);
   args32_.cpl = sweep_cpl == 4 ? 4 : 2;
   int rows = sweep_rows > 0 ? sweep_rows : auto_rows_[args32_.cpl == 4 ? 1 : 0];
   if (rows < 4) rows = 4;
@@ -1008,7 +1011,10 @@ int Sim::to_depth(bool full) {
 
 int Sim::check_device_error() {
   if (!hctl_->error) return 0;
-  err_text_ = "a bounded device-side wait for a bulk copy expired; the step was abandoned";
+  err_text_ = hctl_->error == kErrPhysics
+                  ? "the step kernel was built for other physics than the device held; the step "
+                    "was abandoned"
+                  : "a bounded device-side wait for a bulk copy expired; the step was abandoned";
   hctl_->error = 0;
   cudaMemcpyAsync(&args_.ctl->error, &hctl_->error, sizeof(int), cudaMemcpyHostToDevice, stream_);
   cudaStreamSynchronize(stream_);

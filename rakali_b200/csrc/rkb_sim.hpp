@@ -159,7 +159,7 @@ class Sim {
   GaugeDev snap_gauge_{};  // recorder state at the last snapshot
 
   struct GraphEntry {
-    int steps, hllc, tile, prec, rows;
+    int steps, hllc, tile, prec, rows, plain;
     cudaGraph_t graph;
     cudaGraphExec_t exec;
   };

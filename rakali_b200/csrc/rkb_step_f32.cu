@@ -156,9 +156,10 @@ __device__ __forceinline__ float surface_of(double h, double b) {
   return h > 0.0 ? __double2float_rn(h + b) : __double2float_rd(b);
 }
 
+// minmod(a, b) (rki_kernel_flux.F90:380-393) as the median of (a, b, 0): 0
+// when the signs differ or one is 0, else the value of smaller magnitude.
 __device__ __forceinline__ float minmodf(float a, float b) {
-  if (a * b <= 0.0f) return 0.0f;
-  return fabsf(a) < fabsf(b) ? a : b;
+  return fmaxf(fminf(a, b), fminf(fmaxf(a, b), 0.0f));
 }
 
 struct Slope {
@@ -170,13 +171,9 @@ struct Slope {
 __device__ __forceinline__ Slope slope(unsigned fm, unsigned fc, unsigned fp, float em, float ec,
                                        float ep, float um, float uc, float up, float vm, float vc,
                                        float vp) {
-  Slope s{0.0f, 0.0f, 0.0f};
-  if ((fc & 2u) && (fm & 1u) && (fp & 1u)) {
-    s.e = minmodf(ec - em, ep - ec);
-    s.u = minmodf(uc - um, up - uc);
-    s.v = minmodf(vc - vm, vp - vc);
-  }
-  return s;
+  const bool on = (fc & 2u) && (fm & 1u) && (fp & 1u);
+  return Slope{on ? minmodf(ec - em, ep - ec) : 0.0f, on ? minmodf(uc - um, up - uc) : 0.0f,
+               on ? minmodf(vc - vm, vp - vc) : 0.0f};
 }
 
 // Faces.  The Audusse hydrostatic depths max(0, eta - max(b_L, b_R))
@@ -431,8 +428,9 @@ __device__ __forceinline__ void st_f(float* p, const float (&v)[C]) {
 // Stage kernel
 // ---------------------------------------------------------------------------
 // STAGE 1: U^n (buffer cur) -> U* (S).  STAGE 2: U*, U^n -> U^{n+1} (cur^1).
-// Block `blk` of the `nblk` blocks that cover one simulation.
-template <int C, bool HLLC, int STAGE>
+// Block `blk` of the `nblk` blocks that cover one simulation.  PLAIN: no
+// forcing, Coriolis or sponge (the common case), compiled without those paths.
+template <int C, bool HLLC, int STAGE, bool PLAIN>
 __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, unsigned nblk) {
   using L = Lay<C>;
   constexpr int SLOT = L::slot(STAGE);
@@ -448,19 +446,19 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
   const int cur = ctl->cur;
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  if (threadIdx.x == 0) {
+  if (!PLAIN && threadIdx.x == 0) {
     // Coriolis rotation cos/sin(f dt) (rki_kernel_fused.F90:211-214)
     double sn = 0.0, cs = 1.0;
     if (fabs(phys->coriolis_f) > 1.0e-20) cr_sincos(phys->coriolis_f * dtd, sn, cs);
     rot[0] = (float)cs;
     rot[1] = (float)sn;
   }
-  __syncthreads();
-  const bool has_cor = fabs(phys->coriolis_f) > 1.0e-20;
+  if (!PLAIN) __syncthreads();
+  const bool has_cor = !PLAIN && fabs(phys->coriolis_f) > 1.0e-20;
   const bool friction = phys->manning_n > 0.0;
   const float gn2dt = (float)(kG * phys->manning_n * phys->manning_n) * dt;
-  const bool forcing = phys->forcing_active != 0;
-  const bool sponge_on = a.bc->sponge_width > 0 && a.bc->sponge_strength > 0.0;
+  const bool forcing = !PLAIN && phys->forcing_active != 0;
+  const bool sponge_on = !PLAIN && a.bc->sponge_width > 0 && a.bc->sponge_strength > 0.0;
   const float rdx = (float)(1.0 / g.dx), rdy = (float)(1.0 / g.dy);
   const float cosf_ = rot[0], sinf_ = rot[1];
 
@@ -756,7 +754,7 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
     if (!ok) {
       // a copy did not arrive in time: flag it and let every copy this warp
       // issued land (each wait bounded) before the shared memory goes away
-      if (lane == 0) atomicExch(&ctl->error, 1);
+      if (lane == 0) atomicExch(&ctl->error, kErrWait);
       for (int r = waited + 1; r <= issued; ++r) wait_next();
     }
   }
@@ -790,14 +788,29 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
   finalize_step(g, ctl, phys, a.partials, nw, dtd, cur);
 }
 
-template <int C, bool HLLC, int STAGE>
+// True when the stage has no forcing, Coriolis or sponge terms.
+__device__ __forceinline__ bool plain_physics(const StepArgs32& a) {
+  return a.phys->forcing_active == 0 && !(fabs(a.phys->coriolis_f) > 1.0e-20) &&
+         !(a.bc->sponge_width > 0 && a.bc->sponge_strength > 0.0);
+}
+
+// The host picks the PLAIN build from its copy of the physics; a launch whose
+// device-side physics disagree computes nothing and reports kErrPhysics.
+__device__ __forceinline__ bool plain_mismatch(const StepArgs32& a) {
+  if (plain_physics(a)) return false;
+  if (threadIdx.x == 0) atomicExch(&a.ctl->error, kErrPhysics);
+  return true;
+}
+
+template <int C, bool HLLC, int STAGE, bool PLAIN>
 __global__ void __launch_bounds__(kWarps * 32, C == 2 ? 4 : 2) k_sweep(StepArgs32 a) {
-  sweep_body<C, HLLC, STAGE>(a, blockIdx.x, gridDim.x);
+  if (PLAIN && plain_mismatch(a)) return;
+  sweep_body<C, HLLC, STAGE, PLAIN>(a, blockIdx.x, gridDim.x);
 }
 
 // Every simulation of a batch in one launch: map[blockIdx.x] = (simulation,
 // block index within that simulation's sweep).
-template <int C, bool HLLC, int STAGE>
+template <int C, bool HLLC, int STAGE, bool PLAIN>
 __global__ void __launch_bounds__(kWarps * 32, C == 2 ? 4 : 2)
     k_sweep_batch(const StepArgs32* __restrict__ args, const int2* __restrict__ map) {
   __shared__ StepArgs32 sa;
@@ -805,7 +818,8 @@ __global__ void __launch_bounds__(kWarps * 32, C == 2 ? 4 : 2)
   if (threadIdx.x == 0) sa = args[m.x];
   __syncthreads();
   const unsigned nblk = (unsigned)((sa.nstrips * sa.nrowblk + kWarps - 1) / kWarps);
-  sweep_body<C, HLLC, STAGE>(sa, (unsigned)m.y, nblk);
+  if (PLAIN && plain_mismatch(sa)) return;
+  sweep_body<C, HLLC, STAGE, PLAIN>(sa, (unsigned)m.y, nblk);
 }
 
 // ---------------------------------------------------------------------------
@@ -1065,8 +1079,12 @@ size_t partials_doubles32(const Grid& g, int rows) {
 template <int C, bool HLLC, int STAGE>
 static cudaError_t set_smem() {
   const int bytes = kWarps * kNbuf * Lay<C>::slot(STAGE);
-  return cudaFuncSetAttribute(k_sweep<C, HLLC, STAGE>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaError_t e = cudaFuncSetAttribute(k_sweep<C, HLLC, STAGE, true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_sweep<C, HLLC, STAGE, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  return e;
 }
 
 cudaError_t configure_kernels32() {
@@ -1086,7 +1104,7 @@ static int auto_rows_t(const Grid& g) {
   int per_sm = 0, sms = 0, dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<C, false, 2>, kWarps * 32,
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<C, false, 2, true>, kWarps * 32,
                                                     kWarps * kNbuf * Lay<C>::kSlot2) !=
           cudaSuccess ||
       per_sm < 1)
@@ -1109,10 +1127,17 @@ static cudaError_t launch_sweep_t(const StepArgs32& a, cudaStream_t s) {
   const unsigned work = (unsigned)(a.nstrips * a.nrowblk);
   const unsigned blocks = (work + kWarps - 1) / kWarps;
   const size_t bytes = (size_t)kWarps * kNbuf * Lay<C>::slot(STAGE);
-  if (a.hllc)
-    k_sweep<C, true, STAGE><<<blocks, kWarps * 32, bytes, s>>>(a);
-  else
-    k_sweep<C, false, STAGE><<<blocks, kWarps * 32, bytes, s>>>(a);
+  if (a.hllc) {
+    if (a.plain)
+      k_sweep<C, true, STAGE, true><<<blocks, kWarps * 32, bytes, s>>>(a);
+    else
+      k_sweep<C, true, STAGE, false><<<blocks, kWarps * 32, bytes, s>>>(a);
+  } else {
+    if (a.plain)
+      k_sweep<C, false, STAGE, true><<<blocks, kWarps * 32, bytes, s>>>(a);
+    else
+      k_sweep<C, false, STAGE, false><<<blocks, kWarps * 32, bytes, s>>>(a);
+  }
   return cudaGetLastError();
 }
 
@@ -1209,15 +1234,22 @@ cudaError_t launch_to_depth(const Grid& g32, const Grid& g64, FieldSet32 src, co
 
 int batch_sweep_blocks(const StepArgs32& a) { return (a.nstrips * a.nrowblk + kWarps - 1) / kWarps; }
 
-template <int C, bool HLLC>
-static cudaError_t set_smem_batch() {
-  cudaError_t e = cudaFuncSetAttribute(k_sweep_batch<C, HLLC, 1>,
+template <int C, bool HLLC, bool PLAIN>
+static cudaError_t set_smem_batch_t() {
+  cudaError_t e = cudaFuncSetAttribute(k_sweep_batch<C, HLLC, 1, PLAIN>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        kWarps * kNbuf * Lay<C>::slot(1));
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_sweep_batch<C, HLLC, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_sweep_batch<C, HLLC, 2, PLAIN>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
                              kWarps * kNbuf * Lay<C>::slot(2));
   return e;
+}
+
+template <int C, bool HLLC>
+static cudaError_t set_smem_batch() {
+  cudaError_t e = set_smem_batch_t<C, HLLC, true>();
+  return e == cudaSuccess ? set_smem_batch_t<C, HLLC, false>() : e;
 }
 
 cudaError_t configure_batch32() {
@@ -1231,10 +1263,18 @@ cudaError_t configure_batch32() {
 template <int C, int STAGE>
 static cudaError_t launch_sweep_batch_t(const BatchLaunch32& bl, cudaStream_t s) {
   const size_t bytes = (size_t)kWarps * kNbuf * Lay<C>::slot(STAGE);
-  if (bl.hllc)
-    k_sweep_batch<C, true, STAGE><<<(unsigned)bl.blocks, kWarps * 32, bytes, s>>>(bl.args, bl.map);
-  else
-    k_sweep_batch<C, false, STAGE><<<(unsigned)bl.blocks, kWarps * 32, bytes, s>>>(bl.args, bl.map);
+  const unsigned nb = (unsigned)bl.blocks;
+  if (bl.hllc) {
+    if (bl.plain)
+      k_sweep_batch<C, true, STAGE, true><<<nb, kWarps * 32, bytes, s>>>(bl.args, bl.map);
+    else
+      k_sweep_batch<C, true, STAGE, false><<<nb, kWarps * 32, bytes, s>>>(bl.args, bl.map);
+  } else {
+    if (bl.plain)
+      k_sweep_batch<C, false, STAGE, true><<<nb, kWarps * 32, bytes, s>>>(bl.args, bl.map);
+    else
+      k_sweep_batch<C, false, STAGE, false><<<nb, kWarps * 32, bytes, s>>>(bl.args, bl.map);
+  }
   return cudaGetLastError();
 }
 
