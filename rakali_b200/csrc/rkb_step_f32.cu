@@ -427,10 +427,38 @@ __device__ __forceinline__ void st_f(float* p, const float (&v)[C]) {
 // ---------------------------------------------------------------------------
 // Stage kernel
 // ---------------------------------------------------------------------------
+// A field pointer at its point of use.  Batches keep a member's arguments in
+// shared memory and read each pointer from there when it is needed (held in
+// registers across the row loop they make the kernel spill); single
+// simulations use the kernel-parameter copy.
+template <bool BATCH, typename T>
+__device__ __forceinline__ T* use_ptr(T* const& p) {
+  if constexpr (!BATCH) {
+    return p;
+  } else {
+    unsigned long long v;
+    asm volatile("ld.shared.u64 %0, [%1];" : "=l"(v) : "r"(smem_u32(&p)));
+    return reinterpret_cast<T*>(v);
+  }
+}
+
+// The same for an int of the arguments (grid pitch and extents).
+template <bool BATCH>
+__device__ __forceinline__ int use_int(const int& p) {
+  if constexpr (!BATCH) {
+    return p;
+  } else {
+    int v;
+    asm volatile("ld.shared.s32 %0, [%1];" : "=r"(v) : "r"(smem_u32(&p)));
+    return v;
+  }
+}
+
 // STAGE 1: U^n (buffer cur) -> U* (S).  STAGE 2: U*, U^n -> U^{n+1} (cur^1).
 // Block `blk` of the `nblk` blocks that cover one simulation.  PLAIN: no
 // forcing, Coriolis or sponge (the common case), compiled without those paths.
-template <int C, bool HLLC, int STAGE, bool PLAIN>
+// BATCH: `a` lives in shared memory.
+template <int C, bool HLLC, int STAGE, bool PLAIN, bool BATCH = false>
 __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, unsigned nblk) {
   using L = Lay<C>;
   constexpr int SLOT = L::slot(STAGE);
@@ -439,7 +467,8 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
   __shared__ float rot[2];
   StepCtl* ctl = a.ctl;
   if (!ctl->active) return;
-  const Grid g = a.g;
+  using GRef = std::conditional_t<BATCH, const Grid&, const Grid>;
+  GRef g = a.g;
   const Physics* phys = a.phys;
   const double dtd = ctl->dt;
   const float dt = (float)dtd;
@@ -462,9 +491,10 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
   const float rdx = (float)(1.0 / g.dx), rdy = (float)(1.0 / g.dy);
   const float cosf_ = rot[0], sinf_ = rot[1];
 
-  const FieldSet32 in = STAGE == 2 ? a.S : (cur ? a.U1 : a.U0);
-  const FieldSet32 old = cur ? a.U1 : a.U0;
-  const FieldSet32 out = STAGE == 1 ? a.S : (cur ? a.U0 : a.U1);
+  using FRef = std::conditional_t<BATCH, const FieldSet32&, const FieldSet32>;
+  FRef in = STAGE == 2 ? a.S : (cur ? a.U1 : a.U0);
+  FRef old = cur ? a.U1 : a.U0;
+  FRef out = STAGE == 1 ? a.S : (cur ? a.U0 : a.U1);
 
   const unsigned nw = nblk * kWarps;
   const unsigned gw = blk * kWarps + warp;
@@ -497,16 +527,16 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
       const uint32_t dst = ring_s + s * SLOT, bar = bar0 + 8 * s;
       const bool with_old = STAGE == 2 && r >= y0 && r < yend;
       mbar_expect_tx(bar, with_old ? L::kSlot2 : L::kSlot1);
-      const size_t ro = (size_t)r * (size_t)g.pitch + (size_t)(x0 - 4);
-      bulk_g2s(dst + L::kOffE, in.eta + ro, 4 * L::kSeg, bar);
-      bulk_g2s(dst + L::kOffU, in.hu + ro, 4 * L::kSeg, bar);
-      bulk_g2s(dst + L::kOffV, in.hv + ro, 4 * L::kSeg, bar);
-      bulk_g2s(dst + L::kOffB, a.b + ro, 8 * L::kSeg, bar);
+      const size_t ro = (size_t)r * (size_t)use_int<BATCH>(g.pitch) + (size_t)(x0 - 4);
+      bulk_g2s(dst + L::kOffE, use_ptr<BATCH>(in.eta) + ro, 4 * L::kSeg, bar);
+      bulk_g2s(dst + L::kOffU, use_ptr<BATCH>(in.hu) + ro, 4 * L::kSeg, bar);
+      bulk_g2s(dst + L::kOffV, use_ptr<BATCH>(in.hv) + ro, 4 * L::kSeg, bar);
+      bulk_g2s(dst + L::kOffB, use_ptr<BATCH>(a.b) + ro, 8 * L::kSeg, bar);
       if (with_old) {
         const size_t ro2 = ro + 4;
-        bulk_g2s(dst + L::kOffOE, old.eta + ro2, 4 * L::kStrip, bar);
-        bulk_g2s(dst + L::kOffOU, old.hu + ro2, 4 * L::kStrip, bar);
-        bulk_g2s(dst + L::kOffOV, old.hv + ro2, 4 * L::kStrip, bar);
+        bulk_g2s(dst + L::kOffOE, use_ptr<BATCH>(old.eta) + ro2, 4 * L::kStrip, bar);
+        bulk_g2s(dst + L::kOffOU, use_ptr<BATCH>(old.hu) + ro2, 4 * L::kStrip, bar);
+        bulk_g2s(dst + L::kOffOV, use_ptr<BATCH>(old.hv) + ro2, 4 * L::kStrip, bar);
       }
     };
     auto nxt = [](int s) { return s + 1 == kNbuf ? 0 : s + 1; };
@@ -667,7 +697,8 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
         float h;
         const double hd = protect(e, hu, hv, bc, h);
         const int i = ib + k;
-        const bool valid = out_lane && i < g.nxt - g.ng;  // forcing reads stay in bounds
+        // forcing reads stay in bounds
+        const bool valid = out_lane && i < use_int<BATCH>(g.nxt) - use_int<BATCH>(g.ng);
         if (friction) {
           // Manning friction (rki_kernel_fused.F90:121-130): hu / (1 + dt g n^2 |q| h^-7/3)
           const float den = 1.0f + gn2dt * sqrt_approx(hu * hu + hv * hv) *
@@ -727,18 +758,19 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
         }
       }
       if (out_lane) {
-        const size_t q = (size_t)j * (size_t)g.pitch + (size_t)ib;
-        if (ib + C - 1 < g.nxt - g.ng) {
-          st_f<C>(out.eta + q, ne);
-          st_f<C>(out.hu + q, nu);
-          st_f<C>(out.hv + q, nv);
+        const int xend = use_int<BATCH>(g.nxt) - use_int<BATCH>(g.ng);
+        const size_t q = (size_t)j * (size_t)use_int<BATCH>(g.pitch) + (size_t)ib;
+        if (ib + C - 1 < xend) {
+          st_f<C>(use_ptr<BATCH>(out.eta) + q, ne);
+          st_f<C>(use_ptr<BATCH>(out.hu) + q, nu);
+          st_f<C>(use_ptr<BATCH>(out.hv) + q, nv);
         } else {
 #pragma unroll
           for (int k = 0; k < C; ++k)
-            if (ib + k < g.nxt - g.ng) {
-              out.eta[q + k] = ne[k];
-              out.hu[q + k] = nu[k];
-              out.hv[q + k] = nv[k];
+            if (ib + k < xend) {
+              use_ptr<BATCH>(out.eta)[q + k] = ne[k];
+              use_ptr<BATCH>(out.hu)[q + k] = nu[k];
+              use_ptr<BATCH>(out.hv)[q + k] = nv[k];
             }
         }
       }
@@ -819,7 +851,7 @@ __global__ void __launch_bounds__(kWarps * 32, C == 2 ? 4 : 2)
   __syncthreads();
   const unsigned nblk = (unsigned)((sa.nstrips * sa.nrowblk + kWarps - 1) / kWarps);
   if (PLAIN && plain_mismatch(sa)) return;
-  sweep_body<C, HLLC, STAGE, PLAIN>(sa, (unsigned)m.y, nblk);
+  sweep_body<C, HLLC, STAGE, PLAIN, true>(sa, (unsigned)m.y, nblk);
 }
 
 // ---------------------------------------------------------------------------
