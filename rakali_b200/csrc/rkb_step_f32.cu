@@ -288,6 +288,12 @@ __device__ __forceinline__ float cell_pressure(float hc, float s) {
   return kHalfGf * (pa - pc) * (pa + pc);
 }
 
+// The cell update below rounds every FP32 operation explicitly (the _rn
+// intrinsics are never contracted or regrouped), so every build of the sweep
+// (with or without the optional source terms, single or batched) gives the
+// same bits.
+__device__ __forceinline__ float sq_sum(float a, float b) { return __fmaf_rn(a, a, __fmul_rn(b, b)); }
+
 // Clamp + KP07 + Froude backstop (rki_kernel_fused.F90:93-119) with the
 // threshold tests on the FP64 depth; returns that depth.
 __device__ __forceinline__ double protect(float& e, float& hu, float& hv, double b, float& h) {
@@ -297,21 +303,21 @@ __device__ __forceinline__ double protect(float& e, float& hu, float& hv, double
   e = neg ? __double2float_rd(b) : e;
   hu = wet ? hu : 0.0f;
   hv = wet ? hv : 0.0f;
-  const float h2 = h * h;
-  const float h4 = h2 * h2;
-  const float q2 = hu * hu + hv * hv;
-  const float lim = kFroude2G * h * h2;  // (Fr_max^2 g h) h^2
+  const float h2 = __fmul_rn(h, h);
+  const float h4 = __fmul_rn(h2, h2);
+  const float q2 = sq_sum(hu, hv);
+  const float lim = __fmul_rn(__fmul_rn(kFroude2G, h), h2);  // (Fr_max^2 g h) h^2
   if (wet && (h4 < kEps4F || q2 > lim)) {  // rare: KP07 and / or the Froude backstop
     if (h4 < kEps4F) {
-      const float f = kSqrt2F * h2 * rsqrt_approx(h4 + kEps4F);
-      hu = hu * f;
-      hv = hv * f;
+      const float f = __fmul_rn(__fmul_rn(kSqrt2F, h2), rsqrt_approx(__fadd_rn(h4, kEps4F)));
+      hu = __fmul_rn(hu, f);
+      hv = __fmul_rn(hv, f);
     }
-    const float q2b = hu * hu + hv * hv;
+    const float q2b = sq_sum(hu, hv);
     if (q2b > lim) {
-      const float sc = sqrt_approx(lim) * rsqrt_approx(q2b);
-      hu = hu * sc;
-      hv = hv * sc;
+      const float sc = __fmul_rn(sqrt_approx(lim), rsqrt_approx(q2b));
+      hu = __fmul_rn(hu, sc);
+      hv = __fmul_rn(hv, sc);
     }
   }
   return neg ? 0.0 : hd;
@@ -322,12 +328,12 @@ __device__ __forceinline__ void wave_speed32(double hd, float h, float hu, float
                                              float& sy) {
   sx = 0.0f;
   sy = 0.0f;
-  if (hd > kDry) {
-    const float c = sqrt_approx(kGf * h);
-    const float h2 = h * h;
-    const float f = kSqrt2F * h * rsqrt_approx(h2 * h2 + kEps4F);
-    sx = fabsf(hu) * f + c;
-    sy = fabsf(hv) * f + c;
+  if (hd > kDry) {  // the stage-2 epilogue's terms, rounded the same way
+    const float c = sqrt_approx(__fmul_rn(kGf, h));
+    const float h2 = __fmul_rn(h, h);
+    const float f = __fmul_rn(__fmul_rn(kSqrt2F, h), rsqrt_approx(__fmaf_rn(h2, h2, kEps4F)));
+    sx = __fmaf_rn(fabsf(hu), f, c);
+    sy = __fmaf_rn(fabsf(hv), f, c);
   }
 }
 
@@ -687,12 +693,17 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
         const float Ren = k < C - 1 ? xf[k + 1].en : ren;
         const float Rft = k < C - 1 ? xf[k + 1].ft : rft;
         const float px = cell_pressure(Cr.h[k], sx[k].e), py = cell_pressure(Cr.h[k], sC[k].e);
-        const float dE = -(Rfh - xf[k].fh) * rdx - (top[k].fh - bot[k].fh) * rdy;
-        const float dU = -(((Ren - xf[k].en) + xf[k].dq) + px) * rdx - (top[k].ft - bot[k].ft) * rdy;
-        const float dV = -(Rft - xf[k].ft) * rdx - (((top[k].en - bot[k].en) + bot[k].dq) + py) * rdy;
-        float e = Cr.e[k] + dt * dE;
-        float hu = Cr.u[k] + dt * dU;
-        float hv = Cr.v[k] + dt * dV;
+        const float dE = __fmaf_rn(-__fsub_rn(top[k].fh, bot[k].fh), rdy,
+                                   -__fmul_rn(__fsub_rn(Rfh, xf[k].fh), rdx));
+        const float dU = __fmaf_rn(
+            -__fsub_rn(top[k].ft, bot[k].ft), rdy,
+            -__fmul_rn(__fadd_rn(__fadd_rn(__fsub_rn(Ren, xf[k].en), xf[k].dq), px), rdx));
+        const float dV = __fmaf_rn(
+            -__fadd_rn(__fadd_rn(__fsub_rn(top[k].en, bot[k].en), bot[k].dq), py), rdy,
+            -__fmul_rn(__fsub_rn(Rft, xf[k].ft), rdx));
+        float e = __fmaf_rn(dt, dE, Cr.e[k]);
+        float hu = __fmaf_rn(dt, dU, Cr.u[k]);
+        float hv = __fmaf_rn(dt, dV, Cr.v[k]);
         const double bc = Cr.b[k];
         float h;
         const double hd = protect(e, hu, hv, bc, h);
@@ -701,44 +712,46 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
         const bool valid = out_lane && i < use_int<BATCH>(g.nxt) - use_int<BATCH>(g.ng);
         if (friction) {
           // Manning friction (rki_kernel_fused.F90:121-130): hu / (1 + dt g n^2 |q| h^-7/3)
-          const float den = 1.0f + gn2dt * sqrt_approx(hu * hu + hv * hv) *
-                                       __powf(fmaxf(h, kDryF), -7.0f / 3.0f);
+          const float den = __fmaf_rn(__fmul_rn(gn2dt, sqrt_approx(sq_sum(hu, hv))),
+                                      __powf(fmaxf(h, kDryF), -7.0f / 3.0f), 1.0f);
           const float r = hd > kDry ? rcp_approx(den) : 1.0f;
-          hu = hu * r;
-          hv = hv * r;
+          hu = __fmul_rn(hu, r);
+          hv = __fmul_rn(hv, r);
         }
         if ((forcing || has_cor) && hd > kDry) {
           if (forcing && valid) {  // wind, pressure gradient (rki_kernel_fused.F90:131-146)
             const size_t q = (size_t)i + (size_t)j * (size_t)a.fpitch;
-            hu = hu + dt * (float)(a.fo.wind_x[q] / kRho);
-            hv = hv + dt * (float)(a.fo.wind_y[q] / kRho);
+            hu = __fmaf_rn(dt, (float)(a.fo.wind_x[q] / kRho), hu);
+            hv = __fmaf_rn(dt, (float)(a.fo.wind_y[q] / kRho), hv);
             const float dpdx = (float)((a.fo.atm[q + 1] - a.fo.atm[q - 1]) / (2.0 * g.dx));
             const float dpdy = (float)((a.fo.atm[q + a.fpitch] - a.fo.atm[q - a.fpitch]) / (2.0 * g.dy));
-            hu = hu - dt * h * dpdx * (float)(1.0 / kRho);
-            hv = hv - dt * h * dpdy * (float)(1.0 / kRho);
+            const float dth = __fmul_rn(dt, h);
+            hu = __fmaf_rn(-__fmul_rn(dth, dpdx), (float)(1.0 / kRho), hu);
+            hv = __fmaf_rn(-__fmul_rn(dth, dpdy), (float)(1.0 / kRho), hv);
           }
           if (has_cor) {
             const float uo = hu, vo = hv;
-            hu = uo * cosf_ + vo * sinf_;
-            hv = -(uo * sinf_) + vo * cosf_;
+            hu = __fmaf_rn(uo, cosf_, __fmul_rn(vo, sinf_));
+            hv = __fmaf_rn(vo, cosf_, -__fmul_rn(uo, sinf_));
           }
         }
-        if (forcing && valid) e = e + dt * (float)a.fo.precip[(size_t)i + (size_t)j * (size_t)a.fpitch];
+        if (forcing && valid)
+          e = __fmaf_rn(dt, (float)a.fo.precip[(size_t)i + (size_t)j * (size_t)a.fpitch], e);
         double hfin = hd;
         if (STAGE == 2) {  // RK2 average and second clamp (rki_kernel_fused.F90:435-463)
-          e = 0.5f * (oe[k] + e);
-          hu = 0.5f * (ou[k] + hu);
-          hv = 0.5f * (ov[k] + hv);
+          e = __fmul_rn(0.5f, __fadd_rn(oe[k], e));
+          hu = __fmul_rn(0.5f, __fadd_rn(ou[k], hu));
+          hv = __fmul_rn(0.5f, __fadd_rn(ov[k], hv));
           hfin = protect(e, hu, hv, bc, h);
         }
         if (sponge_on) {
           const double alpha = sponge_alpha(a.bc, g, i, j);
           if (alpha > 0.0) {
-            const float fa = dt * (float)alpha;
-            const float de = -fa * (fmaxf(h, 0.0f) - (float)a.bc->sponge_h_ref);
-            e = e + de;
-            hu = hu - fa * hu;
-            hv = hv - fa * hv;
+            const float fa = __fmul_rn(dt, (float)alpha);
+            const float de = __fmul_rn(-fa, __fadd_rn(fmaxf(h, 0.0f), -(float)a.bc->sponge_h_ref));
+            e = __fadd_rn(e, de);
+            hu = __fmaf_rn(-fa, hu, hu);
+            hv = __fmaf_rn(-fa, hv, hv);
             if (valid) sponge_d += (double)de;
             hfin = (double)e - bc;
             h = fmaxf((float)hfin, 0.0f);
@@ -749,12 +762,13 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
         nv[k] = hv;
         part += valid ? (double)dE : 0.0;
         if (STAGE == 2) {
-          const float c = sqrt_approx(kGf * h);
-          const float h2 = h * h;
-          const float f = kSqrt2F * h * rsqrt_approx(h2 * h2 + kEps4F);
+          const float c = sqrt_approx(__fmul_rn(kGf, h));
+          const float h2 = __fmul_rn(h, h);
+          const float f =
+              __fmul_rn(__fmul_rn(kSqrt2F, h), rsqrt_approx(__fmaf_rn(h2, h2, kEps4F)));
           const bool w = valid && hfin > kDry;
-          wsx = fmaxf(wsx, w ? fabsf(hu) * f + c : 0.0f);
-          wsy = fmaxf(wsy, w ? fabsf(hv) * f + c : 0.0f);
+          wsx = fmaxf(wsx, w ? __fmaf_rn(fabsf(hu), f, c) : 0.0f);
+          wsy = fmaxf(wsy, w ? __fmaf_rn(fabsf(hv), f, c) : 0.0f);
         }
       }
       if (out_lane) {

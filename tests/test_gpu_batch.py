@@ -49,6 +49,41 @@ def test_batch_matches_members_stepped_alone(precision):
         s.close()
 
 
+def test_fp32_batch_mixes_plain_and_forced_members():
+    """One member with wind and rain, the others without: the batch runs the
+    sweep with forcing terms for all, and every member still matches its own
+    single run bit for bit (the single runs use the plain build where they can)."""
+    ms = _members(4, seed=5)
+    rng = np.random.default_rng(8)
+    nx, ny = ms[1]["b"].shape
+    wx = rng.uniform(0.0, 0.2, (nx, ny))
+    wy = rng.uniform(-0.1, 0.1, (nx, ny))
+    rain = np.full((nx, ny), 1.0e-5)
+
+    def build():
+        sims = [wl.build_member(mm, 32) for mm in ms]
+        sims[1].set_wind(wx, wy)
+        sims[1].set_precipitation(rain)
+        return sims
+
+    alone = build()
+    for s in alone:
+        s.step(25)
+    ref = [_state(s) for s in alone]
+    for s in alone:
+        s.close()
+    sims = build()
+    with Ensemble(sims, precision=32) as ens:
+        ens.step(25)
+        for k, (s, r) in enumerate(zip(sims, ref)):
+            got = _state(s)
+            diff = [float(np.abs(x - y).max()) for x, y in zip(got[:3], r[:3])]
+            assert got[3:] == r[3:], (k, got[3:], r[3:])
+            assert max(diff) == 0.0, (k, diff)
+    for s in sims:
+        s.close()
+
+
 def test_fp64_batch_matches_oracle():
     from oracle.oracle import OracleSim
     ms = _members(3, seed=11)

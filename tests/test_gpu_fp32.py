@@ -251,6 +251,39 @@ def test_forcing_and_coriolis():
         assert du <= FILM_MOM_RTOL and dv <= FILM_MOM_RTOL, (du, dv)
 
 
+def test_forcing_switched_on_mid_run():
+    """Steps without forcing (the sweep built without forcing terms, captured in
+    the step graphs), then wind, pressure and rain set on the same handle: the
+    next steps must run the forcing terms, as in the oracle."""
+    nx, ny, dx = 64, 48, 50.0
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, manning_n=0.03, dt_fixed=2.0,
+               init_condition="still_water", eta_initial=0.0)
+    b = gaussian_bed(nx, ny, dx, dx, 6, seed=12, base=-5.0, amp=(-2.0, 6.0),
+                     width=(100.0, 400.0))
+    h = hump_depth(b, dx, dx, amp=0.3, width=300.0)
+    sim, orc = _fp32_pair(cfg, bathymetry=b, initial_h=h)
+    rng = np.random.default_rng(6)
+    wx = rng.uniform(0.0, 0.3, (nx, ny))
+    wy = rng.uniform(-0.1, 0.1, (nx, ny))
+    p = rng.uniform(-50.0, 50.0, (nx, ny))
+    rain = np.full((nx, ny), 1.0e-5)
+    with sim:
+        sim.step(20)
+        orc.step(20)
+        sim.set_wind(wx, wy)
+        sim.set_atm_pressure(p)
+        sim.set_precipitation(rain)
+        g = orc.ng
+        for name, arr in (("wind_x", wx), ("wind_y", wy), ("atm", p), ("precip", rain)):
+            orc.arrays[name][g:-g, g:-g] = arr
+        orc.s.forcing_active = 1
+        sim.step(20)
+        orc.step(20)
+        dh, du, dv = _errors(sim, orc)
+        assert dh <= ETA_TOL, dh
+        assert du <= FILM_MOM_RTOL and dv <= FILM_MOM_RTOL, (du, dv)
+
+
 def test_closed_basin_mass():
     """Walls, wet/dry hump: domain volume kept to FP32 round-off of the surface."""
     nx, ny, dx = 256, 192, 5.0
