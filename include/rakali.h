@@ -119,6 +119,15 @@ void rki_sync_from_device(void *handle);
 int rki_save_restart(void *handle, const char *filename, int len);
 int rki_load_restart(void *handle, const char *filename, int len);
 
+/* Replaces the reference front end's Rakali.save_checkpoint
+ * (python/rakali/_core.py:1433-1499, written there through xarray): a per-step
+ * checkpoint of a finalised handle with every field including ghosts (h, hu,
+ * hv, b and the RK2 saves h0, hu0, hv0 over dimensions x_total, y_total) and
+ * the clock, grid and physics scalars as global attributes, in a NetCDF
+ * classic (64-bit offset) file.  The device state stays canonical.  -1 not
+ * initialised, -2 not finalised, -3 on an empty name or a failed write. */
+int rkb_save_checkpoint(void *handle, const char *filename, int len);
+
 /* rki_api.F90:1473-1507 */
 int rki_set_use_ppm_tracer(void *handle, int flag);
 int rki_set_use_hllc(void *handle, int flag);

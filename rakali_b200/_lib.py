@@ -93,6 +93,7 @@ def load(path: str | None = None):
     _sig(lib, "rki_sync_from_device", [H], None)
     _sig(lib, "rki_save_restart", [H, CP, I], I)
     _sig(lib, "rki_load_restart", [H, CP, I], I)
+    _sig(lib, "rkb_save_checkpoint", [H, CP, I], I)
     _sig(lib, "rki_set_use_ppm_tracer", [H, I], I)
     _sig(lib, "rki_set_use_hllc", [H, I], I)
     _sig(lib, "rki_last_error", [], CP)

@@ -487,6 +487,23 @@ class Rakali:
         raw = str(filename).encode()
         self._rc(self._lib.rki_save_restart(self._handle, raw, len(raw)), "save_restart")
 
+    def save_checkpoint(self, filename):
+        """Write a per-step checkpoint: h, hu, hv, b and the RK2 saves h0, hu0,
+        hv0 with their ghost cells, plus time, step_count, dt, the grid sizes,
+        dx, dy, manning_n, coriolis_f and clamped_elevation as attributes.
+
+        The variables and attributes are those of the reference front end's
+        save_checkpoint (python/rakali/_core.py:1433-1499); the file is NetCDF
+        classic (64-bit offset) instead of NetCDF-4, readable by any NetCDF
+        library.  The simulation keeps running on the device afterwards.
+        """
+        self._check_ready()
+        parent = Path(str(filename)).resolve().parent
+        if not parent.is_dir():
+            raise FileNotFoundError(f"directory {parent} does not exist")
+        raw = str(filename).encode()
+        self._rc(self._lib.rkb_save_checkpoint(self._handle, raw, len(raw)), "save_checkpoint")
+
     # --- gauges (src/io/structured/rki_gauges.F90) --------------------------
     def set_gauges(self, x, y, names=None, interval=0.0, capacity=65536):
         """Record eta, u, v at stations (x, y in metres from the lower-left

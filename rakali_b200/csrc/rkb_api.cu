@@ -338,6 +338,17 @@ int rki_save_restart(void* handle, const char* filename, int len) {
   return rc == 0 ? 0 : fail(-3, err);
 }
 
+int rkb_save_checkpoint(void* handle, const char* filename, int len) {
+  rkb::Sim* s = sim_of(handle);
+  if (!s) return kBadHandle;
+  if (!s->is_initialised) return -1;
+  if (!s->is_finalised) return -2;
+  if (!filename || len <= 0) return fail(-3, "empty checkpoint file name");
+  std::string err;
+  const int rc = s->save_checkpoint(std::string(filename, (size_t)len), err);
+  return rc == 0 ? 0 : fail(-3, err);
+}
+
 int rki_load_restart(void* handle, const char* filename, int len) {
   rkb::Sim* s = sim_of(handle);
   if (!s) return kBadHandle;

@@ -41,6 +41,32 @@ struct Out {
     b.insert(b.end(), v.begin(), v.end());
     while (b.size() % 4) b.push_back(0);
   }
+  void double_att(const std::string& n, double v) {
+    name(n);
+    u32(kDouble);
+    u32(1);
+    uint64_t u;
+    std::memcpy(&u, &v, 8);
+    u64(u);
+  }
+  void int_att(const std::string& n, int v) {
+    name(n);
+    u32(kInt);
+    u32(1);
+    u32((uint32_t)v);
+  }
+};
+
+// A global attribute: text, one NC_DOUBLE or one NC_INT.
+struct Att {
+  std::string name;
+  uint32_t type;
+  std::string text;
+  double d = 0.0;
+  int i = 0;
+  Att(std::string n, const char* v) : name(std::move(n)), type(kChar), text(v) {}
+  Att(std::string n, double v) : name(std::move(n)), type(kDouble), d(v) {}
+  Att(std::string n, int v) : name(std::move(n)), type(kInt), i(v) {}
 };
 
 void put_be_doubles(std::vector<unsigned char>& dst, const double* v, size_t n) {
@@ -199,8 +225,8 @@ struct OutVar {
 
 bool write_classic(const std::string& path,
                    const std::vector<std::pair<std::string, uint32_t>>& dims,
-                   const std::vector<std::pair<std::string, std::string>>& gatts,
-                   const std::vector<OutVar>& vars, std::string& err) {
+                   const std::vector<Att>& gatts, const std::vector<OutVar>& vars,
+                   std::string& err) {
   Out hd;
   hd.b = {'C', 'D', 'F', 2};
   hd.u32(0);
@@ -216,7 +242,14 @@ bool write_classic(const std::string& path,
   } else {
     hd.u32(kAttTag);
     hd.u32((uint32_t)gatts.size());
-    for (const auto& a : gatts) hd.text_att(a.first, a.second);
+    for (const Att& a : gatts) {
+      if (a.type == kDouble)
+        hd.double_att(a.name, a.d);
+      else if (a.type == kInt)
+        hd.int_att(a.name, a.i);
+      else
+        hd.text_att(a.name, a.text);
+    }
   }
   hd.u32(kVarTag);
   hd.u32((uint32_t)vars.size());
@@ -314,6 +347,48 @@ bool write_gauges(const std::string& path, int n, const char* names, int name_le
        v.data(), K * n}};
   return write_classic(path, dims, {{"title", "Rakali gauge time series"}, {"Conventions", "CF-1.8"}},
                        vars, err);
+}
+
+bool write_checkpoint(const std::string& path, int nxt, int nyt, const double* const fields[7],
+                      const CheckpointMeta& m, std::string& err) {
+  // the file's (x_total, y_total) order has y fastest: the transpose of the
+  // Fortran-order arrays
+  const size_t n = (size_t)nxt * (size_t)nyt;
+  std::vector<std::vector<double>> t(7, std::vector<double>(n));
+  for (int v = 0; v < 7; ++v)
+    for (int j = 0; j < nyt; ++j)
+      for (int i = 0; i < nxt; ++i)
+        t[v][(size_t)i * nyt + j] = fields[v][(size_t)i + (size_t)j * nxt];
+  using A = std::vector<std::pair<std::string, std::string>>;
+  const A depth{{"units", "m"}, {"long_name", "water depth (ghost-included)"}};
+  const A qx{{"units", "m2 s-1"}, {"long_name", "x-momentum (ghost-included)"}};
+  const A qy{{"units", "m2 s-1"}, {"long_name", "y-momentum (ghost-included)"}};
+  const A bed{{"units", "m"}, {"long_name", "bottom elevation"}, {"positive", "up"}};
+  const A h0{{"units", "m"}, {"long_name", "RK2 save of h at start of stage 1"}};
+  const A hu0{{"units", "m2 s-1"}, {"long_name", "RK2 save of hu at start of stage 1"}};
+  const A hv0{{"units", "m2 s-1"}, {"long_name", "RK2 save of hv at start of stage 1"}};
+  const std::vector<OutVar> vars = {
+      {"h", {0, 1}, kDouble, depth, t[0].data(), n}, {"hu", {0, 1}, kDouble, qx, t[1].data(), n},
+      {"hv", {0, 1}, kDouble, qy, t[2].data(), n},   {"b", {0, 1}, kDouble, bed, t[3].data(), n},
+      {"h0", {0, 1}, kDouble, h0, t[4].data(), n},   {"hu0", {0, 1}, kDouble, hu0, t[5].data(), n},
+      {"hv0", {0, 1}, kDouble, hv0, t[6].data(), n}};
+  const std::vector<Att> gatts = {{"title", "Rakali per-step checkpoint (2D barotropic)"},
+                                  {"source", "rakali_b200 (Rakali.save_checkpoint)"},
+                                  {"time", m.time},
+                                  {"step_count", m.step_count},
+                                  {"dt", m.dt},
+                                  {"nx_total", nxt},
+                                  {"ny_total", nyt},
+                                  {"nx_phys", m.nx_phys},
+                                  {"ny_phys", m.ny_phys},
+                                  {"nghost", m.nghost},
+                                  {"dx", m.dx},
+                                  {"dy", m.dy},
+                                  {"manning_n", m.manning_n},
+                                  {"coriolis_f", m.coriolis_f},
+                                  {"clamped_elevation", m.clamped_elevation}};
+  return write_classic(path, {{"x_total", (uint32_t)nxt}, {"y_total", (uint32_t)nyt}}, gatts, vars,
+                       err);
 }
 
 namespace {

@@ -40,5 +40,21 @@ bool write_gauges(const std::string& path, int n, const char* names, int name_le
                   const double* x, const double* y, const double* b, int n_records,
                   const double* times, const double* values, std::string& err);
 
+// Per-step checkpoint in the layout of the reference front end's
+// save_checkpoint (python/rakali/_core.py:1433-1499): dimensions x_total,
+// y_total; FP64 variables h, hu, hv, b, h0, hu0, hv0 over (x_total, y_total)
+// with units / long_name (and positive = up for b); global attributes title,
+// source, time, step_count, dt, nx_total, ny_total, nx_phys, ny_phys, nghost,
+// dx, dy, manning_n, coriolis_f, clamped_elevation (doubles as NC_DOUBLE,
+// counts as NC_INT).  The reference writes NetCDF-4 through xarray; this is
+// the same content in a classic (64-bit offset) file.  fields: h, hu, hv, b,
+// h0, hu0, hv0, each (nx_total, ny_total) Fortran order with ghosts.
+struct CheckpointMeta {
+  double time, dt, dx, dy, manning_n, coriolis_f, clamped_elevation;
+  int step_count, nx_phys, ny_phys, nghost;
+};
+bool write_checkpoint(const std::string& path, int nx_total, int ny_total,
+                      const double* const fields[7], const CheckpointMeta& m, std::string& err);
+
 }  // namespace nc
 }  // namespace rkb

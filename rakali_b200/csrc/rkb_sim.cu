@@ -261,7 +261,7 @@ int Sim::finalize(std::string& err) {
   if (rc != 0) return rc;
   RKB_TRY(cudaStreamSynchronize(stream_));
   on_device_ = true;
-  host_is_current_ = false;
+  mark_host_stale();
   is_finalised = true;
   return 0;
 }
@@ -446,6 +446,34 @@ int Sim::read_gauges(int max_records, double* times, double* values, int* overfl
   return k;
 }
 
+// Per-step checkpoint (python/rakali/_core.py:1433-1499): every field with
+// ghosts, RK2 saves included, after a full pull that leaves the device state
+// canonical.
+int Sim::save_checkpoint(const std::string& path, std::string& err) {
+  if (on_device_ && !host_is_current_) {
+    cudaSetDevice(device_);
+    if (pull_state(true) != 0) {
+      err = "copying the state to the host failed";
+      return -1;
+    }
+    host_is_current_ = host_state_current_ = true;
+  }
+  nc::CheckpointMeta m{};
+  m.time = t_current_;
+  m.dt = dt_;
+  m.dx = cfg.dx;
+  m.dy = cfg.dy;
+  m.manning_n = phys.manning_n;
+  m.coriolis_f = phys.coriolis_f;
+  m.clamped_elevation = cfg.clamped_elevation;
+  m.step_count = step_count_;
+  m.nx_phys = cfg.nx;
+  m.ny_phys = cfg.ny;
+  m.nghost = g.ng;
+  const double* f[7] = {hf_[0], hf_[1], hf_[2], hf_[3], hf_[4], hf_[5], hf_[6]};
+  return nc::write_checkpoint(path, g.nxt, g.nyt, f, m, err) ? 0 : -1;
+}
+
 // restart_write (src/io/structured/rki_output.F90:740-853): interior h, hu,
 // hv, b and the clock, after refresh_host.
 int Sim::save_restart(const std::string& path, std::string& err) {
@@ -583,7 +611,7 @@ int Sim::ensure_device() {
     if (upload_state() != 0) return -1;
     on_device_ = true;
   }
-  host_is_current_ = false;
+  mark_host_stale();
   return 0;
 }
 
@@ -630,21 +658,23 @@ int Sim::pull_state(bool full) {
   return pull(args_, cur_, stepped_, full, hf_, g, stream_);
 }
 
+// The host arrays become canonical (a pointer to them is handed out, or they
+// are about to be written): pull what is not current, then the next run
+// uploads them.
 void Sim::ensure_host() {
-  if (host_is_current_) return;
   if (on_device_) {
     cudaSetDevice(device_);
-    pull_state(true);
+    if (!host_is_current_) pull_state(true);
     on_device_ = false;
-    host_is_current_ = true;
+    host_is_current_ = host_state_current_ = true;
   }
 }
 
 void Sim::sync_host() {
-  if (is_initialised && on_device_ && !host_is_current_) {
+  if (is_initialised && on_device_ && !host_is_current_ && !host_state_current_) {
     cudaSetDevice(device_);
     pull_state(false);
-    host_is_current_ = true;
+    host_state_current_ = true;  // h, hu, hv only: the bed and RK2 saves stay on the device
   }
 }
 
@@ -653,7 +683,7 @@ void Sim::sync_from_device() {
     cudaSetDevice(device_);
     pull_state(true);
     on_device_ = false;
-    host_is_current_ = true;
+    host_is_current_ = host_state_current_ = true;
   }
 }
 
@@ -711,7 +741,7 @@ int Sim::set_interior(int which, const double* data, int nx, int ny) {
                         cudaMemcpyHostToDevice, stream_) != cudaSuccess)
       return -1;
     if (cudaStreamSynchronize(stream_) != cudaSuccess) return -1;
-    host_is_current_ = false;
+    mark_host_stale();
   }
   return 0;
 }
@@ -837,7 +867,7 @@ int Sim::run(int mode, double target, int nsteps) {
   if (check_device_error() != 0) return -1;
   if (cudaGetLastError() != cudaSuccess) return -1;
   stepped_ = true;
-  host_is_current_ = false;
+  mark_host_stale();
   return 0;
 }
 
@@ -868,7 +898,7 @@ int Sim::time_steps(int n, double* ms) {
   pull_ctl();
   if (check_device_error() != 0) return -1;
   stepped_ = true;
-  host_is_current_ = false;
+  mark_host_stale();
   return 0;
 }
 
@@ -906,7 +936,7 @@ int Sim::profile_steps(int n, double out[5]) {
   pull_ctl();
   if (check_device_error() != 0) return -1;
   stepped_ = true;
-  host_is_current_ = false;
+  mark_host_stale();
   return 0;
 }
 
@@ -1034,7 +1064,7 @@ int Sim::batch_finish() {
   pull_ctl();
   if (check_device_error() != 0) return -1;
   stepped_ = true;
-  host_is_current_ = false;
+  mark_host_stale();
   return 0;
 }
 
@@ -1085,7 +1115,7 @@ int Sim::restore() {
   step_count_ = snap_steps_;
   stepped_ = snap_stepped_;
   on_device_ = false;  // the next run uploads the host arrays, which hold the snapshot
-  host_is_current_ = true;
+  host_is_current_ = host_state_current_ = true;
   return 0;
 }
 

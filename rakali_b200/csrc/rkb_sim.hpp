@@ -35,6 +35,7 @@ class Sim {
   // the boundary launches summed), out[4] = launches per step.
   int profile_steps(int n, double out[5]);
   int save_restart(const std::string& path, std::string& err);  // NetCDF classic
+  int save_checkpoint(const std::string& path, std::string& err);  // NetCDF classic
   // Gauge stations recorded on the device after every step (rkb_gauges.cu):
   // returns the number of stations inside the domain, or < 0.
   int set_gauges(int n, const double* x, const double* y, double interval, int capacity,
@@ -132,7 +133,11 @@ class Sim {
   void* dmem_ = nullptr;
   StepArgs args_{};
   StepCtl* hctl_ = nullptr;  // pinned
+  // host_is_current_: every host array (state, bed, RK2 saves) equals the
+  // device's; host_state_current_: h, hu, hv do (after rki_sync_host).
   bool on_device_ = false, host_is_current_ = false, stepped_ = false;
+  bool host_state_current_ = false;
+  void mark_host_stale() { host_is_current_ = host_state_current_ = false; }
   int cur_ = 0;
   double t_current_ = 0.0, dt_ = 0.0;
   int step_count_ = 0;

@@ -436,6 +436,64 @@ def test_restart_round_trip_continues_bit_identically(tmp_path, precision):
                 assert np.array_equal(getattr(sim2, fld + "_phys"), getattr(sim, fld + "_phys"))
 
 
+def test_checkpoint_matches_oracle_and_run_continues(tmp_path):
+    """save_checkpoint after 17 steps: every field with its ghosts (RK2 saves
+    included) equals the oracle's bit for bit, the scalar attributes are the
+    handle's, and the run then continues bit-identically with the oracle."""
+    from scipy.io import netcdf_file
+    nx, ny, dx = 72, 56, 5.0
+    b = gaussian_bed(nx, ny, dx, dx, 10, seed=29, width=(20.0, 90.0))
+    h = hump_depth(b, dx, dx, width=50.0)
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, manning_n=0.025,
+               coriolis_f=1.0e-4)
+    sim, orc = pair(cfg, bathymetry=b, initial_h=h)
+    path = tmp_path / "step_17.nc"
+    with sim:
+        sim.step(17)
+        orc.step(17)
+        sim.save_checkpoint(path)
+        ng = orc.ng
+        with netcdf_file(str(path), "r", mmap=False) as f:
+            assert f.dimensions["x_total"] == nx + 2 * ng
+            assert f.dimensions["y_total"] == ny + 2 * ng
+            for name in ("h", "hu", "hv", "b", "h0", "hu0", "hv0"):
+                v = np.asarray(f.variables[name][:])
+                assert f.variables[name].dimensions == ("x_total", "y_total")
+                assert np.array_equal(v, orc.arrays[name]), name
+            assert f.variables["b"].positive == b"up"
+            at = f._attributes
+            assert float(at["time"]) == sim.time
+            assert int(at["step_count"]) == sim.step_count == 17
+            assert float(at["dt"]) == sim.dt
+            assert (int(at["nx_phys"]), int(at["ny_phys"]), int(at["nghost"])) == (nx, ny, ng)
+            assert (int(at["nx_total"]), int(at["ny_total"])) == (nx + 2 * ng, ny + 2 * ng)
+            assert float(at["dx"]) == dx and float(at["dy"]) == dx
+            assert float(at["manning_n"]) == 0.025 and float(at["coriolis_f"]) == 1.0e-4
+            assert float(at["clamped_elevation"]) == sim.clamped_elevation
+        sim.step(9)
+        orc.step(9)
+        compare_state(sim, orc, rtol=0.0, fields=("h", "hu", "hv", "b", "h0", "hu0", "hv0"))
+
+
+def test_sync_host_leaves_bed_and_rk2_saves_readable():
+    """rki_sync_host refreshes h, hu, hv only; reading the bed (whose ghosts
+    the wall fill mirrors every step) or the RK2 saves afterwards still gives
+    their current values, as in the oracle, and stepping continues exactly."""
+    nx, ny, dx = 48, 40, 5.0
+    b = gaussian_bed(nx, ny, dx, dx, 8, seed=31, width=(20.0, 60.0))
+    h = hump_depth(b, dx, dx, width=40.0)
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, manning_n=0.025)
+    sim, orc = pair(cfg, bathymetry=b, initial_h=h)
+    with sim:
+        sim.step(6)
+        orc.step(6)
+        sim.sync_host()
+        compare_state(sim, orc, rtol=0.0, fields=("b", "h0", "hu0", "hv0", "h", "hu", "hv"))
+        sim.step(4)
+        orc.step(4)
+        compare_state(sim, orc, rtol=0.0, fields=("h", "hu", "hv", "b", "h0", "hu0", "hv0"))
+
+
 def test_restart_refuses_grid_mismatch_and_finalised_handle(tmp_path):
     from rakali_b200 import Rakali
     path = tmp_path / "r.nc"
