@@ -290,6 +290,45 @@ class Rakali:
     h0 = property(lambda self: self._field("h0"), doc="RK2 save of h (start of the last step).")
     hu0 = property(lambda self: self._field("hu0"), doc="RK2 save of hu.")
     hv0 = property(lambda self: self._field("hv0"), doc="RK2 save of hv.")
+    def _get_3d_field(self, getter_name):
+        """(nx_total, ny_total, nz) view of a layer field; multilayer mode is
+        not part of this library, so the getter reports -3 and this raises
+        RuntimeError as the reference does when it is inactive
+        (python/rakali/_core.py:713-728)."""
+        self._check_alive()
+        ptr = ctypes.c_void_p()
+        nx, ny, nz = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        rc = getattr(self._lib, getter_name)(self._handle, ctypes.byref(ptr), ctypes.byref(nx),
+                                             ctypes.byref(ny), ctypes.byref(nz))
+        if rc != 0:
+            raise RuntimeError(f"{getter_name} failed (rc={rc})")
+        arr = _view(ptr.value, nx.value * ny.value * nz.value, self)
+        return arr.reshape((nx.value, ny.value, nz.value), order="F")
+
+    @property
+    def h_layer(self):
+        """Layer thickness (multilayer mode only: raises RuntimeError here)."""
+        g = self._ng
+        return self._get_3d_field("rki_get_h_layer_ptr")[g:-g, g:-g, :]
+
+    def _tracer(self, getter_name):
+        q = self._get_3d_field(getter_name)
+        lay = self._get_3d_field("rki_get_h_layer_ptr")
+        g = self._ng
+        q, lay = q[g:-g, g:-g, :], lay[g:-g, g:-g, :]
+        with np.errstate(invalid="ignore", divide="ignore"):
+            return np.where(lay > 1e-6, q / lay, np.nan)
+
+    @property
+    def salinity(self):
+        """Layer salinity (multilayer mode only: raises RuntimeError here)."""
+        return self._tracer("rki_get_salinity_ptr")
+
+    @property
+    def temperature(self):
+        """Layer temperature (multilayer mode only: raises RuntimeError here)."""
+        return self._tracer("rki_get_temperature_ptr")
+
     h_phys = property(lambda self: self._phys(self.h), doc="Water depth, interior only.")
     hu_phys = property(lambda self: self._phys(self.hu), doc="x-momentum, interior only.")
     hv_phys = property(lambda self: self._phys(self.hv), doc="y-momentum, interior only.")
@@ -388,6 +427,61 @@ class Rakali:
         self._check_alive()
         self._lib.rki_sync_host(self._handle)
 
+    def sync_from_device(self):
+        """Copy every field home and make the host arrays canonical (the next
+        step uploads them again)."""
+        self._check_alive()
+        self._lib.rki_sync_from_device(self._handle)
+
+    def to_xarray(self, time_dim=True):
+        """The current interior state as an ``xarray.Dataset`` (copies): h, b,
+        eta, hu, hv and the velocities u, v (NaN where h <= 1e-6) on cell
+        centres x, y, with a length-1 ``time`` dimension unless ``time_dim``
+        is False; the variables, coordinates and attributes of the reference
+        front end's to_xarray (python/rakali/_core.py:1561-1768) without the
+        multilayer fields.  Raises ImportError when xarray is not installed.
+        """
+        try:
+            import xarray as xr
+        except ImportError as e:
+            raise ImportError("to_xarray() requires the xarray package. "
+                              "Install with `pip install xarray`.") from e
+        self._check_ready()
+        self.sync_host()
+        nx, ny, dx, dy = self._nx, self._ny, self.dx, self.dy
+        coords = {
+            "x": ("x", (np.arange(nx) + 0.5) * dx,
+                  {"units": "m", "long_name": "distance east of west boundary", "axis": "X"}),
+            "y": ("y", (np.arange(ny) + 0.5) * dy,
+                  {"units": "m", "long_name": "distance north of south boundary", "axis": "Y"}),
+        }
+        if time_dim:
+            coords["time"] = ("time", np.array([self.time]),
+                              {"units": "seconds since simulation start",
+                               "long_name": "simulation time", "axis": "T"})
+        h, hu, hv, b = (self.h_phys.copy(), self.hu_phys.copy(), self.hv_phys.copy(),
+                        self.b_phys.copy())
+        with np.errstate(invalid="ignore", divide="ignore"):
+            u = np.where(h > 1e-6, hu / h, np.nan)
+            v = np.where(h > 1e-6, hv / h, np.nan)
+
+        def wrap(a):
+            return (("time", "x", "y"), a[np.newaxis]) if time_dim else (("x", "y"), a)
+
+        data_vars = {
+            "h": (*wrap(h), {"units": "m", "long_name": "water depth"}),
+            "b": (*wrap(b), {"units": "m", "long_name": "bottom elevation", "positive": "up"}),
+            "eta": (*wrap(h + b), {"units": "m", "long_name": "surface elevation (h + b)"}),
+            "hu": (*wrap(hu), {"units": "m2 s-1", "long_name": "x-momentum (h*u)"}),
+            "hv": (*wrap(hv), {"units": "m2 s-1", "long_name": "y-momentum (h*v)"}),
+            "u": (*wrap(u), {"units": "m s-1", "long_name": "x-velocity"}),
+            "v": (*wrap(v), {"units": "m s-1", "long_name": "y-velocity"}),
+        }
+        attrs = {"title": "Rakali simulation snapshot", "source": "rakali_b200 (Rakali.to_xarray)",
+                 "Conventions": "CF-1.11", "dx": float(dx), "dy": float(dy), "nx": int(nx),
+                 "ny": int(ny), "time": float(self.time), "step_count": int(self.step_count)}
+        return xr.Dataset(data_vars=data_vars, coords=coords, attrs=attrs)
+
     # --- setters ----------------------------------------------------------
     def _shape(self, a, label):
         a = np.asarray(a, dtype=np.float64)
@@ -415,6 +509,28 @@ class Rakali:
 
     def set_hv(self, hv):
         self._set("rki_set_hv", "set_hv", hv)
+
+    def _set_tracer(self, fn, label, a):
+        self._check_alive()
+        nz = self.nz
+        if nz <= 0:
+            raise RuntimeError(f"{label} requires multilayer mode (nz_layers > 0)")
+        a = np.asfortranarray(a, dtype=np.float64)
+        if a.shape != (self._nx, self._ny, nz):
+            raise ValueError(f"Expected shape {(self._nx, self._ny, nz)}, got {a.shape}")
+        rc = getattr(self._lib, fn)(self._handle, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                    self._nx, self._ny, nz)
+        if rc != 0:
+            raise RuntimeError(f"Failed to {label[4:]} (rc={rc})")
+
+    def set_salinity(self, S):
+        """Per-layer salinity (multilayer mode only: raises RuntimeError here,
+        as the reference does when nz_layers is 0)."""
+        self._set_tracer("rki_set_salinity", "set_salinity", S)
+
+    def set_temperature(self, T):
+        """Per-layer temperature (multilayer mode only: raises RuntimeError here)."""
+        self._set_tracer("rki_set_temperature", "set_temperature", T)
 
     def set_wind(self, wx, wy):
         self._set("rki_set_wind", "set_wind", wx, wy)

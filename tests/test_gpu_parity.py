@@ -494,6 +494,43 @@ def test_sync_host_leaves_bed_and_rk2_saves_readable():
         compare_state(sim, orc, rtol=0.0, fields=("h", "hu", "hv", "b", "h0", "hu0", "hv0"))
 
 
+def test_front_end_layer_accessors_sync_and_xarray():
+    """Front-end methods outside the 2D step: the multilayer accessors and
+    setters raise RuntimeError as the reference's do when multilayer mode is
+    off; sync_from_device hands the host the state and stepping continues
+    exactly; to_xarray raises ImportError without xarray, else returns the
+    interior snapshot."""
+    nx, ny, dx = 40, 32, 5.0
+    b = gaussian_bed(nx, ny, dx, dx, 6, seed=37, width=(20.0, 60.0))
+    h = hump_depth(b, dx, dx, width=40.0)
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, manning_n=0.025)
+    sim, orc = pair(cfg, bathymetry=b, initial_h=h)
+    with sim:
+        assert sim.nz == 0
+        for name in ("h_layer", "salinity", "temperature"):
+            with pytest.raises(RuntimeError):
+                getattr(sim, name)
+        for name in ("set_salinity", "set_temperature"):
+            with pytest.raises(RuntimeError, match="multilayer"):
+                getattr(sim, name)(np.zeros((nx, ny, 1)))
+        sim.step(5)
+        orc.step(5)
+        sim.sync_from_device()
+        compare_state(sim, orc, rtol=0.0, fields=("h", "hu", "hv", "b", "h0", "hu0", "hv0"))
+        sim.step(5)
+        orc.step(5)
+        compare_state(sim, orc, rtol=0.0)
+        try:
+            import xarray  # noqa: F401
+        except ImportError:
+            with pytest.raises(ImportError, match="xarray"):
+                sim.to_xarray()
+        else:
+            ds = sim.to_xarray()
+            assert np.array_equal(ds["h"].values[0], orc.interior("h"))
+            assert float(ds.attrs["time"]) == sim.time
+
+
 def test_restart_refuses_grid_mismatch_and_finalised_handle(tmp_path):
     from rakali_b200 import Rakali
     path = tmp_path / "r.nc"
