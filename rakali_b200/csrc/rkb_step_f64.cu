@@ -632,8 +632,14 @@ __global__ void __launch_bounds__(TX * TY + 32 * XW)
 
 // Every simulation of a batch in one launch: map[blockIdx.x] = (simulation,
 // tile index within that simulation's tiling).
+// Blocks per SM that shared memory allows (2 for the 512- and 448-thread
+// tiles, 3 for the others), as the single-simulation kernels reach by
+// themselves: left free, the compiler gives some batch stages more registers
+// than that occupancy allows.
+constexpr int batch_blocks_per_sm(int threads) { return threads <= 320 ? 3 : 2; }
+
 template <int TX, int TY, bool HLLC, int STAGE, int XW = 0>
-__global__ void __launch_bounds__(TX * TY + 32 * XW)
+__global__ void __launch_bounds__(TX * TY + 32 * XW, batch_blocks_per_sm(TX * TY + 32 * XW))
     k_stage_batch(const StepArgs* __restrict__ args, const int2* __restrict__ map) {
   __shared__ StepArgs sa;
   const int2 m = map[blockIdx.x];
