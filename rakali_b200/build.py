@@ -36,8 +36,9 @@ UNITS = {
     # reciprocal and square root (the well-balanced products are written
     # with explicit round-to-nearest intrinsics and are never contracted)
     "rkb_step_f32.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
-    # FP32 adjoint batches: FP32 arithmetic with fast division and square root
-    "rkb_adjoint32.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
+    # FP32 adjoint batches: FP32 arithmetic with fast division and square root,
+    # uncontracted, so the fused and the taped forward kernels round alike
+    "rkb_adjoint32.cu": ["--fmad=false", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
     "rkb_sim.cu": [],
     "rkb_batch.cu": [],
     "rkb_api.cu": [],

@@ -240,6 +240,146 @@ __global__ void k_cells(Grid g, size_t ms, Fields<T> V, Fields<T> base, const T*
   out.hv[c] = v;
 }
 
+// One forward stage in one launch, for the steps whose slopes and face values
+// the reverse sweep does not read (the checkpointing pass and the segment
+// recomputes): a kBX x kBY tile of cells with a 2-cell halo in shared memory,
+// then the limited slopes, the faces (each once) and the cell update of
+// k_slopes / k_faces / k_cells, with the same device functions in the same
+// expression order, so the trajectory is the taped kernels' bit for bit.
+template <typename T>
+struct FusedSmem {
+  static constexpr int TX = kBX, TY = kBY, TW = TX + 4, NT = TW * (TY + 4);
+  static constexpr int NSX = (TX + 2) * TY, NSY = TX * (TY + 2);
+  static constexpr int NFX = (TX + 1) * TY, NFY = TX * (TY + 1);
+  static constexpr size_t BYTES =
+      sizeof(T) * (4 * (size_t)NT + 3 * NSX + 3 * NSY + 6 * NFX + 6 * NFY);
+};
+
+template <typename T, bool HLLC>
+__global__ void __launch_bounds__(kBX * kBY)
+    k_stage_fused(Grid g, size_t ms, Fields<T> V, Fields<T> base, const T* __restrict__ b,
+                  const T* __restrict__ nf, const double* __restrict__ dts, int stage,
+                  Fields<T> out) {
+  using SM = FusedSmem<T>;
+  constexpr int TX = SM::TX, TY = SM::TY, TW = SM::TW, NTH = kBX * kBY;
+  extern __shared__ __align__(16) unsigned char fused_smem[];
+  T* th = reinterpret_cast<T*>(fused_smem);
+  T* tu = th + SM::NT;
+  T* tv = tu + SM::NT;
+  T* tb = tv + SM::NT;
+  T* sx = tb + SM::NT;       // 3 x NSX: x-slopes of eta, hu, hv, cells -1 .. TX
+  T* sy = sx + 3 * SM::NSX;  // 3 x NSY: y-slopes, rows -1 .. TY
+  T* fx = sy + 3 * SM::NSY;  // 6 x NFX: x-face (c-1 | c) outputs, c = 0 .. TX
+  T* fy = fx + 6 * SM::NFX;  // 6 x NFY: y-face (r-1 | r) outputs, r = 0 .. TY
+  const int tid = threadIdx.x;
+  const size_t zb = member_base(ms);
+  const int gx0 = g.ng + (int)blockIdx.x * TX, gy0 = g.ng + (int)blockIdx.y * TY;
+
+  for (int k = tid; k < SM::NT; k += NTH) {
+    const int gi = gx0 - 2 + k % TW, gj = gy0 - 2 + k / TW;
+    T vh = T(0), vu = T(0), vv = T(0), vb = T(0);
+    if (gi < g.nxt && gj < g.nyt) {
+      const size_t q = g.at(gi, gj) + zb;
+      vh = V.h[q];
+      vu = V.hu[q];
+      vv = V.hv[q];
+      vb = b[q];
+    }
+    th[k] = vh;
+    tu[k] = vu;
+    tv[k] = vv;
+    tb[k] = vb;
+  }
+  __syncthreads();
+
+  auto eta = [&](int q) { return th[q] + tb[q]; };
+  for (int k = tid; k < SM::NSX + SM::NSY; k += NTH) {
+    if (k < SM::NSX) {
+      const int q = (k / (TX + 2) + 2) * TW + (k % (TX + 2) + 1);
+      cell_slope(th[q - 1], th[q], th[q + 1], eta(q - 1), eta(q), eta(q + 1), tu[q - 1], tu[q],
+                 tu[q + 1], tv[q - 1], tv[q], tv[q + 1], sx[k], sx[SM::NSX + k],
+                 sx[2 * SM::NSX + k]);
+    } else {
+      const int kk = k - SM::NSX;
+      const int q = (kk / TX + 1) * TW + (kk % TX + 2);
+      cell_slope(th[q - TW], th[q], th[q + TW], eta(q - TW), eta(q), eta(q + TW), tu[q - TW],
+                 tu[q], tu[q + TW], tv[q - TW], tv[q], tv[q + TW], sy[kk], sy[SM::NSY + kk],
+                 sy[2 * SM::NSY + kk]);
+    }
+  }
+  __syncthreads();
+
+  for (int k = tid; k < SM::NFX + SM::NFY; k += NTH) {
+    FaceOutT<T> o;
+    if (k < SM::NFX) {
+      const int c = k % (TX + 1), r = k / (TX + 1);
+      const int qL = (r + 2) * TW + (c + 1), qR = qL + 1;
+      const int sL = r * (TX + 2) + c, sR = sL + 1;
+      face_flux<0, HLLC>(eta(qL) + T(0.5) * sx[sL], tu[qL] + T(0.5) * sx[SM::NSX + sL],
+                         tv[qL] + T(0.5) * sx[2 * SM::NSX + sL], tb[qL],
+                         eta(qR) - T(0.5) * sx[sR], tu[qR] - T(0.5) * sx[SM::NSX + sR],
+                         tv[qR] - T(0.5) * sx[2 * SM::NSX + sR], tb[qR], o);
+      T* f = fx + k;
+      f[0] = o.fh;
+      f[SM::NFX] = o.fqx;
+      f[2 * SM::NFX] = o.fqy;
+      f[3 * SM::NFX] = o.wbR;
+      f[4 * SM::NFX] = o.hL2;
+      f[5 * SM::NFX] = o.pL2;
+    } else {
+      const int kk = k - SM::NFX;
+      const int c = kk % TX, r = kk / TX;
+      const int qB = (r + 1) * TW + (c + 2), qT = qB + TW;
+      const int sB = r * TX + c, sT = sB + TX;
+      face_flux<1, HLLC>(eta(qB) + T(0.5) * sy[sB], tu[qB] + T(0.5) * sy[SM::NSY + sB],
+                         tv[qB] + T(0.5) * sy[2 * SM::NSY + sB], tb[qB],
+                         eta(qT) - T(0.5) * sy[sT], tu[qT] - T(0.5) * sy[SM::NSY + sT],
+                         tv[qT] - T(0.5) * sy[2 * SM::NSY + sT], tb[qT], o);
+      T* f = fy + kk;
+      f[0] = o.fh;
+      f[SM::NFY] = o.fqx;
+      f[2 * SM::NFY] = o.fqy;
+      f[3 * SM::NFY] = o.wbR;
+      f[4 * SM::NFY] = o.hL2;
+      f[5 * SM::NFY] = o.pL2;
+    }
+  }
+  __syncthreads();
+
+  const int cx = tid % TX, cy = tid / TX;
+  const int i = gx0 + cx, j = gy0 + cy;
+  if (i >= g.nxt - g.ng || j >= g.nyt - g.ng) return;
+  // divergence() on the tile's faces
+  const int l = cy * (TX + 1) + cx, r = l + 1, bo = cy * TX + cx, to = bo + TX;
+  const T dx = T(g.dx), dy = T(g.dy);
+  const T ofh = -((fx[r] - fx[l]) / dx) - (fy[to] - fy[bo]) / dy;
+  const T ofhu = -((fx[SM::NFX + r] - fx[SM::NFX + l]) / dx) -
+                 (fy[SM::NFY + to] - fy[SM::NFY + bo]) / dy -
+                 T(kHalfG) * (fx[3 * SM::NFX + l] - fx[4 * SM::NFX + r] + fx[5 * SM::NFX + r]) / dx;
+  const T ofhv = -((fx[2 * SM::NFX + r] - fx[2 * SM::NFX + l]) / dx) -
+                 (fy[2 * SM::NFY + to] - fy[2 * SM::NFY + bo]) / dy -
+                 T(kHalfG) * (fy[3 * SM::NFY + bo] - fy[4 * SM::NFY + to] + fy[5 * SM::NFY + to]) / dy;
+  // k_cells
+  const size_t c = g.at(i, j) + zb;
+  const T dt = T(dts[blockIdx.z]);
+  const int qc = (cy + 2) * TW + (cx + 2);
+  T a = th[qc], u = tu[qc], v = tv[qc];
+  a = a + dt * ofh;
+  u = u + dt * ofhu;
+  v = v + dt * ofhv;
+  protect(a, u, v);
+  friction(a, u, v, nf[c], dt);
+  if (stage == 2) {
+    a = T(0.5) * (base.h[c] + a);
+    u = T(0.5) * (base.hu[c] + u);
+    v = T(0.5) * (base.hv[c] + v);
+    protect(a, u, v);
+  }
+  out.h[c] = a;
+  out.hu[c] = u;
+  out.hv[c] = v;
+}
+
 // CFL maxima of a state (same wave speed and reduction as the step), per
 // member: mx[2 m], mx[2 m + 1] (FP64 bit patterns of non-negative values).
 template <typename T>
@@ -584,6 +724,13 @@ class Adjoint final : public AdjointBase {
       err = "the adjoint needs an interior at least nghost cells wide in x and y";
       return -2;
     }
+    if (cudaFuncSetAttribute(k_stage_fused<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)FusedSmem<T>::BYTES) != cudaSuccess ||
+        cudaFuncSetAttribute(k_stage_fused<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)FusedSmem<T>::BYTES) != cudaSuccess) {
+      err = "cannot configure the fused forward kernel";
+      return -1;
+    }
     nm_ = nm;
     g_.ng = ng;
     g_.nxt = nx + 2 * ng;
@@ -919,16 +1066,25 @@ class Adjoint final : public AdjointBase {
       k_faces<T, false><<<blocks(g_.ng, ie, g_.ng, je), kBX * kBY, 0, stream_>>>(g_, ms_, V, b_, Tp);
   }
 
-  // Step k: U -> out.  out may alias U: stage 2 reads the RK2 base only at the
-  // cell it writes, and its neighbours come from the stage-1 result.
+  // Step k: U -> out, one fused launch per stage (no tapes).  out may alias
+  // U: stage 2 reads the RK2 base only at the cell it writes, and its
+  // neighbours come from the stage-1 result.
   int step(Fields<T> U, Fields<T> out, int k) {
     walls(U);
-    tape(U, t1_);
-    k_cells<T><<<interior(), kBX * kBY, 0, stream_>>>(g_, ms_, U, U, nf_, t1_, dt_of(k), 1, Us_);
+    fused_stage(U, U, 1, Us_, k);
     walls(Us_);
-    tape(Us_, t2_);
-    k_cells<T><<<interior(), kBX * kBY, 0, stream_>>>(g_, ms_, Us_, U, nf_, t2_, dt_of(k), 2, out);
+    fused_stage(Us_, U, 2, out, k);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  }
+
+  void fused_stage(Fields<T> V, Fields<T> base, int stage, Fields<T> out, int k) {
+    const size_t smem = FusedSmem<T>::BYTES;
+    if (hllc_)
+      k_stage_fused<T, true><<<interior(), kBX * kBY, smem, stream_>>>(g_, ms_, V, base, b_, nf_,
+                                                                       dt_of(k), stage, out);
+    else
+      k_stage_fused<T, false><<<interior(), kBX * kBY, smem, stream_>>>(g_, ms_, V, base, b_, nf_,
+                                                                        dt_of(k), stage, out);
   }
 
   // dt of step k for every member from the CFL condition of U (recorded).
