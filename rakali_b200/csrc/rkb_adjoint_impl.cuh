@@ -1110,10 +1110,12 @@ class Adjoint final : public AdjointBase {
   // gV_ (adjoint of the stage input after the wall fold), gbase_ (stage 2).
   int stage_adj(Fields<T> V, Fields<T> base, Tape<T>& Tp, int k, int stage, Fields<T> gout) {
     const int ie = g_.nxt - g_.ng, je = g_.nyt - g_.ng;
-    const size_t fb = ms_ * nm_ * sizeof(T);
-    ADJ_TRY(cudaMemsetAsync(gV_.h, 0, fb, stream_));  // the outer ghost layers are not gathered
-    ADJ_TRY(cudaMemsetAsync(gV_.hu, 0, fb, stream_));
-    ADJ_TRY(cudaMemsetAsync(gV_.hv, 0, fb, stream_));
+    if (g_.ng > 2) {  // k_gather_adj writes layers ng-2 .. nxt-ng+1: all of them when ng = 2
+      const size_t fb = ms_ * nm_ * sizeof(T);
+      ADJ_TRY(cudaMemsetAsync(gV_.h, 0, fb, stream_));
+      ADJ_TRY(cudaMemsetAsync(gV_.hu, 0, fb, stream_));
+      ADJ_TRY(cudaMemsetAsync(gV_.hv, 0, fb, stream_));
+    }
     k_cells_adj<T><<<interior(), kBX * kBY, 0, stream_>>>(g_, ms_, V, base, nf_, Tp, dt_of(k),
                                                            stage, gout, R_, gbase_, gn_);
     if (hllc_)
@@ -1139,10 +1141,11 @@ class Adjoint final : public AdjointBase {
     walls(Us_);
     tape(Us_, t2_);
     if (stage_adj(Us_, U, t2_, k, 2, lam_) != 0) return -1;  // gV_ = adjoint of U*
-    if (copy(lams_, gV_) != 0) return -1;
+    std::swap(lams_, gV_);  // three distinct buffers: renaming replaces the copies
     if (stage_adj(U, U, t1_, k, 1, lams_) != 0) return -1;  // gV_ = adjoint of U^k (stage 1)
     k_add<T><<<interior(), kBX * kBY, 0, stream_>>>(g_, ms_, gV_, gbase_);
-    return copy(lam_, gV_);
+    std::swap(lam_, gV_);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
   }
 
   Grid g_{};
