@@ -597,6 +597,22 @@ def run_config5(args):
         fd_floor.append(abs(dfl - d64) / abs(d64))
         sec_frozen.append(abs(d64 - secant[k]) / abs(secant[k]))
         sec_exact.append(abs(dex - secant[k]) / abs(secant[k]))
+    # the production FP32 step (surface-form sweep) on member 0's grid, for
+    # the cost of the gradient in forward steps; all members take the same work
+    from rakali_b200 import Rakali
+    import ctypes
+    psim = Rakali(defer_init=True, nx=n, ny=n, dx=dx, dy=dx, nghost=2, t_end=1e9, cfl=0.45,
+                  manning_n=float(ref["n"].flat[0]))
+    psim.set_bathymetry(ref["b"])
+    psim.set_initial_h(ref["h"])
+    psim.finalize()
+    psim.set_precision(32)
+    pms = ctypes.c_double()
+    psim._lib.rkb_time_steps(psim._handle, 5, ctypes.byref(pms))
+    if psim._lib.rkb_time_steps(psim._handle, steps, ctypes.byref(pms)) != 0:
+        raise RuntimeError("production forward timing failed")
+    prod_ms = pms.value * nm
+    psim.close()
     frozen_slopes = {
         "steps": steps,
         "grad_b_rel_l2": rel(frozen[32][0], frozen[64][0]),
@@ -623,6 +639,10 @@ def run_config5(args):
         "forward_cell_updates_per_s": cells / (fwd_ms * 1e-3),
         "forward_plus_adjoint_cell_updates_per_s": cells / (grad_ms * 1e-3),
         "cost_multiple_of_forward": grad_ms / fwd_ms,
+        "production_forward_ms": prod_ms,
+        "cost_multiple_of_production_forward": grad_ms / prod_ms,
+        "production_forward_note": "FP32 surface-form sweep on member 0's grid, "
+                                   f"{steps} CFL steps, times {nm} members",
         "mass_drift_rel_max": drift,
         "vs_fp64_member0_first_steps": first_steps,
         "vs_fp64_member0_frozen_slopes": frozen_slopes,
