@@ -726,22 +726,26 @@ int Sim::set_interior(int which, const double* data, int nx, int ny) {
   }
   if (which == 10 || which == 0) user_set_h = true;
   if (state_field && on_device_) {
-    // push_state_to_device (rki_api.F90:137-143)
+    // push_state_to_device (rki_api.F90:137-143) pushes h, hu and hv; the two
+    // not set here hold what the device holds (refreshed above, and the FP32
+    // form round-trips through the host arrays exactly), so only this one moves
     const size_t wbytes = (size_t)g.nxt * sizeof(double);
     const size_t dpitch = (size_t)g.pitch * sizeof(double);
     FieldSet F = cur_ ? args_.U1 : args_.U0;
     double* dstd[3] = {F.h, F.hu, F.hv};
-    for (int k = 0; k < 3; ++k)
-      if (cudaMemcpy2DAsync(dstd[k], dpitch, hf_[k], wbytes, wbytes, g.nyt,
-                            cudaMemcpyHostToDevice, stream_) != cudaSuccess)
-        return -1;
-    if (precision_ == 32 && to_surface(true) != 0) return -1;
+    if (cudaMemcpy2DAsync(dstd[f], dpitch, hf_[f], wbytes, wbytes, g.nyt, cudaMemcpyHostToDevice,
+                          stream_) != cudaSuccess)
+      return -1;
+    if (precision_ == 32 && to_surface(true, f) != 0) return -1;
     hctl_->ms_valid = 0;
     if (cudaMemcpyAsync(&args_.ctl->ms_valid, &hctl_->ms_valid, sizeof(int),
                         cudaMemcpyHostToDevice, stream_) != cudaSuccess)
       return -1;
     if (cudaStreamSynchronize(stream_) != cudaSuccess) return -1;
-    mark_host_stale();
+    // FP64: h, hu, hv on the host still equal the device's, so the next setter
+    // needs no refresh.  FP32: the device holds the pushed field rounded.
+    host_is_current_ = false;
+    if (precision_ == 32) host_state_current_ = false;
   }
   return 0;
 }
@@ -1014,14 +1018,20 @@ void Sim::sync_args32() {
 
 // FP64 staging buffers -> surface form: all three buffers (after an upload)
 // or the current one (after a setter).
-int Sim::to_surface(bool cur_only) {
+int Sim::to_surface(bool cur_only, int field) {
   if (alloc_device32() != 0) return -1;
   const FieldSet src[3] = {args_.U0, args_.U1, args_.S};
   const FieldSet32 dst[3] = {args32_.U0, args32_.U1, args32_.S};
   for (int k = 0; k < 3; ++k) {
     if (cur_only && k != cur_) continue;
-    RKB_TRY(launch_to_surface(g, args32_.g, src[k], args_.b, dst[k],
-                              k == (cur_only ? cur_ : 0) ? args32_.b : nullptr, stream_));
+    FieldSet s = src[k];
+    if (field >= 0) {  // one state field of the current buffer; the bed is unchanged
+      if (field != 0) s.h = nullptr;
+      if (field != 1) s.hu = nullptr;
+      if (field != 2) s.hv = nullptr;
+    }
+    double* bed = field < 0 && k == (cur_only ? cur_ : 0) ? args32_.b : nullptr;
+    RKB_TRY(launch_to_surface(g, args32_.g, s, args_.b, dst[k], bed, stream_));
   }
   return 0;
 }

@@ -110,7 +110,7 @@ class Sim {
   int upload_state();
   int upload_params();
   int alloc_device32();
-  int to_surface(bool cur_only);
+  int to_surface(bool cur_only, int field = -1);  // field 0..2: that state field only
   int to_depth(bool full);
   int pull_state(bool full);
   void sync_args32();

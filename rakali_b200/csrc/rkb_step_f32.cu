@@ -1060,9 +1060,9 @@ __global__ void k_to_surface(Grid g64, Grid g32, FieldSet src, const double* __r
   for (int j = blockIdx.y; j < g64.nyt; j += gridDim.y) {
     const size_t p = g64.at(i, j), q = g32.at(i, j);
     const double b = b64[p];
-    dst.eta[q] = surface_of(src.h[p], b);
-    dst.hu[q] = (float)src.hu[p];
-    dst.hv[q] = (float)src.hv[p];
+    if (src.h) dst.eta[q] = surface_of(src.h[p], b);  // a null field is left as it is
+    if (src.hu) dst.hu[q] = (float)src.hu[p];
+    if (src.hv) dst.hv[q] = (float)src.hv[p];
     if (bed_out) bed_out[q] = b;
   }
 }
