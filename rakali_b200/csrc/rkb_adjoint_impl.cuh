@@ -565,7 +565,7 @@ __global__ void k_recon_adj(Grid g, size_t ms, Fields<T> V, const T* __restrict_
 // the derivative of the step with the slopes of the current state frozen.
 template <typename T>
 __global__ void k_gather_adj(Grid g, size_t ms, Rev<T> R, Fields<T> gV, T* __restrict__ gb,
-                             int frozen) {
+                             int frozen, Fields<T> gadd) {
   const int i = g.ng - 2 + blockIdx.x * kBX + threadIdx.x % kBX;
   const int j = g.ng - 2 + blockIdx.y * kBY + threadIdx.x / kBX;
   if (i > g.nxt - g.ng + 1 || j > g.nyt - g.ng + 1) return;
@@ -613,6 +613,11 @@ __global__ void k_gather_adj(Grid g, size_t ms, Rev<T> R, Fields<T> gV, T* __res
     gh += R.ga[0][c];
     gu += R.ga[1][c];
     gv += R.ga[2][c];
+    if (gadd.h) {  // stage 1: the RK2 base adjoint of stage 2 (U^k enters both stages)
+      gh += gadd.h[c];
+      gu += gadd.hu[c];
+      gv += gadd.hv[c];
+    }
   }
   gV.h[c] = gh;
   gV.hu[c] = gu;
@@ -672,17 +677,6 @@ __global__ void k_gauges_adj(const long long* __restrict__ gq, const double* __r
   const size_t q = (size_t)gq[k];
   lam.h[q] += T(2.0 * r[k]);  // gauges are distinct cells: no two threads share q
   gb[q] += T(2.0 * r[k]);
-}
-
-template <typename T>
-__global__ void k_add(Grid g, size_t ms, Fields<T> a, Fields<T> b) {  // interior a += b
-  const int i = g.ng + blockIdx.x * kBX + threadIdx.x % kBX;
-  const int j = g.ng + blockIdx.y * kBY + threadIdx.x / kBX;
-  if (i >= g.nxt - g.ng || j >= g.nyt - g.ng) return;
-  const size_t c = g.at(i, j) + member_base(ms);
-  a.h[c] += b.h[c];
-  a.hu[c] += b.hu[c];
-  a.hv[c] += b.hv[c];
 }
 
 // ---------------------------------------------------------------------------
@@ -1127,7 +1121,7 @@ class Adjoint final : public AdjointBase {
     k_recon_adj<T><<<blocks(g_.ng - 1, ie, g_.ng - 1, je), kBX * kBY, 0, stream_>>>(g_, ms_, V, b_,
                                                                                    R_);
     k_gather_adj<T><<<blocks(g_.ng - 2, ie + 1, g_.ng - 2, je + 1), kBX * kBY, 0, stream_>>>(
-        g_, ms_, R_, gV_, gb_, frozen_ ? 1 : 0);
+        g_, ms_, R_, gV_, gb_, frozen_ ? 1 : 0, stage == 1 ? gbase_ : Fields<T>{});
     walls_adj(V, false);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
   }
@@ -1142,8 +1136,8 @@ class Adjoint final : public AdjointBase {
     tape(Us_, t2_);
     if (stage_adj(Us_, U, t2_, k, 2, lam_) != 0) return -1;  // gV_ = adjoint of U*
     std::swap(lams_, gV_);  // three distinct buffers: renaming replaces the copies
-    if (stage_adj(U, U, t1_, k, 1, lams_) != 0) return -1;  // gV_ = adjoint of U^k (stage 1)
-    k_add<T><<<interior(), kBX * kBY, 0, stream_>>>(g_, ms_, gV_, gbase_);
+    // gV_ = adjoint of U^k: stage 1's, with stage 2's RK2 base adjoint added in the gather
+    if (stage_adj(U, U, t1_, k, 1, lams_) != 0) return -1;
     std::swap(lam_, gV_);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
   }

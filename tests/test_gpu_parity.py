@@ -475,6 +475,41 @@ def test_checkpoint_matches_oracle_and_run_continues(tmp_path):
         compare_state(sim, orc, rtol=0.0, fields=("h", "hu", "hv", "b", "h0", "hu0", "hv0"))
 
 
+def test_checkpoint_fp32_form_leaves_the_run_unchanged(tmp_path):
+    """FP32 surface form: the checkpoint holds the fields the handle's views
+    return, and a run that writes one continues bit-identically to one that
+    does not."""
+    from scipy.io import netcdf_file
+
+    from rakali_b200 import Rakali
+    nx, ny, dx = 64, 48, 5.0
+    b = gaussian_bed(nx, ny, dx, dx, 10, seed=41, width=(20.0, 90.0))
+    h = hump_depth(b, dx, dx, width=50.0)
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, manning_n=0.025)
+
+    def make():
+        s = Rakali(defer_init=True, precision=32, **cfg)
+        s.set_bathymetry(b)
+        s.set_initial_h(h)
+        s.finalize()
+        return s
+
+    path = tmp_path / "ck32.nc"
+    with make() as a, make() as c:
+        a.step(17)
+        a.save_checkpoint(path)
+        a.step(9)
+        c.step(26)
+        for f in ("h", "hu", "hv"):
+            assert np.array_equal(getattr(a, f), getattr(c, f)), f
+        assert a.time == c.time
+        with make() as d:
+            d.step(17)
+            with netcdf_file(str(path), "r", mmap=False) as nc:
+                for f in ("h", "hu", "hv", "b", "h0", "hu0", "hv0"):
+                    assert np.array_equal(np.asarray(nc.variables[f][:]), getattr(d, f)), f
+
+
 def test_sync_host_leaves_bed_and_rk2_saves_readable():
     """rki_sync_host refreshes h, hu, hv only; reading the bed (whose ghosts
     the wall fill mirrors every step) or the RK2 saves afterwards still gives
