@@ -428,7 +428,8 @@ __global__ void k_mass(Grid g, size_t ms, const T* __restrict__ h, double* mass)
 // Cells: output adjoint gout -> divergence adjoint go, direct input adjoint
 // ga (a = h + dt o), base adjoint (stage 2), n adjoint.
 template <typename T>
-__global__ void k_cells_adj(Grid g, size_t ms, Fields<T> V, Fields<T> base,
+__global__ void __launch_bounds__(kBX * kBY, 4)
+    k_cells_adj(Grid g, size_t ms, Fields<T> V, Fields<T> base,
                             const T* __restrict__ nf, Tape<T> Tp, const double* __restrict__ dts,
                             int stage, Fields<T> gout, Rev<T> R, Fields<T> gbase,
                             T* __restrict__ gn) {
@@ -471,9 +472,12 @@ __global__ void k_cells_adj(Grid g, size_t ms, Fields<T> V, Fields<T> base,
 
 // Faces: divergence adjoints of the two adjacent cells -> face output
 // adjoints -> adjoints of the reconstructed inputs.
+// Occupancy floors: left free, the FP64 instance of k_faces_adj takes 126-138
+// registers (two blocks per SM) and waits on FP64 latency; three blocks with
+// a few spilled registers run faster.
 template <typename T, bool HLLC>
-__global__ void k_faces_adj(Grid g, size_t ms, Fields<T> V, const T* __restrict__ b, Tape<T> Tp,
-                            Rev<T> R) {
+__global__ void __launch_bounds__(kBX * kBY, 3)
+    k_faces_adj(Grid g, size_t ms, Fields<T> V, const T* __restrict__ b, Tape<T> Tp, Rev<T> R) {
   const int i = g.ng + blockIdx.x * kBX + threadIdx.x % kBX;
   const int j = g.ng + blockIdx.y * kBY + threadIdx.x / kBX;
   const int ie = g.nxt - g.ng, je = g.nyt - g.ng;
