@@ -135,7 +135,7 @@ def test_autograd_function_backward():
 
 
 def test_gradient_matches_torch_autograd_128():
-    """The north-star size for the autograd comparison: 128 x 128, 30 steps, 16 gauges.
+    """The autograd comparison at 128 x 128, 30 steps, 16 gauges.
 
     The transcription agrees with the CUDA forward to ~1e-12, not bit for bit;
     on resting water the limiter and wave-speed branches are decided by
