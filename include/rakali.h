@@ -248,6 +248,14 @@ int rkb_restart_write(const char *path, int nx, int ny, const double *h, const d
                       int nghost);
 int rkb_restart_read(const char *path, int nx, int ny, double *h, double *hu, double *hv,
                      double *b, double *time);
+/* The per-step checkpoint codec of rkb_save_checkpoint without a simulation:
+ * fields = h, hu, hv, b, h0, hu0, hv0, each (nx_total, ny_total) Fortran order
+ * with ghosts; scalars = time, dt, dx, dy, manning_n, coriolis_f,
+ * clamped_elevation; counts = step_count, nx_phys, ny_phys, nghost.  0 written,
+ * -1 write failed, -2 bad arguments. */
+int rkb_checkpoint_write(const char *path, int nx_total, int ny_total,
+                         const double *const *fields, const double *scalars, const int *counts);
+
 /* bathymetry_file input (src/io/rki_bathymetry.F90:21-163): variable b,
  * elevation or depth over dimensions x, y (either order) of a NetCDF classic
  * file into an interior (nx, ny) Fortran-order array; return codes as

@@ -407,6 +407,29 @@ int rkb_restart_write(const char* path, int nx, int ny, const double* h, const d
   return 0;
 }
 
+int rkb_checkpoint_write(const char* path, int nx_total, int ny_total,
+                         const double* const* fields, const double* scalars, const int* counts) {
+  if (!path || !fields || !scalars || !counts || nx_total < 1 || ny_total < 1)
+    return fail(-2, "invalid arguments");
+  for (int k = 0; k < 7; ++k)
+    if (!fields[k]) return fail(-2, "invalid arguments");
+  rkb::nc::CheckpointMeta m{};
+  m.time = scalars[0];
+  m.dt = scalars[1];
+  m.dx = scalars[2];
+  m.dy = scalars[3];
+  m.manning_n = scalars[4];
+  m.coriolis_f = scalars[5];
+  m.clamped_elevation = scalars[6];
+  m.step_count = counts[0];
+  m.nx_phys = counts[1];
+  m.ny_phys = counts[2];
+  m.nghost = counts[3];
+  std::string err;
+  if (!rkb::nc::write_checkpoint(path, nx_total, ny_total, fields, m, err)) return fail(-1, err);
+  return 0;
+}
+
 int rkb_bathymetry_read(const char* path, int nx, int ny, double* b) {
   if (!path || !b || nx < 1 || ny < 1) return fail(-2, "invalid arguments");
   std::string err;

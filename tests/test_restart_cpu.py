@@ -168,3 +168,39 @@ def test_gauge_file_layout_reads_in_scipy(lib, tmp_path):
             assert f.variables[name].dimensions == ("time", "station")
             assert np.array_equal(f.variables[name][:], vals[:, :, c])
         assert f.title == b"Rakali gauge time series"
+
+
+def test_checkpoint_file_layout_reads_in_scipy(lib, tmp_path):
+    """rkb_checkpoint_write (the codec of save_checkpoint) writes the variables
+    and attributes of the reference front end's save_checkpoint
+    (python/rakali/_core.py:1433-1499): fields with ghosts over (x_total,
+    y_total) and the scalars as typed global attributes."""
+    from scipy.io import netcdf_file
+    nxt, nyt = 13, 9
+    rng = np.random.default_rng(12)
+    arrs = [np.asfortranarray(rng.standard_normal((nxt, nyt))) for _ in range(7)]
+    fields = (DP * 7)(*[_p(a) for a in arrs])
+    scal = np.array([123.5, 0.25, 5.0, 7.5, 0.025, 1.0e-4, -0.3])
+    cnt = np.array([42, nxt - 4, nyt - 4, 2], dtype=np.int32)
+    path = tmp_path / "step_42.nc"
+    assert lib.rkb_checkpoint_write(str(path).encode(), nxt, nyt, fields, _p(scal),
+                                    cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int))) == 0
+    names = ("h", "hu", "hv", "b", "h0", "hu0", "hv0")
+    with netcdf_file(str(path), "r", mmap=False) as f:
+        assert f.dimensions == {"x_total": nxt, "y_total": nyt}
+        for name, a in zip(names, arrs):
+            v = f.variables[name]
+            assert v.dimensions == ("x_total", "y_total")
+            assert np.array_equal(v[:], a), name
+        assert f.variables["b"].positive == b"up"
+        assert f.variables["hu"].units == b"m2 s-1"
+        at = f._attributes
+        assert at["title"] == b"Rakali per-step checkpoint (2D barotropic)"
+        for key, val in zip(("time", "dt", "dx", "dy", "manning_n", "coriolis_f",
+                             "clamped_elevation"), scal):
+            assert np.asarray(at[key]).dtype == np.float64 and float(at[key]) == val, key
+        for key, val in zip(("step_count", "nx_phys", "ny_phys", "nghost"), cnt):
+            assert np.asarray(at[key]).dtype.kind == "i" and int(at[key]) == val, key
+        assert (int(at["nx_total"]), int(at["ny_total"])) == (nxt, nyt)
+    assert lib.rkb_checkpoint_write(str(path).encode(), 0, nyt, fields, _p(scal),
+                                    cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int))) == -2
