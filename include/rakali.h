@@ -256,6 +256,17 @@ int rkb_restart_read(const char *path, int nx, int ny, double *h, double *hu, do
 int rkb_checkpoint_write(const char *path, int nx_total, int ny_total,
                          const double *const *fields, const double *scalars, const int *counts);
 
+/* Gauge stencils without a simulation (compute_local_gauges /
+ * compute_interp_weights, src/io/structured/rki_gauges.F90:208-336): of the n
+ * stations (x, y in metres from the lower-left corner) those inside the
+ * nx x ny interior, in order: their index, the 0-based array indices (ghosts
+ * included) of the lower-left stencil cell and the clamped bilinear weights.
+ * Returns how many stations are inside (arrays hold n entries), -2 on bad
+ * arguments. */
+int rkb_gauge_stencils(int nx, int ny, int nghost, double dx, double dy, const double *x,
+                       const double *y, int n, int *station, int *ix0, int *iy0, double *wx,
+                       double *wy);
+
 /* bathymetry_file input (src/io/rki_bathymetry.F90:21-163): variable b,
  * elevation or depth over dimensions x, y (either order) of a NetCDF classic
  * file into an interior (nx, ny) Fortran-order array; return codes as

@@ -134,6 +134,7 @@ def load(path: str | None = None):
     _sig(lib, "rkb_restart_write", [CP, I, I, DP, DP, DP, DP, D, D, D, I], I)
     _sig(lib, "rkb_restart_read", [CP, I, I, DP, DP, DP, DP, DP], I)
     _sig(lib, "rkb_checkpoint_write", [CP, I, I, ctypes.POINTER(DP), DP, IP], I)
+    _sig(lib, "rkb_gauge_stencils", [I, I, I, D, D, DP, DP, I, IP, IP, IP, DP, DP], I)
     _sig(lib, "rkb_bathymetry_read", [CP, I, I, DP], I)
     _sig(lib, "rkb_set_gauges", [H, I, DP, DP, D, I], I)
     _sig(lib, "rkb_gauge_stations", [H, IP, DP], I)

@@ -430,6 +430,31 @@ int rkb_checkpoint_write(const char* path, int nx_total, int ny_total,
   return 0;
 }
 
+int rkb_gauge_stencils(int nx, int ny, int nghost, double dx, double dy, const double* x,
+                       const double* y, int n, int* station, int* ix0, int* iy0, double* wx,
+                       double* wy) {
+  if (nx < 1 || ny < 1 || nghost < 1 || !(dx > 0.0) || !(dy > 0.0) || n < 0 ||
+      (n > 0 && (!x || !y || !station || !ix0 || !iy0 || !wx || !wy)))
+    return fail(-2, "invalid arguments");
+  rkb::Grid g{};
+  g.ng = nghost;
+  g.nxt = nx + 2 * nghost;
+  g.nyt = ny + 2 * nghost;
+  g.pitch = g.nxt;
+  g.dx = dx;
+  g.dy = dy;
+  rkb::GaugeStencils st;
+  rkb::gauge_stencils(g, x, y, n, st);
+  for (size_t k = 0; k < st.station.size(); ++k) {
+    station[k] = st.station[k];
+    ix0[k] = st.ix0[k];
+    iy0[k] = st.iy0[k];
+    wx[k] = st.wx[k];
+    wy[k] = st.wy[k];
+  }
+  return (int)st.station.size();
+}
+
 int rkb_bathymetry_read(const char* path, int nx, int ny, double* b) {
   if (!path || !b || nx < 1 || ny < 1) return fail(-2, "invalid arguments");
   std::string err;
