@@ -334,10 +334,13 @@ int rkb_compute_timestep(const double *h, const double *hu, const double *hv, in
  * nothing: its scratch is a fixed array inside the library (2 doubles per
  * interior row plus one, for at most 32768 interior rows; about 512 KB on
  * every GPU that loads the library, held until exit).  More rows return -2
- * with the reason in rki_last_error().  The first call on each device looks
- * up the array's device address with that device current; make that first
- * call before any stream capture.  Calls share the array, so calls that
- * overlap on the GPU race; the result is read back before returning. */
+ * with the reason in rki_last_error().  Each call looks up the array's
+ * device address with the caller's device current, so a device reset or a
+ * new context is followed; the first call on a device may load the
+ * library's GPU code, so make it before any stream capture.  There is one
+ * array per GPU and every call uses it: calls that overlap on the GPU (other
+ * host threads, other streams) race, so serialise them.  The result is read
+ * back before returning. */
 int rkb_compute_timestep_noalloc(const double *h, const double *hu, const double *hv,
                                  int nx_total, int ny_total, int nghost, int ld, double dx,
                                  double dy, double cfl, double *dt_out);

@@ -413,6 +413,12 @@ int rkb_checkpoint_write(const char* path, int nx_total, int ny_total,
     return fail(-2, "invalid arguments");
   for (int k = 0; k < 7; ++k)
     if (!fields[k]) return fail(-2, "invalid arguments");
+  // the counts must describe the arrays: nx_total = nx_phys + 2 nghost, as
+  // the reference's grid derives it (rki_grid.F90)
+  if (counts[3] < 1 || counts[1] < 1 || counts[2] < 1 ||
+      (long long)nx_total != (long long)counts[1] + 2LL * counts[3] ||
+      (long long)ny_total != (long long)counts[2] + 2LL * counts[3])
+    return fail(-2, "checkpoint counts disagree with the array extents");
   rkb::nc::CheckpointMeta m{};
   m.time = scalars[0];
   m.dt = scalars[1];

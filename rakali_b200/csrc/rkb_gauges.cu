@@ -108,10 +108,15 @@ void gauge_stencils(const Grid& g, const double* x, const double* y, int n, Gaug
   const double dx = g.dx, dy = g.dy;
   out = GaugeStencils{};
   for (int k = 0; k < n; ++k) {
-    // compute_local_gauges (:208-243): the 1-based physical cell of the station
-    const int ig = (int)std::floor(x[k] / dx) + 1;
-    const int jg = (int)std::floor(y[k] / dy) + 1;
-    if (!(ig >= 1 && ig <= nx && jg >= 1 && jg <= ny)) continue;
+    // compute_local_gauges (:208-243): the 1-based physical cell of the
+    // station.  floor(q) + 1 lies in [1, n] exactly when q = x / dx lies in
+    // [0, n), so testing q first gives the reference's inside-domain answer
+    // for every finite coordinate and drops NaN, infinite and huge ones
+    // before any conversion to int.
+    const double qx = x[k] / dx, qy = y[k] / dy;
+    if (!(qx >= 0.0 && qx < (double)nx && qy >= 0.0 && qy < (double)ny)) continue;
+    const int ig = (int)std::floor(qx) + 1;
+    const int jg = (int)std::floor(qy) + 1;
     // compute_interp_weights (:245-336), 1-based array indices ia, ja
     const int ia = ig + ng, ja = jg + ng;
     const double xc = ((double)ig - 0.5) * dx, yc = ((double)jg - 0.5) * dy;

@@ -141,7 +141,6 @@ void rkb_cr_sincos(double x, double* sn, double* cs) { rkb::cr_sincos(x, *sn, *c
 // overlap on the GPU (other host threads, other streams) race on it.
 // ---------------------------------------------------------------------------
 
-#include <mutex>
 #include <string>
 
 namespace rkb {
@@ -209,19 +208,15 @@ __global__ void k_rows_to_dt(Grid g, double cfl, double* scratch) {
   }
 }
 
-// Device address of the scratch array, looked up once per device with that
-// device current (the symbol's host-side name is not a device address).
-double* scratch_address(int device) {
-  static std::mutex mu;
-  static double* addr[64] = {};
-  if (device < 0 || device >= 64) return nullptr;
-  std::lock_guard<std::mutex> lk(mu);
-  if (!addr[device]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) return nullptr;
-    addr[device] = static_cast<double*>(p);
-  }
-  return addr[device];
+// Device address of the scratch array in the current device's context (the
+// symbol's host-side name is not a device address).  Looked up on every
+// call rather than cached: after cudaDeviceReset the runtime loads the module
+// again, possibly elsewhere, and a cached address would go stale.  The
+// lookup is a host-side table read once the module is loaded.
+double* scratch_address() {
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) return nullptr;
+  return static_cast<double*>(p);
 }
 
 }  // namespace
@@ -240,10 +235,11 @@ int rkb_compute_timestep_noalloc(const double* h, const double* hu, const double
                         std::to_string(rkb::kNoAllocMaxRows) + " rows");
     return -2;
   }
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return -1;
-  double* scratch = rkb::scratch_address(dev);
-  if (!scratch) return -1;
+  double* scratch = rkb::scratch_address();
+  if (!scratch) {
+    rkb::set_last_error("rkb_compute_timestep_noalloc: no device address for the scratch array");
+    return -1;
+  }
   rkb::Grid g = rkb::make_grid(nx_total, ny_total, nghost, ld, dx, dy);
   const int rows = g.ny_phys();
   const int warps_per_block = 8;

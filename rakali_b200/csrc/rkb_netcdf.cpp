@@ -8,6 +8,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <string>
 #include <vector>
 
 namespace rkb {
@@ -18,6 +19,7 @@ constexpr uint32_t kDimTag = 0x0A, kVarTag = 0x0B, kAttTag = 0x0C;
 constexpr uint32_t kChar = 2, kShort = 3, kInt = 4, kFloat = 5, kDouble = 6, kByte = 1;
 
 uint32_t pad4(uint32_t n) { return (n + 3u) & ~3u; }
+uint64_t pad4_64(uint64_t n) { return (n + 3ull) & ~3ull; }
 
 // ---- writer -----------------------------------------------------------------
 
@@ -118,7 +120,7 @@ struct In {
       const uint32_t type = u32(), nel = u32();
       const uint32_t sz = type == kByte || type == kChar ? 1 : type == kShort ? 2 :
                           type == kDouble ? 8 : 4;
-      const uint64_t bytes = pad4(nel * sz);
+      const uint64_t bytes = pad4_64((uint64_t)nel * sz);
       if (o + bytes > n) { ok = false; return; }
       o += bytes;
     }
@@ -268,7 +270,9 @@ bool write_classic(const std::string& path,
       for (const auto& a : v.atts) hd.text_att(a.first, a.second);
     }
     hd.u32(v.type);
-    const uint64_t sz = pad4((uint32_t)(v.count * (v.type == kChar ? 1 : 8)));
+    // sizes in 64 bits: a 64-bit-offset file stores each variable's size in
+    // 32 bits, so anything from 4 GiB - 4 on is refused before narrowing
+    const uint64_t sz = pad4_64((uint64_t)v.count * (v.type == kChar ? 1u : 8u));
     if (sz >= 0xFFFFFFFCull) {
       err = "variable " + v.name + " too large for a 64-bit-offset NetCDF file";
       return false;
@@ -354,6 +358,11 @@ bool write_checkpoint(const std::string& path, int nxt, int nyt, const double* c
   // the file's (x_total, y_total) order has y fastest: the transpose of the
   // Fortran-order arrays
   const size_t n = (size_t)nxt * (size_t)nyt;
+  if ((uint64_t)n * 8u >= 0xFFFFFFFCull) {  // checked before the fields are read
+    err = "checkpoint fields of " + std::to_string(nxt) + " x " + std::to_string(nyt) +
+          " cells are too large for a 64-bit-offset NetCDF file";
+    return false;
+  }
   std::vector<std::vector<double>> t(7, std::vector<double>(n));
   for (int v = 0; v < 7; ++v)
     for (int j = 0; j < nyt; ++j)

@@ -67,6 +67,27 @@ def test_stencils_match_the_reference_rules(lib, nx, ny, ng, dx, dy):
     assert got == ref
 
 
+def test_non_finite_and_huge_stations_are_dropped(lib):
+    """NaN, infinite and out-of-range coordinates lie outside the domain:
+    those stations get no stencil, and the finite ones around them keep
+    theirs."""
+    nx, ny, ng, dx, dy = 10, 8, 2, 5.0, 5.0
+    xs = [np.nan, 12.0, np.inf, -np.inf, 1e300, -1e300, 21.0, 3.0e10]
+    ys = [10.0, np.nan, 10.0, 10.0, 10.0, 10.0, 12.5, 10.0]
+    x, y = np.array(xs), np.array(ys)
+    n = len(xs)
+    st, i0, j0 = (np.zeros(n, dtype=np.int32) for _ in range(3))
+    wx, wy = np.zeros(n), np.zeros(n)
+    got_n = lib.rkb_gauge_stencils(nx, ny, ng, dx, dy, x.ctypes.data_as(DP), y.ctypes.data_as(DP),
+                                   n, st.ctypes.data_as(IP), i0.ctypes.data_as(IP),
+                                   j0.ctypes.data_as(IP), wx.ctypes.data_as(DP),
+                                   wy.ctypes.data_as(DP))
+    ref = _stencils_ref(nx, ny, ng, dx, dy, [21.0], [12.5])
+    assert got_n == 1
+    assert (int(st[0]), int(i0[0]), int(j0[0]), float(wx[0]), float(wy[0])) == \
+        (6,) + tuple(ref[0][1:])
+
+
 def test_bad_arguments(lib):
     z = np.zeros(1)
     zi = np.zeros(1, dtype=np.int32)

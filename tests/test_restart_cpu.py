@@ -204,3 +204,29 @@ def test_checkpoint_file_layout_reads_in_scipy(lib, tmp_path):
         assert (int(at["nx_total"]), int(at["ny_total"])) == (nxt, nyt)
     assert lib.rkb_checkpoint_write(str(path).encode(), 0, nyt, fields, _p(scal),
                                     cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int))) == -2
+    # counts that disagree with the extents (nx_total = nx_phys + 2 nghost),
+    # a zero ghost width and negative counts are refused
+    IP = ctypes.POINTER(ctypes.c_int)
+    for bad in ([42, nxt - 2, nyt - 4, 2], [42, nxt - 4, nyt - 4, 3], [42, nxt, nyt, 0],
+                [42, -1, nyt - 4, 2]):
+        b = np.array(bad, dtype=np.int32)
+        assert lib.rkb_checkpoint_write(str(tmp_path / "bad.nc").encode(), nxt, nyt, fields,
+                                        _p(scal), b.ctypes.data_as(IP)) == -2, bad
+    assert not (tmp_path / "bad.nc").exists()
+
+
+def test_checkpoint_too_large_for_the_format_is_refused(lib, tmp_path):
+    """A field of 4 GiB or more cannot be described by a 64-bit-offset file
+    (32-bit variable sizes): the writer refuses it before reading any field,
+    and writes no file.  The arrays passed here are one element long; the
+    writer must not touch them."""
+    n = 23171  # 23171^2 doubles = 4.295e9 bytes > 2^32
+    dummy = [np.zeros(1) for _ in range(7)]
+    fields = (DP * 7)(*[_p(a) for a in dummy])
+    scal = np.zeros(7)
+    cnt = np.array([0, n - 4, n - 4, 2], dtype=np.int32)
+    path = tmp_path / "huge.nc"
+    assert lib.rkb_checkpoint_write(str(path).encode(), n, n, fields, _p(scal),
+                                    cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int))) == -1
+    assert not path.exists()
+    assert b"too large" in lib.rki_last_error()
