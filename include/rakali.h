@@ -327,6 +327,99 @@ int rkb_compute_timestep(const double *h, const double *hu, const double *hv, in
                          int ny_total, int nghost, int ld, double dx, double dy, double cfl,
                          double *dt_out);
 
+/* The remaining structured kernels of src/core/coastal, one entry point each,
+ * on caller-owned device arrays in the same layout.  Each updates the
+ * interior cells nghost .. n_total - nghost - 1 in place, with the
+ * reference's arithmetic (bit-identical results); ghosts are left as they
+ * are.  Optional forcing arrays (wind_x, wind_y, atm, precip) may be NULL
+ * only when forcing_active is 0.  Returns 0, -2 for bad arguments, -1 for a
+ * CUDA error. */
+
+/* fused_update_stage1 (rki_kernel_fused.F90:164-303): (h0, hu0, hv0) <- U,
+ * U <- U + dt F, clamp / KP07 / Froude backstop, Manning friction, wind,
+ * pressure gradient, Coriolis rotation, precipitation. */
+int rkb_fused_update_stage1(double *h, double *hu, double *hv, double *h0, double *hu0,
+                            double *hv0, const double *flux_h, const double *flux_hu,
+                            const double *flux_hv, int nx_total, int ny_total, int nghost, int ld,
+                            double dx, double dy, double dt, double manning_n,
+                            const double *wind_x, const double *wind_y, const double *atm,
+                            const double *precip, double coriolis_f, int forcing_active);
+/* fused_update_stage2 (rki_kernel_fused.F90:305-471): the stage-1 update
+ * without the save, then U <- (U0 + U) / 2 and a second clamp. */
+int rkb_fused_update_stage2(double *h, double *hu, double *hv, const double *h0,
+                            const double *hu0, const double *hv0, const double *flux_h,
+                            const double *flux_hu, const double *flux_hv, int nx_total,
+                            int ny_total, int nghost, int ld, double dx, double dy, double dt,
+                            double manning_n, const double *wind_x, const double *wind_y,
+                            const double *atm, const double *precip, double coriolis_f,
+                            int forcing_active);
+/* fused_update_stage_generic (rki_kernel_fused.F90:22-162): one Euler stage
+ * of the selectable schemes (dt = beta_k dt_step), no save, no average. */
+int rkb_fused_update_stage_generic(double *h, double *hu, double *hv, const double *flux_h,
+                                   const double *flux_hu, const double *flux_hv, int nx_total,
+                                   int ny_total, int nghost, int ld, double dx, double dy,
+                                   double dt, double manning_n, const double *wind_x,
+                                   const double *wind_y, const double *atm,
+                                   const double *precip, double coriolis_f, int forcing_active);
+/* compute_update (rki_kernel_update.F90:35-96): U <- U + dt F, then clamp. */
+int rkb_compute_update(double *h, double *hu, double *hv, const double *flux_h,
+                       const double *flux_hu, const double *flux_hv, int nx_total, int ny_total,
+                       int nghost, int ld, double dt);
+/* compute_rk2_average (rki_kernel_update.F90:98-150): U <- (U0 + U) / 2,
+ * then clamp. */
+int rkb_compute_rk2_average(double *h, double *hu, double *hv, const double *h0,
+                            const double *hu0, const double *hv0, int nx_total, int ny_total,
+                            int nghost, int ld);
+/* compute_ssp_combine (rki_kernel_update.F90:152-208):
+ * U <- a_n U0 + (1 - a_n) U, then clamp. */
+int rkb_compute_ssp_combine(double *h, double *hu, double *hv, const double *h0,
+                            const double *hu0, const double *hv0, double a_n, int nx_total,
+                            int ny_total, int nghost, int ld);
+/* apply_friction (rki_kernel_friction.F90:16-113): semi-implicit Manning
+ * friction, then (forcing_active) wind stress (include_wind), pressure
+ * gradient and precipitation; the reference's optional forcing_active and
+ * include_wind default to 1 there and are explicit here. */
+int rkb_apply_friction(double *h, double *hu, double *hv, int nx_total, int ny_total, int nghost,
+                       int ld, double dx, double dy, double dt, double manning_n,
+                       const double *wind_x, const double *wind_y, const double *atm,
+                       const double *precip, int forcing_active, int include_wind);
+/* apply_coriolis (rki_kernel_friction.F90:115-152): exact rotation of
+ * (hu, hv) by f dt in wet cells. */
+int rkb_apply_coriolis(const double *h, double *hu, double *hv, int nx_total, int ny_total,
+                       int nghost, int ld, double dt, double f);
+
+/* bc_params_t (src/core/structured/rki_boundary_types.F90:38-100) as the
+ * boundary and sponge kernels read it.  type[]: west, east, south, north,
+ * 1 wall, 2 open, 3 tidal, 4 nested, 5 inflow, 6 discharge, 7 clamped,
+ * 8 sponge, 9 chapman (rki_boundary_types.F90:19-36).  eta_old[]: the
+ * Chapman surfaces of the four edges, device arrays of ny_total (W, E) or
+ * nx_total (S, N) doubles, read and refreshed by the fill (NULL where the
+ * edge is not Chapman). */
+#define RKB_MAX_TIDAL 10
+typedef struct {
+  int type[4];
+  int n_tidal;
+  int sponge_width;
+  double tidal_amplitude, tidal_period;
+  double tidal_amp[RKB_MAX_TIDAL], tidal_phase[RKB_MAX_TIDAL], tidal_omega[RKB_MAX_TIDAL];
+  double inflow_velocity, discharge_flux, clamped_elevation;
+  double sponge_strength, sponge_h_ref;
+  double time;  /* bc%time: the boundary clock of this fill */
+  double dt;    /* bc%dt: the step the Chapman condition uses */
+  double *eta_old[4];
+} rkb_bc_params;
+
+/* apply_boundary_conditions (rki_boundary.F90:40-218): ghost layers of the
+ * W, E, S, N edges in that order; wall and sponge edges also mirror the bed
+ * b into their ghosts. */
+int rkb_apply_boundary_conditions(double *h, double *hu, double *hv, double *b, int nx_total,
+                                  int ny_total, int nghost, int ld, double dx, double dy,
+                                  const rkb_bc_params *bc);
+/* apply_sponge (rki_kernel_sponge.F90:16-88): relaxation towards
+ * (sponge_h_ref, 0, 0) within sponge_width cells of sponge edges. */
+int rkb_apply_sponge(double *h, double *hu, double *hv, int nx_total, int ny_total, int nghost,
+                     int ld, double dt, const rkb_bc_params *bc);
+
 /* No counterpart in the reference.  The same dt as rkb_compute_timestep for
  * callers that cannot allocate device memory when they need it: a host
  * application whose memory pool already owns the GPU, or a driver loop that

@@ -129,6 +129,15 @@ def lib():
             [_DP] * 4 + [ctypes.c_double, ctypes.c_int]
         L.orc_fused_stage1.argtypes = stage_args
         L.orc_fused_stage2.argtypes = stage_args
+        L.orc_fused_stage_generic.argtypes = stage_args[:3] + stage_args[6:]
+        I3 = [ctypes.c_int] * 3
+        L.orc_compute_update.argtypes = [_DP] * 6 + I3 + [ctypes.c_double]
+        L.orc_rk2_average.argtypes = [_DP] * 6 + I3
+        L.orc_ssp_combine.argtypes = [_DP] * 6 + [ctypes.c_double] + I3
+        L.orc_apply_friction.argtypes = [_DP] * 3 + I3 + [ctypes.c_double] * 4 + [_DP] * 4 + \
+            [ctypes.c_int, ctypes.c_int]
+        L.orc_apply_coriolis.argtypes = [_DP] * 3 + I3 + [ctypes.c_double] * 2
+        L.orc_apply_sponge.argtypes = [_DP] * 3 + I3 + [ctypes.c_double, ctypes.POINTER(_Bc)]
         L.orc_apply_bc.argtypes = [_DP] * 4 + [ctypes.c_int] * 3 + [ctypes.POINTER(_Bc)]
         L.orc_tidal_eta.argtypes = [ctypes.POINTER(_Bc)]
         L.orc_tidal_eta.restype = ctypes.c_double
@@ -317,6 +326,69 @@ def fused_stage(stage, h, hu, hv, h0, hu0, hv0, fh, fhu, fhv, ng, dt, manning_n=
     fn(ptr(h), ptr(hu), ptr(hv), ptr(h0), ptr(hu0), ptr(hv0), ptr(fh), ptr(fhu), ptr(fhv),
        nx, ny, int(ng), float(dx), float(dy), float(dt), float(manning_n), ptr(wx), ptr(wy),
        ptr(ap), ptr(pr), float(coriolis_f), int(bool(forcing_active)))
+
+
+def fused_stage_generic(h, hu, hv, fh, fhu, fhv, ng, dt, manning_n=0.0, wind_x=None,
+                        wind_y=None, atm=None, precip=None, coriolis_f=0.0,
+                        forcing_active=False, dx=1.0, dy=1.0):
+    """fused_update_stage_generic (rki_kernel_fused.F90:22-162) in place."""
+    nx, ny = h.shape
+    z = np.zeros((nx, ny), order="F")
+    f = [z if a is None else a for a in (wind_x, wind_y, atm, precip)]
+    lib().orc_fused_stage_generic(ptr(h), ptr(hu), ptr(hv), ptr(fh), ptr(fhu), ptr(fhv), nx, ny,
+                                  int(ng), float(dx), float(dy), float(dt), float(manning_n),
+                                  *(ptr(a) for a in f), float(coriolis_f),
+                                  int(bool(forcing_active)))
+
+
+def compute_update(h, hu, hv, fh, fhu, fhv, ng, dt):
+    """compute_update (rki_kernel_update.F90:35-96) in place."""
+    nx, ny = h.shape
+    lib().orc_compute_update(*(ptr(a) for a in (h, hu, hv, fh, fhu, fhv)), nx, ny, int(ng),
+                             float(dt))
+
+
+def rk2_average(h, hu, hv, h0, hu0, hv0, ng):
+    """compute_rk2_average (rki_kernel_update.F90:98-150) in place."""
+    nx, ny = h.shape
+    lib().orc_rk2_average(*(ptr(a) for a in (h, hu, hv, h0, hu0, hv0)), nx, ny, int(ng))
+
+
+def ssp_combine(h, hu, hv, h0, hu0, hv0, a_n, ng):
+    """compute_ssp_combine (rki_kernel_update.F90:152-208) in place."""
+    nx, ny = h.shape
+    lib().orc_ssp_combine(*(ptr(a) for a in (h, hu, hv, h0, hu0, hv0)), float(a_n), nx, ny,
+                          int(ng))
+
+
+def apply_friction(h, hu, hv, ng, dt, manning_n, wind_x=None, wind_y=None, atm=None,
+                   precip=None, forcing_active=False, include_wind=True, dx=1.0, dy=1.0):
+    """apply_friction (rki_kernel_friction.F90:16-113) in place."""
+    nx, ny = h.shape
+    z = np.zeros((nx, ny), order="F")
+    f = [z if a is None else a for a in (wind_x, wind_y, atm, precip)]
+    lib().orc_apply_friction(ptr(h), ptr(hu), ptr(hv), nx, ny, int(ng), float(dx), float(dy),
+                             float(dt), float(manning_n), *(ptr(a) for a in f),
+                             int(bool(forcing_active)), int(bool(include_wind)))
+
+
+def apply_coriolis(h, hu, hv, ng, dt, f):
+    """apply_coriolis (rki_kernel_friction.F90:115-152) in place."""
+    nx, ny = h.shape
+    lib().orc_apply_coriolis(ptr(h), ptr(hu), ptr(hv), nx, ny, int(ng), float(dt), float(f))
+
+
+def apply_sponge(h, hu, hv, ng, dt, west="wall", east="wall", south="wall", north="wall",
+                 sponge_width=0, sponge_strength=0.0, sponge_h_ref=0.0):
+    """apply_sponge (rki_kernel_sponge.F90:16-88) in place."""
+    nx, ny = h.shape
+    bc = _Bc()
+    bc.west, bc.east = BC_CODES[west], BC_CODES[east]
+    bc.south, bc.north = BC_CODES[south], BC_CODES[north]
+    bc.sponge_width, bc.sponge_strength, bc.sponge_h_ref = sponge_width, sponge_strength, \
+        sponge_h_ref
+    lib().orc_apply_sponge(ptr(h), ptr(hu), ptr(hv), nx, ny, int(ng), float(dt),
+                           ctypes.byref(bc))
 
 
 def compute_timestep(h, hu, hv, ng, dx, dy, cfl):

@@ -529,11 +529,12 @@ void orc_ssp_combine(double *h, double *hu, double *hv, const double *h0, const 
   }
 }
 
-/* rki_kernel_friction.F90:16-113 */
+/* rki_kernel_friction.F90:16-113 (forcing_active and include_wind are the
+ * reference's optional arguments, default .true.) */
 void orc_apply_friction(double *h, double *hu, double *hv, int nx, int ny, int ng, double dx,
                         double dy, double dt, double manning_n, const double *wind_x,
                         const double *wind_y, const double *atm, const double *precip,
-                        int forcing_active) {
+                        int forcing_active, int include_wind) {
   int has_fric = manning_n > 0.0;
   if (!has_fric && !forcing_active) return;
   for (int j = ng; j < ny - ng; ++j) {
@@ -550,8 +551,10 @@ void orc_apply_friction(double *h, double *hu, double *hv, int nx, int ny, int n
           AT(hv, i, j) = AT(hv, i, j) / den;
         }
         if (forcing_active) {
-          AT(hu, i, j) = AT(hu, i, j) + dt * AT(wind_x, i, j) / RHO;
-          AT(hv, i, j) = AT(hv, i, j) + dt * AT(wind_y, i, j) / RHO;
+          if (include_wind) { /* :89-94, skipped when wind goes to the surface layer */
+            AT(hu, i, j) = AT(hu, i, j) + dt * AT(wind_x, i, j) / RHO;
+            AT(hv, i, j) = AT(hv, i, j) + dt * AT(wind_y, i, j) / RHO;
+          }
           double dpdx = (AT(atm, i + 1, j) - AT(atm, i - 1, j)) / (2.0 * dx);
           double dpdy = (AT(atm, i, j + 1) - AT(atm, i, j - 1)) / (2.0 * dy);
           AT(hu, i, j) = AT(hu, i, j) - dt * hval * dpdx / RHO;

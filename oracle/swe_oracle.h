@@ -110,7 +110,7 @@ void orc_ssp_combine(double *h, double *hu, double *hv, const double *h0, const 
 void orc_apply_friction(double *h, double *hu, double *hv, int nx, int ny, int ng, double dx,
                         double dy, double dt, double manning_n, const double *wind_x,
                         const double *wind_y, const double *atm, const double *precip,
-                        int forcing_active);
+                        int forcing_active, int include_wind);
 void orc_apply_coriolis(const double *h, double *hu, double *hv, int nx, int ny, int ng,
                         double dt, double f);
 

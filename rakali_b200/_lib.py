@@ -41,6 +41,25 @@ def header_symbols() -> list[str]:
     return re.findall(r"\b(rk[ib]_\w+)\s*\(", text)
 
 
+MAX_TIDAL = 10
+
+
+class BcParams(ctypes.Structure):
+    """rkb_bc_params of include/rakali.h (the reference's bc_params_t as the
+    boundary and sponge kernels read it)."""
+    _fields_ = [
+        ("type", ctypes.c_int * 4), ("n_tidal", ctypes.c_int), ("sponge_width", ctypes.c_int),
+        ("tidal_amplitude", ctypes.c_double), ("tidal_period", ctypes.c_double),
+        ("tidal_amp", ctypes.c_double * MAX_TIDAL), ("tidal_phase", ctypes.c_double * MAX_TIDAL),
+        ("tidal_omega", ctypes.c_double * MAX_TIDAL),
+        ("inflow_velocity", ctypes.c_double), ("discharge_flux", ctypes.c_double),
+        ("clamped_elevation", ctypes.c_double),
+        ("sponge_strength", ctypes.c_double), ("sponge_h_ref", ctypes.c_double),
+        ("time", ctypes.c_double), ("dt", ctypes.c_double),
+        ("eta_old", ctypes.c_void_p * 4),
+    ]
+
+
 def _sig(lib, name, args, res):
     f = getattr(lib, name)
     f.argtypes = args
@@ -147,6 +166,20 @@ def load(path: str | None = None):
     _sig(lib, "rkb_compute_flux", [I, H, H, H, H, H, H, H, H, H, I, I, I, I, D, D], I)
     _sig(lib, "rkb_compute_timestep", [H, H, H, I, I, I, I, D, D, D, DP], I)
     _sig(lib, "rkb_compute_timestep_noalloc", [H, H, H, I, I, I, I, D, D, D, DP], I)
+    # kernel-level structured kernels (device pointers as c_void_p)
+    G4 = [I, I, I, I]  # nx_total, ny_total, nghost, ld
+    stage_tail = [D, D, D, D, H, H, H, H, D, I]  # dx dy dt n  wx wy atm pr  f forcing
+    _sig(lib, "rkb_fused_update_stage1", [H] * 9 + G4 + stage_tail, I)
+    _sig(lib, "rkb_fused_update_stage2", [H] * 9 + G4 + stage_tail, I)
+    _sig(lib, "rkb_fused_update_stage_generic", [H] * 6 + G4 + stage_tail, I)
+    _sig(lib, "rkb_compute_update", [H] * 6 + G4 + [D], I)
+    _sig(lib, "rkb_compute_rk2_average", [H] * 6 + G4, I)
+    _sig(lib, "rkb_compute_ssp_combine", [H] * 6 + [D] + G4, I)
+    _sig(lib, "rkb_apply_friction", [H] * 3 + G4 + [D] * 4 + [H] * 4 + [I, I], I)
+    _sig(lib, "rkb_apply_coriolis", [H] * 3 + G4 + [D, D], I)
+    BP = ctypes.POINTER(BcParams)
+    _sig(lib, "rkb_apply_boundary_conditions", [H] * 4 + G4 + [D, D, BP], I)
+    _sig(lib, "rkb_apply_sponge", [H] * 3 + G4 + [D, BP], I)
     if lib.rki_working_precision() != 8:
         raise RuntimeError("librakali.so must be the FP64 build")
     lib.wp_dtype = np.float64

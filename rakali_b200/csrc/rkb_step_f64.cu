@@ -12,6 +12,8 @@
 // stage-2 epilogue; the first launch of the next step turns it into dt.
 // The boundary mass-out sums (rki_solver.F90:507-537) are per-block partials
 // reduced in a fixed order by the last block of stage 2.
+#include "rkb_bc.cuh"
+#include "rkb_cell.cuh"
 #include "rkb_crmath.cuh"
 #include "rkb_face.cuh"
 #include "rkb_kernels.h"
@@ -63,15 +65,7 @@ __device__ __forceinline__ void bc_body(const StepArgs& a, int stage, int w, int
     ctl->dt = dt;
   }
   if (!active) return;
-  const int type = bc->type[w];
-  if (type == kNested) return;
-  const Edge e = make_edge(w, g);
-  if (t >= e.n_tan) return;
   const FieldSet U0 = a.U0, U1 = a.U1, S = a.S;
-  double* eta_old_w = a.eta_old[0];
-  double* eta_old_e = a.eta_old[1];
-  double* eta_old_s = a.eta_old[2];
-  double* eta_old_n = a.eta_old[3];
 
   const int cur = ctl->cur;
   const int wide = g.ng > 2 ? g.ng : 2;
@@ -103,127 +97,8 @@ __device__ __forceinline__ void bc_body(const StepArgs& a, int stage, int w, int
     else if (narrow)
       also(S);
   }
-  double* h = F.h;
-  double* hu = F.hu;
-  double* hv = F.hv;
-
-  // ghost (k) and first interior cell along the inward normal
-  const int ii = e.ig0 + t * e.dit - e.din;
-  const int ji = e.jg0 + t * e.djt - e.djn;
-
-  auto put = [&](int ig, int jg, double vh, double vu, double vv) {
-    const size_t q = g.at(ig, jg);
-    h[q] = vh; hu[q] = vu; hv[q] = vv;
-    if (h2) { h2[q] = vh; hu2[q] = vu; hv2[q] = vv; }
-  };
-
-  if (type == kWall || type == kSponge) {
-    // bc_wall_edge :220-291 (bed and surface mirrored, normal momentum negated)
-    for (int k = 1; k <= g.ng; ++k) {
-      const int ig = e.ig0 + (k - 1) * e.din + t * e.dit;
-      const int jg = e.jg0 + (k - 1) * e.djn + t * e.djt;
-      const int im = ig - (2 * k - 1) * e.din;
-      const int jm = jg - (2 * k - 1) * e.djn;
-      const size_t m = g.at(im, jm);
-      const double bm = b[m];
-      b[g.at(ig, jg)] = bm;
-      const double vh = pos(h[m] + bm - bm);
-      double vu, vv;
-      if (e.normal_u) { vu = -hu[m]; vv = hv[m]; } else { vv = -hv[m]; vu = hu[m]; }
-      put(ig, jg, vh, vu, vv);
-    }
-    return;
-  }
-
-  const size_t qi = g.at(ii, ji);
-  const double hi = h[qi];
-  const double qu = hu[qi];
-  const double qv = hv[qi];
-  if (type == kOpen || type == kTidal) {
-    // bc_flather_edge :293-345
-    const bool prescribe = type == kTidal;
-    const double eta_ext = prescribe ? tidal_eta(bc, time) : 0.0;
-    const double ei = hi + b[qi];
-    const double hmax = dmax(hi, 1.0e-6);
-    const double c = sqrt(kG * hmax);
-    for (int k = 1; k <= g.ng; ++k) {
-      const int ig = e.ig0 + (k - 1) * e.din + t * e.dit;
-      const int jg = e.jg0 + (k - 1) * e.djn + t * e.djt;
-      const double hg = prescribe ? pos(eta_ext - b[g.at(ig, jg)]) : hi;
-      if (e.normal_u)
-        put(ig, jg, hg, hg * (qu / hmax + e.sgn * c * (ei - eta_ext) / hmax), qv);
-      else
-        put(ig, jg, hg, qu, hg * (qv / hmax + e.sgn * c * (ei - eta_ext) / hmax));
-    }
-  } else if (type == kInflow) {
-    // bc_inflow_edge :347-390
-    const double in_sgn = -e.sgn;
-    for (int k = 1; k <= g.ng; ++k) {
-      const int ig = e.ig0 + (k - 1) * e.din + t * e.dit;
-      const int jg = e.jg0 + (k - 1) * e.djn + t * e.djt;
-      if (e.normal_u)
-        put(ig, jg, hi, in_sgn * hi * bc->inflow_velocity, qv);
-      else
-        put(ig, jg, hi, qu, in_sgn * hi * bc->inflow_velocity);
-    }
-  } else if (type == kDischarge) {
-    // bc_disch_edge :392-434
-    const double in_sgn = -e.sgn;
-    for (int k = 1; k <= g.ng; ++k) {
-      const int ig = e.ig0 + (k - 1) * e.din + t * e.dit;
-      const int jg = e.jg0 + (k - 1) * e.djn + t * e.djt;
-      if (e.normal_u)
-        put(ig, jg, hi, in_sgn * bc->discharge_flux, qv);
-      else
-        put(ig, jg, hi, qu, in_sgn * bc->discharge_flux);
-    }
-  } else if (type == kClamped) {
-    // bc_clamped_edge :436-469
-    for (int k = 1; k <= g.ng; ++k) {
-      const int ig = e.ig0 + (k - 1) * e.din + t * e.dit;
-      const int jg = e.jg0 + (k - 1) * e.djn + t * e.djt;
-      put(ig, jg, pos(bc->clamped_elevation - b[g.at(ig, jg)]), qu, qv);
-    }
-  } else if (type == kChapman) {
-    // bc_chapman_edge :471-552; every layer reads the surface stored before
-    // this call, then position t's surface is refreshed once.
-    double* eo = w == 0 ? eta_old_w : w == 1 ? eta_old_e : w == 2 ? eta_old_s : eta_old_n;
-    const double dd = e.normal_u ? g.dx : g.dy;
-    // The reference fills the ghosts once more before computing dt
-    // (rki_solver.F90:719); for Chapman that extra call refreshes the stored
-    // surface to the current interior one, which the first stage then sees.
-    const double ei0 = hi + b[qi];
-    const double eov = (stage == 1 || stage == 10) ? ei0 : eo[t];
-    const double ei = hi + b[qi];
-    const double hmax = dmax(hi, 1.0e-6);
-    const double c = sqrt(kG * hmax);
-    const int i2 = ii - e.din;
-    const int j2 = ji - e.djn;
-    double eg;
-    if (dtb > 0.0) {
-      const double detadt = (ei - eov) / dtb;
-      double detadx = 0.0;
-      if (i2 >= 0 && i2 < g.nxt && j2 >= 0 && j2 < g.nyt) {
-        const size_t q2 = g.at(i2, j2);
-        detadx = (h[q2] + b[q2] - ei) / dd;
-      }
-      double cp = fabs(detadx) > 1.0e-10 ? -detadt / detadx : 0.0;
-      cp = pos(dmin(cp, c));
-      eg = eov - cp * dtb / dd * (eov - ei);
-    } else {
-      eg = ei;
-    }
-    for (int k = 1; k <= g.ng; ++k) {
-      const int ig = e.ig0 + (k - 1) * e.din + t * e.dit;
-      const int jg = e.jg0 + (k - 1) * e.djn + t * e.djt;
-      const double hg = pos(eg - b[g.at(ig, jg)]);
-      if (e.normal_u)
-        put(ig, jg, hg, hg * (qu / hmax + e.sgn * c * (ei - eg) / hmax), qv);
-      else
-        put(ig, jg, hg, qu, hg * (qv / hmax + e.sgn * c * (ei - eg) / hmax));
-    }
-    eo[t] = ei;
-  }
+  double* eo = a.eta_old[w];
+  fill_edge(g, bc, b, F, h2, hu2, hv2, w, t, time, dtb, eo, stage == 1 || stage == 10);
 }
 
 // Edges [e0, e0 + gridDim.y) of one simulation.
@@ -305,50 +180,6 @@ struct StageSmem {
   static constexpr int DOUBLES = 5 * NT + 3 * NSX + 3 * NSY + 6 * NFX + 6 * NFY;
   static constexpr size_t BYTES = sizeof(double) * (size_t)DOUBLES;
 };
-
-// Pointwise sources after the Euler update: Manning friction, wind,
-// pressure gradient, Coriolis, precipitation (rki_kernel_fused.F90:121-154).
-__device__ __forceinline__ void sources(double& h, double& u, double& v, const Physics* p, double dt,
-                                        double n_sq, double cosf, double sinf, bool has_cor,
-                                        const Grid& g, int i, int j, const Forcing& fo) {
-  if (h > kDry) {
-    if (p->manning_n > 0.0) {
-      const double uu = u / h;
-      const double vv = v / h;
-      const double speed = sqrt(uu * uu + vv * vv);
-      const double cf = kG * n_sq / cr_pow_third(h);
-      const double den = 1.0 + dt * cf * speed / h;
-      u = u / den;
-      v = v / den;
-    }
-    if (p->forcing_active) {
-      const size_t q = g.at(i, j);
-      u = u + dt * fo.wind_x[q] / kRho;
-      v = v + dt * fo.wind_y[q] / kRho;
-      const double dpdx = (fo.atm[g.at(i + 1, j)] - fo.atm[g.at(i - 1, j)]) / (2.0 * g.dx);
-      const double dpdy = (fo.atm[g.at(i, j + 1)] - fo.atm[g.at(i, j - 1)]) / (2.0 * g.dy);
-      u = u - dt * h * dpdx / kRho;
-      v = v - dt * h * dpdy / kRho;
-    }
-    if (has_cor) {
-      const double uo = u, vo = v;
-      u = uo * cosf + vo * sinf;
-      v = -(uo * sinf) + vo * cosf;
-    }
-  }
-  if (p->forcing_active) h = h + dt * fo.precip[g.at(i, j)];
-}
-
-// Sponge relaxation of interior cell (i, j) (rki_kernel_sponge.F90:16-88).
-__device__ __forceinline__ void sponge(double& h, double& u, double& v, const BcParams* bc,
-                                       const Grid& g, int i, int j, double dt) {
-  const double alpha = sponge_alpha(bc, g, i, j);
-  if (alpha > 0.0) {
-    h = h - dt * alpha * (h - bc->sponge_h_ref);
-    u = u - dt * alpha * u;
-    v = v - dt * alpha * v;
-  }
-}
 
 // STAGE 1: U^n (buffer cur) -> U* (scratch S).
 // STAGE 2: U* (S) and U^n (buffer cur) -> U^{n+1} (buffer cur^1).

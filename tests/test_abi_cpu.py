@@ -2,15 +2,20 @@
 
 * librakali.so loads and exports every function include/rakali.h declares;
 * it exports every symbol the reference's Python wrapper binds at import
-  (python/rakali/_core.py:88-283) - and, when the reference package is
-  present in this environment, its unmodified loader binds our library;
+  (python/rakali/_core.py:88-283), declared in include/rakali.h with the
+  argument and result types of the reference's ctypes signatures (recorded
+  in tests/golden/frontend_bindings.json) - and, when RAKALI_REFERENCE_PYTHON
+  names the reference's python/ directory, its unmodified loader binds our
+  library;
 * namelist parsing/validation behaves like the reference's strict schema
   (src/core/rki_config.F90), returning error codes instead of stopping;
 * keyword validation raises ValueError like the reference front end
   (python/tests/test_robustness.py:49-72).
 """
 import ctypes
+import json
 import os
+import re
 import subprocess
 import sys
 from pathlib import Path
@@ -20,19 +25,34 @@ import pytest
 
 ROOT = Path(__file__).resolve().parent.parent
 
-# python/rakali/_core.py:88-283
-REFERENCE_BINDS = """rki_working_precision rki_create rki_finalize rki_create_from_namelist
-rki_create_from_string rki_create_from_namelist_string rki_destroy rki_step rki_advance
-rki_get_time rki_get_dt rki_get_step_count rki_get_nz_ml rki_get_grid_info rki_get_h_ptr
-rki_get_hu_ptr rki_get_hv_ptr rki_get_b_ptr rki_get_h0_ptr rki_get_hu0_ptr rki_get_hv0_ptr
-rki_get_clamped_elevation rki_get_manning_n rki_get_coriolis_f rki_get_h_layer_ptr
-rki_get_hu_layer_ptr rki_get_hv_layer_ptr rki_get_salinity_ptr rki_get_temperature_ptr
-rki_set_bathymetry rki_set_initial_h rki_set_wind rki_set_atm_pressure rki_set_precipitation
-rki_set_heat_flux rki_set_evap_minus_precip rki_set_h rki_set_hu rki_set_hv rki_set_salinity
-rki_set_temperature rki_sync_host rki_sync_from_device rki_save_restart rki_load_restart
-rki_set_inflow_velocity rki_set_inflow_salinity rki_set_inflow_temperature
-rki_set_discharge_flux rki_set_clamped_elevation rki_set_use_ppm_tracer rki_set_use_hllc
-rki_set_tidal_constituents""".split()
+# The signatures the reference's own loader binds (python/rakali/_core.py:
+# 88-283), recorded by tests/golden/make_frontend_bindings.py.
+BINDINGS = json.loads((ROOT / "tests" / "golden" / "frontend_bindings.json").read_text())
+REFERENCE_BINDS = sorted(BINDINGS["functions"])
+
+# C spelling of the ctypes types the reference binds with.
+_C_OF = {"c_int": "int", "c_double": "double", "c_void_p": "void*", "c_char_p": "char*",
+         "POINTER(c_int)": "int*", "POINTER(c_double)": "double*",
+         "POINTER(c_void_p)": "void**", "None": "void"}
+
+
+def _header_prototypes():
+    """name -> (result, [argument types]) of every function include/rakali.h
+    declares, with const, names and spacing removed."""
+    text = (ROOT / "include" / "rakali.h").read_text()
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    protos = {}
+    for m in re.finditer(r"([A-Za-z_][\w \t\*]*?)\b(r[a-z]+_\w+)\s*\(([^;{]*?)\)\s*;", text):
+        def norm(decl, drop_name):
+            decl = decl.replace("const", " ").strip()
+            stars = decl.count("*")
+            words = decl.replace("*", " ").split()
+            if drop_name and len(words) > 1:
+                words = words[:-1]
+            return " ".join(words) + "*" * stars
+        args = [a for a in m.group(3).split(",") if a.strip() and a.strip() != "void"]
+        protos[m.group(2)] = (norm(m.group(1), False), [norm(a, True) for a in args])
+    return protos
 
 
 @pytest.fixture(scope="module")
@@ -51,14 +71,36 @@ def test_header_symbols_exported(lib):
 
 def test_reference_wrapper_symbols_exported(lib):
     missing = [n for n in REFERENCE_BINDS if not hasattr(lib, n)]
+    assert len(REFERENCE_BINDS) >= 50
     assert not missing, missing
     assert lib.rki_working_precision() == 8
+    assert BINDINGS["working_precision_dtype"] == "float64"
 
 
-@pytest.mark.skipif(not Path("/root/reference/python/rakali/_core.py").is_file(),
-                    reason="reference package not present here")
+def test_header_prototypes_match_reference_bindings():
+    """Every function the reference front end binds is declared in
+    include/rakali.h with the same number, order and kind of arguments and
+    the same result type as the reference's ctypes signature."""
+    protos = _header_prototypes()
+    bad = []
+    for name, sig in BINDINGS["functions"].items():
+        if name not in protos:
+            bad.append((name, "not declared"))
+            continue
+        res, args = protos[name]
+        want = [_C_OF[t] for t in sig["argtypes"]]
+        if args != want or res != _C_OF[sig["restype"]]:
+            bad.append((name, res, args, _C_OF[sig["restype"]], want))
+    assert not bad, bad
+
+
+_REF_PY = os.environ.get("RAKALI_REFERENCE_PYTHON")
+
+
+@pytest.mark.skipif(not (_REF_PY and Path(_REF_PY, "rakali", "_core.py").is_file()),
+                    reason="RAKALI_REFERENCE_PYTHON does not name the reference's python/ directory")
 def test_unmodified_reference_loader_binds_library():
-    code = ("import sys; sys.path.insert(0, '/root/reference/python');"
+    code = (f"import sys; sys.path.insert(0, {_REF_PY!r});"
             "from rakali import _core; L = _core._load_lib();"
             "print(L._rki_wp_dtype.__name__)")
     env = dict(os.environ, RAKALI_LIB=str(ROOT / "rakali_b200" / "librakali.so"))
@@ -136,3 +178,42 @@ def test_missing_namelist_raises(tmp_path):
         Rakali(str(tmp_path / "nope.nml"))
     with pytest.raises(FileNotFoundError, match="bathymetry_file"):
         Rakali(nx=8, ny=8, dx=1.0, dy=1.0, t_end=1.0, bathymetry_file=str(tmp_path / "x.nc"))
+
+
+def test_kernel_entry_points_reject_bad_arguments_before_any_launch(lib):
+    """Argument checks of the kernel-level entry points run on the host and
+    return -2 before any CUDA call (so they need no GPU): null arrays, a ghost
+    width below 2, a leading dimension below nx_total, a bad boundary type,
+    a Chapman edge without its surface array."""
+    from rakali_b200._lib import BcParams
+    fake = ctypes.c_void_p(0x1000)  # never dereferenced: the checks fail first
+    n4 = [None] * 4
+    assert lib.rkb_compute_update(None, fake, fake, fake, fake, fake, 10, 10, 2, 10, 0.1) == -2
+    assert lib.rkb_compute_update(fake, fake, fake, fake, fake, fake, 10, 10, 1, 10, 0.1) == -2
+    assert lib.rkb_compute_rk2_average(fake, fake, fake, fake, fake, None, 10, 10, 2, 10) == -2
+    assert lib.rkb_compute_ssp_combine(fake, fake, fake, fake, fake, fake, 0.5, 10, 10, 2, 9) == -2
+    assert lib.rkb_fused_update_stage1(*([fake] * 9), 10, 10, 2, 10, 1.0, 1.0, 0.1, 0.02,
+                                       *n4, 0.0, 1) == -2  # forcing without its arrays
+    assert lib.rkb_fused_update_stage2(*([fake] * 5), None, *([fake] * 3), 10, 10, 2, 10, 1.0,
+                                       1.0, 0.1, 0.02, *n4, 0.0, 0) == -2
+    assert lib.rkb_fused_update_stage_generic(*([fake] * 6), 10, 10, 2, 10, 0.0, 1.0, 0.1, 0.0,
+                                              *n4, 0.0, 0) == -2  # dx = 0
+    assert lib.rkb_apply_friction(fake, fake, fake, 10, 10, 2, 10, 1.0, 1.0, 0.1, 0.02,
+                                  None, None, fake, fake, 1, 1) == -2
+    # nothing to do: the reference's early exits return before any launch
+    assert lib.rkb_apply_friction(fake, fake, fake, 10, 10, 2, 10, 1.0, 1.0, 0.1, 0.0,
+                                  *n4, 0, 1) == 0
+    assert lib.rkb_apply_coriolis(fake, fake, fake, 10, 10, 2, 10, 0.1, 0.0) == 0
+    p = BcParams()
+    for k in range(4):
+        p.type[k] = 1
+    p.type[2] = 12
+    assert lib.rkb_apply_boundary_conditions(fake, fake, fake, fake, 10, 10, 2, 10, 1.0, 1.0,
+                                             ctypes.byref(p)) == -2
+    p.type[2] = 9  # chapman, no surface array
+    assert lib.rkb_apply_boundary_conditions(fake, fake, fake, fake, 10, 10, 2, 10, 1.0, 1.0,
+                                             ctypes.byref(p)) == -2
+    p.type[2] = 1
+    assert lib.rkb_apply_boundary_conditions(fake, fake, fake, fake, 10, 10, 2, 10, 1.0, 1.0,
+                                             None) == -2
+    assert lib.rkb_apply_sponge(fake, fake, fake, 10, 10, 2, 10, 0.1, ctypes.byref(p)) == 0
