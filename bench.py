@@ -10,9 +10,14 @@ librakali.so.  One "step" is one full SSP-RK2 step of the grid.
 
 The headline line is the FP64 depth form (the reference's arithmetic); the
 FP32 surface form is timed on the same handle right after and reported under
-"forms" with its free-surface error against the FP64 step after
-min(K, 500) steps and the FP64 step's own drift under a 1e-7 relative
-perturbation of h (the conditioning floor of this flow).
+"forms" with its free-surface error against the FP64 step after 50 .. 1000
+steps, beside the FP64 step's own drift under 1e-7 and 1e-15 relative
+perturbations of h (the conditioning floors of this flow).  The same line
+carries the CPU baseline (the oracle on every host core, 20 steps of the
+full workload), the parity of the FP64 step with that oracle run
+(`parity_4096`), the lake-at-rest variant over 1000 steps in both forms
+(`lake_at_rest_4096`), the batched ensemble, the adjoint and the batched
+FP32 forward + adjoint of 64 x 2048^2 grids (`adjoint_fp32_batched`).
 
 N > 1 runs N independent replicas (one per rank, launched by torchrun): the
 step does not exchange data between instances, so scaling is weak and no
@@ -135,23 +140,48 @@ def traffic_per_launch(n_cells: int, precision: int = 64):
     return d["dram_bytes_per_launch"] * n_cells / d["cells"]
 
 
-def cpu_baseline(threads: int, side: int = 1024, steps: int = 2, seed: int = 2024):
-    """Oracle (OpenMP) on a side x side window of the workload family."""
+def oracle_run(b, h, n, threads: int, steps: int):
+    """The oracle (OpenMP over `threads` host threads) stepped `steps` times
+    from the workload's initial state; returns (oracle, threads used, seconds)."""
     from oracle import oracle as orc
     from rakali_b200 import workloads as wl
     used = orc.set_threads(threads)
-    b, h = wl.config2(n=side, seed=seed)
-    cfg = dict(nx=side, ny=side, **wl.CONFIG2_KW)
-    o = orc.OracleSim.from_config(cfg, bathymetry=b, initial_h=h)
-    o.step(1)  # warm-up
+    o = orc.OracleSim.from_config(dict(nx=n, ny=n, **wl.CONFIG2_KW), bathymetry=b, initial_h=h)
     t0 = time.perf_counter()
     o.step(steps)
-    dt = time.perf_counter() - t0
-    return {"value": side * side * steps / dt, "unit": "cell-updates/s", "cores": used,
+    return o, used, time.perf_counter() - t0
+
+
+def cpu_baseline_and_parity(b, h, n, steps=20):
+    """The CPU baseline on the full workload (the oracle on every host core,
+    `steps` SSP-RK2 steps from the initial state) and, from the same run, the
+    parity check of the FP64 step at full size: a fresh simulation stepped as
+    many times on the device, compared with the oracle bit for bit (ghosts
+    included)."""
+    from rakali_b200 import Rakali
+    from rakali_b200 import workloads as wl
+    o, used, secs = oracle_run(b, h, n, os.cpu_count() or 1, steps)
+    base = {"value": n * n * steps / secs, "unit": "cell-updates/s", "cores": used,
             "kind": "port",
-            "sample": f"{steps} SSP-RK2 steps of a {side}x{side} window of the 4096^2 "
-                      f"configuration (same bed family, dx = 5 m, n = 0.025), FP64, "
-                      f"{used} OpenMP threads"}
+            "sample": f"{steps} SSP-RK2 steps of the full {n}x{n} workload from its initial "
+                      f"state, FP64, {used} OpenMP threads ({secs:.1f} s)"}
+    s = Rakali(defer_init=True, nx=n, ny=n, **wl.CONFIG2_KW)
+    s.set_bathymetry(b)
+    s.set_initial_h(h)
+    s.finalize()
+    s.step(steps)
+    diff = {}
+    for name in ("h", "hu", "hv"):
+        got, want = getattr(s, name), o.arrays[name]
+        diff[name] = {"max_abs_diff": float(np.max(np.abs(got - want))),
+                      "cells_differing": int(np.sum(got != want))}
+    parity = {"workload": f"{n}x{n}, the benchmark workload, FP64", "steps": steps,
+              "bit_identical": all(d["cells_differing"] == 0 for d in diff.values()),
+              "time_equal": s.time == o.time, "dt_equal": s.dt == o.dt, "fields": diff,
+              "tolerance": "0 (bit-identical; the required bar is 1e-12 relative)"}
+    s.close()
+    del o
+    return base, parity
 
 
 FORM_DESC = {64: "FP64 depth form (the reference's arithmetic, bit-identical to the oracle)",
@@ -167,14 +197,17 @@ def arm_config(n: int, world: int, precision: int) -> dict:
 
 
 def run_reference(args, rank, world):
-    """CPU implementation of the path (the oracle port), all host threads."""
+    """CPU implementation of the path (the oracle port), all host threads, on
+    the benchmark workload itself (4096^2) while K + W steps take well under
+    a minute; beyond that each step is a window of the workload (said in the
+    line's config and sample)."""
     if rank != 0:
         return 0
     from oracle import oracle as orc
     from rakali_b200 import workloads as wl
     threads = os.cpu_count() or 1
     used = orc.set_threads(threads)
-    side = 1024
+    side = N_CELLS_SIDE if args.steps + args.warmup <= 40 else 1024
     b, h = wl.config2(n=side, seed=2024)
     cfg = dict(nx=side, ny=side, **wl.CONFIG2_KW)
     o = orc.OracleSim.from_config(cfg, bathymetry=b, initial_h=h)
@@ -183,14 +216,19 @@ def run_reference(args, rank, world):
     o.step(args.steps)
     elapsed = time.perf_counter() - t0
     value = side * side * args.steps / elapsed
-    sample = (f"each step: one SSP-RK2 step of a {side}x{side} window of the 4096^2 "
-              f"configuration (same bed family), FP64, {used} OpenMP threads")
+    if side == N_CELLS_SIDE:
+        sample = (f"each step: one SSP-RK2 step of the full {side}x{side} workload, FP64, "
+                  f"{used} OpenMP threads")
+    else:
+        sample = (f"each step: one SSP-RK2 step of a {side}x{side} window of the "
+                  f"{N_CELLS_SIDE}^2 workload (same bed family), FP64, {used} OpenMP threads")
+    config = arm_config(side, world, 64)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-updates/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": arm_config(N_CELLS_SIDE, world, 64),
+        "config": config,
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": used,
                          "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
@@ -200,7 +238,7 @@ def run_reference(args, rank, world):
     return 0
 
 
-def _form_numbers(sim, args, world, local_rank, dist, cells):
+def _form_numbers(sim, args, world, local_rank, dist, cells, inputs):
     """Time one arithmetic form on the current state: device time of K steps,
     per-kernel events and the end-to-end run through the public API."""
     import ctypes
@@ -231,10 +269,12 @@ def _form_numbers(sim, args, world, local_rank, dist, cells):
     if lib.rkb_profile_steps(sim._handle, 5, prof) != 0:
         raise RuntimeError("rkb_profile_steps failed")
 
-    # end to end through the public API with host buffers: upload the state,
-    # K steps, read the fields back (D2H) - wall clock around all of it.
-    state = [np.asfortranarray(a) for a in (sim.h_phys.copy(), sim.hu_phys.copy(),
-                                            sim.hv_phys.copy())]
+    # end to end through the public API with host buffers: the inputs (the
+    # workload's initial h, hu, hv in host memory) go up through the setters,
+    # K steps run, the result (h) comes back through its zero-copy view -
+    # wall clock around all of it.  The setters send the interiors straight
+    # to the device; the view brings home h alone, ghosts included.
+    state = [np.asfortranarray(a) for a in inputs]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     sim.set_h(state[0])
@@ -248,7 +288,8 @@ def _form_numbers(sim, args, world, local_rank, dist, cells):
     nxt = n + 2 * sim.nghost
     e2e = {"value": world * cells * args.steps / e2e_s, "unit": "cell-updates/s",
            "h2d_bytes_per_step": 3 * 8 * cells / args.steps,   # interior h, hu, hv
-           "d2h_bytes_per_step": 7 * 8 * nxt * nxt / args.steps}  # h, hu, hv, b, h0, hu0, hv0
+           "d2h_bytes_per_step": 8 * nxt * nxt / args.steps,   # h with its ghosts
+           "flow": "set_h/set_hu/set_hv from host arrays, K steps, h read through its view"}
     return {"value": value, "ms": ms, "e2e": e2e, "clocks": clk.summary(),
             "stage_ms": {"bc_stage1": prof[0], "stage1": prof[1], "bc_stage2": prof[2],
                          "stage2": prof[3]},
@@ -271,16 +312,18 @@ def _roofline(form, precision, cells, world):
             "step_frac_of_hbm": b_cell * form["value"] / world / 1e9 / hbm}
 
 
-def _fp32_error(b, h, n, steps):
+def _accuracy(b, h, n, steps):
     """Free-surface error of the FP32 form against the FP64 step (which the
-    parity tests hold bit-identical to the oracle) after `steps` steps from the
-    same state, and the FP64 step's own drift when h is perturbed by 1e-7
-    relative noise (the conditioning floor of this configuration); the same
-    two figures after 50, 100 and 200 steps show how both grow."""
+    parity tests hold bit-identical to the oracle) after 50 .. `steps` steps
+    from the same state, beside two floors of the FP64 step against itself:
+    h perturbed by 1e-7 relative noise (FP32 round-off) and by 1e-15 (FP64
+    round-off).  The second floor is the error any arithmetic other than the
+    reference's own would show on this flow.  Also the domain volume drift of
+    each run (closed walls: the volume is conserved)."""
     from rakali_b200 import Rakali
     from rakali_b200 import workloads as wl
 
-    marks = sorted({k for k in (50, 100, 200) if k < steps} | {steps})
+    marks = sorted({k for k in (50, 100, 200, 500) if k < steps} | {steps})
 
     def run(hh, prec, sink):
         s = Rakali(defer_init=True, nx=n, ny=n, **wl.CONFIG2_KW)
@@ -288,32 +331,71 @@ def _fp32_error(b, h, n, steps):
         s.set_initial_h(hh)
         s.finalize()
         s.set_precision(prec)
+        v0 = float(np.sum(s.h_phys))
         done = 0
         for k in marks:
             s.step(k - done)
             done = k
             sink(k, s.h_phys)
+        v1 = float(np.sum(s.h_phys))
         s.close()
+        return (v1 - v0) / v0
 
     ref = {}
-    run(h, 64, lambda k, a: ref.__setitem__(k, a.copy()))
-    err32, floor = {}, {}
+    drift = {"fp64": run(h, 64, lambda k, a: ref.__setitem__(k, a.copy()))}
+    err32, floor7, floor15 = {}, {}, {}
 
     def stats(store):
-        return lambda k, a: store.__setitem__(k, (float(np.abs(a - ref[k]).max()),
-                                                  float(np.sqrt(np.mean((a - ref[k]) ** 2)))))
+        def put(k, a):
+            d = a - ref[k]
+            store[k] = (float(np.abs(d).max()), float(np.sqrt(np.mean(d * d))))
+        return put
 
-    run(h, 32, stats(err32))
+    drift["fp32"] = run(h, 32, stats(err32))
     rng = np.random.default_rng(17)
-    hp = np.asfortranarray(h * (1.0 + 1.0e-7 * rng.standard_normal(h.shape)))
-    run(hp, 64, stats(floor))
-    return {"steps": steps, "unit": "m",
-            "max": err32[steps][0], "rms": err32[steps][1],
-            "fp64_floor_max": floor[steps][0], "fp64_floor_rms": floor[steps][1],
-            "by_steps": {str(k): {"max": err32[k][0], "rms": err32[k][1],
-                                  "fp64_floor_max": floor[k][0], "fp64_floor_rms": floor[k][1]}
-                         for k in marks},
-            "note": "free surface vs the FP64 step; floor = FP64 step vs itself with h x (1 + 1e-7 noise)"}
+    noise = rng.standard_normal(h.shape)
+    drift["fp64_1e-7"] = run(np.asfortranarray(h * (1.0 + 1.0e-7 * noise)), 64, stats(floor7))
+    drift["fp64_1e-15"] = run(np.asfortranarray(h * (1.0 + 1.0e-15 * noise)), 64, stats(floor15))
+    by = {str(k): {"max": err32[k][0], "rms": err32[k][1],
+                   "fp64_floor_1e-7_max": floor7[k][0], "fp64_floor_1e-7_rms": floor7[k][1],
+                   "fp64_floor_1e-15_max": floor15[k][0], "fp64_floor_1e-15_rms": floor15[k][1]}
+          for k in marks}
+    return {"steps": steps, "unit": "m", "max": err32[steps][0], "rms": err32[steps][1],
+            "fp64_floor_max": floor15[steps][0], "fp64_floor_rms": floor15[steps][1],
+            "by_steps": by, "volume_drift_rel": drift,
+            "note": "free surface vs the FP64 step; floors = the FP64 step vs itself from h x "
+                    "(1 + eps noise), eps = 1e-7 (FP32 round-off) and 1e-15 (FP64 round-off)"}
+
+
+def _lake_at_rest(n, steps):
+    """The workload's bed with a flat surface (eta = 0, emergent islands):
+    after `steps` steps in each form, max |eta| over wet cells, max |hu|,
+    |hv| and the domain volume drift."""
+    from rakali_b200 import Rakali
+    from rakali_b200 import workloads as wl
+    b, h = wl.config2(n=n, seed=2024, hump=False)
+    out = {"workload": f"{n}x{n}, the benchmark bed, eta = 0, no hump", "steps": steps}
+    for prec in (64, 32):
+        s = Rakali(defer_init=True, nx=n, ny=n, **wl.CONFIG2_KW)
+        s.set_bathymetry(b)
+        s.set_initial_h(h)
+        s.finalize()
+        s.set_precision(prec)
+        s.step(steps)
+        hh = s.h_phys
+        wet = hh > 0
+        out[f"fp{prec}"] = {
+            "eta_max_abs": float(np.abs((hh + b)[wet]).max()),
+            "momentum_max_abs": max(float(np.abs(s.hu_phys).max()),
+                                    float(np.abs(s.hv_phys).max())),
+            "state_unchanged": bool(np.array_equal(hh, h)),
+            "volume_drift_rel": (float(np.sum(hh)) - float(np.sum(h))) / float(np.sum(h))}
+        s.close()
+    hmax = float(h.max())
+    out["bound"] = {"eta_m": 1e-13, "momentum_m2_s": 1e-12 * hmax * float(np.sqrt(9.80665 * hmax)),
+                    "source": "|eta| <= 1e-13 m; momentum 1e-12 H sqrt(gH) with H the deepest "
+                              "water (the reference's test_c_property.F90:97-104 scaling)"}
+    return out
 
 
 def run_ensemble(args, world, local_rank, dist):
@@ -687,13 +769,15 @@ def run_b200(args, rank, world, local_rank, dist):
     forms = {}
     for prec in (head, other) if args.both_forms else (head,):
         sim.set_precision(prec)
-        forms[prec] = _form_numbers(sim, args, world, local_rank, dist, cells)
+        forms[prec] = _form_numbers(sim, args, world, local_rank, dist, cells,
+                                    (h, np.zeros_like(h), np.zeros_like(h)))
         forms[prec]["roofline"] = _roofline(forms[prec], prec, cells, world)
     sim.close()
     ens = run_ensemble(args, world, local_rank, dist) if args.ensemble_steps > 0 else None
-    err = None
+    err = lake = None
     if args.both_forms and rank == 0 and not args.no_accuracy:
-        err = _fp32_error(b, h, n, min(args.steps, 500))
+        err = _accuracy(b, h, n, args.accuracy_steps)
+        lake = _lake_at_rest(n, args.accuracy_steps)
     if rank != 0:
         return 0
 
@@ -722,7 +806,9 @@ def run_b200(args, rank, world, local_rank, dist):
                 entry["error_vs_fp64"] = err
             line["forms"][f"fp{prec}"] = entry
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
+        line["cpu_baseline"], line["parity_4096"] = cpu_baseline_and_parity(b, h, n)
+    if lake is not None:
+        line["lake_at_rest_4096"] = lake
     if args.ensemble_steps > 0:
         line["ensemble"] = ens
     if world == 1 and args.adjoint_steps > 0:
@@ -760,16 +846,18 @@ def main():
                     help="random directions of the finite-difference check")
     ap.add_argument("--adjoint-fd-steps", type=int, default=100,
                     help="steps of the finite-difference check (the gradient's first steps)")
-    ap.add_argument("--config5", action="store_true",
-                    help="also run the batched FP32 forward + adjoint (64 x 2048^2, 500 steps; "
-                         "a few minutes)")
+    ap.add_argument("--no-config5", dest="config5", action="store_false",
+                    help="skip the batched FP32 forward + adjoint (64 x 2048^2, 500 steps; "
+                         "about a minute, run by default on one GPU)")
     ap.add_argument("--c5-members", type=int, default=64)
     ap.add_argument("--c5-side", type=int, default=2048)
     ap.add_argument("--c5-steps", type=int, default=500)
     ap.add_argument("--c5-cmp-steps", type=int, default=50,
                     help="steps of the FP32-vs-FP64 gradient comparison on member 0")
     ap.add_argument("--no-accuracy", action="store_true",
-                    help="skip the FP32-vs-FP64 error measurement")
+                    help="skip the FP32-vs-FP64 error and lake-at-rest measurements")
+    ap.add_argument("--accuracy-steps", type=int, default=1000,
+                    help="steps of the FP32-vs-FP64 error and lake-at-rest runs")
     ap.add_argument("--sweep-cols", type=int, choices=(0, 2, 4), default=0,
                     help="FP32 form: columns per lane of the sweep kernel (0 = default)")
     ap.add_argument("--sweep-rows", type=int, default=0,

@@ -107,6 +107,7 @@ int Batch::build() {
       StepArgs a = s->device_args();
       a.tile = tile_;
       a.hllc = hllc_;
+      plain = plain && a.plain;
       a64.push_back(a);
       blocks[i] = batch_stage_blocks(s->g, tile_);
     } else {
@@ -143,7 +144,7 @@ int Batch::build() {
   const int nblocks = (int)map.size();
   const bool same = prec_ == 64
                         ? (bl_.blocks == nblocks && bl_.max_nxt == max_nxt && bl_.max_nyt == max_nyt &&
-                           bl_.tile == tile_)
+                           bl_.tile == tile_ && bl_.plain == plain)
                         : (bl32_.blocks == nblocks && bl32_.max_nxt == max_nxt &&
                            bl32_.max_nyt == max_nyt && bl32_.cpl == cpl_ && bl32_.plain == plain);
   std::vector<int> gsig(n);
@@ -151,7 +152,8 @@ int Batch::build() {
   // graphs hold launch shapes and pointers, and the members' gauge recorders
   if (realloc_ || !same || gsig != gauge_sig_) clear_graphs();
   gauge_sig_ = gsig;
-  bl_ = BatchLaunch{(const StepArgs*)dargs_, dmap_, n, nblocks, max_nxt, max_nyt, tile_, hllc_};
+  bl_ = BatchLaunch{(const StepArgs*)dargs_, dmap_, n, nblocks, max_nxt, max_nyt, tile_, hllc_,
+                    plain};
   bl32_ = BatchLaunch32{(const StepArgs32*)dargs_, dmap_, n, nblocks, max_nxt, max_nyt,
                         cpl_, hllc_, plain};
   return 0;

@@ -11,21 +11,24 @@
 
 namespace rkb {
 
+// Semi-implicit Manning friction of a wet cell (rki_kernel_fused.F90:121-131).
+__device__ __forceinline__ void manning(double h, double& u, double& v, double dt, double n_sq) {
+  const double uu = u / h;
+  const double vv = v / h;
+  const double speed = sqrt(uu * uu + vv * vv);
+  const double cf = kG * n_sq / cr_pow_third(h);
+  const double den = 1.0 + dt * cf * speed / h;
+  u = u / den;
+  v = v / den;
+}
+
 // Pointwise sources after the Euler update: Manning friction, wind,
 // pressure gradient, Coriolis, precipitation (rki_kernel_fused.F90:121-154).
 __device__ __forceinline__ void sources(double& h, double& u, double& v, const Physics* p, double dt,
                                         double n_sq, double cosf, double sinf, bool has_cor,
                                         const Grid& g, int i, int j, const Forcing& fo) {
   if (h > kDry) {
-    if (p->manning_n > 0.0) {
-      const double uu = u / h;
-      const double vv = v / h;
-      const double speed = sqrt(uu * uu + vv * vv);
-      const double cf = kG * n_sq / cr_pow_third(h);
-      const double den = 1.0 + dt * cf * speed / h;
-      u = u / den;
-      v = v / den;
-    }
+    if (p->manning_n > 0.0) manning(h, u, v, dt, n_sq);
     if (p->forcing_active) {
       const size_t q = g.at(i, j);
       u = u + dt * fo.wind_x[q] / kRho;
@@ -42,6 +45,20 @@ __device__ __forceinline__ void sources(double& h, double& u, double& v, const P
     }
   }
   if (p->forcing_active) h = h + dt * fo.precip[g.at(i, j)];
+}
+
+// The sources of a stage without forcing, Coriolis or sponge terms: Manning
+// friction alone (the same expressions as sources()).
+__device__ __forceinline__ void sources_plain(double& h, double& u, double& v, double manning_n,
+                                              double dt, double n_sq) {
+  if (h > kDry && manning_n > 0.0) manning(h, u, v, dt, n_sq);
+}
+
+// True when a stage has no forcing, Coriolis or sponge terms: the stage
+// kernels then run their plain-physics build.
+__host__ __device__ __forceinline__ bool plain_physics(const Physics& p, const BcParams& bc) {
+  return p.forcing_active == 0 && !(fabs(p.coriolis_f) > 1.0e-20) &&
+         !(bc.sponge_width > 0 && bc.sponge_strength > 0.0);
 }
 
 // Sponge relaxation of interior cell (i, j) (rki_kernel_sponge.F90:16-88).

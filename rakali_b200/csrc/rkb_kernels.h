@@ -54,6 +54,7 @@ struct StepArgs {
   int hllc;
   int scheme;    // time scheme: 2 SSP-RK2 (fused stages), 1 euler, 3 rk3, 4 rk43
   int n_stages;  // stages of the generic schemes
+  int plain;     // no forcing, Coriolis or sponge: the SSP-RK2 stages built without those terms
 };
 
 // Doubles of per-block partial storage the step kernels need.
@@ -140,6 +141,7 @@ struct BatchLaunch {
   int blocks;   // blocks of one stage launch
   int max_nxt, max_nyt;
   int tile, hllc;
+  int plain;  // every member plain (StepArgs::plain)
 };
 int batch_stage_blocks(const Grid& g, int tile);
 cudaError_t configure_batch(int tile, int hllc);

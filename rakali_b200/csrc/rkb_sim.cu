@@ -1,5 +1,6 @@
 // Host driver of one structured simulation (see rkb_sim.hpp).
 #include "rkb_sim.hpp"
+#include "rkb_cell.cuh"
 
 #include "rkb_netcdf.hpp"
 
@@ -450,13 +451,12 @@ int Sim::read_gauges(int max_records, double* times, double* values, int* overfl
 // ghosts, RK2 saves included, after a full pull that leaves the device state
 // canonical.
 int Sim::save_checkpoint(const std::string& path, std::string& err) {
-  if (on_device_ && !host_is_current_) {
+  if (on_device_) {
     cudaSetDevice(device_);
-    if (pull_state(true) != 0) {
+    if (pull_missing(7) != 0) {
       err = "copying the state to the host failed";
       return -1;
     }
-    host_is_current_ = host_state_current_ = true;
   }
   nc::CheckpointMeta m{};
   m.time = t_current_;
@@ -600,6 +600,7 @@ int Sim::upload_params() {
   args_.tile = tile;
   args_.scheme = phys.scheme;
   args_.n_stages = phys.n_stages;
+  args_.plain = plain_physics(phys, bc) ? 1 : 0;
   RKB_TRY(configure_kernels(args_.tile, args_.hllc));
   params_dirty = false;
   return 0;
@@ -610,7 +611,21 @@ int Sim::ensure_device() {
   if (!on_device_) {
     if (upload_state() != 0) return -1;
     on_device_ = true;
+  } else if (handed_[0] || handed_[1] || handed_[2] || handed_[3]) {
+    // Fields whose host arrays went out through a pointer since the last run
+    // may have been written there: they move back, and only they (the
+    // reference's ensure_device uploads every array, rki_api.F90:116-123).
+    if (precision_ == 32 && handed_[3]) {
+      // a new bed changes every surface eta = h + b: the depths come home
+      // under the old bed, then the whole state goes up again
+      if (pull_missing(7) != 0) return -1;
+      if (upload_state() != 0) return -1;
+    } else {
+      for (int f = 0; f < 4; ++f)
+        if (handed_[f] && push_field(f) != 0) return -1;
+    }
   }
+  for (bool& h : handed_) h = false;
   mark_host_stale();
   return 0;
 }
@@ -655,7 +670,62 @@ static int pull(const StepArgs& a, int cur, bool stepped, bool full, double* con
 
 int Sim::pull_state(bool full) {
   if (precision_ == 32 && to_depth(full) != 0) return -1;
-  return pull(args_, cur_, stepped_, full, hf_, g, stream_);
+  if (pull(args_, cur_, stepped_, full, hf_, g, stream_) != 0) return -1;
+  for (int f = 0; f < (full ? 7 : 3); ++f) fcur_[f] = true;
+  return 0;
+}
+
+// One field of pull(): 0..2 the current state, 3 the bed, 4..6 the RK2 saves
+// (written by the first step; before it the host arrays hold their values).
+int Sim::pull_field(int f) {
+  if (f >= 4 && !stepped_) {
+    fcur_[f] = true;
+    return 0;
+  }
+  if (precision_ == 32 && to_depth(f >= 4) != 0) return -1;
+  const size_t wbytes = (size_t)g.nxt * sizeof(double);
+  const size_t spitch = (size_t)g.pitch * sizeof(double);
+  const FieldSet F = cur_ ? args_.U1 : args_.U0;
+  const FieldSet O = cur_ ? args_.U0 : args_.U1;
+  const double* src[7] = {F.h, F.hu, F.hv, args_.b, O.h, O.hu, O.hv};
+  if (f < 4 || args_.scheme != 2) {
+    RKB_TRY(cudaMemcpy2DAsync(hf_[f], wbytes, src[f], spitch, wbytes, g.nyt,
+                              cudaMemcpyDeviceToHost, stream_));
+  } else {
+    const size_t off_d = (size_t)g.ng + (size_t)g.ng * (size_t)g.pitch;
+    const size_t off_h = (size_t)g.ng + (size_t)g.ng * (size_t)g.nxt;
+    RKB_TRY(cudaMemcpy2DAsync(hf_[f] + off_h, wbytes, src[f] + off_d, spitch,
+                              (size_t)g.nx_phys() * sizeof(double), g.ny_phys(),
+                              cudaMemcpyDeviceToHost, stream_));
+  }
+  RKB_TRY(cudaStreamSynchronize(stream_));
+  fcur_[f] = true;
+  return 0;
+}
+
+int Sim::pull_missing(int upto) {
+  for (int f = 0; f < upto; ++f)
+    if (!field_current(f) && pull_field(f) != 0) return -1;
+  return 0;
+}
+
+// Host array f (0..2 a state field of the current buffer, 3 the bed) to the
+// device, ghosts included; the CFL maxima are recomputed before the next step.
+int Sim::push_field(int f) {
+  const size_t wbytes = (size_t)g.nxt * sizeof(double);
+  const size_t dpitch = (size_t)g.pitch * sizeof(double);
+  const FieldSet F = cur_ ? args_.U1 : args_.U0;
+  double* dst[4] = {F.h, F.hu, F.hv, args_.b};
+  RKB_TRY(cudaMemcpy2DAsync(dst[f], dpitch, hf_[f], wbytes, wbytes, g.nyt,
+                            cudaMemcpyHostToDevice, stream_));
+  if (f <= 2) {
+    if (precision_ == 32 && to_surface(true, f) != 0) return -1;
+    hctl_->ms_valid = 0;
+    RKB_TRY(cudaMemcpyAsync(&args_.ctl->ms_valid, &hctl_->ms_valid, sizeof(int),
+                            cudaMemcpyHostToDevice, stream_));
+  }
+  RKB_TRY(cudaStreamSynchronize(stream_));
+  return 0;
 }
 
 // The host arrays become canonical (a pointer to them is handed out, or they
@@ -664,17 +734,20 @@ int Sim::pull_state(bool full) {
 void Sim::ensure_host() {
   if (on_device_) {
     cudaSetDevice(device_);
-    if (!host_is_current_) pull_state(true);
+    // fields already current (some perhaps written through a view since)
+    // are kept; the others come home
+    pull_missing(7);
     on_device_ = false;
-    host_is_current_ = host_state_current_ = true;
+    mark_host_current();
+    for (bool& h : handed_) h = false;
   }
 }
 
 void Sim::sync_host() {
-  if (is_initialised && on_device_ && !host_is_current_ && !host_state_current_) {
+  if (is_initialised && on_device_) {
     cudaSetDevice(device_);
-    pull_state(false);
-    host_state_current_ = true;  // h, hu, hv only: the bed and RK2 saves stay on the device
+    pull_missing(3);  // h, hu, hv only: the bed and RK2 saves stay on the device
+    host_state_current_ = true;
   }
 }
 
@@ -683,12 +756,22 @@ void Sim::sync_from_device() {
     cudaSetDevice(device_);
     pull_state(true);
     on_device_ = false;
-    host_is_current_ = host_state_current_ = true;
+    mark_host_current();
+    for (bool& h : handed_) h = false;
   }
 }
 
+// rki_get_*_ptr (rki_api.F90:502-700): the reference brings every array home
+// and unmaps the device copy (ensure_host); here only the field asked for
+// comes home, and the next run uploads it again in case the caller wrote
+// through the pointer.  Before finalize and after ensure_host the host
+// arrays are canonical already.
 double* Sim::field_ptr(int which) {
-  ensure_host();
+  if (on_device_) {
+    cudaSetDevice(device_);
+    if (!field_current(which)) pull_field(which);
+    handed_[which] = true;
+  }
   return hf_[which];
 }
 
@@ -698,15 +781,19 @@ int Sim::set_interior(int which, const double* data, int nx, int ny) {
   const bool pre_final = (which == 3) || (which == 10);  // bathymetry, initial h
   if (pre_final) {
     if (on_device_) ensure_host();
-  } else if (state_field) {
-    // refresh_host (rki_api.F90:126-135)
-    if (is_initialised && !host_is_current_ && on_device_) sync_host();
   }
   const int f = which == 10 ? 0 : which;
+  // A state field set while the device holds the state goes straight from
+  // the caller's array to the device, and the host array is marked stale
+  // (the next pointer to it brings the new values home) - unless a pointer
+  // to it is out, in which case the host array is the caller's view and
+  // takes the values too.
+  const bool direct = state_field && on_device_ && !handed_[f];
   double* dst = hf_[f];
-  for (int j = 0; j < ny; ++j)
-    std::memcpy(dst + (size_t)g.ng + (size_t)(g.ng + j) * g.nxt, data + (size_t)j * nx,
-                (size_t)nx * sizeof(double));
+  if (!direct)
+    for (int j = 0; j < ny; ++j)
+      std::memcpy(dst + (size_t)g.ng + (size_t)(g.ng + j) * g.nxt, data + (size_t)j * nx,
+                  (size_t)nx * sizeof(double));
   if (which == 3) {
     user_set_bathymetry = true;
     if (is_finalised) {
@@ -726,15 +813,23 @@ int Sim::set_interior(int which, const double* data, int nx, int ny) {
   }
   if (which == 10 || which == 0) user_set_h = true;
   if (state_field && on_device_) {
-    // push_state_to_device (rki_api.F90:137-143) pushes h, hu and hv; the two
-    // not set here hold what the device holds (refreshed above, and the FP32
-    // form round-trips through the host arrays exactly), so only this one moves
+    // The reference refreshes the host state, writes the interior and pushes
+    // h, hu and hv (rki_api.F90:126-143); the device already holds the other
+    // two fields and this one's ghosts, so only this field's interior moves.
+    cudaSetDevice(device_);
     const size_t wbytes = (size_t)g.nxt * sizeof(double);
     const size_t dpitch = (size_t)g.pitch * sizeof(double);
+    // FP32: the depth staging buffers take the current state first, so the
+    // conversion of this field back carries the device's ghosts
+    if (precision_ == 32 && to_depth(false) != 0) return -1;
     FieldSet F = cur_ ? args_.U1 : args_.U0;
     double* dstd[3] = {F.h, F.hu, F.hv};
-    if (cudaMemcpy2DAsync(dstd[f], dpitch, hf_[f], wbytes, wbytes, g.nyt, cudaMemcpyHostToDevice,
-                          stream_) != cudaSuccess)
+    const size_t off_d = (size_t)g.ng + (size_t)g.ng * (size_t)g.pitch;
+    const size_t off_h = (size_t)g.ng + (size_t)g.ng * (size_t)g.nxt;
+    const double* src = direct ? data : hf_[f] + off_h;
+    const size_t spitch = direct ? (size_t)nx * sizeof(double) : wbytes;
+    if (cudaMemcpy2DAsync(dstd[f] + off_d, dpitch, src, spitch, (size_t)nx * sizeof(double), ny,
+                          cudaMemcpyHostToDevice, stream_) != cudaSuccess)
       return -1;
     if (precision_ == 32 && to_surface(true, f) != 0) return -1;
     hctl_->ms_valid = 0;
@@ -742,10 +837,12 @@ int Sim::set_interior(int which, const double* data, int nx, int ny) {
                         cudaMemcpyHostToDevice, stream_) != cudaSuccess)
       return -1;
     if (cudaStreamSynchronize(stream_) != cudaSuccess) return -1;
-    // FP64: h, hu, hv on the host still equal the device's, so the next setter
-    // needs no refresh.  FP32: the device holds the pushed field rounded.
-    host_is_current_ = false;
-    if (precision_ == 32) host_state_current_ = false;
+    // FP64 through the host array: a host array that was current stays
+    // current (same interior on both sides).  Direct, or FP32 (the device
+    // holds the field rounded to the surface form): the host copy is stale.
+    for (int k = 0; k < 7; ++k) fcur_[k] = field_current(k);
+    host_is_current_ = host_state_current_ = false;
+    if (direct || precision_ == 32) fcur_[f] = false;
   }
   return 0;
 }
@@ -781,7 +878,7 @@ void Sim::pull_ctl() {
 
 cudaGraphExec_t Sim::graph_for(int steps) {
   const int rows = precision_ == 32 ? args32_.rows * 8 + args32_.cpl : 0;
-  const int plain = precision_ == 32 ? args32_.plain : 0;
+  const int plain = precision_ == 32 ? args32_.plain : args_.plain;
   for (auto& ge : graphs_)
     if (ge.steps == steps && ge.hllc == args_.hllc && ge.tile == args_.tile &&
         ge.prec == precision_ && ge.rows == rows && ge.plain == plain)
@@ -1125,7 +1222,8 @@ int Sim::restore() {
   step_count_ = snap_steps_;
   stepped_ = snap_stepped_;
   on_device_ = false;  // the next run uploads the host arrays, which hold the snapshot
-  host_is_current_ = host_state_current_ = true;
+  mark_host_current();
+  for (bool& h : handed_) h = false;
   return 0;
 }
 

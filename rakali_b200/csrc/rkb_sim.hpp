@@ -137,7 +137,27 @@ class Sim {
   // device's; host_state_current_: h, hu, hv do (after rki_sync_host).
   bool on_device_ = false, host_is_current_ = false, stepped_ = false;
   bool host_state_current_ = false;
-  void mark_host_stale() { host_is_current_ = host_state_current_ = false; }
+  // Per-field bookkeeping while the device holds the state (fields 0 h, 1 hu,
+  // 2 hv, 3 b, 4-6 the RK2 saves): fcur_[f], host array f equals the
+  // device's value; handed_[f], a pointer to host array f went out since the
+  // last device run, so the caller may have written through it and the next
+  // run uploads it (the RK2 saves are rewritten by every step and are not).
+  bool fcur_[7] = {};
+  bool handed_[7] = {};
+  void mark_host_stale() {
+    host_is_current_ = host_state_current_ = false;
+    for (bool& f : fcur_) f = false;
+  }
+  void mark_host_current() {
+    host_is_current_ = host_state_current_ = true;
+    for (bool& f : fcur_) f = true;
+  }
+  bool field_current(int f) const {
+    return host_is_current_ || fcur_[f] || (f <= 2 && host_state_current_);
+  }
+  int pull_field(int f);      // device -> host array f (FP32: through the depth form)
+  int pull_missing(int upto);  // every field f < upto whose host array is not current
+  int push_field(int f);      // host array f -> device (f <= 3)
   int cur_ = 0;
   double t_current_ = 0.0, dt_ = 0.0;
   int step_count_ = 0;

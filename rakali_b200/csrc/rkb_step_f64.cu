@@ -164,7 +164,8 @@ __global__ void k_max_speed(Grid g, StepCtl* ctl, FieldSet U0, FieldSet U1) {
 // ---------------------------------------------------------------------------
 
 // Shared-memory plan of one TX x TY tile (doubles):
-//   tile  5 x (TX+4)(TY+4)   h, hu, hv, b, eta with a 2-cell halo
+//   tile  4 x (TX+4)(TY+4)   h, hu, hv, b with a 2-cell halo (eta = h + b is
+//                            formed where it is read, with the same rounding)
 //   sx    3 x (TX+2) TY      limited x-slopes of eta, hu, hv
 //   sy    3 x TX (TY+2)      limited y-slopes
 //   fx    6 x (TX+1) TY      x-face fluxes + well-balanced terms
@@ -177,7 +178,7 @@ struct StageSmem {
   static constexpr int NSY = TX * (TY + 2);
   static constexpr int NFX = (TX + 1) * TY;
   static constexpr int NFY = TX * (TY + 1);
-  static constexpr int DOUBLES = 5 * NT + 3 * NSX + 3 * NSY + 6 * NFX + 6 * NFY;
+  static constexpr int DOUBLES = 4 * NT + 3 * NSX + 3 * NSY + 6 * NFX + 6 * NFY;
   static constexpr size_t BYTES = sizeof(double) * (size_t)DOUBLES;
 };
 
@@ -192,7 +193,9 @@ struct StageSmem {
 // Tile (bx, by) of a gx x gy tiling of one simulation, with TX * TY + 32 XW
 // threads: XW extra warps share the slope and face loops (so that no warp
 // runs a third, mostly empty face round) and sit out the cell update.
-template <int TX, int TY, bool HLLC, int STAGE, int XW = 0>
+// PLAIN: the build for stages without forcing, Coriolis or sponge terms
+// (Manning friction only), chosen by the host from its copy of the physics.
+template <int TX, int TY, bool HLLC, int STAGE, int XW = 0, bool PLAIN = false>
 __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Physics* phys,
                                            const BcParams* bcp, const FieldSet& U0,
                                            const FieldSet& U1, const FieldSet& S,
@@ -208,8 +211,7 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
   double* tu = th + SM::NT;
   double* tv = tu + SM::NT;
   double* tb = tv + SM::NT;
-  double* te = tb + SM::NT;
-  double* sxe = te + SM::NT;
+  double* sxe = tb + SM::NT;
   double* sxu = sxe + SM::NSX;
   double* sxv = sxu + SM::NSX;
   double* sye = sxv + SM::NSX;
@@ -239,7 +241,7 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
   // Coriolis rotation of this stage, cos/sin(f dt), correctly rounded once
   // per block (rki_kernel_fused.F90:211-214)
   __shared__ double rot[2];
-  if (STAGE != 0 && tid == 0) {
+  if (STAGE != 0 && !PLAIN && tid == 0) {
     double sn = 0.0, cs = 0.0;
     if (fabs(phys->coriolis_f) > 1.0e-20) cr_sincos(phys->coriolis_f * dt, sn, cs);
     rot[0] = cs;
@@ -256,7 +258,6 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
       vh = in.h[q]; vu = in.hu[q]; vv = in.hv[q]; vb = b[q];
     }
     th[k] = vh; tu[k] = vu; tv[k] = vv; tb[k] = vb;
-    te[k] = vh + vb;
   }
   if (STAGE == 2 && tid < TX * TY) {
     // the RK2 average reads U^n of this thread's cell after the face phase:
@@ -272,18 +273,20 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
   }
   __syncthreads();
 
+  auto te = [&](int q) { return th[q] + tb[q]; };  // the surface eta = h + b
+
   // 2. limited slopes: x for cells c in [-1, TX], y for rows r in [-1, TY]
   for (int k = tid; k < SM::NSX + SM::NSY; k += NTH) {
     if (k < SM::NSX) {
       const int c = k % (TX + 2) - 1, r = k / (TX + 2);
       const int q = (r + 2) * TW + (c + 2);
-      cell_slope(th[q - 1], th[q], th[q + 1], te[q - 1], te[q], te[q + 1], tu[q - 1], tu[q],
+      cell_slope(th[q - 1], th[q], th[q + 1], te(q - 1), te(q), te(q + 1), tu[q - 1], tu[q],
                  tu[q + 1], tv[q - 1], tv[q], tv[q + 1], sxe[k], sxu[k], sxv[k]);
     } else {
       const int kk = k - SM::NSX;
       const int c = kk % TX, r = kk / TX - 1;
       const int q = (r + 2) * TW + (c + 2);
-      cell_slope(th[q - TW], th[q], th[q + TW], te[q - TW], te[q], te[q + TW], tu[q - TW], tu[q],
+      cell_slope(th[q - TW], th[q], th[q + TW], te(q - TW), te(q), te(q + TW), tu[q - TW], tu[q],
                  tu[q + TW], tv[q - TW], tv[q], tv[q + TW], sye[kk], syu[kk], syv[kk]);
     }
   }
@@ -296,8 +299,8 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
       const int c = k % (TX + 1), r = k / (TX + 1);  // face between c-1 and c
       const int qL = (r + 2) * TW + (c + 1), qR = qL + 1;
       const int sL = r * (TX + 2) + c, sR = sL + 1;  // slope index of cell c-1 and c
-      face_flux<0, HLLC>(te[qL] + 0.5 * sxe[sL], tu[qL] + 0.5 * sxu[sL], tv[qL] + 0.5 * sxv[sL],
-                         tb[qL], te[qR] - 0.5 * sxe[sR], tu[qR] - 0.5 * sxu[sR],
+      face_flux<0, HLLC>(te(qL) + 0.5 * sxe[sL], tu[qL] + 0.5 * sxu[sL], tv[qL] + 0.5 * sxv[sL],
+                         tb[qL], te(qR) - 0.5 * sxe[sR], tu[qR] - 0.5 * sxu[sR],
                          tv[qR] - 0.5 * sxv[sR], tb[qR], o);
       fxa[k] = o.fh;
       fxa[SM::NFX + k] = o.fqx;
@@ -310,8 +313,8 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
       const int c = kk % TX, r = kk / TX;  // face between rows r-1 and r
       const int qB = (r + 1) * TW + (c + 2), qT = qB + TW;
       const int sB = r * TX + c, sT = sB + TX;  // y-slope index of rows r-1 and r
-      face_flux<1, HLLC>(te[qB] + 0.5 * sye[sB], tu[qB] + 0.5 * syu[sB], tv[qB] + 0.5 * syv[sB],
-                         tb[qB], te[qT] - 0.5 * sye[sT], tu[qT] - 0.5 * syu[sT],
+      face_flux<1, HLLC>(te(qB) + 0.5 * sye[sB], tu[qB] + 0.5 * syu[sB], tv[qB] + 0.5 * syv[sB],
+                         tb[qB], te(qT) - 0.5 * sye[sT], tu[qT] - 0.5 * syu[sT],
                          tv[qT] - 0.5 * syv[sT], tb[qT], o);
       fya[kk] = o.fh;
       fya[SM::NFY + kk] = o.fqx;
@@ -365,8 +368,12 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
       v = v + dt * o_fhv;
       protect(a, u, v);
       const double n_sq = phys->manning_n * phys->manning_n;
-      const bool has_cor = fabs(phys->coriolis_f) > 1.0e-20;
-      sources(a, u, v, phys, dt, n_sq, rot[0], rot[1], has_cor, g, i, j, fo);
+      if (PLAIN) {
+        sources_plain(a, u, v, phys->manning_n, dt, n_sq);
+      } else {
+        const bool has_cor = fabs(phys->coriolis_f) > 1.0e-20;
+        sources(a, u, v, phys, dt, n_sq, rot[0], rot[1], has_cor, g, i, j, fo);
+      }
       FieldSet out;
       if (STAGE == 1) {
         out = S;
@@ -392,12 +399,12 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
         protect(a, u, v);
       }
       const double h_pre_sponge = a;
-      sponge(a, u, v, bcp, g, i, j, dt);
+      if (!PLAIN) sponge(a, u, v, bcp, g, i, j, dt);
       out.h[q] = a;
       out.hu[q] = u;
       out.hv[q] = v;
       part = o_fh;
-      sponge_d = a - h_pre_sponge;
+      sponge_d = PLAIN ? 0.0 : a - h_pre_sponge;
       if (STAGE == 2 || (STAGE == 3 && gk == nst - 1)) wave_speed(a, u, v, wsx, wsy);
     }
   }
@@ -450,15 +457,28 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
   finalize_step(g, ctl, phys, partials, nblocks, step_dt, cur, kBudget);
 }
 
-template <int TX, int TY, bool HLLC, int STAGE, int XW = 0>
+// The host picks the PLAIN build from its copy of the physics; a launch whose
+// device-side physics disagree computes nothing and reports kErrPhysics (the
+// host then fails the step).  Every block sees the same physics, so either
+// all blocks return here or none does.
+__device__ __forceinline__ bool plain_mismatch64(StepCtl* ctl, const Physics* phys,
+                                                 const BcParams* bcp) {
+  if (plain_physics(*phys, *bcp)) return false;
+  if (threadIdx.x == 0) atomicExch(&ctl->error, kErrPhysics);
+  return true;
+}
+
+template <int TX, int TY, bool HLLC, int STAGE, int XW = 0, bool PLAIN = false>
 __global__ void __launch_bounds__(TX * TY + 32 * XW)
     k_stage(Grid g, StepCtl* ctl, const Physics* phys, const BcParams* bcp, FieldSet U0,
             FieldSet U1, FieldSet S, const double* __restrict__ b, Forcing fo,
             double* __restrict__ partials, FluxOut fl, int gk) {
+  if (PLAIN && plain_mismatch64(ctl, phys, bcp)) return;
   // one-dimensional grid over the gx x gy tiles (no limit on the row count)
   const unsigned gx = (unsigned)((g.nx_phys() + TX - 1) / TX);
-  stage_body<TX, TY, HLLC, STAGE, XW>(g, ctl, phys, bcp, U0, U1, S, b, fo, partials, fl,
-                                      blockIdx.x % gx, blockIdx.x / gx, gx, gridDim.x / gx, gk);
+  stage_body<TX, TY, HLLC, STAGE, XW, PLAIN>(g, ctl, phys, bcp, U0, U1, S, b, fo, partials, fl,
+                                             blockIdx.x % gx, blockIdx.x / gx, gx,
+                                             gridDim.x / gx, gk);
 }
 
 // Every simulation of a batch in one launch: map[blockIdx.x] = (simulation,
@@ -469,19 +489,20 @@ __global__ void __launch_bounds__(TX * TY + 32 * XW)
 // than that occupancy allows.
 constexpr int batch_blocks_per_sm(int threads) { return threads <= 320 ? 3 : 2; }
 
-template <int TX, int TY, bool HLLC, int STAGE, int XW = 0>
+template <int TX, int TY, bool HLLC, int STAGE, int XW = 0, bool PLAIN = false>
 __global__ void __launch_bounds__(TX * TY + 32 * XW, batch_blocks_per_sm(TX * TY + 32 * XW))
     k_stage_batch(const StepArgs* __restrict__ args, const int2* __restrict__ map) {
   __shared__ StepArgs sa;
   const int2 m = map[blockIdx.x];
   if (threadIdx.x == 0) sa = args[m.x];
   __syncthreads();
+  if (PLAIN && plain_mismatch64(sa.ctl, sa.phys, sa.bc)) return;
   const unsigned gx = (unsigned)((sa.g.nx_phys() + TX - 1) / TX);
   const unsigned gy = (unsigned)((sa.g.ny_phys() + TY - 1) / TY);
   const FluxOut none{};
-  stage_body<TX, TY, HLLC, STAGE, XW>(sa.g, sa.ctl, sa.phys, sa.bc, sa.U0, sa.U1, sa.S, sa.b,
-                                      sa.fo, sa.partials, none, (unsigned)m.y % gx,
-                                      (unsigned)m.y / gx, gx, gy);
+  stage_body<TX, TY, HLLC, STAGE, XW, PLAIN>(sa.g, sa.ctl, sa.phys, sa.bc, sa.U0, sa.U1, sa.S,
+                                             sa.b, sa.fo, sa.partials, none, (unsigned)m.y % gx,
+                                             (unsigned)m.y / gx, gx, gy);
 }
 
 // ---------------------------------------------------------------------------
@@ -743,10 +764,13 @@ size_t partials_doubles(const Grid& g, int tile) {
 template <int TX, int TY, bool HLLC, int STAGE, int XW = 0>
 static cudaError_t launch_stage_t(const StepArgs& a, FluxOut fl, cudaStream_t s, int gk) {
   using SM = StageSmem<TX, TY>;
-  auto kern = k_stage<TX, TY, HLLC, STAGE, XW>;
+  // the plain-physics build serves the SSP-RK2 stages
+  constexpr bool kRk2 = STAGE == 1 || STAGE == 2;
+  auto kern = (kRk2 && a.plain) ? k_stage<TX, TY, HLLC, STAGE, XW, kRk2>
+                                : k_stage<TX, TY, HLLC, STAGE, XW, false>;
   const dim3 d = stage_grid(a.g, a.tile);
-  kern<<<d.x * d.y, TX * TY + 32 * XW, SM::BYTES, s>>>(a.g, a.ctl, a.phys, a.bc, a.U0, a.U1, a.S, a.b, a.fo,
-                                        a.partials, fl, gk);
+  kern<<<d.x * d.y, TX * TY + 32 * XW, SM::BYTES, s>>>(a.g, a.ctl, a.phys, a.bc, a.U0, a.U1, a.S,
+                                                       a.b, a.fo, a.partials, fl, gk);
   return cudaGetLastError();
 }
 
@@ -767,6 +791,8 @@ static cudaError_t configure_t() {
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<TX, TY, HLLC, 1, XW>, attr, bytes);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<TX, TY, HLLC, 2, XW>, attr, bytes);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<TX, TY, HLLC, 3, XW>, attr, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<TX, TY, HLLC, 1, XW, true>, attr, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<TX, TY, HLLC, 2, XW, true>, attr, bytes);
   return e;
 }
 
@@ -918,11 +944,13 @@ int batch_stage_blocks(const Grid& g, int tile) {
 template <int TX, int TY, bool HLLC, int XW = 0>
 static cudaError_t configure_batch_t() {
   const int bytes = (int)StageSmem<TX, TY>::BYTES;
-  cudaError_t e = cudaFuncSetAttribute(k_stage_batch<TX, TY, HLLC, 1, XW>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  cudaError_t e = cudaFuncSetAttribute(k_stage_batch<TX, TY, HLLC, 1, XW>, attr, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage_batch<TX, TY, HLLC, 2, XW>, attr, bytes);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_stage_batch<TX, TY, HLLC, 2, XW>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    e = cudaFuncSetAttribute(k_stage_batch<TX, TY, HLLC, 1, XW, true>, attr, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_stage_batch<TX, TY, HLLC, 2, XW, true>, attr, bytes);
   return e;
 }
 
@@ -941,9 +969,9 @@ cudaError_t configure_batch(int tile, int hllc) {
 
 template <int TX, int TY, bool HLLC, int STAGE, int XW = 0>
 static cudaError_t launch_stage_batch_t(const BatchLaunch& bl, cudaStream_t s) {
-  k_stage_batch<TX, TY, HLLC, STAGE, XW>
-      <<<(unsigned)bl.blocks, TX * TY + 32 * XW, StageSmem<TX, TY>::BYTES, s>>>(
-      bl.args, bl.map);
+  auto kern = bl.plain ? k_stage_batch<TX, TY, HLLC, STAGE, XW, true>
+                       : k_stage_batch<TX, TY, HLLC, STAGE, XW, false>;
+  kern<<<(unsigned)bl.blocks, TX * TY + 32 * XW, StageSmem<TX, TY>::BYTES, s>>>(bl.args, bl.map);
   return cudaGetLastError();
 }
 

@@ -35,6 +35,9 @@ def test_reference_arm_prints_the_contract_line():
     assert cb["kind"] in ("port", "reference") and cb["value"] == line["value"]
     assert cb["cores"] >= 1 and cb["sample"]
     assert "workload" in line["config"]
+    # K + W small: every step is the full benchmark workload, and the config says so
+    assert "4096x4096" in line["config"]["workload"] and line["config"]["cells_per_gpu"] == 4096 ** 2
+    assert "full 4096x4096" in cb["sample"]
 
 
 def test_reference_arm_other_ranks_exit_quietly():

@@ -214,7 +214,7 @@ def test_boundary_conditions(lib, edges, kw, shape):
     d = [_dev(a) for a in (h, hu, hv, b)]
     import torch
     eod = [torch.from_numpy(eo[e].copy()).cuda() for e in ("west", "east", "south", "north")]
-    p = _bc_params(edges, tidal=tidal, **kw)
+    p = _bc_params(edges, tidal=tidal, **okw)
     for k in range(4):
         p.eta_old[k] = eod[k].data_ptr()
     rc = lib.rkb_apply_boundary_conditions(*(t.data_ptr() for t in d), nxt, nyt, ng, nxt, dx, dy,
