@@ -124,6 +124,7 @@ def load(path: str | None = None):
     _sig(lib, "rkb_set_precision", [H, I], I)
     _sig(lib, "rkb_get_precision", [H], I)
     _sig(lib, "rkb_set_sweep", [H, I, I], I)
+    _sig(lib, "rkb_set_wait_limit", [H, ctypes.c_longlong], I)
     _sig(lib, "rkb_batch_create", [HP, I, I, HP], I)
     _sig(lib, "rkb_batch_destroy", [HP], None)
     _sig(lib, "rkb_batch_step", [H, I], I)

@@ -678,6 +678,15 @@ int rkb_set_sweep(void* handle, int cols_per_lane, int rows) {
   return 0;
 }
 
+int rkb_set_wait_limit(void* handle, long long cycles) {
+  rkb::Sim* s = sim_of(handle);
+  if (!s) return kBadHandle;
+  s->wait_cycles = cycles > 0 ? cycles : rkb::kWaitCyclesDefault;
+  s->drop_step_graphs();  // the step graphs hold the sweep's arguments by value
+  s->params_dirty = true;
+  return 0;
+}
+
 }  // extern "C"
 
 namespace rkb {

@@ -95,12 +95,18 @@ struct StepCtl {
   unsigned int done_blocks;  // last-block counter of the final stage kernel
   unsigned int ms_done_blocks;
   int steps_run;       // steps executed since the host last cleared it
-  int error;           // nonzero: kErrWait or kErrPhysics (FP32 sweep)
+  int error;           // nonzero: kErrWait, kErrPhysics or kErrNonFinite
 };
 
-// StepCtl::error codes of the FP32 sweep.
-constexpr int kErrWait = 1;     // a bounded device-side wait for a bulk copy gave up
-constexpr int kErrPhysics = 2;  // a launch built without forcing / Coriolis / sponge met them
+// StepCtl::error codes.  A step that sets one completes; the steps after it
+// in the same graph chunk do not run (step_begin), and the host reports it.
+constexpr int kErrWait = 1;       // a bounded device-side wait for a bulk copy gave up (FP32)
+constexpr int kErrPhysics = 2;    // a launch built without forcing / Coriolis / sponge met them
+constexpr int kErrNonFinite = 3;  // the new state holds a NaN or an infinity
+
+// Default limit of the FP32 sweep's waits for its bulk copies (~1 s at B200
+// clocks); the drain after a wait gave up always uses this one.
+constexpr long long kWaitCyclesDefault = 2000000000ll;
 
 // ---------------------------------------------------------------------------
 // Small FP64 helpers in the reference's evaluation order.

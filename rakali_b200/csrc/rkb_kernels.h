@@ -87,6 +87,7 @@ struct StepArgs32 {
   int cpl;             // columns per lane of the sweep (2 or 4)
   int rows;            // rows per warp sweep
   int nstrips, nrowblk;
+  long long wait_cycles;  // limit of the waits for the bulk copies (kWaitCyclesDefault)
 };
 
 // Strips and row blocks of the sweep for `rows` rows per warp and `cpl`

@@ -1110,6 +1110,7 @@ void Sim::sync_args32() {
   int rows = sweep_rows > 0 ? sweep_rows : auto_rows_[args32_.cpl == 4 ? 1 : 0];
   if (rows < 4) rows = 4;
   args32_.rows = rows;
+  args32_.wait_cycles = wait_cycles > 0 ? wait_cycles : kWaitCyclesDefault;
   sweep_shape(g, rows, args32_.cpl, args32_.nstrips, args32_.nrowblk);
 }
 
@@ -1148,9 +1149,14 @@ int Sim::to_depth(bool full) {
 
 int Sim::check_device_error() {
   if (!hctl_->error) return 0;
-  err_text_ = hctl_->error == kErrPhysics
+  const int code = hctl_->error;
+  err_text_ = code == kErrPhysics
                   ? "the step kernel was built for other physics than the device held; the step "
                     "was abandoned"
+              : code == kErrNonFinite
+                  ? "a non-finite value (NaN or infinity) appeared in the state at step " +
+                        std::to_string(step_count_) + " (t = " + std::to_string(t_current_) +
+                        "); the run stopped after that step"
                   : "a bounded device-side wait for a bulk copy expired; the step was abandoned";
   hctl_->error = 0;
   cudaMemcpyAsync(&args_.ctl->error, &hctl_->error, sizeof(int), cudaMemcpyHostToDevice, stream_);

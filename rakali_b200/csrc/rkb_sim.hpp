@@ -76,6 +76,10 @@ class Sim {
   int steps_per_graph_cap = 256;
   int sweep_rows = 0;     // FP32 sweep: rows per warp (0: one wave of resident warps)
   int sweep_cpl = 2;      // FP32 sweep: columns per lane (2 or 4)
+  // FP32 sweep: limit of its waits for bulk copies, in clock cycles (the
+  // default unless a test shortens it to make a wait give up)
+  long long wait_cycles = kWaitCyclesDefault;
+  void drop_step_graphs() { drop_graphs(); }
 
   // Arithmetic form of the step: 64 = FP64 depth form (the reference's
   // arithmetic), 32 = FP32 surface form (rkb_step_f32.cu).  Switching brings

@@ -74,7 +74,6 @@ struct Lay {
                 "bulk copies need 16-byte aligned rows and slots");
   static constexpr int slot(int stage) { return stage == 2 ? kSlot2 : kSlot1; }
 };
-constexpr long long kWaitCycles = 2000000000ll;  // ~1 s at B200 clocks
 
 // ---------------------------------------------------------------------------
 // PTX helpers: bulk copies, mbarriers, approximate FP32 math
@@ -121,13 +120,29 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Wait for a phase of `bar` for at most kWaitCycles; warp-uniform result.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  bool ok = mbar_try_wait(bar, parity);
+__device__ __forceinline__ bool mbar_test_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Wait for a phase of `bar` for at most `limit` cycles; warp-uniform result.
+// The default limit (kWaitCyclesDefault, ~1 s) polls with try_wait, which
+// may suspend the thread in hardware while the copy is in flight; a shorter
+// limit (set from the host to test this error path) polls with the
+// non-blocking test_wait, so the limit alone decides when it gives up.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
+  const bool quick = limit < kWaitCyclesDefault;
+  bool ok = quick ? mbar_test_wait(bar, parity) : mbar_try_wait(bar, parity);
   if (!ok) {
     const long long t0 = clock64();
-    while (!(ok = mbar_try_wait(bar, parity)))
-      if (clock64() - t0 > kWaitCycles) break;
+    while (!(ok = quick ? mbar_test_wait(bar, parity) : mbar_try_wait(bar, parity)))
+      if (clock64() - t0 > limit) break;
   }
   return __all_sync(kFull, ok);
 }
@@ -460,6 +475,17 @@ __device__ __forceinline__ int use_int(const int& p) {
   }
 }
 
+template <bool BATCH>
+__device__ __forceinline__ long long use_ll(const long long& p) {
+  if constexpr (!BATCH) {
+    return p;
+  } else {
+    long long v;
+    asm volatile("ld.shared.s64 %0, [%1];" : "=l"(v) : "r"(smem_u32(&p)));
+    return v;
+  }
+}
+
 // STAGE 1: U^n (buffer cur) -> U* (S).  STAGE 2: U*, U^n -> U^{n+1} (cur^1).
 // Block `blk` of the `nblk` blocks that cover one simulation.  PLAIN: no
 // forcing, Coriolis or sponge (the common case), compiled without those paths.
@@ -506,6 +532,8 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
   const unsigned gw = blk * kWarps + warp;
   double part = 0.0, sponge_d = 0.0;
   float wsx = 0.0f, wsy = 0.0f;
+  bool bad = false;  // a new surface of this lane is not finite (a NaN in the
+                     // momenta reaches the surface through the next fluxes)
 
   if (gw < (unsigned)(a.nstrips * a.nrowblk)) {  // warp-uniform
     const int strip = (int)(gw % (unsigned)a.nstrips);
@@ -548,12 +576,14 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
     auto nxt = [](int s) { return s + 1 == kNbuf ? 0 : s + 1; };
     uint32_t ph = 0;
     int ws = 0;  // slot of the next row to wait for
-    auto wait_next = [&]() {
-      const bool r_ok = mbar_wait(bar0 + 8 * ws, (ph >> ws) & 1u);
+    // A wait that gives up leaves its slot the next to wait for, so the
+    // drain below waits for that row's copies again.
+    auto wait_next = [&](long long limit) {
+      if (!mbar_wait(bar0 + 8 * ws, (ph >> ws) & 1u, limit)) return -1;
       ph ^= 1u << ws;
       const int s_done = ws;
       ws = nxt(ws);
-      return r_ok ? s_done : -1;
+      return s_done;
     };
 
     int issued = min(r0 + kNbuf - 1, rlast);
@@ -566,7 +596,7 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
     int waited = r0 - 1;  // last row whose copies have landed
     auto take = [&](int r, Row<C>& R) {
       if (!ok) return;
-      const int sl = wait_next();
+      const int sl = wait_next(use_ll<BATCH>(a.wait_cycles));
       ok = sl >= 0;
       if (ok) {
         read_row<C>(ring + sl * SLOT, base, R);
@@ -598,7 +628,7 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
     const int src_r = (lane + 1) & 31, src_l = (lane + 31) & 31;
     int sj = 2;  // slot of row j
     for (int j = y0; ok && j < yend; ++j) {
-      const int sn = wait_next();  // row j + 2
+      const int sn = wait_next(use_ll<BATCH>(a.wait_cycles));  // row j + 2
       ok = sn >= 0;
       if (!ok) break;
       waited = j + 2;
@@ -769,6 +799,7 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
           const bool w = valid && hfin > kDry;
           wsx = fmaxf(wsx, w ? __fmaf_rn(fabsf(hu), f, c) : 0.0f);
           wsy = fmaxf(wsy, w ? __fmaf_rn(fabsf(hv), f, c) : 0.0f);
+          bad = bad || (valid && !isfinite(e));
         }
       }
       if (out_lane) {
@@ -799,9 +830,11 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
     }
     if (!ok) {
       // a copy did not arrive in time: flag it and let every copy this warp
-      // issued land (each wait bounded) before the shared memory goes away
+      // issued land (each wait bounded by the default limit, whatever limit
+      // gave up) before the shared memory goes away
       if (lane == 0) atomicExch(&ctl->error, kErrWait);
-      for (int r = waited + 1; r <= issued; ++r) wait_next();
+      for (int r = waited + 1; r <= issued; ++r)
+        if (wait_next(kWaitCyclesDefault) < 0) break;
     }
   }
 
@@ -811,6 +844,7 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
   if (STAGE == 2) {
     wsx = (float)warp_max((double)wsx);
     wsy = (float)warp_max((double)wsy);
+    bad = __any_sync(kFull, bad);
   }
   if (lane == 0) {
     double* P = a.partials + (size_t)(STAGE - 1) * 2 * nw;
@@ -819,6 +853,7 @@ __device__ __forceinline__ void sweep_body(const StepArgs32& a, unsigned blk, un
     if (STAGE == 2) {
       atomic_max_pos(&ctl->msx_next, (double)wsx);
       atomic_max_pos(&ctl->msy_next, (double)wsy);
+      if (bad) atomicExch(&ctl->error, kErrNonFinite);
     }
   }
   if (STAGE != 2) return;

@@ -346,6 +346,7 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
       kHalfG * (fya[3 * SM::NFY + fb_] - fya[4 * SM::NFY + ft_] + fya[5 * SM::NFY + ft_]) / dy;
 
   double part = 0.0, sponge_d = 0.0, wsx = 0.0, wsy = 0.0;
+  bool bad = false;  // the new state of this cell is not finite
   if (valid) {
     const size_t q = g.at(i, j);
     if (STAGE == 0) {
@@ -405,7 +406,10 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
       out.hv[q] = v;
       part = o_fh;
       sponge_d = PLAIN ? 0.0 : a - h_pre_sponge;
-      if (STAGE == 2 || (STAGE == 3 && gk == nst - 1)) wave_speed(a, u, v, wsx, wsy);
+      if (STAGE == 2 || (STAGE == 3 && gk == nst - 1)) {
+        wave_speed(a, u, v, wsx, wsy);
+        bad = !isfinite(a + u + v);
+      }
     }
   }
   if (STAGE == 0) return;
@@ -416,9 +420,11 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
   if (STAGE != 1) {
     wsx = warp_max(wsx);
     wsy = warp_max(wsy);
+    bad = __any_sync(0xffffffffu, bad);
     if ((tid & 31) == 0) {
       atomic_max_pos(&ctl->msx_next, wsx);
       atomic_max_pos(&ctl->msy_next, wsy);
+      if (bad) atomicExch(&ctl->error, kErrNonFinite);
     }
   }
   const unsigned int nblocks = gx * gy;

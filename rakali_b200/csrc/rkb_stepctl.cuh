@@ -23,6 +23,7 @@ __device__ __forceinline__ bool step_begin(const StepCtl* c, const Physics* p, c
     dt_max = p->t_end - c->t;
   }
   dt = c->dt_prev;
+  if (c->error != 0) active = false;  // a step reported an error: the rest of the chunk idles
   if (!active) return false;
   if (p->dt_fixed > 0.0) {
     dt = dmin(p->dt_fixed, dt_max);

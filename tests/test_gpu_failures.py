@@ -1,0 +1,73 @@
+"""Failure detection on the device, made to happen without faulting the GPU.
+
+* A bulk-copy wait that runs out (FP32 sweep): the limit of the sweep's waits
+  is set to one cycle, so the first wait of every warp gives up; the kernel
+  flags the step, still waits (with the default limit) for the copies it
+  issued, and returns.  The step fails with a message naming the wait; with
+  the default limit restored the same handle steps normally.
+* A non-finite state: a NaN put into the momentum through the setter is
+  caught by the stage-2 epilogue; the step that produced it completes, the
+  rest of the requested steps do not run, and the call fails with a message
+  naming the step.  Restoring a finite state makes the handle usable again.
+"""
+import numpy as np
+import pytest
+
+from helpers import gaussian_bed, hump_depth
+
+pytestmark = pytest.mark.gpu
+
+NX, NY, DX = 200, 150, 5.0
+
+
+def _sim(precision):
+    from rakali_b200 import Rakali
+    b = gaussian_bed(NX, NY, DX, DX, 8, seed=2, width=(30.0, 150.0))
+    h = hump_depth(b, DX, DX, width=80.0)
+    s = Rakali(defer_init=True, nx=NX, ny=NY, dx=DX, dy=DX, t_end=1e6, cfl=0.45,
+               manning_n=0.025)
+    s.set_bathymetry(b)
+    s.set_initial_h(h)
+    s.finalize()
+    s.set_precision(precision)
+    return s
+
+
+def test_expired_bulk_copy_wait_fails_the_step_and_the_handle_recovers():
+    with _sim(32) as s:
+        s.step(2)
+        state = [a.copy() for a in (s.h_phys, s.hu_phys, s.hv_phys)]
+        lib = s._lib
+        assert lib.rkb_set_wait_limit(s._handle, 1) == 0
+        with pytest.raises(RuntimeError, match="wait for a bulk copy expired"):
+            s.step(3)
+        assert lib.rkb_set_wait_limit(s._handle, 0) == 0
+        s.set_h(state[0])
+        s.set_hu(state[1])
+        s.set_hv(state[2])
+        n0 = s.step_count
+        s.step(3)
+        assert s.step_count == n0 + 3
+        assert np.all(np.isfinite(s.h_phys))
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_nan_in_the_state_is_reported_not_propagated_silently(precision):
+    with _sim(precision) as s:
+        s.step(2)
+        good = [a.copy() for a in (s.h_phys, s.hu_phys, s.hv_phys)]
+        wet = np.argwhere(good[0] > 0.5)
+        i, j = wet[len(wet) // 2]
+        bad_hu = good[1].copy()
+        bad_hu[i, j] = np.nan
+        s.set_hu(bad_hu)
+        n0 = s.step_count
+        with pytest.raises(RuntimeError, match="non-finite"):
+            s.step(5)
+        assert s.step_count == n0 + 1  # the step that met the NaN, none after it
+        s.set_h(good[0])
+        s.set_hu(good[1])
+        s.set_hv(good[2])
+        s.step(3)
+        assert s.step_count == n0 + 4
+        assert np.all(np.isfinite(s.h_phys)) and np.all(np.isfinite(s.hu_phys))
