@@ -427,12 +427,20 @@ def run_ensemble(args, world, local_rank, dist):
             with ClockSampler(rp.visible_gpu_index(local_rank)) as clk:
                 ms = ens.time_steps(args.ensemble_steps)
             ms = rp.max_over_ranks(ms, dist)
+            # the same steps launch by launch, with events between the phases:
+            # what the six launches of a step cost beyond their kernels
+            phases = ens.profile_steps(20)
+            kernel_sum = sum(phases[k] for k in ("bc_stage1", "stage1", "bc_stage2", "stage2"))
+            graph_ms = ms / args.ensemble_steps
             out["forms"][f"fp{prec}"] = {
                 "value": rp.weak_value(world, cells, args.ensemble_steps, ms),
                 "unit": "cell-updates/s", "steps": args.ensemble_steps,
-                "ms_per_step": ms / args.ensemble_steps, "variant": list(ens.variant),
+                "ms_per_step": graph_ms, "variant": list(ens.variant),
                 "autotune_best_ms_per_step": best, "clocks": clk.summary(),
-                "launches_per_step": 6}
+                "launches_per_step": 6,
+                "phases_ms_per_step": phases,
+                "launch_overhead": {"kernel_sum_ms": kernel_sum, "graph_ms_per_step": graph_ms,
+                                    "share_outside_kernels": (graph_ms - kernel_sum) / graph_ms}}
     for s in sims:
         s.close()
     return out
@@ -826,8 +834,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--tile", type=int, default=1,
-                    help="stage-kernel variant (rkb_set_tile): 0-3 shared-memory tiles, "
+    ap.add_argument("--tile", type=int, default=3,
+                    help="stage-kernel variant (rkb_set_tile): 0-3 shared-memory tiles "
+                         "32x8, 32x16, 64x4, 16x16 (default 16x16, the fastest measured), "
                          "4/5 marching strips of 64/32 rows, 6/7 tiles 32x8 / 32x12 with two "
                          "extra warps")
     ap.add_argument("--precision", type=int, choices=(32, 64), default=64,

@@ -185,6 +185,12 @@ int rkb_batch_step(void *batch, int n_steps);
 int rkb_batch_advance(void *batch, double target_time);
 /* n steps of every member between CUDA events on the batch's stream. */
 int rkb_batch_time_steps(void *batch, int n, double *ms);
+/* n steps of every member launched phase by phase with CUDA events between
+ * the launches: out5[0..3] = mean ms per step of the stage-1 boundary fills,
+ * stage 1, the stage-2 fills and stage 2; out5[4] = mean ms per step of the
+ * whole sequence.  Set beside rkb_batch_time_steps (the same steps replayed
+ * from CUDA graphs) it shows what the launches themselves cost. */
+int rkb_batch_profile_steps(void *batch, int n, double *out5);
 /* Times each candidate kernel shape (FP64: the four tiles; FP32: 2 or 4
  * columns per lane x rows per warp sweep) for trial_steps steps on the live
  * state, restores the state exactly, keeps the fastest shape. */

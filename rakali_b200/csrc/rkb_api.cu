@@ -639,6 +639,14 @@ int rkb_batch_time_steps(void* batch, int n, double* ms) {
   return rc ? fail(rc, b->error().empty() ? "batch timing failed" : b->error()) : 0;
 }
 
+int rkb_batch_profile_steps(void* batch, int n, double* out5) {
+  rkb::Batch* b = batch_of(batch);
+  if (!b) return kBadHandle;
+  if (!out5) return -2;
+  const int rc = b->profile_steps(n, out5);
+  return rc ? fail(rc, b->error().empty() ? "batch profiling failed" : b->error()) : 0;
+}
+
 int rkb_batch_autotune(void* batch, int trial_steps, double* best_ms_per_step) {
   rkb::Batch* b = batch_of(batch);
   if (!b) return kBadHandle;

@@ -279,6 +279,38 @@ int Batch::time_steps(int n, double* ms) {
   return finish();
 }
 
+int Batch::profile_steps(int n, double out[5]) {
+  if (n <= 0) return -2;
+  if (prepare(1, 0.0, n) != 0) return -1;
+  cudaEvent_t ev[5];
+  for (auto& e : ev) RKB_TRY(cudaEventCreate(&e));
+  double acc[5] = {0, 0, 0, 0, 0};
+  for (int k = 0; k < n; ++k) {
+    const bool f32 = prec_ == 32;
+    RKB_TRY(cudaEventRecord(ev[0], stream_));
+    RKB_TRY(f32 ? launch_bc32_batch(bl32_, 1, stream_) : launch_bc_batch(bl_, 1, stream_));
+    RKB_TRY(cudaEventRecord(ev[1], stream_));
+    RKB_TRY(f32 ? launch_stage32_batch(bl32_, 1, stream_) : launch_stage_batch_only(bl_, 1, stream_));
+    RKB_TRY(cudaEventRecord(ev[2], stream_));
+    RKB_TRY(f32 ? launch_bc32_batch(bl32_, 2, stream_) : launch_bc_batch(bl_, 2, stream_));
+    RKB_TRY(cudaEventRecord(ev[3], stream_));
+    RKB_TRY(f32 ? launch_stage32_batch(bl32_, 2, stream_) : launch_stage_batch_only(bl_, 2, stream_));
+    RKB_TRY(cudaEventRecord(ev[4], stream_));
+    RKB_TRY(cudaEventSynchronize(ev[4]));
+    for (int p = 0; p < 4; ++p) {
+      float f = 0.0f;
+      RKB_TRY(cudaEventElapsedTime(&f, ev[p], ev[p + 1]));
+      acc[p] += f;
+    }
+    float f = 0.0f;
+    RKB_TRY(cudaEventElapsedTime(&f, ev[0], ev[4]));
+    acc[4] += f;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (int p = 0; p < 5; ++p) out[p] = acc[p] / n;
+  return finish();
+}
+
 // Candidate shapes: FP64 the four shared-memory tiles; FP32 2 or 4 columns
 // per lane times rows per warp sweep (0 = one wave of resident warps per member).
 int Batch::autotune(int trial_steps, double* best_ms) {

@@ -25,6 +25,12 @@ class Batch {
   int step(int n);                    // n steps of every member
   int advance(double target);         // every member to `target` (own dt)
   int time_steps(int n, double* ms);  // n steps between CUDA events
+  // n steps launched phase by phase with events between the phases:
+  // out[0..3] = mean ms per step of the stage-1 boundary fills, stage 1, the
+  // stage-2 fills and stage 2 (every member in each launch); out[4] = mean ms
+  // per step of the whole launch-by-launch sequence (phases plus the gaps
+  // between launches).
+  int profile_steps(int n, double out[5]);
   // Time each candidate kernel shape for `trial_steps` steps on the live
   // state (restored afterwards), keep the fastest; *best_ms = its time per step.
   int autotune(int trial_steps, double* best_ms);

@@ -147,6 +147,8 @@ struct BatchLaunch {
 int batch_stage_blocks(const Grid& g, int tile);
 cudaError_t configure_batch(int tile, int hllc);
 cudaError_t launch_step_batch(const BatchLaunch& bl, cudaStream_t s);
+cudaError_t launch_bc_batch(const BatchLaunch& bl, int stage, cudaStream_t s);
+cudaError_t launch_stage_batch_only(const BatchLaunch& bl, int stage, cudaStream_t s);
 
 struct BatchLaunch32 {
   const StepArgs32* args;

@@ -474,8 +474,16 @@ __device__ __forceinline__ bool plain_mismatch64(StepCtl* ctl, const Physics* ph
   return true;
 }
 
+// Resident blocks per SM the stage kernels are built for: as many as 64
+// registers a thread and the tile's shared memory allow (4 for the 256-thread
+// tiles, 3 for 288 threads, 2 for 448 and 512).  Left free, the compiler
+// gives the stages more registers than that occupancy allows.
+constexpr int stage_blocks_per_sm(int threads) {
+  return threads <= 256 ? 4 : threads <= 320 ? 3 : 2;
+}
+
 template <int TX, int TY, bool HLLC, int STAGE, int XW = 0, bool PLAIN = false>
-__global__ void __launch_bounds__(TX * TY + 32 * XW)
+__global__ void __launch_bounds__(TX * TY + 32 * XW, stage_blocks_per_sm(TX * TY + 32 * XW))
     k_stage(Grid g, StepCtl* ctl, const Physics* phys, const BcParams* bcp, FieldSet U0,
             FieldSet U1, FieldSet S, const double* __restrict__ b, Forcing fo,
             double* __restrict__ partials, FluxOut fl, int gk) {
@@ -489,14 +497,8 @@ __global__ void __launch_bounds__(TX * TY + 32 * XW)
 
 // Every simulation of a batch in one launch: map[blockIdx.x] = (simulation,
 // tile index within that simulation's tiling).
-// Blocks per SM that shared memory allows (2 for the 512- and 448-thread
-// tiles, 3 for the others), as the single-simulation kernels reach by
-// themselves: left free, the compiler gives some batch stages more registers
-// than that occupancy allows.
-constexpr int batch_blocks_per_sm(int threads) { return threads <= 320 ? 3 : 2; }
-
 template <int TX, int TY, bool HLLC, int STAGE, int XW = 0, bool PLAIN = false>
-__global__ void __launch_bounds__(TX * TY + 32 * XW, batch_blocks_per_sm(TX * TY + 32 * XW))
+__global__ void __launch_bounds__(TX * TY + 32 * XW, stage_blocks_per_sm(TX * TY + 32 * XW))
     k_stage_batch(const StepArgs* __restrict__ args, const int2* __restrict__ map) {
   __shared__ StepArgs sa;
   const int2 m = map[blockIdx.x];
@@ -1011,6 +1013,10 @@ cudaError_t launch_bc_batch(const BatchLaunch& bl, int stage, cudaStream_t s) {
   const dim3 gy((unsigned)((bl.max_nxt + tpb - 1) / tpb), 2, (unsigned)bl.n);
   k_bc_batch<<<gy, tpb, 0, s>>>(bl.args, stage, 2, 0);
   return cudaGetLastError();
+}
+
+cudaError_t launch_stage_batch_only(const BatchLaunch& bl, int stage, cudaStream_t s) {
+  return stage == 1 ? launch_stage_batch<1>(bl, s) : launch_stage_batch<2>(bl, s);
 }
 
 cudaError_t launch_step_batch(const BatchLaunch& bl, cudaStream_t s) {

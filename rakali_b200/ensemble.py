@@ -55,6 +55,16 @@ class Ensemble:
         self._rc(self._lib.rkb_batch_time_steps(self._b, int(n), ctypes.byref(ms)), "time_steps")
         return ms.value
 
+    def profile_steps(self, n: int) -> dict:
+        """Mean device ms per step of each launch phase over ``n`` steps issued
+        launch by launch (boundary fills and stages of every member), and of
+        the whole sequence."""
+        self._check()
+        out = (ctypes.c_double * 5)()
+        self._rc(self._lib.rkb_batch_profile_steps(self._b, int(n), out), "profile_steps")
+        return {"bc_stage1": out[0], "stage1": out[1], "bc_stage2": out[2], "stage2": out[3],
+                "launch_by_launch": out[4]}
+
     def autotune(self, trial_steps: int = 3) -> float:
         """Pick the fastest kernel shape on the live state (restored); ms per step."""
         self._check()
