@@ -165,11 +165,12 @@ int rkb_get_precision(void *handle);
  * not depend on either. */
 int rkb_set_sweep(void *handle, int cols_per_lane, int rows);
 /* FP32 form: limit, in GPU clock cycles, of the sweep's waits for its bulk
- * row copies (<= 0: the default, about one second).  A wait that runs out
- * makes the step fail with -1 and a message in rki_last_error(); the copies
- * in flight are still waited for (with the default limit) before the kernel
- * returns.  No counterpart in the reference: it exists so that the error
- * path can be exercised. */
+ * row copies (<= 0: the default, about one second; a limit shorter than one
+ * clock read gives up at once).  A wait that runs out makes the step fail
+ * with -1 and a message in rki_last_error(); the copies in flight are still
+ * waited for (with the default limit) before the kernel returns.  No
+ * counterpart in the reference: it exists so that the error path can be
+ * exercised. */
 int rkb_set_wait_limit(void *handle, long long cycles);
 
 /* Batches of independent simulations (ensembles of uneven sizes): every

@@ -133,16 +133,24 @@ __device__ __forceinline__ bool mbar_test_wait(uint32_t bar, uint32_t parity) {
 
 // Wait for a phase of `bar` for at most `limit` cycles; warp-uniform result.
 // The default limit (kWaitCyclesDefault, ~1 s) polls with try_wait, which
-// may suspend the thread in hardware while the copy is in flight; a shorter
+// may suspend the thread in hardware while the copy is in flight.  A shorter
 // limit (set from the host to test this error path) polls with the
-// non-blocking test_wait, so the limit alone decides when it gives up.
+// non-blocking test_wait and only while the limit has not passed, so the
+// limit alone decides when the wait gives up: one shorter than a clock read
+// gives up at once.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
-  const bool quick = limit < kWaitCyclesDefault;
-  bool ok = quick ? mbar_test_wait(bar, parity) : mbar_try_wait(bar, parity);
-  if (!ok) {
+  bool ok = false;
+  if (limit >= kWaitCyclesDefault) {
+    ok = mbar_try_wait(bar, parity);
+    if (!ok) {
+      const long long t0 = clock64();
+      while (!(ok = mbar_try_wait(bar, parity)))
+        if (clock64() - t0 > limit) break;
+    }
+  } else {
     const long long t0 = clock64();
-    while (!(ok = quick ? mbar_test_wait(bar, parity) : mbar_try_wait(bar, parity)))
-      if (clock64() - t0 > limit) break;
+    while (clock64() - t0 <= limit)
+      if ((ok = mbar_test_wait(bar, parity))) break;
   }
   return __all_sync(kFull, ok);
 }
