@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 
 namespace rkb {
 
@@ -77,7 +78,66 @@ Sim::~Sim() {
     p = nullptr;
   }
   if (hctl_) cudaFreeHost(hctl_);
+  for (int k = 0; k < 2; ++k) {
+    if (stage_buf_[k]) cudaFreeHost(stage_buf_[k]);
+    if (stage_ev_[k]) cudaEventDestroy(stage_ev_[k]);
+  }
   if (stream_) cudaStreamDestroy(stream_);
+}
+
+namespace {
+constexpr size_t kStageBytes = size_t(16) << 20;  // per staging buffer
+
+// rows [r0, r1) of an (nx)-wide row-major block copied with up to `nt`
+// threads (each a contiguous band of rows)
+void copy_rows(double* dst, const double* src, size_t nx, int r0, int r1) {
+  const int rows = r1 - r0;
+  const unsigned hw = std::thread::hardware_concurrency();
+  const int nt = (int)std::max(1u, std::min(hw ? hw : 1u, 8u));
+  const size_t bytes = (size_t)rows * nx * sizeof(double);
+  if (nt == 1 || bytes < (size_t(1) << 20)) {
+    std::memcpy(dst, src + (size_t)r0 * nx, bytes);
+    return;
+  }
+  std::vector<std::thread> th;
+  th.reserve(nt);
+  for (int t = 0; t < nt; ++t) {
+    const int a = r0 + rows * t / nt, b = r0 + rows * (t + 1) / nt;
+    if (a < b)
+      th.emplace_back([=] {
+        std::memcpy(dst + (size_t)(a - r0) * nx, src + (size_t)a * nx,
+                    (size_t)(b - a) * nx * sizeof(double));
+      });
+  }
+  for (auto& t : th) t.join();
+}
+}  // namespace
+
+int Sim::upload_rows(double* dst, const double* src, int nx, int ny) {
+  const size_t row_bytes = (size_t)nx * sizeof(double);
+  const int chunk = (int)std::max<size_t>(1, kStageBytes / row_bytes);
+  if ((size_t)chunk * row_bytes > kStageBytes) {  // one row exceeds a buffer
+    RKB_TRY(cudaMemcpy2DAsync(dst, (size_t)g.pitch * sizeof(double), src, row_bytes, row_bytes,
+                              ny, cudaMemcpyHostToDevice, stream_));
+    return 0;
+  }
+  for (int k = 0; k < 2; ++k) {
+    if (!stage_buf_[k]) RKB_TRY(cudaMallocHost(&stage_buf_[k], kStageBytes));
+    if (!stage_ev_[k]) RKB_TRY(cudaEventCreateWithFlags(&stage_ev_[k], cudaEventDisableTiming));
+  }
+  int k = 0;
+  bool used[2] = {false, false};
+  for (int r0 = 0; r0 < ny; r0 += chunk, k ^= 1) {
+    const int r1 = std::min(ny, r0 + chunk);
+    if (used[k]) RKB_TRY(cudaEventSynchronize(stage_ev_[k]));  // its previous DMA is done
+    copy_rows(static_cast<double*>(stage_buf_[k]), src, (size_t)nx, r0, r1);
+    RKB_TRY(cudaMemcpy2DAsync(dst + (size_t)r0 * g.pitch, (size_t)g.pitch * sizeof(double),
+                              stage_buf_[k], row_bytes, row_bytes, r1 - r0,
+                              cudaMemcpyHostToDevice, stream_));
+    RKB_TRY(cudaEventRecord(stage_ev_[k], stream_));
+    used[k] = true;
+  }
+  return 0;
 }
 
 int Sim::create(const std::string& text, std::string& err) {
@@ -826,11 +886,13 @@ int Sim::set_interior(int which, const double* data, int nx, int ny) {
     double* dstd[3] = {F.h, F.hu, F.hv};
     const size_t off_d = (size_t)g.ng + (size_t)g.ng * (size_t)g.pitch;
     const size_t off_h = (size_t)g.ng + (size_t)g.ng * (size_t)g.nxt;
-    const double* src = direct ? data : hf_[f] + off_h;
-    const size_t spitch = direct ? (size_t)nx * sizeof(double) : wbytes;
-    if (cudaMemcpy2DAsync(dstd[f] + off_d, dpitch, src, spitch, (size_t)nx * sizeof(double), ny,
-                          cudaMemcpyHostToDevice, stream_) != cudaSuccess)
+    if (direct) {
+      if (upload_rows(dstd[f] + off_d, data, nx, ny) != 0) return -1;
+    } else if (cudaMemcpy2DAsync(dstd[f] + off_d, dpitch, hf_[f] + off_h, wbytes,
+                                 (size_t)nx * sizeof(double), ny, cudaMemcpyHostToDevice,
+                                 stream_) != cudaSuccess) {
       return -1;
+    }
     if (precision_ == 32 && to_surface(true, f) != 0) return -1;
     hctl_->ms_valid = 0;
     if (cudaMemcpyAsync(&args_.ctl->ms_valid, &hctl_->ms_valid, sizeof(int),

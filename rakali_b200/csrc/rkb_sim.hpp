@@ -159,6 +159,12 @@ class Sim {
   bool field_current(int f) const {
     return host_is_current_ || fcur_[f] || (f <= 2 && host_state_current_);
   }
+  // Caller's (nx, ny) interior rows -> device rows starting at `dst` (pitch
+  // in elements), through two pinned staging buffers: host threads copy one
+  // chunk of rows while the previous chunk's DMA runs.
+  int upload_rows(double* dst, const double* src, int nx, int ny);
+  void* stage_buf_[2] = {nullptr, nullptr};
+  cudaEvent_t stage_ev_[2] = {nullptr, nullptr};
   int pull_field(int f);      // device -> host array f (FP32: through the depth form)
   int pull_missing(int upto);  // every field f < upto whose host array is not current
   int push_field(int f);      // host array f -> device (f <= 3)
