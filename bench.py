@@ -777,8 +777,11 @@ def run_b200(args, rank, world, local_rank, dist):
     forms = {}
     for prec in (head, other) if args.both_forms else (head,):
         sim.set_precision(prec)
+        # the inputs of the end-to-end leg: the initial state in ordinary
+        # (written, so resident) host arrays
+        zeros = np.full(h.shape, 0.0, order="F")
         forms[prec] = _form_numbers(sim, args, world, local_rank, dist, cells,
-                                    (h, np.zeros_like(h), np.zeros_like(h)))
+                                    (h, zeros, zeros.copy(order="F")))
         forms[prec]["roofline"] = _roofline(forms[prec], prec, cells, world)
     sim.close()
     ens = run_ensemble(args, world, local_rank, dist) if args.ensemble_steps > 0 else None

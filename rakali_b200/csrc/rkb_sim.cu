@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <thread>
 
 namespace rkb {
@@ -78,15 +79,39 @@ Sim::~Sim() {
     p = nullptr;
   }
   if (hctl_) cudaFreeHost(hctl_);
-  for (int k = 0; k < 2; ++k) {
-    if (stage_buf_[k]) cudaFreeHost(stage_buf_[k]);
-    if (stage_ev_[k]) cudaEventDestroy(stage_ev_[k]);
-  }
   if (stream_) cudaStreamDestroy(stream_);
 }
 
 namespace {
 constexpr size_t kStageBytes = size_t(16) << 20;  // per staging buffer
+
+// Two pinned staging buffers shared by every simulation of the process (one
+// upload at a time holds them), allocated by the first finalize on a device
+// so no timed upload pays for the pinned allocation.  Their events are
+// recorded on whichever stream used them last.
+struct Staging {
+  std::mutex mu;
+  void* buf[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  bool used[2] = {false, false};
+  int ensure() {
+    for (int k = 0; k < 2; ++k) {
+      if (!buf[k] && cudaMallocHost(&buf[k], kStageBytes) != cudaSuccess) {
+        buf[k] = nullptr;
+        return -1;
+      }
+      if (!ev[k] && cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming) != cudaSuccess) {
+        ev[k] = nullptr;
+        return -1;
+      }
+    }
+    return 0;
+  }
+};
+Staging& staging() {
+  static Staging* st = new Staging();  // lives until exit (pinned memory freed by the driver)
+  return *st;
+}
 
 // rows [r0, r1) of an (nx)-wide row-major block copied with up to `nt`
 // threads (each a contiguous band of rows)
@@ -121,22 +146,22 @@ int Sim::upload_rows(double* dst, const double* src, int nx, int ny) {
                               ny, cudaMemcpyHostToDevice, stream_));
     return 0;
   }
-  for (int k = 0; k < 2; ++k) {
-    if (!stage_buf_[k]) RKB_TRY(cudaMallocHost(&stage_buf_[k], kStageBytes));
-    if (!stage_ev_[k]) RKB_TRY(cudaEventCreateWithFlags(&stage_ev_[k], cudaEventDisableTiming));
-  }
+  Staging& st = staging();
+  std::lock_guard<std::mutex> lk(st.mu);
+  if (st.ensure() != 0) return -1;
   int k = 0;
-  bool used[2] = {false, false};
   for (int r0 = 0; r0 < ny; r0 += chunk, k ^= 1) {
     const int r1 = std::min(ny, r0 + chunk);
-    if (used[k]) RKB_TRY(cudaEventSynchronize(stage_ev_[k]));  // its previous DMA is done
-    copy_rows(static_cast<double*>(stage_buf_[k]), src, (size_t)nx, r0, r1);
+    if (st.used[k]) RKB_TRY(cudaEventSynchronize(st.ev[k]));  // its previous DMA is done
+    copy_rows(static_cast<double*>(st.buf[k]), src, (size_t)nx, r0, r1);
     RKB_TRY(cudaMemcpy2DAsync(dst + (size_t)r0 * g.pitch, (size_t)g.pitch * sizeof(double),
-                              stage_buf_[k], row_bytes, row_bytes, r1 - r0,
-                              cudaMemcpyHostToDevice, stream_));
-    RKB_TRY(cudaEventRecord(stage_ev_[k], stream_));
-    used[k] = true;
+                              st.buf[k], row_bytes, row_bytes, r1 - r0, cudaMemcpyHostToDevice,
+                              stream_));
+    RKB_TRY(cudaEventRecord(st.ev[k], stream_));
+    st.used[k] = true;
   }
+  // the buffers are free again once this stream's copies are done
+  RKB_TRY(cudaEventSynchronize(st.ev[k ^ 1]));
   return 0;
 }
 
@@ -314,6 +339,14 @@ int Sim::finalize(std::string& err) {
 
   int rc = alloc_device(err);
   if (rc != 0) return rc;
+  {  // the setters' staging buffers, once per process
+    Staging& st = staging();
+    std::lock_guard<std::mutex> lk(st.mu);
+    if (st.ensure() != 0) {
+      err = "pinned staging allocation failed";
+      return -1;
+    }
+  }
   for (int w = 0; w < 4; ++w)
     RKB_TRY(cudaMemcpyAsync(args_.eta_old[w], eta_old_[w].data(),
                             eta_old_[w].size() * sizeof(double), cudaMemcpyHostToDevice,

@@ -163,8 +163,6 @@ class Sim {
   // in elements), through two pinned staging buffers: host threads copy one
   // chunk of rows while the previous chunk's DMA runs.
   int upload_rows(double* dst, const double* src, int nx, int ny);
-  void* stage_buf_[2] = {nullptr, nullptr};
-  cudaEvent_t stage_ev_[2] = {nullptr, nullptr};
   int pull_field(int f);      // device -> host array f (FP32: through the depth form)
   int pull_missing(int upto);  // every field f < upto whose host array is not current
   int push_field(int f);      // host array f -> device (f <= 3)
