@@ -166,19 +166,21 @@ __global__ void k_max_speed(Grid g, StepCtl* ctl, FieldSet U0, FieldSet U1) {
 // Shared-memory plan of one TX x TY tile (doubles):
 //   tile  4 x (TX+4)(TY+4)   h, hu, hv, b with a 2-cell halo (eta = h + b is
 //                            formed where it is read, with the same rounding)
-//   sx    3 x (TX+2) TY      limited x-slopes of eta, hu, hv
-//   sy    3 x TX (TY+2)      limited y-slopes
 //   fx    6 x (TX+1) TY      x-face fluxes + well-balanced terms
 //   fy    6 x TX (TY+1)      y-face fluxes + well-balanced terms
+//   old   3 x TX TY          U^n of the tile's cells (stage 2: the RK2 average)
+// The limited slopes are not stored: each face computes the slopes of its
+// two cells along its normal from the tile (every slope twice, the same
+// expressions, so the same bits), which spares the slope arrays and a block
+// barrier.
 template <int TX, int TY>
 struct StageSmem {
   static constexpr int TW = TX + 4, TH = TY + 4;
   static constexpr int NT = TW * TH;
-  static constexpr int NSX = (TX + 2) * TY;
-  static constexpr int NSY = TX * (TY + 2);
   static constexpr int NFX = (TX + 1) * TY;
   static constexpr int NFY = TX * (TY + 1);
-  static constexpr int DOUBLES = 4 * NT + 3 * NSX + 3 * NSY + 6 * NFX + 6 * NFY;
+  static constexpr int NC = TX * TY;
+  static constexpr int DOUBLES = 4 * NT + 6 * NFX + 6 * NFY + 3 * NC;
   static constexpr size_t BYTES = sizeof(double) * (size_t)DOUBLES;
 };
 
@@ -211,14 +213,11 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
   double* tu = th + SM::NT;
   double* tv = tu + SM::NT;
   double* tb = tv + SM::NT;
-  double* sxe = tb + SM::NT;
-  double* sxu = sxe + SM::NSX;
-  double* sxv = sxu + SM::NSX;
-  double* sye = sxv + SM::NSX;
-  double* syu = sye + SM::NSY;
-  double* syv = syu + SM::NSY;
-  double* fxa = syv + SM::NSY;  // 6 arrays of NFX: fh, fqx, fqy, wbR, hL2, pL2
+  double* fxa = tb + SM::NT;  // 6 arrays of NFX: fh, fqx, fqy, wbR, hL2, pL2
   double* fya = fxa + 6 * SM::NFX;
+  double* oh = fya + 6 * SM::NFY;  // U^n of the tile's cells (stage 2)
+  double* ou = oh + SM::NC;
+  double* ov = ou + SM::NC;
 
   double dt = 0.0;
   int cur = 0;
@@ -259,49 +258,42 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
     }
     th[k] = vh; tu[k] = vu; tv[k] = vv; tb[k] = vb;
   }
-  if (STAGE == 2 && tid < TX * TY) {
-    // the RK2 average reads U^n of this thread's cell after the face phase:
-    // start bringing those lines into L2 now
-    const int pi = gx0 + tid % TX, pj = gy0 + tid / TX;
-    if (pi < g.nxt - g.ng && pj < g.nyt - g.ng) {
-      const FieldSet old = cur ? U1 : U0;
-      const size_t q = g.at(pi, pj);
-      asm volatile("prefetch.global.L2 [%0];" ::"l"(old.h + q));
-      asm volatile("prefetch.global.L2 [%0];" ::"l"(old.hu + q));
-      asm volatile("prefetch.global.L2 [%0];" ::"l"(old.hv + q));
+  if (STAGE == 2) {
+    // U^n of the tile's cells for the RK2 average, loaded with the tile so
+    // its latency passes during the face phase (each cell thread reads back
+    // what it loaded)
+    const FieldSet old = cur ? U1 : U0;
+    for (int k = tid; k < SM::NC; k += NTH) {
+      const int pi = gx0 + k % TX, pj = gy0 + k / TX;
+      if (pi < g.nxt - g.ng && pj < g.nyt - g.ng) {
+        const size_t q = g.at(pi, pj);
+        oh[k] = old.h[q];
+        ou[k] = old.hu[q];
+        ov[k] = old.hv[q];
+      }
     }
   }
   __syncthreads();
 
   auto te = [&](int q) { return th[q] + tb[q]; };  // the surface eta = h + b
+  // limited slope (eta, hu, hv) of tile cell q along the direction whose
+  // neighbours are q - d and q + d
+  auto slope_at = [&](int q, int d, double& se, double& su, double& sv) {
+    cell_slope(th[q - d], th[q], th[q + d], te(q - d), te(q), te(q + d), tu[q - d], tu[q],
+               tu[q + d], tv[q - d], tv[q], tv[q + d], se, su, sv);
+  };
 
-  // 2. limited slopes: x for cells c in [-1, TX], y for rows r in [-1, TY]
-  for (int k = tid; k < SM::NSX + SM::NSY; k += NTH) {
-    if (k < SM::NSX) {
-      const int c = k % (TX + 2) - 1, r = k / (TX + 2);
-      const int q = (r + 2) * TW + (c + 2);
-      cell_slope(th[q - 1], th[q], th[q + 1], te(q - 1), te(q), te(q + 1), tu[q - 1], tu[q],
-                 tu[q + 1], tv[q - 1], tv[q], tv[q + 1], sxe[k], sxu[k], sxv[k]);
-    } else {
-      const int kk = k - SM::NSX;
-      const int c = kk % TX, r = kk / TX - 1;
-      const int q = (r + 2) * TW + (c + 2);
-      cell_slope(th[q - TW], th[q], th[q + TW], te(q - TW), te(q), te(q + TW), tu[q - TW], tu[q],
-                 tu[q + TW], tv[q - TW], tv[q], tv[q + TW], sye[kk], syu[kk], syv[kk]);
-    }
-  }
-  __syncthreads();
-
-  // 3. faces, each evaluated once
+  // 2. faces, each evaluated once, with the slopes of its two cells
   for (int k = tid; k < SM::NFX + SM::NFY; k += NTH) {
     FaceOut o;
     if (k < SM::NFX) {
       const int c = k % (TX + 1), r = k / (TX + 1);  // face between c-1 and c
       const int qL = (r + 2) * TW + (c + 1), qR = qL + 1;
-      const int sL = r * (TX + 2) + c, sR = sL + 1;  // slope index of cell c-1 and c
-      face_flux<0, HLLC>(te(qL) + 0.5 * sxe[sL], tu[qL] + 0.5 * sxu[sL], tv[qL] + 0.5 * sxv[sL],
-                         tb[qL], te(qR) - 0.5 * sxe[sR], tu[qR] - 0.5 * sxu[sR],
-                         tv[qR] - 0.5 * sxv[sR], tb[qR], o);
+      double sLe, sLu, sLv, sRe, sRu, sRv;
+      slope_at(qL, 1, sLe, sLu, sLv);
+      slope_at(qR, 1, sRe, sRu, sRv);
+      face_flux<0, HLLC>(te(qL) + 0.5 * sLe, tu[qL] + 0.5 * sLu, tv[qL] + 0.5 * sLv, tb[qL],
+                         te(qR) - 0.5 * sRe, tu[qR] - 0.5 * sRu, tv[qR] - 0.5 * sRv, tb[qR], o);
       fxa[k] = o.fh;
       fxa[SM::NFX + k] = o.fqx;
       fxa[2 * SM::NFX + k] = o.fqy;
@@ -312,10 +304,11 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
       const int kk = k - SM::NFX;
       const int c = kk % TX, r = kk / TX;  // face between rows r-1 and r
       const int qB = (r + 1) * TW + (c + 2), qT = qB + TW;
-      const int sB = r * TX + c, sT = sB + TX;  // y-slope index of rows r-1 and r
-      face_flux<1, HLLC>(te(qB) + 0.5 * sye[sB], tu[qB] + 0.5 * syu[sB], tv[qB] + 0.5 * syv[sB],
-                         tb[qB], te(qT) - 0.5 * sye[sT], tu[qT] - 0.5 * syu[sT],
-                         tv[qT] - 0.5 * syv[sT], tb[qT], o);
+      double sBe, sBu, sBv, sTe, sTu, sTv;
+      slope_at(qB, TW, sBe, sBu, sBv);
+      slope_at(qT, TW, sTe, sTu, sTv);
+      face_flux<1, HLLC>(te(qB) + 0.5 * sBe, tu[qB] + 0.5 * sBu, tv[qB] + 0.5 * sBv, tb[qB],
+                         te(qT) - 0.5 * sTe, tu[qT] - 0.5 * sTu, tv[qT] - 0.5 * sTv, tb[qT], o);
       fya[kk] = o.fh;
       fya[SM::NFY + kk] = o.fqx;
       fya[2 * SM::NFY + kk] = o.fqy;
@@ -326,7 +319,7 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
   }
   __syncthreads();
 
-  // 4. cell update: one cell per thread (the extra warps repeat cell 0 and
+  // 3. cell update: one cell per thread (the extra warps repeat cell 0 and
   // store nothing)
   const int tc = tid < TX * TY ? tid : 0;
   const int c = tc % TX, r = tc / TX;
@@ -392,11 +385,10 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
         }
       } else {
         // RK2 average with U^n and the second clamp (rki_kernel_fused.F90:435-463)
-        const FieldSet old = cur ? U1 : U0;
         out = cur ? U0 : U1;
-        a = 0.5 * (old.h[q] + a);
-        u = 0.5 * (old.hu[q] + u);
-        v = 0.5 * (old.hv[q] + v);
+        a = 0.5 * (oh[tc] + a);
+        u = 0.5 * (ou[tc] + u);
+        v = 0.5 * (ov[tc] + v);
         protect(a, u, v);
       }
       const double h_pre_sponge = a;
@@ -415,7 +407,7 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
   if (STAGE == 0) return;
   if (STAGE == 3 && gk != nst - 1) return;  // block-uniform
 
-  // 5. block partials (fixed order) and the CFL maxima of the new state
+  // 4. block partials (fixed order) and the CFL maxima of the new state
   constexpr bool kBudget = STAGE != 3;
   if (STAGE != 1) {
     wsx = warp_max(wsx);
@@ -451,7 +443,7 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
   }
   if (STAGE == 1) return;
 
-  // 6. last block closes the step
+  // 5. last block closes the step
   __shared__ bool last;
   if (tid == 0) {
     __threadfence();
