@@ -140,6 +140,28 @@ def traffic_per_launch(n_cells: int, precision: int = 64):
     return d["dram_bytes_per_launch"] * n_cells / d["cells"]
 
 
+# Issue capacity of a B200: 148 SMs x 4 schedulers x 1 warp instruction per
+# clock at 1965 MHz, in thread instructions per second.
+ISSUE_THREAD_INST_PER_S = 148 * 4 * 32 * 1965e6
+
+
+def issue_bound(value: float, precision: int):
+    """The instruction-issue roofline beside the HBM one: warp instructions
+    per cell of the two stage kernels from the committed ncu capture, the
+    cell-update rate full issue would give, and the fraction reached."""
+    p = ROOT / "profiles" / f"stage2_fp{precision}_ncu.json"
+    if not p.is_file():
+        return None
+    d = json.loads(p.read_text())
+    w = d.get("warp_inst_per_cell")
+    if not w:
+        return None
+    per_update = 32.0 * (w["stage1"] + w["stage2"])
+    bound = ISSUE_THREAD_INST_PER_S / per_update
+    return {"thread_inst_per_cell_update": per_update, "bound_cell_updates_per_s": bound,
+            "frac": value / bound, "source": d.get("inst_source", "")}
+
+
 def oracle_run(b, h, n, threads: int, steps: int):
     """The oracle (OpenMP over `threads` host threads) stepped `steps` times
     from the workload's initial state; returns (oracle, threads used, seconds)."""
@@ -309,7 +331,8 @@ def _roofline(form, precision, cells, world):
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
             if peak_kind == "measured" else "fallback 6650 GB/s",
             "stage_ms": form["stage_ms"], "bytes_per_cell_update": b_cell,
-            "step_frac_of_hbm": b_cell * form["value"] / world / 1e9 / hbm}
+            "step_frac_of_hbm": b_cell * form["value"] / world / 1e9 / hbm,
+            "issue": issue_bound(form["value"] / world, precision)}
 
 
 def _accuracy(b, h, n, steps):
