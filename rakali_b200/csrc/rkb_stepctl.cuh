@@ -104,15 +104,28 @@ static __device__ void finalize_step(const Grid& g, StepCtl* ctl, const Physics*
                               double* partials, unsigned int nparts, double dt, int cur,
                               bool budget = true) {
   const int tid = threadIdx.x;
+  const int nthr = (int)blockDim.x;  // a multiple of 32
   const double area = g.dx * g.dy;
-  volatile double* VP = partials;
-  double sums[4];
+  // Fixed-order sums of the per-block partials over every thread of this
+  // (last) block: thread t adds partials t, t + nthr, ... in order (L2 loads:
+  // the other blocks wrote them before their fence and counter increment),
+  // each warp combines its lanes by butterfly, and thread 0 adds the warp
+  // results in warp order.  With tens of thousands of partials a step, one
+  // warp doing it alone left the rest of the GPU idle for a long tail.
+  __shared__ double red[4][32];
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  if (budget)
+    for (unsigned int k = tid; k < nparts; k += nthr)
+      for (int s = 0; s < 4; ++s) acc[s] = acc[s] + __ldcg(partials + (size_t)s * nparts + k);
   for (int s = 0; s < 4; ++s) {
-    double acc = 0.0;
-    if (tid < 32 && budget)
-      for (unsigned int k = tid; k < nparts; k += 32) acc = acc + VP[(size_t)s * nparts + k];
-    sums[s] = warp_sum(acc);
+    const double w = warp_sum(acc[s]);
+    if ((tid & 31) == 0) red[s][tid >> 5] = w;
   }
+  __syncthreads();
+  double sums[4] = {0.0, 0.0, 0.0, 0.0};
+  if (tid == 0)
+    for (int w = 0; w < nthr / 32; ++w)
+      for (int s = 0; s < 4; ++s) sums[s] = sums[s] + red[s][w];
   if (tid == 0 && budget) {
     double mo = ctl->mass_out;
     mo = mo - 0.5 * dt * sums[0] * area;
