@@ -407,32 +407,30 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
   if (STAGE == 0) return;
   if (STAGE == 3 && gk != nst - 1) return;  // block-uniform
 
-  // 4. block partials (fixed order) and the block's CFL maxima of the new
-  // state, written to the partials array: the last block reduces them (no
-  // atomics on two addresses from every warp of the grid)
+  // 4. block partials (fixed order) and the CFL maxima of the new state
   constexpr bool kBudget = STAGE != 3;
-  const unsigned int nblocks = gx * gy;
-  const unsigned int bid = by * gx + bx;
-  if (kBudget) {
-    part = warp_sum(part);
-    sponge_d = warp_sum(sponge_d);
-  }
   if (STAGE != 1) {
     wsx = warp_max(wsx);
     wsy = warp_max(wsy);
     bad = __any_sync(0xffffffffu, bad);
-    if ((tid & 31) == 0 && bad) atomicExch(&ctl->error, kErrNonFinite);
+    if ((tid & 31) == 0) {
+      atomic_max_pos(&ctl->msx_next, wsx);
+      atomic_max_pos(&ctl->msy_next, wsy);
+      if (bad) atomicExch(&ctl->error, kErrNonFinite);
+    }
   }
-  __shared__ double red[4][NTH / 32];
-  if ((tid & 31) == 0) {
-    red[0][tid >> 5] = part;
-    red[1][tid >> 5] = sponge_d;
-    red[2][tid >> 5] = wsx;
-    red[3][tid >> 5] = wsy;
-  }
-  __syncthreads();
-  if (tid == 0) {
-    if (kBudget) {
+  const unsigned int nblocks = gx * gy;
+  if (kBudget) {
+    part = warp_sum(part);
+    sponge_d = warp_sum(sponge_d);
+    __shared__ double red[2][NTH / 32];
+    if ((tid & 31) == 0) {
+      red[0][tid >> 5] = part;
+      red[1][tid >> 5] = sponge_d;
+    }
+    __syncthreads();
+    const unsigned int bid = by * gx + bx;
+    if (tid == 0) {
       double s0 = 0.0, s1 = 0.0;
       for (int w = 0; w < NTH / 32; ++w) {
         s0 = s0 + red[0][w];
@@ -441,16 +439,6 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
       double* P = partials + (size_t)(STAGE - 1) * 2 * nblocks;
       P[bid] = s0;
       P[nblocks + bid] = s1;
-    }
-    if (STAGE != 1) {
-      double mx = 0.0, my = 0.0;
-      for (int w = 0; w < NTH / 32; ++w) {
-        mx = fmax(mx, red[2][w]);  // fmax: a NaN (a non-finite state, flagged) is skipped
-        my = fmax(my, red[3][w]);
-      }
-      double* M = partials + 4 * (size_t)nblocks;
-      M[bid] = mx;
-      M[nblocks + bid] = my;
     }
   }
   if (STAGE == 1) return;
@@ -464,8 +452,7 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
   __syncthreads();
   if (!last) return;
   __threadfence();
-  finalize_step(g, ctl, phys, partials, nblocks, step_dt, cur, kBudget,
-                partials + 4 * (size_t)nblocks);
+  finalize_step(g, ctl, phys, partials, nblocks, step_dt, cur, kBudget);
 }
 
 // The host picks the PLAIN build from its copy of the physics; a launch whose
@@ -771,7 +758,7 @@ static dim3 stage_grid(const Grid& g, int tile) {
 size_t partials_doubles(const Grid& g, int tile) {
   dim3 d = stage_grid(g, tile);
   const size_t parts = (size_t)d.x * (size_t)d.y * (is_march(tile) ? kMarchWarps : 1);
-  return 6 * parts;  // stage sums (4 arrays) and the CFL maxima (2) of every block
+  return 4 * parts;
 }
 
 template <int TX, int TY, bool HLLC, int STAGE, int XW = 0>

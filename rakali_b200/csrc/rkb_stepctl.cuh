@@ -100,11 +100,9 @@ __device__ __forceinline__ double warp_sum(double v) {
 // (rki_solver.F90:507-657), the CFL maxima of the new state and the clock.
 // `budget` false: the generic Shu-Osher schemes, which do not accumulate the
 // boundary mass budget (rki_solver.F90:861-926).
-// `maxima`: per-block CFL maxima (nparts each along x and y) to reduce here;
-// null when the kernels accumulated them with atomics in msx_next / msy_next.
 static __device__ void finalize_step(const Grid& g, StepCtl* ctl, const Physics* phys,
                               double* partials, unsigned int nparts, double dt, int cur,
-                              bool budget = true, const double* maxima = nullptr) {
+                              bool budget = true) {
   const int tid = threadIdx.x;
   const int nthr = (int)blockDim.x;  // a multiple of 32
   const double area = g.dx * g.dy;
@@ -114,35 +112,20 @@ static __device__ void finalize_step(const Grid& g, StepCtl* ctl, const Physics*
   // each warp combines its lanes by butterfly, and thread 0 adds the warp
   // results in warp order.  With tens of thousands of partials a step, one
   // warp doing it alone left the rest of the GPU idle for a long tail.
-  __shared__ double red[6][32];
+  __shared__ double red[4][32];
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  double mx = 0.0, my = 0.0;
   if (budget)
     for (unsigned int k = tid; k < nparts; k += nthr)
       for (int s = 0; s < 4; ++s) acc[s] = acc[s] + __ldcg(partials + (size_t)s * nparts + k);
-  if (maxima)
-    for (unsigned int k = tid; k < nparts; k += nthr) {
-      mx = fmax(mx, __ldcg(maxima + k));
-      my = fmax(my, __ldcg(maxima + nparts + k));
-    }
   for (int s = 0; s < 4; ++s) {
     const double w = warp_sum(acc[s]);
     if ((tid & 31) == 0) red[s][tid >> 5] = w;
   }
-  mx = warp_max(mx);
-  my = warp_max(my);
-  if ((tid & 31) == 0) {
-    red[4][tid >> 5] = mx;
-    red[5][tid >> 5] = my;
-  }
   __syncthreads();
   double sums[4] = {0.0, 0.0, 0.0, 0.0};
   if (tid == 0)
-    for (int w = 0; w < nthr / 32; ++w) {
+    for (int w = 0; w < nthr / 32; ++w)
       for (int s = 0; s < 4; ++s) sums[s] = sums[s] + red[s][w];
-      mx = fmax(mx, red[4][w]);
-      my = fmax(my, red[5][w]);
-    }
   if (tid == 0 && budget) {
     double mo = ctl->mass_out;
     mo = mo - 0.5 * dt * sums[0] * area;
@@ -157,13 +140,8 @@ static __device__ void finalize_step(const Grid& g, StepCtl* ctl, const Physics*
   }
   if (tid == 0) {
     volatile StepCtl* vc = ctl;
-    if (maxima) {
-      ctl->msx = mx;
-      ctl->msy = my;
-    } else {
-      ctl->msx = __longlong_as_double((long long)vc->msx_next);
-      ctl->msy = __longlong_as_double((long long)vc->msy_next);
-    }
+    ctl->msx = __longlong_as_double((long long)vc->msx_next);
+    ctl->msy = __longlong_as_double((long long)vc->msy_next);
     ctl->msx_next = 0ull;
     ctl->msy_next = 0ull;
     ctl->ms_valid = 1;
