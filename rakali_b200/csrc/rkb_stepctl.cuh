@@ -114,9 +114,12 @@ static __device__ void finalize_step(const Grid& g, StepCtl* ctl, const Physics*
   // warp doing it alone left the rest of the GPU idle for a long tail.
   __shared__ double red[4][32];
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  if (budget)
+  if (budget) {
+    // eight rows of loads in flight per thread; the additions keep their order
+#pragma unroll 8
     for (unsigned int k = tid; k < nparts; k += nthr)
       for (int s = 0; s < 4; ++s) acc[s] = acc[s] + __ldcg(partials + (size_t)s * nparts + k);
+  }
   for (int s = 0; s < 4; ++s) {
     const double w = warp_sum(acc[s]);
     if ((tid & 31) == 0) red[s][tid >> 5] = w;
