@@ -460,7 +460,7 @@ def run_ensemble(args, world, local_rank, dist):
                 "unit": "cell-updates/s", "steps": args.ensemble_steps,
                 "ms_per_step": graph_ms, "variant": list(ens.variant),
                 "autotune_best_ms_per_step": best, "clocks": clk.summary(),
-                "launches_per_step": 6,
+                "launches_per_step": 7 if prec == 64 else 6,  # FP64: + the step close
                 "phases_ms_per_step": phases,
                 "launch_overhead": {"kernel_sum_ms": kernel_sum, "graph_ms_per_step": graph_ms,
                                     "share_outside_kernels": (graph_ms - kernel_sum) / graph_ms}}

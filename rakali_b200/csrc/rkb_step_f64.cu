@@ -441,18 +441,33 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
       P[nblocks + bid] = s1;
     }
   }
-  if (STAGE == 1) return;
+  // 5. the step is closed by k_close, launched right after this stage: a
+  // grid-wide "last block" counter would hold every block for an atomic
+  // round trip and leave the closing sums to one block at the tail
+  (void)step_dt;
+  (void)cur;
+}
 
-  // 5. last block closes the step
-  __shared__ bool last;
-  if (tid == 0) {
-    __threadfence();
-    last = atomicAdd(&ctl->done_blocks, 1u) == nblocks - 1;
-  }
+// Close a step after its last stage kernel (one block): the fixed-order sums
+// of the per-block partials, the mass budget, the CFL maxima and the clock.
+__global__ void __launch_bounds__(1024)
+    k_close(Grid g, StepCtl* ctl, const Physics* phys, double* partials, unsigned int nblocks,
+            int budget) {
+  if (!ctl->active) return;
+  finalize_step(g, ctl, phys, partials, nblocks, ctl->dt, ctl->cur, budget != 0);
+}
+
+// The same for every simulation of a batch (blockIdx.x = simulation), tiles
+// of tx x ty cells.
+__global__ void __launch_bounds__(1024)
+    k_close_batch(const StepArgs* __restrict__ args, int tx, int ty) {
+  __shared__ StepArgs sa;
+  if (threadIdx.x == 0) sa = args[blockIdx.x];
   __syncthreads();
-  if (!last) return;
-  __threadfence();
-  finalize_step(g, ctl, phys, partials, nblocks, step_dt, cur, kBudget);
+  if (!sa.ctl->active) return;
+  const unsigned int nb = (unsigned)((sa.g.nx_phys() + tx - 1) / tx) *
+                          (unsigned)((sa.g.ny_phys() + ty - 1) / ty);
+  finalize_step(sa.g, sa.ctl, sa.phys, sa.partials, nb, sa.ctl->dt, sa.ctl->cur, true);
 }
 
 // The host picks the PLAIN build from its copy of the physics; a launch whose
@@ -811,6 +826,13 @@ cudaError_t configure_kernels(int tile, int hllc) {
   }
 }
 
+// The close of a step whose last stage ran on shared-memory tiles.
+static cudaError_t launch_close(const StepArgs& a, bool budget, cudaStream_t s) {
+  const dim3 d = stage_grid(a.g, a.tile);
+  k_close<<<1, 1024, 0, s>>>(a.g, a.ctl, a.phys, a.partials, d.x * d.y, budget ? 1 : 0);
+  return cudaGetLastError();
+}
+
 template <int STAGE>
 static cudaError_t launch_stage(const StepArgs& a, FluxOut fl, cudaStream_t s, int gk = 0) {
   const bool h = a.hllc != 0;
@@ -896,7 +918,7 @@ static cudaError_t launch_step_generic(const StepArgs& a, cudaStream_t s) {
     e = launch_stage<3>(ga, none, s, k);
     if (e != cudaSuccess) return e;
   }
-  return cudaSuccess;
+  return launch_close(ga, false, s);  // the generic schemes keep no boundary budget
 }
 
 cudaError_t launch_step(const StepArgs& a, cudaStream_t s) {
@@ -908,12 +930,18 @@ cudaError_t launch_step(const StepArgs& a, cudaStream_t s) {
   if (e != cudaSuccess) return e;
   e = launch_bc(a, 2, s);
   if (e != cudaSuccess) return e;
-  return launch_stage<2>(a, none, s);
+  e = launch_stage<2>(a, none, s);
+  if (e != cudaSuccess || is_march(a.tile)) return e;  // marching kernels close the step themselves
+  return launch_close(a, true, s);
 }
 
+// Stage 2 includes the close of the step.
 cudaError_t launch_stage_only(const StepArgs& a, int stage, cudaStream_t s) {
   FluxOut none{};
-  return stage == 1 ? launch_stage<1>(a, none, s) : launch_stage<2>(a, none, s);
+  if (stage == 1) return launch_stage<1>(a, none, s);
+  const cudaError_t e = launch_stage<2>(a, none, s);
+  if (e != cudaSuccess || is_march(a.tile)) return e;
+  return launch_close(a, true, s);
 }
 
 int launches_per_step(const StepArgs& a) {
@@ -921,8 +949,8 @@ int launches_per_step(const StepArgs& a) {
   const int need = g.ng > 2 ? g.ng : 2;
   const int bc = (g.nx_phys() >= need ? 1 : 2) + (g.ny_phys() >= need ? 1 : 2);
   const int pre = narrow_grid(g) ? bc : 0;
-  if (a.scheme != 2) return a.n_stages * (bc + 1) + pre;
-  return 2 * bc + 2 + pre;
+  if (a.scheme != 2) return a.n_stages * (bc + 1) + pre + 1;  // + the close
+  return 2 * bc + 2 + pre + (is_march(a.tile) ? 0 : 1);
 }
 
 cudaError_t launch_max_speed(const StepArgs& a, cudaStream_t s) {
@@ -1007,8 +1035,18 @@ cudaError_t launch_bc_batch(const BatchLaunch& bl, int stage, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+static cudaError_t launch_close_batch(const BatchLaunch& bl, cudaStream_t s) {
+  int tx, ty;
+  tile_dims(bl.tile, tx, ty);
+  k_close_batch<<<(unsigned)bl.n, 1024, 0, s>>>(bl.args, tx, ty);
+  return cudaGetLastError();
+}
+
+// Stage 2 includes the close of every member's step.
 cudaError_t launch_stage_batch_only(const BatchLaunch& bl, int stage, cudaStream_t s) {
-  return stage == 1 ? launch_stage_batch<1>(bl, s) : launch_stage_batch<2>(bl, s);
+  if (stage == 1) return launch_stage_batch<1>(bl, s);
+  const cudaError_t e = launch_stage_batch<2>(bl, s);
+  return e == cudaSuccess ? launch_close_batch(bl, s) : e;
 }
 
 cudaError_t launch_step_batch(const BatchLaunch& bl, cudaStream_t s) {
@@ -1016,6 +1054,7 @@ cudaError_t launch_step_batch(const BatchLaunch& bl, cudaStream_t s) {
   if (e == cudaSuccess) e = launch_stage_batch<1>(bl, s);
   if (e == cudaSuccess) e = launch_bc_batch(bl, 2, s);
   if (e == cudaSuccess) e = launch_stage_batch<2>(bl, s);
+  if (e == cudaSuccess) e = launch_close_batch(bl, s);
   return e;
 }
 
