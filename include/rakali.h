@@ -315,8 +315,8 @@ int rkb_write_gauges_netcdf(const char *path, int n, const char *names, int name
  * *ms = device time of the n steps (state already resident). */
 int rkb_time_steps(void *handle, int n, double *ms);
 /* Run n steps one launch at a time; out5[0..3] = mean ms per step of the
- * stage-1 boundary fill, stage 1, stage-2 boundary fill, stage 2;
- * out5[4] = kernel launches per step. */
+ * stage-1 boundary fill, stage 1, stage-2 boundary fill, stage 2 (with the
+ * close of the step); out5[4] = kernel launches per step. */
 int rkb_profile_steps(void *handle, int n, double *out5);
 
 /* Correctly rounded h**fl(1/3) and sin/cos, the host builds of the device
