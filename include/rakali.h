@@ -149,9 +149,21 @@ int rkb_get_mass_budget(void *handle, double *out);
  * next step (the state ping-pongs between two buffers). */
 int rkb_get_device_fields(void *handle, void **ptrs, int *pitch);
 
-/* Tile shape of the fused stage kernel (0: 32x8, 1: 32x16, 2: 64x4, 3: 16x16). */
+/* Kernel shape of the FP64 stage (0: 32x8, 1: 32x16, 2: 64x4, 3: 16x16
+ * tiles; 4 / 5: marching strips of 64 / 32 rows; 6 / 7: 32x8 / 32x12 tiles
+ * with two extra warps; 8: 16x15 tiles; 9: 32x7 tiles with one extra warp;
+ * 10: 16x15 tiles in a persistent kernel that TMA-loads each block's next
+ * tile while it updates the current one (the 16x15 kernel where its maps
+ * cannot be encoded, see rkb_tma_tile_status)).  Results do not depend on the shape.  -2 for any other
+ * value. */
 int rkb_set_tile(void *handle, int tile);
 int rkb_get_tile(void *handle);
+/* Whether tile 10 runs TMA-staged on this simulation: 0 yes; -1 not yet
+ * finalised; otherwise why not (1 misaligned rows, 2 misaligned buffer, 3 no
+ * tensor-map encoder, 100 + a runtime error or 200 + an entry-point query
+ * result while finding it, 1000 + the encoder's CUresult).  No counterpart
+ * in the reference. */
+int rkb_tma_tile_status(void *handle);
 
 /* Arithmetic form of the step: 64 = FP64 depth form (the reference's
  * arithmetic, the default), 32 = FP32 surface form (eta = h + b, hu, hv in
@@ -164,9 +176,10 @@ int rkb_get_precision(void *handle);
  * and rows each warp sweeps (0 = one wave of resident warps).  Results do
  * not depend on either. */
 int rkb_set_sweep(void *handle, int cols_per_lane, int rows);
-/* FP32 form: limit, in GPU clock cycles, of the sweep's waits for its bulk
- * row copies (<= 0: the default, about one second; a limit shorter than one
- * clock read gives up at once).  A wait that runs out makes the step fail
+/* Limit, in GPU clock cycles, of the device-side waits for asynchronous
+ * copies: the FP32 sweep's bulk row copies and the TMA tile copies of the
+ * FP64 TMA-staged tile kernel (tile 10) (<= 0: the default, about one second;
+ * a limit shorter than one clock read gives up at once).  A wait that runs out makes the step fail
  * with -1 and a message in rki_last_error(); the copies in flight are still
  * waited for (with the default limit) before the kernel returns.  No
  * counterpart in the reference: it exists so that the error path can be
@@ -192,7 +205,7 @@ int rkb_batch_time_steps(void *batch, int n, double *ms);
  * whole sequence.  Set beside rkb_batch_time_steps (the same steps replayed
  * from CUDA graphs) it shows what the launches themselves cost. */
 int rkb_batch_profile_steps(void *batch, int n, double *out5);
-/* Times each candidate kernel shape (FP64: the four tiles; FP32: 2 or 4
+/* Times each candidate kernel shape (FP64: the shared-memory tiles; FP32: 2 or 4
  * columns per lane x rows per warp sweep) for trial_steps steps on the live
  * state, restores the state exactly, keeps the fastest shape. */
 int rkb_batch_autotune(void *batch, int trial_steps, double *best_ms_per_step);

@@ -121,6 +121,7 @@ def load(path: str | None = None):
     _sig(lib, "rkb_get_device_fields", [H, HP, IP], I)
     _sig(lib, "rkb_set_tile", [H, I], I)
     _sig(lib, "rkb_get_tile", [H], I)
+    _sig(lib, "rkb_tma_tile_status", [H], I)
     _sig(lib, "rkb_set_precision", [H, I], I)
     _sig(lib, "rkb_get_precision", [H], I)
     _sig(lib, "rkb_set_sweep", [H, I, I], I)

@@ -568,6 +568,11 @@ int rkb_get_tile(void* handle) {
   return s ? s->tile : kBadHandle;
 }
 
+int rkb_tma_tile_status(void* handle) {
+  rkb::Sim* s = sim_of(handle);
+  return s ? s->tma_status() : kBadHandle;
+}
+
 // ---- batches ----------------------------------------------------------------
 
 static rkb::Batch* batch_of(void* p) {

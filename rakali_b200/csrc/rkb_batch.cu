@@ -317,7 +317,8 @@ int Batch::autotune(int trial_steps, double* best_ms) {
   if (trial_steps <= 0) trial_steps = 3;
   std::vector<std::pair<int, int>> cands;
   if (prec_ == 64) {
-    for (int t : {kTile32x16, kTile32x8, kTile64x4, kTile16x16, kTile32x8w, kTile32x12w})
+    for (int t : {kTile32x16, kTile32x8, kTile64x4, kTile16x16, kTile32x8w, kTile32x12w,
+                  kTile16x15, kTile32x7w})
       cands.push_back({t, 0});
   } else {
     for (int c : {2, 4})

@@ -100,12 +100,13 @@ struct StepCtl {
 
 // StepCtl::error codes.  A step that sets one completes; the steps after it
 // in the same graph chunk do not run (step_begin), and the host reports it.
-constexpr int kErrWait = 1;       // a bounded device-side wait for a bulk copy gave up (FP32)
+constexpr int kErrWait = 1;       // a bounded device-side wait for a bulk or TMA copy gave up
 constexpr int kErrPhysics = 2;    // a launch built without forcing / Coriolis / sponge met them
 constexpr int kErrNonFinite = 3;  // the new state holds a NaN or an infinity
 
-// Default limit of the FP32 sweep's waits for its bulk copies (~1 s at B200
-// clocks); the drain after a wait gave up always uses this one.
+// Default limit of the device-side waits for bulk and TMA copies (FP32
+// sweep, FP64 TMA-staged tiles; ~1 s at B200 clocks); the drain after a wait
+// gave up always uses this one.
 constexpr long long kWaitCyclesDefault = 2000000000ll;
 
 // ---------------------------------------------------------------------------

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstddef>
+#include <cuda.h>  // CUtensorMap (the maps are encoded through the runtime's driver entry point)
 #include <cuda_runtime.h>
 
 #include "rkb_common.cuh"
@@ -34,10 +35,28 @@ enum TileShape : int {
   kTile32x8 = 0, kTile32x16 = 1, kTile64x4 = 2, kTile16x16 = 3,  // shared-memory tiles
   kMarch64 = 4, kMarch32 = 5,  // warp-per-strip marching kernel, 64 / 32 rows per warp
   kTile32x8w = 6, kTile32x12w = 7,  // shared-memory tiles with two extra warps
-  kNumTiles = 8
+  // tiles whose face loop takes exactly two rounds of 256 threads: 16x15
+  // (511 faces) and 32x7 with one extra warp (487 faces)
+  kTile16x15 = 8, kTile32x7w = 9,
+  // 16x15 tiles in a persistent kernel: each block walks a list of tiles and
+  // TMA-loads the next tile's halo box while it updates the current one's
+  // cells (the plain 16x15 kernel runs where the maps cannot be encoded)
+  kTile16x15t = 10,
+  kNumTiles = 11
 };
 const char* tile_name(int tile);
 void tile_dims(int tile, int& tx, int& ty);
+
+// TMA maps (2D, FP64, pitched rows, zero fill outside) of the state buffers
+// for the TMA-staged tile kernel: the halo box of a tile (TX + 6 by TY + 4:
+// boxes start on an even column) over U0, U1 and S, the same box over the
+// bed, and the box of the tile's cells (TX + 2 by TY) over U0 and U1 (U^n in
+// stage 2).
+struct alignas(64) TileMaps {
+  CUtensorMap tile[3][3];   // [U0, U1, S][h, hu, hv]
+  CUtensorMap bed;
+  CUtensorMap cells[2][3];  // [U0, U1][h, hu, hv]
+};
 
 // Everything one step needs; all pointers are device pointers.
 struct StepArgs {
@@ -55,7 +74,15 @@ struct StepArgs {
   int scheme;    // time scheme: 2 SSP-RK2 (fused stages), 1 euler, 3 rk3, 4 rk43
   int n_stages;  // stages of the generic schemes
   int plain;     // no forcing, Coriolis or sponge: the SSP-RK2 stages built without those terms
+  const TileMaps* maps;    // HOST copy of the TMA maps of these buffers (null: none)
+  long long wait_cycles;   // limit of the TMA tile kernel's waits (kWaitCyclesDefault)
 };
+
+// Encodes the TMA maps of a's buffers for the TMA-staged tile kernel.  0, or
+// why that kernel cannot serve this grid: 1 rows not on 16-byte boundaries, 2 a misaligned buffer, 3 no encoder, 100 + a runtime
+// error or 200 + an entry-point query result while finding the encoder,
+// 1000 + the encoder's own result.
+int encode_tile_maps(const StepArgs& a, TileMaps* m);
 
 // Doubles of per-block partial storage the step kernels need.
 size_t partials_doubles(const Grid& g, int tile);

@@ -409,6 +409,9 @@ int Sim::alloc_device(std::string& err) {
   args_.hllc = phys.use_hllc;
   args_.scheme = phys.scheme;
   args_.n_stages = phys.n_stages;
+  args_.wait_cycles = wait_cycles;
+  tma_status_ = encode_tile_maps(args_, &maps_);
+  args_.maps = tma_status_ == 0 ? &maps_ : nullptr;
   cur_ = 0;
   // the clock starts at the restart time when a restart file was loaded
   hctl_->t = t_current_;
@@ -694,6 +697,7 @@ int Sim::upload_params() {
   args_.scheme = phys.scheme;
   args_.n_stages = phys.n_stages;
   args_.plain = plain_physics(phys, bc) ? 1 : 0;
+  args_.wait_cycles = wait_cycles > 0 ? wait_cycles : kWaitCyclesDefault;
   RKB_TRY(configure_kernels(args_.tile, args_.hllc));
   params_dirty = false;
   return 0;
@@ -1252,7 +1256,8 @@ int Sim::check_device_error() {
                   ? "a non-finite value (NaN or infinity) appeared in the state at step " +
                         std::to_string(step_count_) + " (t = " + std::to_string(t_current_) +
                         "); the run stopped after that step"
-                  : "a bounded device-side wait for a bulk copy expired; the step was abandoned";
+                  : "a bounded device-side wait for a bulk copy expired (a bulk or TMA copy into "
+                    "shared memory); the step was abandoned";
   hctl_->error = 0;
   cudaMemcpyAsync(&args_.ctl->error, &hctl_->error, sizeof(int), cudaMemcpyHostToDevice, stream_);
   cudaStreamSynchronize(stream_);

@@ -72,7 +72,7 @@ class Sim {
   BcParams bc{};
   Physics phys{};
   bool params_dirty = true;
-  int tile = kTile16x16;  // fastest measured FP64 variant on B200 (4096^2 workload)
+  int tile = kTile16x15;  // fastest measured FP64 variant on B200 (4096^2 workload)
   int steps_per_graph_cap = 256;
   int sweep_rows = 0;     // FP32 sweep: rows per warp (0: one wave of resident warps)
   int sweep_cpl = 2;      // FP32 sweep: columns per lane (2 or 4)
@@ -103,6 +103,7 @@ class Sim {
 
   // Device pointers for the torch / kernel-level paths.
   StepArgs device_args() const { return args_; }
+  int tma_status() const { return tma_status_; }
   int current_buffer() const { return cur_; }
   cudaStream_t stream() const { return stream_; }
   int ensure_device();
@@ -136,6 +137,8 @@ class Sim {
   cudaStream_t stream_ = nullptr;
   void* dmem_ = nullptr;
   StepArgs args_{};
+  TileMaps maps_{};  // TMA maps of the state buffers (args_.maps points here when encoded)
+  int tma_status_ = -1;  // encode_tile_maps' result (-1: no device buffers yet)
   StepCtl* hctl_ = nullptr;  // pinned
   // host_is_current_: every host array (state, bed, RK2 saves) equals the
   // device's; host_state_current_: h, hu, hv do (after rki_sync_host).

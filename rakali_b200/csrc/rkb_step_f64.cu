@@ -10,8 +10,11 @@
 //
 // The CFL reduction (rki_kernel_timestep.F90:16-74) is folded into the
 // stage-2 epilogue; the first launch of the next step turns it into dt.
-// The boundary mass-out sums (rki_solver.F90:507-537) are per-block partials
-// reduced in a fixed order by the last block of stage 2.
+// The boundary mass-out sums (rki_solver.F90:507-537) are per-tile partials
+// reduced in a fixed order by a one-block close kernel after stage 2.
+#include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled
+
+#include "rkb_async.cuh"
 #include "rkb_bc.cuh"
 #include "rkb_cell.cuh"
 #include "rkb_crmath.cuh"
@@ -173,15 +176,89 @@ __global__ void k_max_speed(Grid g, StepCtl* ctl, FieldSet U0, FieldSet U1) {
 // two cells along its normal from the tile (every slope twice, the same
 // expressions, so the same bits), which spares the slope arrays and a block
 // barrier.
-template <int TX, int TY>
+// Threads of a TX x TY tile with XW extra warps: the cells rounded up to
+// whole warps, plus the extra warps.
+constexpr int stage_threads(int tx, int ty, int xw) { return (tx * ty + 31) / 32 * 32 + 32 * xw; }
+
+// TMA: the layout of the TMA-staged kernel.  Its boxes start on an even
+// column (16 bytes), one column left of the tile when the ghost width is odd,
+// so their rows are two columns wider (TX + 6 with the halo, TX + 2 for U^n)
+// and the arrays are read from an offset of (ng & 1); every array starts on
+// a 128-byte line, and the dynamic buffer carries 128 bytes of slack to
+// align its start.
+template <int TX, int TY, bool TMA = false>
 struct StageSmem {
-  static constexpr int TW = TX + 4, TH = TY + 4;
+  static constexpr int TW = TX + 4 + (TMA ? 2 : 0), TH = TY + 4;  // tile row stride, rows
   static constexpr int NT = TW * TH;
+  static constexpr int NTP = TMA ? (NT + 15) / 16 * 16 : NT;  // tile array stride
   static constexpr int NFX = (TX + 1) * TY;
   static constexpr int NFY = TX * (TY + 1);
-  static constexpr int NC = TX * TY;
-  static constexpr int DOUBLES = 4 * NT + 6 * NFX + 6 * NFY + 3 * NC;
-  static constexpr size_t BYTES = sizeof(double) * (size_t)DOUBLES;
+  static constexpr int NC = TX * TY;                        // cells
+  static constexpr int CW = TX + (TMA ? 2 : 0);             // U^n row stride
+  static constexpr int NCP = TMA ? (CW * TY + 15) / 16 * 16 : NC;  // U^n array stride
+  static constexpr int DOUBLES = 4 * NTP + 3 * NCP + 6 * NFX + 6 * NFY;
+  static constexpr size_t BYTES = sizeof(double) * (size_t)DOUBLES + (TMA ? 128 : 0);
+  static_assert(!TMA || TX % 2 == 0, "TMA boxes start on even columns");
+};
+
+// Shared-memory arrays of one stage block: tile (h, hu, hv, b with a 2-cell
+// halo), U^n of the cells, x- and y-face terms.
+struct StagePtrs {
+  double *th, *tu, *tv, *tb, *oh, *ou, *ov, *fxa, *fya;
+};
+
+// The arrays where the copies land (TMA: 128-byte aligned).
+template <int TX, int TY, bool TMA>
+__device__ __forceinline__ StagePtrs stage_ptrs(double* base) {
+  using SM = StageSmem<TX, TY, TMA>;
+  if (TMA) base = (double*)(((uintptr_t)base + 127) & ~(uintptr_t)127);
+  StagePtrs p;
+  p.th = base;
+  p.tu = p.th + SM::NTP;
+  p.tv = p.tu + SM::NTP;
+  p.tb = p.tv + SM::NTP;
+  p.oh = p.tb + SM::NTP;
+  p.ou = p.oh + SM::NCP;
+  p.ov = p.ou + SM::NCP;
+  p.fxa = p.ov + SM::NCP;  // 6 arrays of NFX: fh, fqx, fqy, wbR, hL2, pL2
+  p.fya = p.fxa + 6 * SM::NFX;
+  return p;
+}
+
+// TMA copies of tile (bx, by) for the TMA-staged kernel (one thread): the
+// halo box of h, hu, hv from field set `in_set` (0 U0, 1 U1, 2 S) and of the
+// bed, and in stage 2 the cell box of U^n from `old_set`, all completing on
+// `bar`.  The caller has passed a block barrier after the last reads of
+// these arrays; the proxy fence orders those reads before the copies.  The
+// box x coordinates, ng + bx TX - 2 - (ng & 1) and that + 2, are even (TX is),
+// which puts every box start on a 16-byte boundary.
+template <int TX, int TY, int STAGE>
+__device__ __forceinline__ void issue_tile(const TileMaps& tm, int in_set, int old_set,
+                                           const Grid& g, unsigned bx, unsigned by,
+                                           uint32_t bar, const StagePtrs& p) {
+  using SM = StageSmem<TX, TY, true>;
+  constexpr uint32_t kBox = 8u * SM::TW * SM::TH, kCells = 8u * SM::CW * TY;
+  const int x = g.ng + (int)bx * TX - 2 - (g.ng & 1), y = g.ng + (int)by * TY - 2;
+  fence_proxy_async();
+  mbar_expect_tx(bar, 4 * kBox + (STAGE == 2 ? 3 * kCells : 0));
+  tma_load_2d(smem_u32(p.th), &tm.tile[in_set][0], x, y, bar);
+  tma_load_2d(smem_u32(p.tu), &tm.tile[in_set][1], x, y, bar);
+  tma_load_2d(smem_u32(p.tv), &tm.tile[in_set][2], x, y, bar);
+  tma_load_2d(smem_u32(p.tb), &tm.bed, x, y, bar);
+  if (STAGE == 2) {
+    tma_load_2d(smem_u32(p.oh), &tm.cells[old_set][0], x + 2, y + 2, bar);
+    tma_load_2d(smem_u32(p.ou), &tm.cells[old_set][1], x + 2, y + 2, bar);
+    tma_load_2d(smem_u32(p.ov), &tm.cells[old_set][2], x + 2, y + 2, bar);
+  }
+}
+
+// The next tile of a TMA-staged block: issued by thread 0 once the face
+// loop of the current tile has read the tile arrays for the last time.
+struct TmaNext {
+  const TileMaps* maps = nullptr;  // parameter-space copy
+  uint32_t bar = 0;
+  int tile = -1;                   // next tile index of this block, < 0: none
+  int in_set = 0, old_set = 0;
 };
 
 // STAGE 1: U^n (buffer cur) -> U* (scratch S).
@@ -197,32 +274,38 @@ struct StageSmem {
 // runs a third, mostly empty face round) and sit out the cell update.
 // PLAIN: the build for stages without forcing, Coriolis or sponge terms
 // (Manning friction only), chosen by the host from its copy of the physics.
-template <int TX, int TY, bool HLLC, int STAGE, int XW = 0, bool PLAIN = false>
+// TMA: the tile arrays were filled by TMA copies the caller has waited for
+// (the TMA-staged kernel, stages 1 and 2); `nx` names the block's next tile,
+// whose copies thread 0 issues after the face loop.
+template <int TX, int TY, bool HLLC, int STAGE, int XW = 0, bool PLAIN = false, bool TMA = false>
 __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Physics* phys,
                                            const BcParams* bcp, const FieldSet& U0,
                                            const FieldSet& U1, const FieldSet& S,
                                            const double* __restrict__ b, const Forcing& fo,
                                            double* __restrict__ partials, const FluxOut& fl,
                                            unsigned bx, unsigned by, unsigned gx, unsigned gy,
-                                           int gk = 0) {
-  using SM = StageSmem<TX, TY>;
+                                           int gk = 0, TmaNext nx = TmaNext{}) {
+  static_assert(!TMA || STAGE == 1 || STAGE == 2, "TMA staging serves the SSP-RK2 stages");
+  using SM = StageSmem<TX, TY, TMA>;
   constexpr int TW = SM::TW;
-  constexpr int NTH = TX * TY + 32 * XW;
+  constexpr int NTH = stage_threads(TX, TY, XW);
   extern __shared__ double smem[];
-  double* th = smem;
-  double* tu = th + SM::NT;
-  double* tv = tu + SM::NT;
-  double* tb = tv + SM::NT;
-  double* fxa = tb + SM::NT;  // 6 arrays of NFX: fh, fqx, fqy, wbR, hL2, pL2
-  double* fya = fxa + 6 * SM::NFX;
-  double* oh = fya + 6 * SM::NFY;  // U^n of the tile's cells (stage 2)
-  double* ou = oh + SM::NC;
-  double* ov = ou + SM::NC;
+  const StagePtrs P = stage_ptrs<TX, TY, TMA>(smem);
+  const int xo = TMA ? (g.ng & 1) : 0;  // column of the tile's first x in the TMA boxes
+  double* th = P.th + xo;
+  double* tu = P.tu + xo;
+  double* tv = P.tv + xo;
+  double* tb = P.tb + xo;
+  double* fxa = P.fxa;
+  double* fya = P.fya;
+  double* oh = P.oh + xo;  // U^n of the tile's cells (stage 2), rows SM::CW apart
+  double* ou = P.ou + xo;
+  double* ov = P.ov + xo;
 
   double dt = 0.0;
   int cur = 0;
   if (STAGE != 0) {
-    if (!ctl->active) return;
+    if (!TMA && !ctl->active) return;  // the TMA-staged kernel checks before its first copy
     dt = ctl->dt;
     cur = ctl->cur;
   }
@@ -247,8 +330,9 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
     rot[1] = sn;
   }
 
-  // 1. tile load with halo (ghost cells come from the BC launches)
-  for (int k = tid; k < SM::NT; k += NTH) {
+  // 1. tile load with halo (ghost cells come from the BC launches); the
+  // TMA-staged kernel has its tile already
+  for (int k = tid; !TMA && k < SM::NT; k += NTH) {
     const int x = k % TW, y = k / TW;
     const int gi = gx0 - 2 + x, gj = gy0 - 2 + y;
     double vh = 0.0, vu = 0.0, vv = 0.0, vb = 0.0;
@@ -258,10 +342,9 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
     }
     th[k] = vh; tu[k] = vu; tv[k] = vv; tb[k] = vb;
   }
-  if (STAGE == 2) {
+  if (STAGE == 2 && !TMA) {
     // U^n of the tile's cells for the RK2 average, loaded with the tile so
-    // its latency passes during the face phase (each cell thread reads back
-    // what it loaded)
+    // its latency passes during the face phase
     const FieldSet old = cur ? U1 : U0;
     for (int k = tid; k < SM::NC; k += NTH) {
       const int pi = gx0 + k % TX, pj = gy0 + k / TX;
@@ -317,13 +400,26 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
       fya[5 * SM::NFY + kk] = o.pL2;
     }
   }
-  __syncthreads();
-
   // 3. cell update: one cell per thread (the extra warps repeat cell 0 and
-  // store nothing)
+  // store nothing).  The cell's own state and U^n are read before the
+  // barrier: behind it the TMA-staged kernel refills the tile arrays.
   const int tc = tid < TX * TY ? tid : 0;
   const int c = tc % TX, r = tc / TX;
   const int i = gx0 + c, j = gy0 + r;
+  const int qc = (r + 2) * TW + (c + 2);
+  const double h_c = th[qc], hu_c = tu[qc], hv_c = tv[qc];
+  double h_n = 0.0, hu_n = 0.0, hv_n = 0.0;
+  if (STAGE == 2) {
+    const int qn = r * SM::CW + c;
+    h_n = oh[qn];
+    hu_n = ou[qn];
+    hv_n = ov[qn];
+  }
+  __syncthreads();
+  if (TMA && tid == 0 && nx.tile >= 0)
+    issue_tile<TX, TY, STAGE>(*nx.maps, nx.in_set, nx.old_set, g, (unsigned)nx.tile % gx,
+                              (unsigned)nx.tile / gx, nx.bar, P);
+
   const bool valid = tid < TX * TY && i < g.nxt - g.ng && j < g.nyt - g.ng;
   const int fl_ = r * (TX + 1) + c, fr_ = fl_ + 1;
   const int fb_ = r * TX + c, ft_ = fb_ + TX;
@@ -355,8 +451,7 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
         if (j == g.ng) fl.mflux_y[q - g.pitch] = fya[fb_];
       }
     } else {
-      const int qc = (r + 2) * TW + (c + 2);
-      double a = th[qc], u = tu[qc], v = tv[qc];
+      double a = h_c, u = hu_c, v = hv_c;
       a = a + dt * o_fh;
       u = u + dt * o_fhu;
       v = v + dt * o_fhv;
@@ -386,9 +481,9 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
       } else {
         // RK2 average with U^n and the second clamp (rki_kernel_fused.F90:435-463)
         out = cur ? U0 : U1;
-        a = 0.5 * (oh[tc] + a);
-        u = 0.5 * (ou[tc] + u);
-        v = 0.5 * (ov[tc] + v);
+        a = 0.5 * (h_n + a);
+        u = 0.5 * (hu_n + u);
+        v = 0.5 * (hv_n + v);
         protect(a, u, v);
       }
       const double h_pre_sponge = a;
@@ -484,13 +579,22 @@ __device__ __forceinline__ bool plain_mismatch64(StepCtl* ctl, const Physics* ph
 // Resident blocks per SM the stage kernels are built for: as many as 64
 // registers a thread and the tile's shared memory allow (4 for the 256-thread
 // tiles, 3 for 288 threads, 2 for 448 and 512).  Left free, the compiler
-// gives the stages more registers than that occupancy allows.
-constexpr int stage_blocks_per_sm(int threads) {
-  return threads <= 256 ? 4 : threads <= 320 ? 3 : 2;
+// gives the stages more registers than that occupancy allows.  The
+// plain-physics stage 1 of a 256-thread tile whose shared memory (with the
+// 1 KB each block reserves) fits five blocks in the SM's 228 KB is built for
+// five: 48 registers and a few spilled bytes, measured 3% faster.  Stage 2
+// holds U^n as well and measured 1% slower so, and the full-physics build
+// spills several times more: both keep four.
+constexpr int stage_blocks_per_sm(int threads, int smem_bytes = 0, bool five = false) {
+  return threads <= 256 ? (five && 5 * (smem_bytes + 128 + 1024) <= 228 * 1024 ? 5 : 4)
+                        : threads <= 320 ? 3 : 2;
 }
 
 template <int TX, int TY, bool HLLC, int STAGE, int XW = 0, bool PLAIN = false>
-__global__ void __launch_bounds__(TX * TY + 32 * XW, stage_blocks_per_sm(TX * TY + 32 * XW))
+__global__ void __launch_bounds__(stage_threads(TX, TY, XW),
+                                  stage_blocks_per_sm(stage_threads(TX, TY, XW),
+                                                      (int)StageSmem<TX, TY>::BYTES,
+                                                      STAGE == 1 && PLAIN))
     k_stage(Grid g, StepCtl* ctl, const Physics* phys, const BcParams* bcp, FieldSet U0,
             FieldSet U1, FieldSet S, const double* __restrict__ b, Forcing fo,
             double* __restrict__ partials, FluxOut fl, int gk) {
@@ -505,7 +609,10 @@ __global__ void __launch_bounds__(TX * TY + 32 * XW, stage_blocks_per_sm(TX * TY
 // Every simulation of a batch in one launch: map[blockIdx.x] = (simulation,
 // tile index within that simulation's tiling).
 template <int TX, int TY, bool HLLC, int STAGE, int XW = 0, bool PLAIN = false>
-__global__ void __launch_bounds__(TX * TY + 32 * XW, stage_blocks_per_sm(TX * TY + 32 * XW))
+__global__ void __launch_bounds__(stage_threads(TX, TY, XW),
+                                  stage_blocks_per_sm(stage_threads(TX, TY, XW),
+                                                      (int)StageSmem<TX, TY>::BYTES,
+                                                      STAGE == 1 && PLAIN))
     k_stage_batch(const StepArgs* __restrict__ args, const int2* __restrict__ map) {
   __shared__ StepArgs sa;
   const int2 m = map[blockIdx.x];
@@ -518,6 +625,61 @@ __global__ void __launch_bounds__(TX * TY + 32 * XW, stage_blocks_per_sm(TX * TY
   stage_body<TX, TY, HLLC, STAGE, XW, PLAIN>(sa.g, sa.ctl, sa.phys, sa.bc, sa.U0, sa.U1, sa.S,
                                              sa.b, sa.fo, sa.partials, none, (unsigned)m.y % gx,
                                              (unsigned)m.y / gx, gx, gy);
+}
+
+// TMA-staged SSP-RK2 stage (STAGE 1 or 2) on TX x TY tiles: a persistent
+// grid of the resident blocks, block k taking tiles k, k + gridDim.x, ...
+// Each tile's halo box arrives by TMA on the block's mbarrier; thread 0
+// issues the next tile's copies as soon as the face loop has read the tile
+// arrays for the last time, so the copies overlap the cell update and the
+// partial sums.  Every tile writes its own partials, as in k_stage, so the
+// step's sums and bits are the same.  A wait that runs out of `limit` cycles
+// marks the step (kErrWait), waits for the copies in flight with the default
+// limit and ends the block.
+template <int TX, int TY, bool HLLC, int STAGE, bool PLAIN = false>
+__global__ void __launch_bounds__(stage_threads(TX, TY, 0),
+                                  stage_blocks_per_sm(stage_threads(TX, TY, 0),
+                                                      (int)StageSmem<TX, TY, true>::BYTES,
+                                                      STAGE == 1 && PLAIN))
+    k_stage_tma(Grid g, StepCtl* ctl, const Physics* phys, const BcParams* bcp, FieldSet U0,
+                FieldSet U1, FieldSet S, const double* __restrict__ b, Forcing fo,
+                double* __restrict__ partials, long long limit, const __grid_constant__ TileMaps tm) {
+  if (PLAIN && plain_mismatch64(ctl, phys, bcp)) return;
+  if (!ctl->active) return;
+  const int cur = ctl->cur;
+  const unsigned gx = (unsigned)((g.nx_phys() + TX - 1) / TX);
+  const unsigned gy = (unsigned)((g.ny_phys() + TY - 1) / TY);
+  const unsigned ntiles = gx * gy;
+  extern __shared__ double smem[];
+  const StagePtrs P = stage_ptrs<TX, TY, true>(smem);
+  __shared__ __align__(8) unsigned long long bar_word;
+  TmaNext nx;
+  nx.maps = &tm;
+  nx.bar = smem_u32(&bar_word);
+  nx.in_set = STAGE == 2 ? 2 : cur;
+  nx.old_set = cur;
+  if (threadIdx.x == 0) {
+    mbar_init(nx.bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  unsigned t = blockIdx.x;
+  if (threadIdx.x == 0 && t < ntiles)
+    issue_tile<TX, TY, STAGE>(tm, nx.in_set, nx.old_set, g, t % gx, t / gx, nx.bar, P);
+  uint32_t parity = 0;
+  for (; t < ntiles; t += gridDim.x) {
+    const bool ok = mbar_wait(nx.bar, parity, limit);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) atomicExch(&ctl->error, kErrWait);
+      mbar_wait(nx.bar, parity, kWaitCyclesDefault);  // the copies still in flight
+      return;
+    }
+    parity ^= 1u;
+    const unsigned next = t + gridDim.x;
+    nx.tile = next < ntiles ? (int)next : -1;
+    stage_body<TX, TY, HLLC, STAGE, 0, PLAIN, true>(g, ctl, phys, bcp, U0, U1, S, b, fo, partials,
+                                                    FluxOut{}, t % gx, t / gx, gx, gy, 0, nx);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -744,6 +906,9 @@ const char* tile_name(int tile) {
     case kTile16x16: return "16x16";
     case kTile32x8w: return "32x8+2w";
     case kTile32x12w: return "32x12+2w";
+    case kTile16x15: return "16x15";
+    case kTile32x7w: return "32x7+1w";
+    case kTile16x15t: return "16x15 TMA";
     case kMarch64: return "march28x64";
     default: return "march28x32";
   }
@@ -757,6 +922,9 @@ void tile_dims(int tile, int& tx, int& ty) {
     case kTile16x16: tx = 16; ty = 16; break;
     case kTile32x8w: tx = 32; ty = 8; break;
     case kTile32x12w: tx = 32; ty = 12; break;
+    case kTile16x15: tx = 16; ty = 15; break;
+    case kTile32x7w: tx = 32; ty = 7; break;
+    case kTile16x15t: tx = 16; ty = 15; break;
     case kMarch64: tx = kMarchCols * kMarchWarps; ty = 64; break;
     default: tx = kMarchCols * kMarchWarps; ty = 32; break;
   }
@@ -784,8 +952,29 @@ static cudaError_t launch_stage_t(const StepArgs& a, FluxOut fl, cudaStream_t s,
   auto kern = (kRk2 && a.plain) ? k_stage<TX, TY, HLLC, STAGE, XW, kRk2>
                                 : k_stage<TX, TY, HLLC, STAGE, XW, false>;
   const dim3 d = stage_grid(a.g, a.tile);
-  kern<<<d.x * d.y, TX * TY + 32 * XW, SM::BYTES, s>>>(a.g, a.ctl, a.phys, a.bc, a.U0, a.U1, a.S,
+  kern<<<d.x * d.y, stage_threads(TX, TY, XW), SM::BYTES, s>>>(a.g, a.ctl, a.phys, a.bc, a.U0, a.U1, a.S,
                                                        a.b, a.fo, a.partials, fl, gk);
+  return cudaGetLastError();
+}
+
+// The TMA-staged kernel: one block per resident slot (at most one per tile).
+template <int TX, int TY, bool HLLC, int STAGE>
+static cudaError_t launch_stage_tma_t(const StepArgs& a, cudaStream_t s) {
+  using SM = StageSmem<TX, TY, true>;
+  auto kern = a.plain ? k_stage_tma<TX, TY, HLLC, STAGE, true> : k_stage_tma<TX, TY, HLLC, STAGE, false>;
+  constexpr int threads = stage_threads(TX, TY, 0);
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, SM::BYTES);
+  if (e != cudaSuccess) return e;
+  const dim3 d = stage_grid(a.g, a.tile);
+  const unsigned ntiles = d.x * d.y;
+  const unsigned slots = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));
+  const long long limit = a.wait_cycles > 0 ? a.wait_cycles : kWaitCyclesDefault;
+  kern<<<ntiles < slots ? ntiles : slots, threads, SM::BYTES, s>>>(
+      a.g, a.ctl, a.phys, a.bc, a.U0, a.U1, a.S, a.b, a.fo, a.partials, limit, *a.maps);
   return cudaGetLastError();
 }
 
@@ -795,6 +984,17 @@ static cudaError_t launch_march_t(const StepArgs& a, cudaStream_t s) {
   k_march<HLLC, STAGE, ROWS><<<grid, kMarchWarps * 32, 0, s>>>(a.g, a.ctl, a.phys, a.bc, a.U0,
                                                               a.U1, a.S, a.b, a.fo, a.partials);
   return cudaGetLastError();
+}
+
+template <int TX, int TY, bool HLLC>
+static cudaError_t configure_tma_t() {
+  const int bytes = (int)StageSmem<TX, TY, true>::BYTES;
+  const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  cudaError_t e = cudaFuncSetAttribute(k_stage_tma<TX, TY, HLLC, 1, false>, attr, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage_tma<TX, TY, HLLC, 2, false>, attr, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage_tma<TX, TY, HLLC, 1, true>, attr, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage_tma<TX, TY, HLLC, 2, true>, attr, bytes);
+  return e;
 }
 
 template <int TX, int TY, bool HLLC, int XW = 0>
@@ -820,6 +1020,14 @@ cudaError_t configure_kernels(int tile, int hllc) {
     case kTile16x16: return h ? configure_t<16, 16, true>() : configure_t<16, 16, false>();
     case kTile32x8w: return h ? configure_t<32, 8, true, 2>() : configure_t<32, 8, false, 2>();
     case kTile32x12w: return h ? configure_t<32, 12, true, 2>() : configure_t<32, 12, false, 2>();
+    case kTile16x15: return h ? configure_t<16, 15, true>() : configure_t<16, 15, false>();
+    case kTile32x7w: return h ? configure_t<32, 7, true, 1>() : configure_t<32, 7, false, 1>();
+    case kTile16x15t: {
+      // the plain 16x15 kernel serves the other stages and grids without maps
+      const cudaError_t e = h ? configure_t<16, 15, true>() : configure_t<16, 15, false>();
+      if (e != cudaSuccess) return e;
+      return h ? configure_tma_t<16, 15, true>() : configure_tma_t<16, 15, false>();
+    }
     // marching kernels use no dynamic shared memory; the generic stages run
     // on 32x16 tiles under them
     default: return h ? configure_t<32, 16, true>() : configure_t<32, 16, false>();
@@ -849,6 +1057,16 @@ static cudaError_t launch_stage(const StepArgs& a, FluxOut fl, cudaStream_t s, i
       return h ? launch_stage_t<32, 8, true, STAGE, 2>(a, fl, s, gk) : launch_stage_t<32, 8, false, STAGE, 2>(a, fl, s, gk);
     case kTile32x12w:
       return h ? launch_stage_t<32, 12, true, STAGE, 2>(a, fl, s, gk) : launch_stage_t<32, 12, false, STAGE, 2>(a, fl, s, gk);
+    case kTile16x15:
+      return h ? launch_stage_t<16, 15, true, STAGE>(a, fl, s, gk) : launch_stage_t<16, 15, false, STAGE>(a, fl, s, gk);
+    case kTile32x7w:
+      return h ? launch_stage_t<32, 7, true, STAGE, 1>(a, fl, s, gk) : launch_stage_t<32, 7, false, STAGE, 1>(a, fl, s, gk);
+    case kTile16x15t:
+      if constexpr (STAGE == 1 || STAGE == 2) {
+        if (a.maps)
+          return h ? launch_stage_tma_t<16, 15, true, STAGE>(a, s) : launch_stage_tma_t<16, 15, false, STAGE>(a, s);
+      }
+      return h ? launch_stage_t<16, 15, true, STAGE>(a, fl, s, gk) : launch_stage_t<16, 15, false, STAGE>(a, fl, s, gk);
     default:
       break;
   }
@@ -944,6 +1162,66 @@ cudaError_t launch_stage_only(const StepArgs& a, int stage, cudaStream_t s) {
   return launch_close(a, true, s);
 }
 
+// ---- TMA maps of the state buffers ----
+
+// The driver's tensor-map encoder through the runtime (no link against the
+// driver library); *status: 0, or 100 + the runtime error, or 200 + the
+// entry-point query result.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder(int* status) {
+  static int st = 0;
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    const cudaError_t e =
+        cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q);
+    if (e != cudaSuccess) {
+      st = 100 + (int)e;
+      p = nullptr;
+    } else if (q != cudaDriverEntryPointSuccess) {
+      st = 200 + (int)q;
+      p = nullptr;
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  *status = st;
+  return fn;
+}
+
+// One FP64 field of g's layout (nxt x nyt elements, rows `pitch` apart),
+// boxes of bw x bh elements, zeros outside; 0 or 1000 + the driver's result.
+static int encode_field(PFN_cuTensorMapEncodeTiled_v12000 enc, CUtensorMap* m,
+                        const double* base, const Grid& g, int bw, int bh) {
+  if (((uintptr_t)base & 15) != 0) return 2;
+  cuuint64_t dims[2] = {(cuuint64_t)g.nxt, (cuuint64_t)g.nyt};
+  cuuint64_t strides[1] = {(cuuint64_t)g.pitch * sizeof(double)};
+  cuuint32_t box[2] = {(cuuint32_t)bw, (cuuint32_t)bh};
+  cuuint32_t estride[2] = {1, 1};
+  const CUresult r =
+      enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dims, strides, box,
+          estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 0 : 1000 + (int)r;
+}
+
+int encode_tile_maps(const StepArgs& a, TileMaps* m) {
+  const Grid& g = a.g;
+  // rows must start on 16-byte boundaries (the boxes' x starts are even)
+  if ((g.pitch * sizeof(double)) % 16 != 0 || g.nx_phys() < 1 || g.ny_phys() < 1) return 1;
+  int st = 0;
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder(&st);
+  if (!enc) return st != 0 ? st : 3;
+  using SM = StageSmem<16, 15, true>;  // kTile16x15t
+  const FieldSet sets[3] = {a.U0, a.U1, a.S};
+  for (int k = 0; k < 3; ++k) {
+    const double* f[3] = {sets[k].h, sets[k].hu, sets[k].hv};
+    for (int c = 0; c < 3; ++c) {
+      if ((st = encode_field(enc, &m->tile[k][c], f[c], g, SM::TW, SM::TH)) != 0) return st;
+      if (k < 2 && (st = encode_field(enc, &m->cells[k][c], f[c], g, SM::CW, 15)) != 0) return st;
+    }
+  }
+  return encode_field(enc, &m->bed, a.b, g, SM::TW, SM::TH);
+}
+
 int launches_per_step(const StepArgs& a) {
   const Grid& g = a.g;
   const int need = g.ng > 2 ? g.ng : 2;
@@ -991,6 +1269,8 @@ cudaError_t configure_batch(int tile, int hllc) {
     case kTile16x16: return h ? configure_batch_t<16, 16, true>() : configure_batch_t<16, 16, false>();
     case kTile32x8w: return h ? configure_batch_t<32, 8, true, 2>() : configure_batch_t<32, 8, false, 2>();
     case kTile32x12w: return h ? configure_batch_t<32, 12, true, 2>() : configure_batch_t<32, 12, false, 2>();
+    case kTile16x15: return h ? configure_batch_t<16, 15, true>() : configure_batch_t<16, 15, false>();
+    case kTile32x7w: return h ? configure_batch_t<32, 7, true, 1>() : configure_batch_t<32, 7, false, 1>();
     default: return cudaErrorInvalidValue;  // batches use the shared-memory tiles
   }
 }
@@ -999,7 +1279,8 @@ template <int TX, int TY, bool HLLC, int STAGE, int XW = 0>
 static cudaError_t launch_stage_batch_t(const BatchLaunch& bl, cudaStream_t s) {
   auto kern = bl.plain ? k_stage_batch<TX, TY, HLLC, STAGE, XW, true>
                        : k_stage_batch<TX, TY, HLLC, STAGE, XW, false>;
-  kern<<<(unsigned)bl.blocks, TX * TY + 32 * XW, StageSmem<TX, TY>::BYTES, s>>>(bl.args, bl.map);
+  kern<<<(unsigned)bl.blocks, stage_threads(TX, TY, XW), StageSmem<TX, TY>::BYTES, s>>>(bl.args,
+                                                                                      bl.map);
   return cudaGetLastError();
 }
 
@@ -1019,6 +1300,10 @@ static cudaError_t launch_stage_batch(const BatchLaunch& bl, cudaStream_t s) {
       return h ? launch_stage_batch_t<32, 8, true, STAGE, 2>(bl, s) : launch_stage_batch_t<32, 8, false, STAGE, 2>(bl, s);
     case kTile32x12w:
       return h ? launch_stage_batch_t<32, 12, true, STAGE, 2>(bl, s) : launch_stage_batch_t<32, 12, false, STAGE, 2>(bl, s);
+    case kTile16x15:
+      return h ? launch_stage_batch_t<16, 15, true, STAGE>(bl, s) : launch_stage_batch_t<16, 15, false, STAGE>(bl, s);
+    case kTile32x7w:
+      return h ? launch_stage_batch_t<32, 7, true, STAGE, 1>(bl, s) : launch_stage_batch_t<32, 7, false, STAGE, 1>(bl, s);
     default:
       return cudaErrorInvalidValue;
   }

@@ -1,10 +1,11 @@
 """Failure detection on the device, made to happen without faulting the GPU.
 
-* A bulk-copy wait that runs out (FP32 sweep): the limit of the sweep's waits
-  is set to one cycle, so the first wait of every warp gives up; the kernel
-  flags the step, still waits (with the default limit) for the copies it
-  issued, and returns.  The step fails with a message naming the wait; with
-  the default limit restored the same handle steps normally.
+* A bulk-copy wait that runs out (FP32 sweep; FP64 TMA-staged tiles): the
+  limit of the device-side waits is set to one cycle, so the first wait of
+  every warp (block) gives up; the kernel flags the step, still waits (with
+  the default limit) for the copies it issued, and returns.  The step fails
+  with a message naming the wait; with the default limit restored the same
+  handle steps normally.
 * A non-finite state: a NaN put into the momentum through the setter is
   caught by the stage-2 epilogue; the step that produced it completes, the
   rest of the requested steps do not run, and the call fails with a message
@@ -33,8 +34,12 @@ def _sim(precision):
     return s
 
 
-def test_expired_bulk_copy_wait_fails_the_step_and_the_handle_recovers():
-    with _sim(32) as s:
+@pytest.mark.parametrize("precision,tile", [(32, None), (64, 10)])
+def test_expired_bulk_copy_wait_fails_the_step_and_the_handle_recovers(precision, tile):
+    with _sim(precision) as s:
+        if tile is not None:
+            s.set_tile(tile)
+            assert s._lib.rkb_tma_tile_status(s._handle) == 0  # the TMA-staged kernel runs
         s.step(2)
         state = [a.copy() for a in (s.h_phys, s.hu_phys, s.hv_phys)]
         lib = s._lib

@@ -293,10 +293,12 @@ def test_tiles_agree():
     h = hump_depth(b, dx, dx, width=40.0)
     cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, t_end=1e6, cfl=0.45, use_hllc=True)
     ref = None
-    for tile in range(8):
+    for tile in range(11):
         sim, _ = pair(cfg, bathymetry=b, initial_h=h)
         with sim:
             sim.set_tile(tile)
+            if tile == 10:  # the TMA-staged kernel, not its fallback
+                assert sim._lib.rkb_tma_tile_status(sim._handle) == 0
             sim.step(25)
             cur = sim.h.copy(), sim.hu.copy(), sim.hv.copy()
         if ref is None:
