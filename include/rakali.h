@@ -152,9 +152,8 @@ int rkb_get_device_fields(void *handle, void **ptrs, int *pitch);
 /* Kernel shape of the FP64 stage (0: 32x8, 1: 32x16, 2: 64x4, 3: 16x16
  * tiles; 4 / 5: marching strips of 64 / 32 rows; 6 / 7: 32x8 / 32x12 tiles
  * with two extra warps; 8: 16x15 tiles; 9: 32x7 tiles with one extra warp;
- * 10: 16x15 tiles in a persistent kernel that TMA-loads each block's next
- * tile while it updates the current one (the 16x15 kernel where its maps
- * cannot be encoded, see rkb_tma_tile_status)).  Results do not depend on the shape.  -2 for any other
+ * 10: 16x15 tiles loaded by TMA copies of their halo boxes (the 16x15
+ * kernel where its maps cannot be encoded, see rkb_tma_tile_status)).  Results do not depend on the shape.  -2 for any other
  * value. */
 int rkb_set_tile(void *handle, int tile);
 int rkb_get_tile(void *handle);

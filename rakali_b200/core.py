@@ -761,8 +761,8 @@ class Rakali:
     def set_tile(self, tile: int):
         """Kernel shape of the FP64 stage (0: 32x8, 1: 32x16, 2: 64x4, 3: 16x16 tiles;
         4 / 5: marching strips of 64 / 32 rows; 6 / 7: 32x8 / 32x12 tiles with two extra
-        warps; 8: 16x15 tiles; 9: 32x7 tiles with one extra warp; 10: 16x15 tiles in a
-        persistent kernel with TMA-staged tiles)."""
+        warps; 8: 16x15 tiles; 9: 32x7 tiles with one extra warp; 10: 16x15 tiles
+        loaded by TMA copies of their halo boxes)."""
         self._check_alive()
         self._rc(self._lib.rkb_set_tile(self._handle, int(tile)), "set_tile")
 

@@ -38,9 +38,8 @@ enum TileShape : int {
   // tiles whose face loop takes exactly two rounds of 256 threads: 16x15
   // (511 faces) and 32x7 with one extra warp (487 faces)
   kTile16x15 = 8, kTile32x7w = 9,
-  // 16x15 tiles in a persistent kernel: each block walks a list of tiles and
-  // TMA-loads the next tile's halo box while it updates the current one's
-  // cells (the plain 16x15 kernel runs where the maps cannot be encoded)
+  // 16x15 tiles loaded by TMA copies of their halo boxes (the plain 16x15
+  // kernel runs where the maps cannot be encoded)
   kTile16x15t = 10,
   kNumTiles = 11
 };

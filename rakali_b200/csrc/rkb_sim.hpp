@@ -72,7 +72,7 @@ class Sim {
   BcParams bc{};
   Physics phys{};
   bool params_dirty = true;
-  int tile = kTile16x15;  // fastest measured FP64 variant on B200 (4096^2 workload)
+  int tile = kTile16x15t;  // fastest measured FP64 variant on B200 (4096^2 workload)
   int steps_per_graph_cap = 256;
   int sweep_rows = 0;     // FP32 sweep: rows per warp (0: one wave of resident warps)
   int sweep_cpl = 2;      // FP32 sweep: columns per lane (2 or 4)

@@ -228,10 +228,8 @@ __device__ __forceinline__ StagePtrs stage_ptrs(double* base) {
 // TMA copies of tile (bx, by) for the TMA-staged kernel (one thread): the
 // halo box of h, hu, hv from field set `in_set` (0 U0, 1 U1, 2 S) and of the
 // bed, and in stage 2 the cell box of U^n from `old_set`, all completing on
-// `bar`.  The caller has passed a block barrier after the last reads of
-// these arrays; the proxy fence orders those reads before the copies.  The
-// box x coordinates, ng + bx TX - 2 - (ng & 1) and that + 2, are even (TX is),
-// which puts every box start on a 16-byte boundary.
+// `bar`.  The box x coordinates, ng + bx TX - 2 - (ng & 1) and that + 2, are
+// even (TX is), which puts every box start on a 16-byte boundary.
 template <int TX, int TY, int STAGE>
 __device__ __forceinline__ void issue_tile(const TileMaps& tm, int in_set, int old_set,
                                            const Grid& g, unsigned bx, unsigned by,
@@ -252,14 +250,7 @@ __device__ __forceinline__ void issue_tile(const TileMaps& tm, int in_set, int o
   }
 }
 
-// The next tile of a TMA-staged block: issued by thread 0 once the face
-// loop of the current tile has read the tile arrays for the last time.
-struct TmaNext {
-  const TileMaps* maps = nullptr;  // parameter-space copy
-  uint32_t bar = 0;
-  int tile = -1;                   // next tile index of this block, < 0: none
-  int in_set = 0, old_set = 0;
-};
+
 
 // STAGE 1: U^n (buffer cur) -> U* (scratch S).
 // STAGE 2: U* (S) and U^n (buffer cur) -> U^{n+1} (buffer cur^1).
@@ -275,8 +266,7 @@ struct TmaNext {
 // PLAIN: the build for stages without forcing, Coriolis or sponge terms
 // (Manning friction only), chosen by the host from its copy of the physics.
 // TMA: the tile arrays were filled by TMA copies the caller has waited for
-// (the TMA-staged kernel, stages 1 and 2); `nx` names the block's next tile,
-// whose copies thread 0 issues after the face loop.
+// (the TMA-staged kernel, stages 1 and 2).
 template <int TX, int TY, bool HLLC, int STAGE, int XW = 0, bool PLAIN = false, bool TMA = false>
 __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Physics* phys,
                                            const BcParams* bcp, const FieldSet& U0,
@@ -284,7 +274,7 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
                                            const double* __restrict__ b, const Forcing& fo,
                                            double* __restrict__ partials, const FluxOut& fl,
                                            unsigned bx, unsigned by, unsigned gx, unsigned gy,
-                                           int gk = 0, TmaNext nx = TmaNext{}) {
+                                           int gk = 0) {
   static_assert(!TMA || STAGE == 1 || STAGE == 2, "TMA staging serves the SSP-RK2 stages");
   using SM = StageSmem<TX, TY, TMA>;
   constexpr int TW = SM::TW;
@@ -402,7 +392,8 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
   }
   // 3. cell update: one cell per thread (the extra warps repeat cell 0 and
   // store nothing).  The cell's own state and U^n are read before the
-  // barrier: behind it the TMA-staged kernel refills the tile arrays.
+  // barrier, where their latency passes while the slower warps finish
+  // their faces.
   const int tc = tid < TX * TY ? tid : 0;
   const int c = tc % TX, r = tc / TX;
   const int i = gx0 + c, j = gy0 + r;
@@ -416,9 +407,6 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
     hv_n = ov[qn];
   }
   __syncthreads();
-  if (TMA && tid == 0 && nx.tile >= 0)
-    issue_tile<TX, TY, STAGE>(*nx.maps, nx.in_set, nx.old_set, g, (unsigned)nx.tile % gx,
-                              (unsigned)nx.tile / gx, nx.bar, P);
 
   const bool valid = tid < TX * TY && i < g.nxt - g.ng && j < g.nyt - g.ng;
   const int fl_ = r * (TX + 1) + c, fr_ = fl_ + 1;
@@ -576,18 +564,20 @@ __device__ __forceinline__ bool plain_mismatch64(StepCtl* ctl, const Physics* ph
   return true;
 }
 
-// Resident blocks per SM the stage kernels are built for: as many as 64
-// registers a thread and the tile's shared memory allow (4 for the 256-thread
-// tiles, 3 for 288 threads, 2 for 448 and 512).  Left free, the compiler
-// gives the stages more registers than that occupancy allows.  The
-// plain-physics stage 1 of a 256-thread tile whose shared memory (with the
-// 1 KB each block reserves) fits five blocks in the SM's 228 KB is built for
-// five: 48 registers and a few spilled bytes, measured 3% faster.  Stage 2
-// holds U^n as well and measured 1% slower so, and the full-physics build
-// spills several times more: both keep four.
-constexpr int stage_blocks_per_sm(int threads, int smem_bytes = 0, bool five = false) {
-  return threads <= 256 ? (five && 5 * (smem_bytes + 128 + 1024) <= 228 * 1024 ? 5 : 4)
-                        : threads <= 320 ? 3 : 2;
+// Resident blocks per SM the stage kernels are built for: 32 warps per SM,
+// i.e. 64 registers a thread (4 blocks of 256 threads, 8 of 128, 3 of 320, 2
+// of 448 and 512).  Left free, the compiler gives the stages more registers
+// than that occupancy allows.  `forty`: 40 warps (48 registers) where the
+// tile's shared memory, with the 1 KB each block reserves, holds that many
+// blocks in the SM's 228 KB; the plain-physics stage 1 is built so (48
+// registers and a few spilled bytes, measured 3% faster with 256-thread
+// tiles).  Stage 2 holds U^n as well and measured 1% slower so, and the
+// full-physics build spills several times more: both keep 32 warps.
+constexpr int stage_blocks_per_sm(int threads, int smem_bytes = 0, bool forty = false) {
+  const int warps = (threads + 31) / 32;
+  const int fit = smem_bytes > 0 ? 228 * 1024 / (smem_bytes + 128 + 1024) : 0;
+  if (forty && fit * warps >= 40) return 40 / warps;
+  return 32 / warps > 0 ? 32 / warps : 1;
 }
 
 template <int TX, int TY, bool HLLC, int STAGE, int XW = 0, bool PLAIN = false>
@@ -627,15 +617,13 @@ __global__ void __launch_bounds__(stage_threads(TX, TY, XW),
                                              (unsigned)m.y / gx, gx, gy);
 }
 
-// TMA-staged SSP-RK2 stage (STAGE 1 or 2) on TX x TY tiles: a persistent
-// grid of the resident blocks, block k taking tiles k, k + gridDim.x, ...
-// Each tile's halo box arrives by TMA on the block's mbarrier; thread 0
-// issues the next tile's copies as soon as the face loop has read the tile
-// arrays for the last time, so the copies overlap the cell update and the
-// partial sums.  Every tile writes its own partials, as in k_stage, so the
-// step's sums and bits are the same.  A wait that runs out of `limit` cycles
-// marks the step (kErrWait), waits for the copies in flight with the default
-// limit and ends the block.
+// TMA-staged SSP-RK2 stage (STAGE 1 or 2) on TX x TY tiles: thread 0 loads
+// the tile's halo boxes (and in stage 2 its U^n) with TMA copies completing
+// on the block's mbarrier, which every thread waits on; the rest is k_stage.
+// A wait that runs out of `limit` cycles marks the step (kErrWait), waits
+// for the copies in flight with the default limit and ends the block.
+// (A persistent form, each block walking a list of tiles and loading the
+// next while it updated the current one, measured 9% slower.)
 template <int TX, int TY, bool HLLC, int STAGE, bool PLAIN = false>
 __global__ void __launch_bounds__(stage_threads(TX, TY, 0),
                                   stage_blocks_per_sm(stage_threads(TX, TY, 0),
@@ -648,38 +636,25 @@ __global__ void __launch_bounds__(stage_threads(TX, TY, 0),
   if (!ctl->active) return;
   const int cur = ctl->cur;
   const unsigned gx = (unsigned)((g.nx_phys() + TX - 1) / TX);
-  const unsigned gy = (unsigned)((g.ny_phys() + TY - 1) / TY);
-  const unsigned ntiles = gx * gy;
+  const unsigned bx = blockIdx.x % gx, by = blockIdx.x / gx;
   extern __shared__ double smem[];
-  const StagePtrs P = stage_ptrs<TX, TY, true>(smem);
   __shared__ __align__(8) unsigned long long bar_word;
-  TmaNext nx;
-  nx.maps = &tm;
-  nx.bar = smem_u32(&bar_word);
-  nx.in_set = STAGE == 2 ? 2 : cur;
-  nx.old_set = cur;
+  const uint32_t bar = smem_u32(&bar_word);
   if (threadIdx.x == 0) {
-    mbar_init(nx.bar, 1);
+    mbar_init(bar, 1);
     fence_mbar_init();
+    issue_tile<TX, TY, STAGE>(tm, STAGE == 2 ? 2 : cur, cur, g, bx, by, bar,
+                              stage_ptrs<TX, TY, true>(smem));
   }
   __syncthreads();
-  unsigned t = blockIdx.x;
-  if (threadIdx.x == 0 && t < ntiles)
-    issue_tile<TX, TY, STAGE>(tm, nx.in_set, nx.old_set, g, t % gx, t / gx, nx.bar, P);
-  uint32_t parity = 0;
-  for (; t < ntiles; t += gridDim.x) {
-    const bool ok = mbar_wait(nx.bar, parity, limit);
-    if (__syncthreads_or(!ok)) {
-      if (threadIdx.x == 0) atomicExch(&ctl->error, kErrWait);
-      mbar_wait(nx.bar, parity, kWaitCyclesDefault);  // the copies still in flight
-      return;
-    }
-    parity ^= 1u;
-    const unsigned next = t + gridDim.x;
-    nx.tile = next < ntiles ? (int)next : -1;
-    stage_body<TX, TY, HLLC, STAGE, 0, PLAIN, true>(g, ctl, phys, bcp, U0, U1, S, b, fo, partials,
-                                                    FluxOut{}, t % gx, t / gx, gx, gy, 0, nx);
+  const bool ok = mbar_wait(bar, 0, limit);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) atomicExch(&ctl->error, kErrWait);
+    mbar_wait(bar, 0, kWaitCyclesDefault);  // the copies still in flight
+    return;
   }
+  stage_body<TX, TY, HLLC, STAGE, 0, PLAIN, true>(g, ctl, phys, bcp, U0, U1, S, b, fo, partials,
+                                                  FluxOut{}, bx, by, gx, gridDim.x / gx);
 }
 
 // ---------------------------------------------------------------------------
@@ -957,23 +932,14 @@ static cudaError_t launch_stage_t(const StepArgs& a, FluxOut fl, cudaStream_t s,
   return cudaGetLastError();
 }
 
-// The TMA-staged kernel: one block per resident slot (at most one per tile).
+// The TMA-staged kernel: one block per tile.
 template <int TX, int TY, bool HLLC, int STAGE>
 static cudaError_t launch_stage_tma_t(const StepArgs& a, cudaStream_t s) {
   using SM = StageSmem<TX, TY, true>;
   auto kern = a.plain ? k_stage_tma<TX, TY, HLLC, STAGE, true> : k_stage_tma<TX, TY, HLLC, STAGE, false>;
-  constexpr int threads = stage_threads(TX, TY, 0);
-  int dev = 0, sms = 0, per_sm = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, SM::BYTES);
-  if (e != cudaSuccess) return e;
   const dim3 d = stage_grid(a.g, a.tile);
-  const unsigned ntiles = d.x * d.y;
-  const unsigned slots = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));
   const long long limit = a.wait_cycles > 0 ? a.wait_cycles : kWaitCyclesDefault;
-  kern<<<ntiles < slots ? ntiles : slots, threads, SM::BYTES, s>>>(
+  kern<<<d.x * d.y, stage_threads(TX, TY, 0), SM::BYTES, s>>>(
       a.g, a.ctl, a.phys, a.bc, a.U0, a.U1, a.S, a.b, a.fo, a.partials, limit, *a.maps);
   return cudaGetLastError();
 }
