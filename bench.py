@@ -318,7 +318,7 @@ def _form_numbers(sim, args, world, local_rank, dist, cells, inputs):
             "launches_per_step": int(prof[4])}
 
 
-def _roofline(form, precision, cells, world):
+def _roofline(form, precision, cells, world, tile):
     hbm, peak_kind = peaks()
     f32 = precision == 32
     b_s2 = BYTES_STAGE2_32 if f32 else BYTES_STAGE2
@@ -327,7 +327,9 @@ def _roofline(form, precision, cells, world):
     return {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "traffic": traffic_per_launch(cells, precision),
             "kernel": ("k_sweep<stage 2> (FP32 surface form: flux + update + RK2 average)"
-                       if f32 else "k_stage<stage 2> (fused flux + update + RK2 average)"),
+                       if f32 else "k_stage_tma<16,15, stage 2> (TMA-staged tiles: fused flux + "
+                       "update + RK2 average)" if tile == 10
+                       else "k_stage<stage 2> (fused flux + update + RK2 average)"),
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
             if peak_kind == "measured" else "fallback 6650 GB/s",
             "stage_ms": form["stage_ms"], "bytes_per_cell_update": b_cell,
@@ -805,7 +807,7 @@ def run_b200(args, rank, world, local_rank, dist):
         zeros = np.full(h.shape, 0.0, order="F")
         forms[prec] = _form_numbers(sim, args, world, local_rank, dist, cells,
                                     (h, zeros, zeros.copy(order="F")))
-        forms[prec]["roofline"] = _roofline(forms[prec], prec, cells, world)
+        forms[prec]["roofline"] = _roofline(forms[prec], prec, cells, world, args.tile)
     sim.close()
     ens = run_ensemble(args, world, local_rank, dist) if args.ensemble_steps > 0 else None
     err = lake = None

@@ -542,6 +542,34 @@ __global__ void __launch_bounds__(1024)
   finalize_step(g, ctl, phys, partials, nblocks, ctl->dt, ctl->cur, budget != 0);
 }
 
+// First level of the close, before k_close: block b of the kCloseBlocks sums
+// its contiguous share of each of the four per-tile partial arrays (nparts
+// long, one after the other) in a fixed order into out[s * gridDim.x + b].
+// One block alone reads the tens of thousands of partials of a large grid at
+// the latency of its own loads (45 us a step at 4096^2).
+__global__ void __launch_bounds__(256)
+    k_close_part(const StepCtl* ctl, const double* __restrict__ partials, unsigned int nparts,
+                 double* __restrict__ out) {
+  if (!ctl->active) return;
+  const unsigned int per = (nparts + gridDim.x - 1) / gridDim.x;
+  const unsigned int k0 = blockIdx.x * per;
+  const unsigned int k1 = k0 + per < nparts ? k0 + per : nparts;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (unsigned int k = k0 + threadIdx.x; k < k1; k += blockDim.x)
+    for (int s = 0; s < 4; ++s) acc[s] = acc[s] + __ldcg(partials + (size_t)s * nparts + k);
+  __shared__ double red[4][8];
+  for (int s = 0; s < 4; ++s) {
+    const double w = warp_sum(acc[s]);
+    if ((threadIdx.x & 31) == 0) red[s][threadIdx.x >> 5] = w;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t = t + red[threadIdx.x][w];
+    out[threadIdx.x * gridDim.x + blockIdx.x] = t;
+  }
+}
+
 // The same for every simulation of a batch (blockIdx.x = simulation), tiles
 // of tx x ty cells.
 __global__ void __launch_bounds__(1024)
@@ -917,10 +945,13 @@ static dim3 stage_grid(const Grid& g, int tile) {
   return dim3((unsigned)((g.nx_phys() + tx - 1) / tx), (unsigned)((g.ny_phys() + ty - 1) / ty));
 }
 
+// Blocks of the close's first level (k_close_part).
+constexpr unsigned int kCloseBlocks = 148;
+
 size_t partials_doubles(const Grid& g, int tile) {
   dim3 d = stage_grid(g, tile);
   const size_t parts = (size_t)d.x * (size_t)d.y * (is_march(tile) ? kMarchWarps : 1);
-  return 4 * parts;
+  return 4 * parts + 4 * kCloseBlocks;  // + the first level of the close
 }
 
 template <int TX, int TY, bool HLLC, int STAGE, int XW = 0>
@@ -1005,9 +1036,18 @@ cudaError_t configure_kernels(int tile, int hllc) {
 }
 
 // The close of a step whose last stage ran on shared-memory tiles.
+// With the boundary budget, k_close_part first reduces the per-tile partials
+// to kCloseBlocks per array (stored after them), which k_close then sums.
 static cudaError_t launch_close(const StepArgs& a, bool budget, cudaStream_t s) {
   const dim3 d = stage_grid(a.g, a.tile);
-  k_close<<<1, 1024, 0, s>>>(a.g, a.ctl, a.phys, a.partials, d.x * d.y, budget ? 1 : 0);
+  const unsigned int nparts = d.x * d.y;
+  if (!budget) {
+    k_close<<<1, 1024, 0, s>>>(a.g, a.ctl, a.phys, a.partials, nparts, 0);
+    return cudaGetLastError();
+  }
+  double* first = a.partials + 4 * (size_t)nparts;
+  k_close_part<<<kCloseBlocks, 256, 0, s>>>(a.ctl, a.partials, nparts, first);
+  k_close<<<1, 1024, 0, s>>>(a.g, a.ctl, a.phys, first, kCloseBlocks, 1);
   return cudaGetLastError();
 }
 
@@ -1198,7 +1238,7 @@ int launches_per_step(const StepArgs& a) {
   const int bc = (g.nx_phys() >= need ? 1 : 2) + (g.ny_phys() >= need ? 1 : 2);
   const int pre = narrow_grid(g) ? bc : 0;
   if (a.scheme != 2) return a.n_stages * (bc + 1) + pre + 1;  // + the close
-  return 2 * bc + 2 + pre + (is_march(a.tile) ? 0 : 1);
+  return 2 * bc + 2 + pre + (is_march(a.tile) ? 0 : 2);  // + the close's two levels
 }
 
 cudaError_t launch_max_speed(const StepArgs& a, cudaStream_t s) {

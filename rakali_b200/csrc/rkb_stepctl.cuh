@@ -95,8 +95,9 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// Close a step (last block of the final stage kernel): fixed-order sums of
-// the per-block partials, the mass budget in the reference's order
+// Close a step (one block: k_close after the last FP64 stage, or the last
+// block of a marching or FP32 sweep kernel): fixed-order sums of the
+// partials, the mass budget in the reference's order
 // (rki_solver.F90:507-657), the CFL maxima of the new state and the clock.
 // `budget` false: the generic Shu-Osher schemes, which do not accumulate the
 // boundary mass budget (rki_solver.F90:861-926).
@@ -106,12 +107,10 @@ static __device__ void finalize_step(const Grid& g, StepCtl* ctl, const Physics*
   const int tid = threadIdx.x;
   const int nthr = (int)blockDim.x;  // a multiple of 32
   const double area = g.dx * g.dy;
-  // Fixed-order sums of the per-block partials over every thread of this
-  // (last) block: thread t adds partials t, t + nthr, ... in order (L2 loads:
-  // the other blocks wrote them before their fence and counter increment),
-  // each warp combines its lanes by butterfly, and thread 0 adds the warp
-  // results in warp order.  With tens of thousands of partials a step, one
-  // warp doing it alone left the rest of the GPU idle for a long tail.
+  // Fixed-order sums of the partials over every thread of this block: thread
+  // t adds partials t, t + nthr, ... in order (L2 loads: earlier kernels or
+  // blocks wrote them), each warp combines its lanes by butterfly, and thread
+  // 0 adds the warp results in warp order.
   __shared__ double red[4][32];
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   if (budget) {
