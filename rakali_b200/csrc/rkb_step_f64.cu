@@ -1,17 +1,18 @@
 // FP64 kernels of the structured SSP-RK2 step (sm_100a).
 //
-// One step is four launches, all reading their clock from the device-side
+// One step is eight launches, all reading their clock from the device-side
 // StepCtl so a whole chunk of steps can be captured once in a CUDA graph:
 //
 //   bc_we / bc_sn (stage 1, time t)   ghost fill of U^n          rki_boundary.F90:40-218
 //   stage<1>                          U^n -> U*                  rki_kernel_flux.F90 + rki_kernel_fused.F90:164-303
 //   bc_we / bc_sn (stage 2, t + dt)   ghost fill of U*           (ghosts also copied into the U^{n+1} buffer)
 //   stage<2>                          U*, U^n -> U^{n+1}         rki_kernel_fused.F90:305-471
+//   close_part, close                 sums, budget, clock        rki_solver.F90:507-657
 //
 // The CFL reduction (rki_kernel_timestep.F90:16-74) is folded into the
 // stage-2 epilogue; the first launch of the next step turns it into dt.
 // The boundary mass-out sums (rki_solver.F90:507-537) are per-tile partials
-// reduced in a fixed order by a one-block close kernel after stage 2.
+// reduced in a fixed order by the two close kernels after stage 2.
 #include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled
 
 #include "rkb_async.cuh"
