@@ -393,24 +393,13 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
       fya[5 * SM::NFY + kk] = o.pL2;
     }
   }
+  __syncthreads();
+
   // 3. cell update: one cell per thread (the extra warps repeat cell 0 and
-  // store nothing).  The cell's own state and U^n are read before the
-  // barrier, where their latency passes while the slower warps finish
-  // their faces.
+  // store nothing)
   const int tc = tid < TX * TY ? tid : 0;
   const int c = tc % TX, r = tc / TX;
   const int i = gx0 + c, j = gy0 + r;
-  const int qc = (r + 2) * TW + (c + 2);
-  const double h_c = th[qc], hu_c = tu[qc], hv_c = tv[qc];
-  double h_n = 0.0, hu_n = 0.0, hv_n = 0.0;
-  if (STAGE == 2) {
-    const int qn = r * SM::CW + c;
-    h_n = oh[qn];
-    hu_n = ou[qn];
-    hv_n = ov[qn];
-  }
-  __syncthreads();
-
   const bool valid = tid < TX * TY && i < g.nxt - g.ng && j < g.nyt - g.ng;
   const int fl_ = r * (TX + 1) + c, fr_ = fl_ + 1;
   const int fb_ = r * TX + c, ft_ = fb_ + TX;
@@ -442,7 +431,8 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
         if (j == g.ng) fl.mflux_y[q - g.pitch] = fya[fb_];
       }
     } else {
-      double a = h_c, u = hu_c, v = hv_c;
+      const int qc = (r + 2) * TW + (c + 2);
+      double a = th[qc], u = tu[qc], v = tv[qc];
       a = a + dt * o_fh;
       u = u + dt * o_fhu;
       v = v + dt * o_fhv;
@@ -472,9 +462,10 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
       } else {
         // RK2 average with U^n and the second clamp (rki_kernel_fused.F90:435-463)
         out = cur ? U0 : U1;
-        a = 0.5 * (h_n + a);
-        u = 0.5 * (hu_n + u);
-        v = 0.5 * (hv_n + v);
+        const int qn = r * SM::CW + c;  // U^n of this cell
+        a = 0.5 * (oh[qn] + a);
+        u = 0.5 * (ou[qn] + u);
+        v = 0.5 * (ov[qn] + v);
         protect(a, u, v);
       }
       const double h_pre_sponge = a;
