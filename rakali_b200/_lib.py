@@ -142,6 +142,7 @@ def load(path: str | None = None):
     _sig(lib, "rkb_adjoint_forward", [H, DP, DP, D, I, DP, DP], I)
     _sig(lib, "rkb_adjoint_gradient", [H, DP, DP, D, DP, DP, DP], I)
     _sig(lib, "rkb_adjoint_checkpoint_interval", [H], I)
+    _sig(lib, "rkb_adjoint_set_state_budget", [H, ctypes.c_longlong], I)
     _sig(lib, "rkb_adjoint_last_ms", [H], D)
     _sig(lib, "rkb_adjoint_batch_create",
          [I, I, I, I, I, D, D, D, I, I, DP, DP, DP, IP, IP, I, HP], I)

@@ -122,7 +122,16 @@ class GaugeMisfit:
 
     @property
     def checkpoint_interval(self):
+        """1 once a gradient run kept every state in device memory, else the
+        sqrt(n_steps) checkpoint interval."""
         return int(self._lib.rkb_adjoint_checkpoint_interval(self._a))
+
+    def set_state_budget(self, nbytes):
+        """Device bytes a gradient run may allocate to keep every state: None
+        (the default) half the free device memory, 0 never (sqrt(n_steps)
+        checkpoints and recomputation).  The gradients are the same bits."""
+        self._rc(self._lib.rkb_adjoint_set_state_budget(self._a, -1 if nbytes is None else int(nbytes)),
+                 "set_state_budget")
 
     @property
     def last_ms(self) -> float:
@@ -271,7 +280,16 @@ class GaugeMisfitBatch:
 
     @property
     def checkpoint_interval(self):
+        """1 once a gradient run kept every state in device memory, else the
+        sqrt(n_steps) checkpoint interval."""
         return int(self._lib.rkb_adjoint_checkpoint_interval(self._a))
+
+    def set_state_budget(self, nbytes):
+        """Device bytes a gradient run may allocate to keep every state: None
+        (the default) half the free device memory, 0 never (sqrt(n_steps)
+        checkpoints and recomputation).  The gradients are the same bits."""
+        self._rc(self._lib.rkb_adjoint_set_state_budget(self._a, -1 if nbytes is None else int(nbytes)),
+                 "set_state_budget")
 
     @property
     def last_ms(self) -> float:

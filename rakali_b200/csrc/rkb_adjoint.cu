@@ -103,6 +103,12 @@ int rkb_adjoint_checkpoint_interval(void* adj) {
   return adj ? as_adj(adj)->checkpoint_interval() : -2;
 }
 
+int rkb_adjoint_set_state_budget(void* adj, long long bytes) {
+  if (!adj) return -2;
+  as_adj(adj)->set_state_budget(bytes);
+  return 0;
+}
+
 double rkb_adjoint_last_ms(void* adj) { return adj ? as_adj(adj)->last_ms() : -1.0; }
 
 int rkb_adjoint_members(void* adj) { return adj ? as_adj(adj)->members() : -2; }

@@ -12,8 +12,12 @@
 //   reverse, per stage:  cells -> faces -> reconstruction -> slope gather -> walls
 //
 // Every reverse kernel gathers (each output element is written by one thread),
-// so there are no atomics and the gradient is deterministic.  States are
-// checkpointed every K ~ sqrt(N) steps and recomputed segment by segment.
+// so there are no atomics and the gradient is deterministic.  A gradient run
+// keeps every state U^0..U^N in device memory when they fit in the state
+// budget (by default half the free memory at the first run: 12.7 GB for
+// 1024^2 FP64 over 500 steps), so the reverse sweep reads U^k directly;
+// otherwise states are checkpointed every K ~ sqrt(N) steps and recomputed
+// segment by segment.  Both give the same bits.
 // Each launch covers every member (blockIdx.z = member; member m's arrays start
 // m * ms elements after member 0's).
 //
@@ -47,7 +51,12 @@ class AdjointBase {
                       double* eta_out) = 0;
   virtual int gradient(const double* b, const double* n, double n_scalar, double* J,
                        double* gb_out, double* gn_out) = 0;
+  // 1 once a gradient run kept every state, else K ~ sqrt(N).
   virtual int checkpoint_interval() const = 0;
+  // Bytes the gradient may allocate to keep every state: < 0 half the free
+  // device memory at the next gradient run, 0 never (sqrt(N) checkpoints
+  // and recomputation only).  Frees a kept-state allocation above it.
+  virtual void set_state_budget(long long bytes) = 0;
   virtual double last_ms() = 0;
   virtual int members() const = 0;
   virtual int precision() const = 0;
@@ -699,6 +708,7 @@ class Adjoint final : public AdjointBase {
   ~Adjoint() override {
     for (auto& e : ev_)
       if (e) cudaEventDestroy(e);
+    if (all_mem_) cudaFree(all_mem_);
     if (mem_) cudaFree(mem_);
     if (obs_d_) cudaFree(obs_d_);
     if (stream_) cudaStreamDestroy(stream_);
@@ -864,7 +874,7 @@ class Adjoint final : public AdjointBase {
         if (cfl_step(U_, k) != 0) return -1;
       }
       if (step(U_, U_, k) != 0) return -1;
-      gauges(k);
+      gauges(k, U_);
     }
     if (record) have_dt_ = true;
     if (mark(1) != 0) return -1;
@@ -878,14 +888,24 @@ class Adjoint final : public AdjointBase {
     if (!have_dt_) return -2;
     if (upload_params(b, n, n_scalar) != 0) return -1;
     const size_t fb = ms_ * nm_ * sizeof(T);
+    const bool all = keep_all_states();
     if (mark(0) != 0) return -1;
-    // forward with checkpoints
-    if (copy(U_, ck_[0]) != 0) return -1;
-    for (int k = 0; k < nsteps_; ++k) {
-      if (step(U_, U_, k) != 0) return -1;
-      gauges(k);
-      if ((k + 1) % K_ == 0 && (k + 1) / K_ < nck_)
-        if (copy(ck_[(k + 1) / K_], U_) != 0) return -1;
+    if (all) {
+      // forward keeping every state
+      if (copy(all_[0], ck_[0]) != 0) return -1;
+      for (int k = 0; k < nsteps_; ++k) {
+        if (step(all_[k], all_[k + 1], k) != 0) return -1;
+        gauges(k, all_[k + 1]);
+      }
+    } else {
+      // forward with checkpoints
+      if (copy(U_, ck_[0]) != 0) return -1;
+      for (int k = 0; k < nsteps_; ++k) {
+        if (step(U_, U_, k) != 0) return -1;
+        gauges(k, U_);
+        if ((k + 1) % K_ == 0 && (k + 1) / K_ < nck_)
+          if (copy(ck_[(k + 1) / K_], U_) != 0) return -1;
+      }
     }
     // reverse
     ADJ_TRY(cudaMemsetAsync(lam_.h, 0, fb, stream_));
@@ -893,8 +913,14 @@ class Adjoint final : public AdjointBase {
     ADJ_TRY(cudaMemsetAsync(lam_.hv, 0, fb, stream_));
     ADJ_TRY(cudaMemsetAsync(gb_, 0, fb, stream_));
     ADJ_TRY(cudaMemsetAsync(gn_, 0, fb, stream_));
-    const int nseg = (nsteps_ + K_ - 1) / K_;
+    const int nseg = all ? 0 : (nsteps_ + K_ - 1) / K_;
     const int ng = nm_ * ngauge_;
+    for (int k = all ? nsteps_ - 1 : -1; k >= 0; --k) {
+      if (ng > 0)  // misfit at U^{k+1}
+        k_gauges_adj<T><<<(ng + 127) / 128, 128, 0, stream_>>>(gq_, r_ + (size_t)k * ng, ng,
+                                                               lam_, gb_);
+      if (step_adj(all_[k], k) != 0) return -1;
+    }
     for (int s = nseg - 1; s >= 0; --s) {
       const int k0 = s * K_, k1 = std::min(nsteps_, k0 + K_);
       if (copy(seg_[0], ck_[s]) != 0) return -1;
@@ -916,7 +942,16 @@ class Adjoint final : public AdjointBase {
     return download_interior(gn_out, gn_);
   }
 
-  int checkpoint_interval() const override { return K_; }
+  int checkpoint_interval() const override { return kept_all_ ? 1 : K_; }
+  void set_state_budget(long long bytes) override {
+    budget_ = bytes;
+    if (all_mem_ && bytes >= 0 && (long long)all_bytes() > bytes) {
+      cudaFree(all_mem_);
+      all_mem_ = nullptr;
+      all_.clear();
+      kept_all_ = false;
+    }
+  }
   // Device milliseconds of the last forward / gradient run (CUDA events on
   // the adjoint's stream, from the initial state to the last kernel).
   double last_ms() override {
@@ -1003,11 +1038,47 @@ class Adjoint final : public AdjointBase {
     return 0;
   }
 
-  void gauges(int k) {
+  // Gauge residuals of step k from its new state V (= U^{k+1}).
+  void gauges(int k, const Fields<T>& V) {
     const int ng = nm_ * ngauge_;
     if (ng > 0)
-      k_gauges<T><<<(ng + 127) / 128, 128, 0, stream_>>>(U_, b_, gq_, obs_dev() + (size_t)k * ng,
+      k_gauges<T><<<(ng + 127) / 128, 128, 0, stream_>>>(V, b_, gq_, obs_dev() + (size_t)k * ng,
                                                          ng, r_ + (size_t)k * ng);
+  }
+
+  size_t all_bytes() const {
+    const size_t fbytes = (ms_ * nm_ * sizeof(T) + 255) / 256 * 256;
+    return 3 * fbytes * (size_t)(nsteps_ + 1);
+  }
+
+  // Every state U^0..U^N in device memory, allocated at the first gradient
+  // run that the budget allows (kept for later runs); false: checkpoints.
+  bool keep_all_states() {
+    kept_all_ = false;
+    if (budget_ == 0) return false;
+    if (!all_mem_) {
+      size_t free_b = 0, total_b = 0;
+      if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return false;
+      const size_t limit = budget_ < 0 ? free_b / 2 : (size_t)budget_;
+      if (all_bytes() > limit) return false;
+      if (cudaMalloc(&all_mem_, all_bytes()) != cudaSuccess) {
+        all_mem_ = nullptr;
+        cudaGetLastError();  // the failed allocation is not an error of the run
+        return false;
+      }
+      // zero, like the checkpoint buffers: cells no kernel writes (row
+      // padding, corners) then hold the same values in both modes
+      if (cudaMemsetAsync(all_mem_, 0, all_bytes(), stream_) != cudaSuccess) return false;
+      const size_t fbytes = (ms_ * nm_ * sizeof(T) + 255) / 256 * 256;
+      char* p = (char*)all_mem_;
+      all_.resize((size_t)nsteps_ + 1);
+      for (auto& st : all_) {
+        st = Fields<T>{(T*)p, (T*)(p + fbytes), (T*)(p + 2 * fbytes)};
+        p += 3 * fbytes;
+      }
+    }
+    kept_all_ = true;
+    return true;
   }
 
   // Per-member J = sum of squared residuals (FP64) and the gauge surfaces.
@@ -1151,6 +1222,11 @@ class Adjoint final : public AdjointBase {
   int nm_ = 1;
   double cfl_ = 0.45;
   int hllc_ = 0, nsteps_ = 0, ngauge_ = 0, K_ = 1, nck_ = 1;
+  // every state of a gradient run (keep_all_states)
+  void* all_mem_ = nullptr;
+  std::vector<Fields<T>> all_;
+  long long budget_ = -1;
+  bool kept_all_ = false;
   size_t nfields_ = 0;
   cudaStream_t stream_ = nullptr;
   void* mem_ = nullptr;

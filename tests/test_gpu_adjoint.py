@@ -104,8 +104,10 @@ def test_gradient_matches_torch_autograd(hllc):
 def test_gradient_matches_central_differences():
     nx, ny, steps = 40, 32, 29  # 29 steps: checkpoint segments of 6, the last one short
     p, b, h, n, _, _ = _problem(nx, ny, steps, 10, seed=7, generic=True)
+    p.set_state_budget(0)  # the checkpointed path: segments recomputed
     assert p.checkpoint_interval == 6
     J, gb, gn = p.gradient(b, n)
+    assert p.checkpoint_interval == 6
     rng = np.random.default_rng(11)
     for k in range(5):
         db = np.asfortranarray(gaussian_bed(nx, ny, 10.0, 10.0, 3, seed=100 + k, base=0.0,
@@ -117,6 +119,25 @@ def test_gradient_matches_central_differences():
         fd = (Jp - Jm) / (2 * eps)
         ad = float(np.sum(gb * db) + np.sum(gn * dn))
         assert abs(fd - ad) <= 1e-6 * max(abs(fd), 1e-12), (k, fd, ad)
+    p.close()
+
+
+def test_kept_states_and_checkpoints_give_the_same_bits():
+    """A gradient run that keeps every state (the default when they fit) and
+    one that checkpoints every ~sqrt(N) steps and recomputes the segments
+    return identical J and gradients."""
+    nx, ny, steps = 40, 32, 29
+    p, b, h, n, _, _ = _problem(nx, ny, steps, 10, seed=7, generic=True)
+    J1, gb1, gn1 = p.gradient(b, n)
+    assert p.checkpoint_interval == 1  # every state kept
+    p.set_state_budget(0)
+    J0, gb0, gn0 = p.gradient(b, n)
+    assert p.checkpoint_interval == 6
+    assert J0 == J1 and np.array_equal(gb0, gb1) and np.array_equal(gn0, gn1)
+    p.set_state_budget(None)
+    J2, gb2, gn2 = p.gradient(b, n)
+    assert p.checkpoint_interval == 1
+    assert J2 == J1 and np.array_equal(gb2, gb1) and np.array_equal(gn2, gn1)
     p.close()
 
 
@@ -199,14 +220,33 @@ def test_batch_fp64_equals_single_problems():
         pb.set_observations(obs)
         J, gb, gn = pb.gradient(b, n)
         dts = pb.dt
+        assert pb.checkpoint_interval == 1  # every state kept
     for m in range(nm):
         with GaugeMisfit(nx, ny, 10.0, 10.0, h[m], gauges[m], steps) as p:
+            p.set_state_budget(0)  # checkpoints: the other storage mode
             p.record_dt(b[m], n[m])
             assert np.array_equal(p.dt, dts[m])
             p.set_observations(obs[:, m, :])
             Jm, gbm, gnm = p.gradient(b[m], n[m])
         assert Jm == J[m]
         assert np.array_equal(gbm, gb[m]) and np.array_equal(gnm, gn[m])
+
+
+def test_batch_fp32_kept_states_and_checkpoints_give_the_same_bits():
+    from rakali_b200.adjoint import GaugeMisfitBatch
+    nm, nx, ny, steps = 2, 30, 24, 17
+    b, h, gauges, ob = _batch_inputs(nm, nx, ny, steps, 4, seed=37)
+    n = np.full((nm, nx, ny), 0.025)
+    with GaugeMisfitBatch(nm, nx, ny, 10.0, 10.0, h, gauges, steps, precision=32) as pb:
+        pb.record_dt(b, n)
+        _, obs = pb.forward(ob, n)
+        pb.set_observations(obs)
+        J1, gb1, gn1 = pb.gradient(b, n)
+        assert pb.checkpoint_interval == 1
+        pb.set_state_budget(0)
+        J0, gb0, gn0 = pb.gradient(b, n)
+        assert pb.checkpoint_interval == 5
+    assert np.array_equal(J0, J1) and np.array_equal(gb0, gb1) and np.array_equal(gn0, gn1)
 
 
 def test_batch_fp32_against_fp64():
