@@ -473,7 +473,8 @@ def run_ensemble(args, world, local_rank, dist):
 
 def run_adjoint(args):
     """Gauge-misfit gradient w.r.t. bed and Manning n at 1024^2 over 500 steps:
-    device time of the forward and of forward + adjoint (sqrt(N) checkpoints),
+    device time of the forward and of forward + adjoint (sqrt(N) checkpoints
+    and recomputation, and beside it every state kept in device memory),
     the production FP64 forward of the same grid, and central differences on
     random directions."""
     from rakali_b200 import Rakali
@@ -491,6 +492,14 @@ def run_adjoint(args):
     fwd_ms = p.last_ms
     J, gb, gn = p.gradient(b, nf)
     grad_ms = p.last_ms
+    interval = p.checkpoint_interval
+    # every state kept in device memory (12.7 GB here): no segment recompute
+    p.set_state_budget(None)
+    Jk, gbk, gnk = p.gradient(b, nf)
+    kept_ms = p.last_ms
+    kept = p.checkpoint_interval == 1
+    same_bits = bool(Jk == J and np.array_equal(gbk, gb) and np.array_equal(gnk, gn))
+    p.set_state_budget(0)  # frees them
     # the production FP64 step on the same grid and dt sequence
     sim = Rakali(defer_init=True, nx=n, ny=n, dx=w["dx"], dy=w["dx"], nghost=2, t_end=1e9,
                  cfl=0.45, manning_n=0.025)
@@ -531,11 +540,17 @@ def run_adjoint(args):
     out = {"workload": f"{n}x{n}, dx = {w['dx']} m, 16-Gaussian bed, 0.5 m hump on a smooth "
                        f"surface undulation, Manning n field 0.025, walls, FP64, {steps} steps, "
                        f"{len(w['gauges'])} gauges; observations from the bed + 0.2 m smooth noise",
-           "J": J, "checkpoint_interval": p.checkpoint_interval,
+           "J": J, "checkpoint_interval": interval,
            "forward_ms": fwd_ms, "forward_plus_adjoint_ms": grad_ms,
            "cost_multiple_of_forward": grad_ms / fwd_ms,
            "production_forward_ms": prod_ms,
            "cost_multiple_of_production_forward": grad_ms / prod_ms,
+           "kept_states": {"note": "every state U^0..U^N kept in device memory instead of "
+                                   "sqrt(N) checkpoints + segment recompute "
+                                   "(rkb_adjoint_set_state_budget)",
+                           "used": kept, "forward_plus_adjoint_ms": kept_ms,
+                           "cost_multiple_of_production_forward": kept_ms / prod_ms,
+                           "same_bits_as_checkpointed": same_bits},
            "fd_check": {"steps": args.adjoint_fd_steps, "directions": len(errs), "eps": 1e-6,
                         "max_rel_err": max(errs) if errs else None,
                         "median_rel_err": float(np.median(errs)) if errs else None},

@@ -214,8 +214,8 @@ int rkb_batch_variant(void *batch, int *a, int *b);
 /* Gauge-misfit adjoint of the FP64 step (walls, HLL or HLLC, Manning
  * friction with a per-cell n field).  J = sum over steps 1..n_steps and the
  * gauges of (h + b - obs)^2 on a fixed dt sequence; gradients by
- * hand-written reverse kernels, every state kept in device memory when the
- * state budget allows, else sqrt(n_steps) checkpointing.  Interior
+ * hand-written reverse kernels with sqrt(n_steps) checkpointing (or every
+ * state kept in device memory, rkb_adjoint_set_state_budget).  Interior
  * arrays are (nx, ny) Fortran order on the host; gauges are interior
  * (i, j), 0-based, distinct; obs is (n_steps, n_gauges) row-major. */
 int rkb_adjoint_create(int nx, int ny, int nghost, double dx, double dy, double cfl, int use_hllc,
@@ -236,9 +236,9 @@ int rkb_adjoint_gradient(void *adj, const double *b, const double *n_field, doub
 /* 1 once a gradient run kept every state, else the sqrt(n_steps) interval. */
 int rkb_adjoint_checkpoint_interval(void *adj);
 /* Device bytes a gradient run may allocate to keep every state U^0..U^N
- * (3 (N + 1) fields): < 0 (the default) half the free device memory at that
- * run, 0 never (sqrt(N) checkpoints and recomputation).  The gradients are
- * the same bits either way.  No counterpart in the reference. */
+ * (3 (N + 1) fields) instead of recomputing them from sqrt(N) checkpoints:
+ * 0 (the default) never, < 0 half the free device memory at that run.  The
+ * gradients are the same bits either way.  No counterpart in the reference. */
 int rkb_adjoint_set_state_budget(void *adj, long long bytes);
 /* Device milliseconds of the last forward / gradient call (CUDA events). */
 double rkb_adjoint_last_ms(void *adj);

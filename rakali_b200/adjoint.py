@@ -127,9 +127,10 @@ class GaugeMisfit:
         return int(self._lib.rkb_adjoint_checkpoint_interval(self._a))
 
     def set_state_budget(self, nbytes):
-        """Device bytes a gradient run may allocate to keep every state: None
-        (the default) half the free device memory, 0 never (sqrt(n_steps)
-        checkpoints and recomputation).  The gradients are the same bits."""
+        """Device bytes a gradient run may allocate to keep every state instead
+        of recomputing them from sqrt(n_steps) checkpoints: 0 (the default)
+        never, None half the free device memory.  The gradients are the same
+        bits either way."""
         self._rc(self._lib.rkb_adjoint_set_state_budget(self._a, -1 if nbytes is None else int(nbytes)),
                  "set_state_budget")
 
@@ -285,9 +286,10 @@ class GaugeMisfitBatch:
         return int(self._lib.rkb_adjoint_checkpoint_interval(self._a))
 
     def set_state_budget(self, nbytes):
-        """Device bytes a gradient run may allocate to keep every state: None
-        (the default) half the free device memory, 0 never (sqrt(n_steps)
-        checkpoints and recomputation).  The gradients are the same bits."""
+        """Device bytes a gradient run may allocate to keep every state instead
+        of recomputing them from sqrt(n_steps) checkpoints: 0 (the default)
+        never, None half the free device memory.  The gradients are the same
+        bits either way."""
         self._rc(self._lib.rkb_adjoint_set_state_budget(self._a, -1 if nbytes is None else int(nbytes)),
                  "set_state_budget")
 

@@ -12,12 +12,12 @@
 //   reverse, per stage:  cells -> faces -> reconstruction -> slope gather -> walls
 //
 // Every reverse kernel gathers (each output element is written by one thread),
-// so there are no atomics and the gradient is deterministic.  A gradient run
-// keeps every state U^0..U^N in device memory when they fit in the state
-// budget (by default half the free memory at the first run: 12.7 GB for
-// 1024^2 FP64 over 500 steps), so the reverse sweep reads U^k directly;
-// otherwise states are checkpointed every K ~ sqrt(N) steps and recomputed
-// segment by segment.  Both give the same bits.
+// so there are no atomics and the gradient is deterministic.  States are
+// checkpointed every K ~ sqrt(N) steps and recomputed segment by segment;
+// given a state budget (set_state_budget), a gradient run instead keeps every
+// state U^0..U^N in device memory when they fit (12.7 GB for 1024^2 FP64 over
+// 500 steps) and the reverse sweep reads U^k directly.  Both give the same
+// bits.
 // Each launch covers every member (blockIdx.z = member; member m's arrays start
 // m * ms elements after member 0's).
 //
@@ -55,7 +55,8 @@ class AdjointBase {
   virtual int checkpoint_interval() const = 0;
   // Bytes the gradient may allocate to keep every state: < 0 half the free
   // device memory at the next gradient run, 0 never (sqrt(N) checkpoints
-  // and recomputation only).  Frees a kept-state allocation above it.
+  // and recomputation only, the default).  Frees a kept-state allocation
+  // above it.
   virtual void set_state_budget(long long bytes) = 0;
   virtual double last_ms() = 0;
   virtual int members() const = 0;
@@ -1225,7 +1226,7 @@ class Adjoint final : public AdjointBase {
   // every state of a gradient run (keep_all_states)
   void* all_mem_ = nullptr;
   std::vector<Fields<T>> all_;
-  long long budget_ = -1;
+  long long budget_ = 0;
   bool kept_all_ = false;
   size_t nfields_ = 0;
   cudaStream_t stream_ = nullptr;

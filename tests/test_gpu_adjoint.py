@@ -104,8 +104,7 @@ def test_gradient_matches_torch_autograd(hllc):
 def test_gradient_matches_central_differences():
     nx, ny, steps = 40, 32, 29  # 29 steps: checkpoint segments of 6, the last one short
     p, b, h, n, _, _ = _problem(nx, ny, steps, 10, seed=7, generic=True)
-    p.set_state_budget(0)  # the checkpointed path: segments recomputed
-    assert p.checkpoint_interval == 6
+    assert p.checkpoint_interval == 6  # the default: segments recomputed
     J, gb, gn = p.gradient(b, n)
     assert p.checkpoint_interval == 6
     rng = np.random.default_rng(11)
@@ -123,11 +122,12 @@ def test_gradient_matches_central_differences():
 
 
 def test_kept_states_and_checkpoints_give_the_same_bits():
-    """A gradient run that keeps every state (the default when they fit) and
-    one that checkpoints every ~sqrt(N) steps and recomputes the segments
-    return identical J and gradients."""
+    """A gradient run that keeps every state (given a state budget) and one
+    that checkpoints every ~sqrt(N) steps and recomputes the segments (the
+    default) return identical J and gradients."""
     nx, ny, steps = 40, 32, 29
     p, b, h, n, _, _ = _problem(nx, ny, steps, 10, seed=7, generic=True)
+    p.set_state_budget(None)
     J1, gb1, gn1 = p.gradient(b, n)
     assert p.checkpoint_interval == 1  # every state kept
     p.set_state_budget(0)
@@ -215,6 +215,7 @@ def test_batch_fp64_equals_single_problems():
     n = np.full((nm, nx, ny), 0.025)
     with GaugeMisfitBatch(nm, nx, ny, 10.0, 10.0, h, gauges, steps, precision=64) as pb:
         assert pb.precision == 64
+        pb.set_state_budget(None)  # every state kept: the singles checkpoint
         pb.record_dt(b, n)
         _, obs = pb.forward(ob, n)
         pb.set_observations(obs)
@@ -223,7 +224,6 @@ def test_batch_fp64_equals_single_problems():
         assert pb.checkpoint_interval == 1  # every state kept
     for m in range(nm):
         with GaugeMisfit(nx, ny, 10.0, 10.0, h[m], gauges[m], steps) as p:
-            p.set_state_budget(0)  # checkpoints: the other storage mode
             p.record_dt(b[m], n[m])
             assert np.array_equal(p.dt, dts[m])
             p.set_observations(obs[:, m, :])
@@ -238,6 +238,7 @@ def test_batch_fp32_kept_states_and_checkpoints_give_the_same_bits():
     b, h, gauges, ob = _batch_inputs(nm, nx, ny, steps, 4, seed=37)
     n = np.full((nm, nx, ny), 0.025)
     with GaugeMisfitBatch(nm, nx, ny, 10.0, 10.0, h, gauges, steps, precision=32) as pb:
+        pb.set_state_budget(None)
         pb.record_dt(b, n)
         _, obs = pb.forward(ob, n)
         pb.set_observations(obs)
