@@ -20,15 +20,19 @@ namespace rkb {
 RKB_HD double pow_third(double h) { return cr_pow_third(h); }
 RKB_HD float pow_third(float h) { return cbrtf(h); }
 
-// Derivative of velocity(): u = q/h when h > DRY_THRESHOLD, else 0.
+// Derivative of velocity(): u = q/h when h > DRY_THRESHOLD, else 0.  The
+// five quotients by h share one reciprocal: they only scale adjoints (no
+// branch depends on them), so a last-bit difference from the divisions is
+// immaterial, and the reverse sweep is dominated by division sequences.
 template <typename T>
 RKB_HD void velocity_adj(T h, T qx, T qy, T gu, T gv, T& gh,
                          T& gqx, T& gqy) {
   if (h > T(kDry)) {
-    const T u = qx / h, v = qy / h;
-    gqx += gu / h;
-    gqy += gv / h;
-    gh += -(gu * u + gv * v) / h;
+    const T rh = T(1) / h;
+    const T u = qx * rh, v = qy * rh;
+    gqx += gu * rh;
+    gqy += gv * rh;
+    gh += -(gu * u + gv * v) * rh;
   }
 }
 
@@ -276,28 +280,34 @@ RKB_HD void friction(T h, T& u, T& v, T n, T dt) {
 
 // Adjoint of friction at input (h, u, v, n): (gu, gv) output adjoints in,
 // input adjoints out; gh, gn accumulated.
+// The quotients share one reciprocal per denominator (h, h^(1/3), den, sp):
+// they only scale adjoints, and no branch depends on them.
 template <typename T>
 RKB_HD void friction_adj(T h, T u, T v, T n, T dt, T& gh,
                          T& gu, T& gv, T& gn) {
   if (!(h > T(kDry) && n > T(0))) return;
-  const T uu = u / h, vv = v / h;
+  const T rh = T(1) / h;
+  const T uu = u * rh, vv = v * rh;
   const T sp = sqrt(uu * uu + vv * vv);
   const T c3 = pow_third(h);
-  const T cf = T(kG) * n * n / c3;
-  const T den = T(1) + dt * cf * sp / h;
-  const T gden = -(gu * u + gv * v) / (den * den);
-  T gu0 = gu / den, gv0 = gv / den;
-  const T gcf = gden * dt * sp / h;
-  const T gsp = gden * dt * cf / h;
-  gh += gden * (-dt * cf * sp / (h * h));
-  gn += gcf * T(2) * T(kG) * n / c3;
-  const T gc3 = -gcf * cf / c3;
-  gh += gc3 * c3 / (T(3) * h);
+  const T rc3 = T(1) / c3;
+  const T cf = T(kG) * n * n * rc3;
+  const T den = T(1) + dt * cf * sp * rh;
+  const T rden = T(1) / den;
+  const T gden = -(gu * u + gv * v) * rden * rden;
+  T gu0 = gu * rden, gv0 = gv * rden;
+  const T gcf = gden * dt * sp * rh;
+  const T gsp = gden * dt * cf * rh;
+  gh += gden * (-dt * cf * sp * rh * rh);
+  gn += gcf * T(2) * T(kG) * n * rc3;
+  const T gc3 = -gcf * cf * rc3;
+  gh += gc3 * c3 * rh * T(1.0 / 3.0);
   if (sp > T(0)) {
-    const T guu = gsp * uu / sp, gvv = gsp * vv / sp;
-    gu0 += guu / h;
-    gv0 += gvv / h;
-    gh += -(guu * uu + gvv * vv) / h;
+    const T rsp = T(1) / sp;
+    const T guu = gsp * uu * rsp, gvv = gsp * vv * rsp;
+    gu0 += guu * rh;
+    gv0 += gvv * rh;
+    gh += -(guu * uu + gvv * vv) * rh;
   }
   gu = gu0;
   gv = gv0;
