@@ -497,23 +497,25 @@ __global__ void __launch_bounds__(kBX * kBY, 3)
   auto go = [&](int k, int ii, int jj) {  // zero outside the interior
     return (ii >= g.ng && ii < ie && jj >= g.ng && jj < je) ? R.go[k][g.at(ii, jj) + zb] : T(0);
   };
+  // the divergence's divisions by dx and dy, as products with the
+  // reciprocals: they only scale adjoints
   if (j < je) {
-    const T dx = T(g.dx);
+    const T rdx = T(1) / T(g.dx);
     const T lh = go(0, i - 1, j), lu = go(1, i - 1, j), lv = go(2, i - 1, j);
     const T rh = go(0, i, j), ru = go(1, i, j), rv = go(2, i, j);
-    const T gout[6] = {(-lh + rh) / dx, (-lu + ru) / dx, (-lv + rv) / dx,
-                       -T(kHalfG) * ru / dx, T(kHalfG) * lu / dx, -T(kHalfG) * lu / dx};
+    const T gout[6] = {(-lh + rh) * rdx, (-lu + ru) * rdx, (-lv + rv) * rdx,
+                       -T(kHalfG) * ru * rdx, T(kHalfG) * lu * rdx, -T(kHalfG) * lu * rdx};
     const FaceIn<T> f = face_in(V, b, Tp, c - 1, c, 0);
     T gin[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     face_adj<0, HLLC>(f.eL, f.qxL, f.qyL, f.bL, f.eR, f.qxR, f.qyR, f.bR, gout, gin);
     for (int k = 0; k < 8; ++k) R.gfx[k][c] = gin[k];
   }
   if (i < ie) {
-    const T dy = T(g.dy);
+    const T rdy = T(1) / T(g.dy);
     const T bh = go(0, i, j - 1), bu = go(1, i, j - 1), bv = go(2, i, j - 1);
     const T th = go(0, i, j), tu = go(1, i, j), tv = go(2, i, j);
-    const T gout[6] = {(-bh + th) / dy, (-bu + tu) / dy, (-bv + tv) / dy,
-                       -T(kHalfG) * tv / dy, T(kHalfG) * bv / dy, -T(kHalfG) * bv / dy};
+    const T gout[6] = {(-bh + th) * rdy, (-bu + tu) * rdy, (-bv + tv) * rdy,
+                       -T(kHalfG) * tv * rdy, T(kHalfG) * bv * rdy, -T(kHalfG) * bv * rdy};
     const FaceIn<T> f = face_in(V, b, Tp, c - g.pitch, c, 1);
     T gin[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     face_adj<1, HLLC>(f.eL, f.qxL, f.qyL, f.bL, f.eR, f.qxR, f.qyR, f.bR, gout, gin);
