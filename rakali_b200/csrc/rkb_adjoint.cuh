@@ -280,8 +280,10 @@ RKB_HD void friction(T h, T& u, T& v, T n, T dt) {
 
 // Adjoint of friction at input (h, u, v, n): (gu, gv) output adjoints in,
 // input adjoints out; gh, gn accumulated.
-// The quotients share one reciprocal per denominator (h, h^(1/3), den, sp):
-// they only scale adjoints, and no branch depends on them.
+// The quotients share one reciprocal per denominator (h, h^(1/3), den, sp),
+// and h^(1/3) is the math library's cube root rather than the correctly
+// rounded one of the forward step: here they only scale adjoints, and no
+// branch depends on them.
 template <typename T>
 RKB_HD void friction_adj(T h, T u, T v, T n, T dt, T& gh,
                          T& gu, T& gv, T& gn) {
@@ -289,7 +291,7 @@ RKB_HD void friction_adj(T h, T u, T v, T n, T dt, T& gh,
   const T rh = T(1) / h;
   const T uu = u * rh, vv = v * rh;
   const T sp = sqrt(uu * uu + vv * vv);
-  const T c3 = pow_third(h);
+  const T c3 = cbrt(h);
   const T rc3 = T(1) / c3;
   const T cf = T(kG) * n * n * rc3;
   const T den = T(1) + dt * cf * sp * rh;

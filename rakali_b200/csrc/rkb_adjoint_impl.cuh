@@ -494,9 +494,10 @@ __global__ void __launch_bounds__(kBX * kBY, 3)
   if (i > ie || j > je) return;
   const size_t zb = member_base(ms);
   const size_t c = g.at(i, j) + zb;
-  auto go = [&](int k, int ii, int jj) {  // zero outside the interior
-    return (ii >= g.ng && ii < ie && jj >= g.ng && jj < je) ? R.go[k][g.at(ii, jj) + zb] : T(0);
-  };
+  // R.go is written at interior cells only (k_cells_adj) and was zeroed at
+  // creation, so the ghost ring around the interior reads as zero: the
+  // neighbours (i-1, j), (i, j), (i, j-1) need no bounds test
+  auto go = [&](int k, int ii, int jj) { return R.go[k][g.at(ii, jj) + zb]; };
   // the divergence's divisions by dx and dy, as products with the
   // reciprocals: they only scale adjoints
   if (j < je) {
