@@ -287,6 +287,45 @@ def test_generic_schemes_refuse_fp32_and_batches():
         sim.step(3)  # still usable
 
 
+@pytest.mark.parametrize("nghost", [2, 3, 4, 5])
+@pytest.mark.parametrize("physics", ["plain", "forcing_coriolis_sponge"])
+def test_tma_tiles_against_the_oracle(nghost, physics):
+    """The TMA-staged tile kernel (the default) on every ghost parity: its boxes
+    start one column left of the tile when nghost is odd.  77 x 50 leaves
+    ragged tiles on both axes; the full-physics case runs the kernel built
+    with forcing, Coriolis and sponge terms."""
+    nx, ny, dx = 77, 50, 20.0
+    cfg = dict(nx=nx, ny=ny, dx=dx, dy=dx, nghost=nghost, t_end=1e6, cfl=0.45, manning_n=0.03,
+               use_hllc=True)
+    if physics != "plain":
+        cfg.update(coriolis_f=1.0e-4, bc_west="sponge", sponge_width=5, sponge_strength=0.01,
+                   sponge_h_ref=8.0)
+    b = gaussian_bed(nx, ny, dx, dx, 8, seed=40 + nghost, base=-6.0, amp=(-2.0, 8.0),
+                     width=(60.0, 300.0))
+    h = hump_depth(b, dx, dx, width=150.0)
+    sim, orc = pair(cfg, bathymetry=b, initial_h=h)
+    with sim:
+        assert sim._lib.rkb_tma_tile_status(sim._handle) == 0
+        assert sim._lib.rkb_get_tile(sim._handle) == 10
+        if physics != "plain":
+            rng = np.random.default_rng(nghost)
+            wx = rng.uniform(0.0, 0.3, (nx, ny))
+            wy = rng.uniform(-0.1, 0.1, (nx, ny))
+            pr = rng.uniform(-50.0, 50.0, (nx, ny))
+            rain = np.full((nx, ny), 1.0e-5)
+            sim.set_wind(wx, wy)
+            sim.set_atm_pressure(pr)
+            sim.set_precipitation(rain)
+            g = orc.ng
+            for name, arr in (("wind_x", wx), ("wind_y", wy), ("atm", pr), ("precip", rain)):
+                orc.arrays[name][g:-g, g:-g] = arr
+            orc.s.forcing_active = 1
+        sim.step(40)
+        orc.step(40)
+        assert sim.dt == orc.dt
+        compare_state(sim, orc, rtol=0.0)
+
+
 def test_tiles_agree():
     nx, ny, dx = 150, 70, 5.0
     b = gaussian_bed(nx, ny, dx, dx, 10, seed=9, width=(20.0, 80.0))
