@@ -210,6 +210,11 @@ int rkb_batch_profile_steps(void *batch, int n, double *out5);
 int rkb_batch_autotune(void *batch, int trial_steps, double *best_ms_per_step);
 /* Kernel shape in use: FP64 (tile, 0); FP32 (columns per lane, rows). */
 int rkb_batch_variant(void *batch, int *a, int *b);
+/* Sets the kernel shape without trials: FP64 (a shared-memory tile: 0-3,
+ * 6-10; tile 10, TMA-staged, needs every member's tensor maps and otherwise
+ * runs the 16x15 kernel), 0); FP32 (2 or 4 columns per lane, rows per warp
+ * sweep >= 0, 0 = one wave of resident warps).  -2 for any other shape. */
+int rkb_batch_set_variant(void *batch, int a, int b);
 
 /* Gauge-misfit adjoint of the FP64 step (walls, HLL or HLLC, Manning
  * friction with a per-cell n field).  J = sum over steps 1..n_steps and the

@@ -133,6 +133,7 @@ def load(path: str | None = None):
     _sig(lib, "rkb_batch_time_steps", [H, I, DP], I)
     _sig(lib, "rkb_batch_autotune", [H, I, DP], I)
     _sig(lib, "rkb_batch_profile_steps", [H, I, DP], I)
+    _sig(lib, "rkb_batch_set_variant", [H, I, I], I)
     _sig(lib, "rkb_batch_variant", [H, IP, IP], I)
     _sig(lib, "rkb_adjoint_create", [I, I, I, D, D, D, I, I, DP, DP, DP, IP, IP, I, HP], I)
     _sig(lib, "rkb_adjoint_destroy", [HP], None)

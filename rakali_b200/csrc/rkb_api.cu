@@ -666,6 +666,13 @@ int rkb_batch_variant(void* batch, int* a, int* b_) {
   return 0;
 }
 
+int rkb_batch_set_variant(void* batch, int a, int b_) {
+  rkb::Batch* b = batch_of(batch);
+  if (!b) return kBadHandle;
+  const int rc = b->set_variant(a, b_);
+  return rc == 0 ? 0 : fail(rc, b->error().empty() ? "batch variant refused" : b->error());
+}
+
 int rkb_set_precision(void* handle, int bits) {
   rkb::Sim* s = sim_of(handle);
   if (!s) return kBadHandle;

@@ -24,6 +24,7 @@ Batch::~Batch() {
   clear_graphs();
   if (dargs_) cudaFree(dargs_);
   if (dmap_) cudaFree(dmap_);
+  if (dmaps_) cudaFree(dmaps_);
   if (stream_) cudaStreamDestroy(stream_);
   for (Sim* s : sims_)
     if (s && s->batch == this) s->batch = nullptr;
@@ -41,6 +42,29 @@ void Batch::detach(Sim* s) {
   for (Sim*& m : sims_)
     if (m == s) m = nullptr;
   broken_ = true;
+}
+
+int Batch::set_variant(int a, int b) {
+  if (prec_ == 64) {
+    const bool ok = b == 0 && (a == kTile32x8 || a == kTile32x16 || a == kTile64x4 ||
+                               a == kTile16x16 || a == kTile32x8w || a == kTile32x12w ||
+                               a == kTile16x15 || a == kTile32x7w || a == kTile16x15t);
+    if (!ok) {
+      err_ = "FP64 batches take a shared-memory tile (0-3, 6-10) and b = 0";
+      return -2;
+    }
+    if (configure_batch(a, hllc_) != cudaSuccess) return -1;
+    tile_ = a;
+  } else {
+    if ((a != 2 && a != 4) || b < 0) {
+      err_ = "FP32 batches take 2 or 4 columns per lane and rows >= 0";
+      return -2;
+    }
+    cpl_ = a;
+    rows_ = b;
+  }
+  clear_graphs();
+  return 0;
 }
 
 void Batch::variant(int* a, int* b) const {
@@ -140,6 +164,17 @@ int Batch::build() {
                           args_bytes, cudaMemcpyHostToDevice, stream_));
   RKB_TRY(cudaMemcpyAsync(dmap_, map.data(), map.size() * sizeof(int2), cudaMemcpyHostToDevice,
                           stream_));
+  // the TMA-staged tiles need every member's maps (encoded when it was
+  // finalised); the maps follow the members' buffers, which never move
+  bool maps_ok = prec_ == 64;
+  for (Sim* s : sims_) maps_ok = maps_ok && s->tma_status() == 0;
+  if (maps_ok && !dmaps_) {
+    RKB_TRY(cudaMalloc((void**)&dmaps_, (size_t)n * sizeof(TileMaps)));
+    std::vector<TileMaps> hm(n);
+    for (int i = 0; i < n; ++i) hm[i] = sims_[i]->tile_maps();
+    RKB_TRY(cudaMemcpyAsync(dmaps_, hm.data(), (size_t)n * sizeof(TileMaps),
+                            cudaMemcpyHostToDevice, stream_));
+  }
   RKB_TRY(cudaStreamSynchronize(stream_));
   const int nblocks = (int)map.size();
   const bool same = prec_ == 64
@@ -153,7 +188,7 @@ int Batch::build() {
   if (realloc_ || !same || gsig != gauge_sig_) clear_graphs();
   gauge_sig_ = gsig;
   bl_ = BatchLaunch{(const StepArgs*)dargs_, dmap_, n, nblocks, max_nxt, max_nyt, tile_, hllc_,
-                    plain};
+                    plain, maps_ok ? dmaps_ : nullptr};
   bl32_ = BatchLaunch32{(const StepArgs32*)dargs_, dmap_, n, nblocks, max_nxt, max_nyt,
                         cpl_, hllc_, plain};
   return 0;
@@ -318,7 +353,7 @@ int Batch::autotune(int trial_steps, double* best_ms) {
   std::vector<std::pair<int, int>> cands;
   if (prec_ == 64) {
     for (int t : {kTile32x16, kTile32x8, kTile64x4, kTile16x16, kTile32x8w, kTile32x12w,
-                  kTile16x15, kTile32x7w})
+                  kTile16x15, kTile32x7w, kTile16x15t})
       cands.push_back({t, 0});
   } else {
     for (int c : {2, 4})

@@ -37,6 +37,9 @@ class Batch {
   // Current kernel shape: FP64 tile, or FP32 columns per lane and rows
   // (0 rows = automatic per member).
   void variant(int* a, int* b) const;
+  // Sets the kernel shape (FP64: a = a shared-memory tile, b = 0; FP32: a =
+  // 2 or 4 columns per lane, b >= 0 rows per warp sweep); -2 for others.
+  int set_variant(int a, int b);
   void detach(Sim* s);  // a member is being destroyed
   const std::string& error() const { return err_; }
 
@@ -59,6 +62,7 @@ class Batch {
   cudaStream_t stream_ = nullptr;
   void* dargs_ = nullptr;
   int2* dmap_ = nullptr;
+  TileMaps* dmaps_ = nullptr;  // the members' TMA maps (FP64; null unless all are encoded)
   size_t map_cap_ = 0;
   BatchLaunch bl_{};
   BatchLaunch32 bl32_{};

@@ -169,6 +169,7 @@ struct BatchLaunch {
   int max_nxt, max_nyt;
   int tile, hllc;
   int plain;  // every member plain (StepArgs::plain)
+  const TileMaps* maps;  // device array: every member's TMA maps (null: not all encoded)
 };
 int batch_stage_blocks(const Grid& g, int tile);
 cudaError_t configure_batch(int tile, int hllc);

@@ -104,6 +104,7 @@ class Sim {
   // Device pointers for the torch / kernel-level paths.
   StepArgs device_args() const { return args_; }
   int tma_status() const { return tma_status_; }
+  const TileMaps& tile_maps() const { return maps_; }
   int current_buffer() const { return cur_; }
   cudaStream_t stream() const { return stream_; }
   int ensure_device();

@@ -681,6 +681,46 @@ __global__ void __launch_bounds__(stage_threads(TX, TY, 0),
                                                   FluxOut{}, bx, by, gx, gridDim.x / gx);
 }
 
+// The TMA-staged stage for every simulation of a batch (blocks as in
+// k_stage_batch): member m's tiles come through its own maps, maps[m], in
+// global memory.
+template <int TX, int TY, bool HLLC, int STAGE, bool PLAIN = false>
+__global__ void __launch_bounds__(stage_threads(TX, TY, 0),
+                                  stage_blocks_per_sm(stage_threads(TX, TY, 0),
+                                                      (int)StageSmem<TX, TY, true>::BYTES, PLAIN))
+    k_stage_batch_tma(const StepArgs* __restrict__ args, const int2* __restrict__ map,
+                      const TileMaps* __restrict__ maps) {
+  __shared__ StepArgs sa;
+  const int2 m = map[blockIdx.x];
+  if (threadIdx.x == 0) sa = args[m.x];
+  __syncthreads();
+  if (PLAIN && plain_mismatch64(sa.ctl, sa.phys, sa.bc)) return;
+  if (!sa.ctl->active) return;
+  const int cur = sa.ctl->cur;
+  const unsigned gx = (unsigned)((sa.g.nx_phys() + TX - 1) / TX);
+  const unsigned gy = (unsigned)((sa.g.ny_phys() + TY - 1) / TY);
+  const unsigned bx = (unsigned)m.y % gx, by = (unsigned)m.y / gx;
+  extern __shared__ double smem[];
+  __shared__ __align__(8) unsigned long long bar_word;
+  const uint32_t bar = smem_u32(&bar_word);
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+    issue_tile<TX, TY, STAGE>(maps[m.x], STAGE == 2 ? 2 : cur, cur, sa.g, bx, by, bar,
+                              stage_ptrs<TX, TY, true>(smem));
+  }
+  __syncthreads();
+  const bool ok = mbar_wait(bar, 0, sa.wait_cycles > 0 ? sa.wait_cycles : kWaitCyclesDefault);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) atomicExch(&sa.ctl->error, kErrWait);
+    mbar_wait(bar, 0, kWaitCyclesDefault);  // the copies still in flight
+    return;
+  }
+  const FluxOut none{};
+  stage_body<TX, TY, HLLC, STAGE, 0, PLAIN, true>(sa.g, sa.ctl, sa.phys, sa.bc, sa.U0, sa.U1, sa.S,
+                                                  sa.b, sa.fo, sa.partials, none, bx, by, gx, gy);
+}
+
 // ---------------------------------------------------------------------------
 // Marching stage kernel: one warp per 28-column strip, stepping up the rows.
 // ---------------------------------------------------------------------------
@@ -1262,6 +1302,19 @@ static cudaError_t configure_batch_t() {
   return e;
 }
 
+template <int TX, int TY, bool HLLC>
+static cudaError_t configure_batch_tma_t() {
+  const int bytes = (int)StageSmem<TX, TY, true>::BYTES;
+  const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  cudaError_t e = cudaFuncSetAttribute(k_stage_batch_tma<TX, TY, HLLC, 1>, attr, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage_batch_tma<TX, TY, HLLC, 2>, attr, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_stage_batch_tma<TX, TY, HLLC, 1, true>, attr, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_stage_batch_tma<TX, TY, HLLC, 2, true>, attr, bytes);
+  return e;
+}
+
 cudaError_t configure_batch(int tile, int hllc) {
   const bool h = hllc != 0;
   switch (tile) {
@@ -1273,6 +1326,13 @@ cudaError_t configure_batch(int tile, int hllc) {
     case kTile32x12w: return h ? configure_batch_t<32, 12, true, 2>() : configure_batch_t<32, 12, false, 2>();
     case kTile16x15: return h ? configure_batch_t<16, 15, true>() : configure_batch_t<16, 15, false>();
     case kTile32x7w: return h ? configure_batch_t<32, 7, true, 1>() : configure_batch_t<32, 7, false, 1>();
+    case kTile16x15t: {
+      // the plain 16x15 kernel serves batches whose maps are not all encoded
+      const cudaError_t e =
+          h ? configure_batch_t<16, 15, true>() : configure_batch_t<16, 15, false>();
+      if (e != cudaSuccess) return e;
+      return h ? configure_batch_tma_t<16, 15, true>() : configure_batch_tma_t<16, 15, false>();
+    }
     default: return cudaErrorInvalidValue;  // batches use the shared-memory tiles
   }
 }
@@ -1283,6 +1343,15 @@ static cudaError_t launch_stage_batch_t(const BatchLaunch& bl, cudaStream_t s) {
                        : k_stage_batch<TX, TY, HLLC, STAGE, XW, false>;
   kern<<<(unsigned)bl.blocks, stage_threads(TX, TY, XW), StageSmem<TX, TY>::BYTES, s>>>(bl.args,
                                                                                       bl.map);
+  return cudaGetLastError();
+}
+
+template <int TX, int TY, bool HLLC, int STAGE>
+static cudaError_t launch_stage_batch_tma_t(const BatchLaunch& bl, cudaStream_t s) {
+  auto kern = bl.plain ? k_stage_batch_tma<TX, TY, HLLC, STAGE, true>
+                       : k_stage_batch_tma<TX, TY, HLLC, STAGE, false>;
+  kern<<<(unsigned)bl.blocks, stage_threads(TX, TY, 0), StageSmem<TX, TY, true>::BYTES, s>>>(
+      bl.args, bl.map, bl.maps);
   return cudaGetLastError();
 }
 
@@ -1306,6 +1375,10 @@ static cudaError_t launch_stage_batch(const BatchLaunch& bl, cudaStream_t s) {
       return h ? launch_stage_batch_t<16, 15, true, STAGE>(bl, s) : launch_stage_batch_t<16, 15, false, STAGE>(bl, s);
     case kTile32x7w:
       return h ? launch_stage_batch_t<32, 7, true, STAGE, 1>(bl, s) : launch_stage_batch_t<32, 7, false, STAGE, 1>(bl, s);
+    case kTile16x15t:
+      if (bl.maps)
+        return h ? launch_stage_batch_tma_t<16, 15, true, STAGE>(bl, s) : launch_stage_batch_tma_t<16, 15, false, STAGE>(bl, s);
+      return h ? launch_stage_batch_t<16, 15, true, STAGE>(bl, s) : launch_stage_batch_t<16, 15, false, STAGE>(bl, s);
     default:
       return cudaErrorInvalidValue;
   }

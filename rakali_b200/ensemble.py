@@ -73,6 +73,12 @@ class Ensemble:
                  "autotune")
         return ms.value
 
+    def set_variant(self, a: int, b: int = 0):
+        """Set the kernel shape without trials: FP64 (tile, 0), tiles 0-3 and
+        6-10 (10: TMA-staged 16x15); FP32 (2 or 4 columns per lane, rows)."""
+        self._check()
+        self._rc(self._lib.rkb_batch_set_variant(self._b, int(a), int(b)), "set_variant")
+
     @property
     def variant(self):
         """FP64: (tile, 0); FP32: (columns per lane, rows per warp sweep)."""

@@ -84,11 +84,16 @@ def test_fp32_batch_mixes_plain_and_forced_members():
         s.close()
 
 
-def test_fp64_batch_matches_oracle():
+@pytest.mark.parametrize("tile", [1, 10])
+def test_fp64_batch_matches_oracle(tile):
+    """Tile 1 (32x16) and tile 10 (16x15, TMA-loaded through each member's own
+    tensor maps)."""
     from oracle.oracle import OracleSim
     ms = _members(3, seed=11)
     sims = [wl.build_member(m) for m in ms]
     with Ensemble(sims) as ens:
+        ens.set_variant(tile, 0)
+        assert ens.variant == (tile, 0)
         ens.step(25)
         for m, s in zip(ms, sims):
             o = OracleSim.from_config(m["kw"], bathymetry=m["b"], initial_h=m["h"])
@@ -134,8 +139,27 @@ def test_autotune_leaves_state_unchanged(precision):
         for s, r in zip(sims, ref):
             _assert_same(_state(s), r)
         a, b = ens.variant
-        assert (a in (0, 1, 2, 3, 6, 7)) if precision == 64 else (a in (2, 4))
+        assert (a in (0, 1, 2, 3, 6, 7, 8, 9, 10)) if precision == 64 else (a in (2, 4))
     for s in ref_sims + sims:
+        s.close()
+
+
+def test_set_variant_checks_the_shape():
+    sims = [wl.build_member(m) for m in _members(2, seed=4)]
+    with Ensemble(sims) as ens:
+        for a, b in ((4, 0), (11, 0), (1, 3), (-1, 0)):
+            with pytest.raises(RuntimeError, match="variant"):
+                ens.set_variant(a, b)
+        ens.set_variant(8, 0)
+        ens.step(2)
+    sims32 = [wl.build_member(m, 32) for m in _members(2, seed=4)]
+    with Ensemble(sims32, precision=32) as ens:
+        with pytest.raises(RuntimeError, match="variant"):
+            ens.set_variant(3, 0)
+        ens.set_variant(4, 16)
+        assert ens.variant == (4, 16)
+        ens.step(2)
+    for s in sims + sims32:
         s.close()
 
 
