@@ -433,12 +433,14 @@ __global__ void k_mass(Grid g, size_t ms, const T* __restrict__ h, double* mass)
 // ---- reverse ------------------------------------------------------------------
 
 // Cells: output adjoint gout -> divergence adjoint go, direct input adjoint
-// ga (a = h + dt o), base adjoint (stage 2), n adjoint.
-template <typename T>
+// ga (a = h + dt o), base adjoint (stage 2), n adjoint.  STAGE is a template
+// argument so that stage 1, which needs no post-friction state (no RK2
+// average), does not recompute the forward friction.
+template <typename T, int STAGE>
 __global__ void __launch_bounds__(kBX * kBY, 4)
     k_cells_adj(Grid g, size_t ms, Fields<T> V, Fields<T> base,
                             const T* __restrict__ nf, Tape<T> Tp, const double* __restrict__ dts,
-                            int stage, Fields<T> gout, Rev<T> R, Fields<T> gbase,
+                            Fields<T> gout, Rev<T> R, Fields<T> gbase,
                             T* __restrict__ gn) {
   const int i = g.ng + blockIdx.x * kBX + threadIdx.x % kBX;
   const int j = g.ng + blockIdx.y * kBY + threadIdx.x / kBX;
@@ -454,7 +456,7 @@ __global__ void __launch_bounds__(kBX * kBY, 4)
   T a2 = a1, u2 = u1, v2 = v1;
   friction(a2, u2, v2, nf[c], dt);
   T ga = gout.h[c], gu = gout.hu[c], gv = gout.hv[c];
-  if (stage == 2) {
+  if (STAGE == 2) {
     const T ap = T(0.5) * (base.h[c] + a2), up = T(0.5) * (base.hu[c] + u2),
             vp = T(0.5) * (base.hv[c] + v2);
     protect_adj(ap, up, vp, ga, gu, gv);
@@ -920,7 +922,7 @@ class Adjoint final : public AdjointBase {
       if (ng > 0)  // misfit at U^{k+1}
         k_gauges_adj<T><<<(ng + 127) / 128, 128, 0, stream_>>>(gq_, r_ + (size_t)k * ng, ng,
                                                                lam_, gb_);
-      if (step_adj(all_[k], k) != 0) return -1;
+      if (step_adj(all_[k], k, true) != 0) return -1;  // every kept U^k went through step()
     }
     for (int s = nseg - 1; s >= 0; --s) {
       const int k0 = s * K_, k1 = std::min(nsteps_, k0 + K_);
@@ -932,7 +934,8 @@ class Adjoint final : public AdjointBase {
         if (ng > 0)
           k_gauges_adj<T><<<(ng + 127) / 128, 128, 0, stream_>>>(gq_, r_ + (size_t)k * ng, ng,
                                                                  lam_, gb_);
-        if (step_adj(seg_[k - k0], k) != 0) return -1;
+        // the segment's last state was not the input of a recomputed step
+        if (step_adj(seg_[k - k0], k, k < k1 - 1) != 0) return -1;
       }
     }
     // bed ghosts mirror interior cells: fold their adjoints in (S/N then W/E)
@@ -1188,8 +1191,12 @@ class Adjoint final : public AdjointBase {
       ADJ_TRY(cudaMemsetAsync(gV_.hu, 0, fb, stream_));
       ADJ_TRY(cudaMemsetAsync(gV_.hv, 0, fb, stream_));
     }
-    k_cells_adj<T><<<interior(), kBX * kBY, 0, stream_>>>(g_, ms_, V, base, nf_, Tp, dt_of(k),
-                                                           stage, gout, R_, gbase_, gn_);
+    if (stage == 2)
+      k_cells_adj<T, 2><<<interior(), kBX * kBY, 0, stream_>>>(g_, ms_, V, base, nf_, Tp,
+                                                              dt_of(k), gout, R_, gbase_, gn_);
+    else
+      k_cells_adj<T, 1><<<interior(), kBX * kBY, 0, stream_>>>(g_, ms_, V, base, nf_, Tp,
+                                                              dt_of(k), gout, R_, gbase_, gn_);
     if (hllc_)
       k_faces_adj<T, true><<<blocks(g_.ng, ie, g_.ng, je), kBX * kBY, 0, stream_>>>(g_, ms_, V, b_,
                                                                                     Tp, R_);
@@ -1205,9 +1212,11 @@ class Adjoint final : public AdjointBase {
   }
 
   // Reverse of step k from U (= U^k): lam_ (adjoint of U^{k+1}) -> lam_
-  // (adjoint of U^k).  Recomputes U* and both tapes.
-  int step_adj(Fields<T> U, int k) {
-    walls(U);
+  // (adjoint of U^k).  Recomputes U* and both tapes.  `walled`: U's wall
+  // ghosts were filled from its interior already (a forward step() took it as
+  // its input), so the fill, which would write the same values, is skipped.
+  int step_adj(Fields<T> U, int k, bool walled) {
+    if (!walled) walls(U);
     tape(U, t1_);
     k_cells<T><<<interior(), kBX * kBY, 0, stream_>>>(g_, ms_, U, U, nf_, t1_, dt_of(k), 1, Us_);
     walls(Us_);
