@@ -94,6 +94,7 @@ struct Tape {
   T* s[6];   // x-slopes (eta, hu, hv), y-slopes (eta, hu, hv)
   T* fx[6];  // x-face i-1/2 at (i, j): fh, fqx, fqy, wbR, hL2, pL2
   T* fy[6];  // y-face j-1/2 at (i, j)
+  T* od[3];  // flux divergence of the cell (stage 1, written by k_cells)
 };
 
 template <typename T>
@@ -233,6 +234,9 @@ __global__ void k_cells(Grid g, size_t ms, Fields<T> V, Fields<T> base, const T*
   const T dt = T(dts[blockIdx.z]);
   T ofh, ofhu, ofhv;
   divergence(g, Tp, c, ofh, ofhu, ofhv);
+  Tp.od[0][c] = ofh;  // for k_cells_adj<T, 1>
+  Tp.od[1][c] = ofhu;
+  Tp.od[2][c] = ofhv;
   T a = V.h[c], u = V.hu[c], v = V.hv[c];
   a = a + dt * ofh;
   u = u + dt * ofhu;
@@ -448,7 +452,13 @@ __global__ void __launch_bounds__(kBX * kBY, 4)
   const size_t c = g.at(i, j) + member_base(ms);
   const T dt = T(dts[blockIdx.z]);
   T ofh, ofhu, ofhv;
-  divergence(g, Tp, c, ofh, ofhu, ofhv);
+  if (STAGE == 1) {  // taped by k_cells, the same bits
+    ofh = Tp.od[0][c];
+    ofhu = Tp.od[1][c];
+    ofhv = Tp.od[2][c];
+  } else {
+    divergence(g, Tp, c, ofh, ofhu, ofhv);
+  }
   // forward with intermediates
   const T a0 = V.h[c] + dt * ofh, u0 = V.hu[c] + dt * ofhu, v0 = V.hv[c] + dt * ofhv;
   T a1 = a0, u1 = u0, v1 = v0;
@@ -775,9 +785,9 @@ class Adjoint final : public AdjointBase {
     if (cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking) != cudaSuccess) return -1;
     const size_t f = ms_ * (size_t)nm;  // elements of one batched field
     // fields: b, n; U, Us, lam, lam*, gbase, gV (3 each); gb, gn; tapes
-    // (2 x 18); reverse scratch (3+3+8+8+6+4) + branch bits; checkpoints;
+    // (2 x 21); reverse scratch (3+3+8+8+6+4) + branch bits; checkpoints;
     // segment states
-    nfields_ = 2 + 6 * 3 + 2 + 2 * 18 + (3 + 3 + 8 + 8 + 6 + 4) + 1 + 3 * (size_t)nck_ +
+    nfields_ = 2 + 6 * 3 + 2 + 2 * 21 + (3 + 3 + 8 + 8 + 6 + 4) + 1 + 3 * (size_t)nck_ +
                3 * (size_t)(K_ + 1);
     const size_t fbytes = (f * sizeof(T) + 255) / 256 * 256;
     const size_t nres = (size_t)nsteps * nm * ngauge;
@@ -806,6 +816,7 @@ class Adjoint final : public AdjointBase {
       for (auto& x : t->s) x = take();
       for (auto& x : t->fx) x = take();
       for (auto& x : t->fy) x = take();
+      for (auto& x : t->od) x = take();
     }
     for (auto& x : R_.go) x = take();
     for (auto& x : R_.ga) x = take();
