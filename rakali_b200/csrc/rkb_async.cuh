@@ -83,6 +83,17 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long lo
   return __all_sync(0xffffffffu, ok);
 }
 
+// Named CTA barrier `id` (1..15) of `count` threads (a multiple of 32), as a
+// producer (arrive: does not wait) or a consumer (sync: waits for `count`
+// arrivals including its own warp's); orders the producers' prior memory
+// accesses before the consumers' later ones.  Warp-uniform.
+__device__ __forceinline__ void named_arrive(int id, int count) {
+  asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+__device__ __forceinline__ void named_sync(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
 // TMA load of one box of a 2D tensor map (a CUtensorMap in parameter, constant
 // or global memory) at element coordinates (x, y) into shared memory,
 // completing on `bar`.  The box lands row after row, x fastest; elements

@@ -359,8 +359,12 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
                tu[q + d], tv[q - d], tv[q], tv[q + d], se, su, sv);
   };
 
-  // 2. faces, each evaluated once, with the slopes of its two cells
-  for (int k = tid; k < SM::NFX + SM::NFY; k += NTH) {
+  // 2. faces, each evaluated once, with the slopes of its two cells.  In the
+  // paired form (below) thread t takes x-face t in the first round and y-face
+  // t in the second; otherwise faces go round-robin over the threads.
+  constexpr bool kPaired = TMA && TX == 16 && TY == 15 && XW == 0;
+  static_assert(!kPaired || (NTH == 256 && SM::NFX == 255 && SM::NFY == 256), "paired layout");
+  auto face = [&](int k) {
     FaceOut o;
     if (k < SM::NFX) {
       const int c = k % (TX + 1), r = k / (TX + 1);  // face between c-1 and c
@@ -392,8 +396,27 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
       fya[4 * SM::NFY + kk] = o.hL2;
       fya[5 * SM::NFY + kk] = o.pL2;
     }
+  };
+  if (kPaired) {
+    if (tid < SM::NFX) face(tid);
+    face(SM::NFX + tid);
+    // The cells of warp w (rows 2w, 2w+1) read x-faces 34w .. 34w+33 and
+    // y-faces 32w .. 32w+47: faces of warps w and w+1 only, and warp 7 reads
+    // its own.  So instead of a block barrier, warp w+1 arrives on named
+    // barrier w+1 (64 threads) and warp w waits on it; warp 7 orders its own
+    // lanes.  Every warp reaches this point (the early exits above are
+    // block-uniform), so each barrier gets its 64 threads.
+    const int w = tid >> 5;
+    __syncwarp();
+    if (w > 0) named_arrive(w, 64);
+    if (w < NTH / 32 - 1)
+      named_sync(w + 1, 64);
+    else
+      __syncwarp();
+  } else {
+    for (int k = tid; k < SM::NFX + SM::NFY; k += NTH) face(k);
+    __syncthreads();
   }
-  __syncthreads();
 
   // 3. cell update: one cell per thread (the extra warps repeat cell 0 and
   // store nothing)
