@@ -36,6 +36,7 @@
 #include <vector>
 
 #include "rkb_adjoint.cuh"
+#include "rkb_async.cuh"
 #include "rkb_kernels.h"
 
 namespace rkb {
@@ -316,7 +317,9 @@ __global__ void __launch_bounds__(kFThreads, 5)
     cell_slope(th[q - d], th[q], th[q + d], eta(q - d), eta(q), eta(q + d), tu[q - d], tu[q],
                tu[q + d], tv[q - d], tv[q], tv[q + d], se, su, sv);
   };
-  for (int k = tid; k < SM::NFX + SM::NFY; k += NTH) {
+  // thread t takes x-face t, then y-face t
+  static_assert(NTH == 256 && SM::NFX == 255 && SM::NFY == 256, "face layout");
+  auto face = [&](int k) {
     FaceOutT<T> o;
     if (k < SM::NFX) {
       const int c = k % (TX + 1), r = k / (TX + 1);
@@ -352,8 +355,21 @@ __global__ void __launch_bounds__(kFThreads, 5)
       f[4 * SM::NFY] = o.hL2;
       f[5 * SM::NFY] = o.pL2;
     }
+  };
+  if (tid < SM::NFX) face(tid);
+  face(SM::NFX + tid);
+  // The cells of warp w read the faces of warps w and w+1 only (warp 7 its
+  // own): warp w+1 arrives on named barrier w+1 and warp w waits on it.
+  // Every warp gets here (no exit above).
+  {
+    const int w = tid >> 5;
+    __syncwarp();
+    if (w > 0) named_arrive(w, 64);
+    if (w < NTH / 32 - 1)
+      named_sync(w + 1, 64);
+    else
+      __syncwarp();
   }
-  __syncthreads();
 
   if (tid >= TX * TY) return;  // the 16 threads beyond the tile's cells only took faces
   const int cx = tid % TX, cy = tid / TX;
