@@ -104,9 +104,6 @@ struct Rev {
   T* ga[3];   // direct adjoint of the stage input at interior cells (a = h + dt o)
   T* gfx[8];  // x-face input adjoints (eL, qxL, qyL, bL, eR, qxR, qyR, bR)
   T* gfy[8];
-  T* gs[6];   // slope adjoints
-  int* ch;    // minmod branches, 2 bits per slope (6 slopes)
-  T* gd[4];   // reconstruction adjoints of eta, hu, hv, b at the cell
 };
 
 __device__ __forceinline__ bool in_box(int i, int j, int i0, int i1, int j0, int j1) {
@@ -549,19 +546,21 @@ __global__ void __launch_bounds__(kBX * kBY, 3)
   }
 }
 
-// Reconstruction: face input adjoints -> adjoints of the cell's eta, hu, hv,
-// b (direct) and of its six slopes, with the minmod branch of each slope.
+// Reconstruction adjoint of cell (i, j) (global index c): the face input
+// adjoints of its four faces -> the direct adjoints gd of its eta, hu, hv, b
+// and the adjoints gs of its six limited slopes, with the minmod branch of
+// each slope (2 bits per slope) in ch.  Cells of [ng-1, ie] x [ng-1, je].
 template <typename T>
-__global__ void k_recon_adj(Grid g, size_t ms, Fields<T> V, const T* __restrict__ b, Rev<T> R) {
-  const int i = g.ng - 1 + blockIdx.x * kBX + threadIdx.x % kBX;
-  const int j = g.ng - 1 + blockIdx.y * kBY + threadIdx.x / kBX;
+__device__ __forceinline__ void recon_cell(const Grid& g, const Fields<T>& V,
+                                           const T* __restrict__ b, const Rev<T>& R, size_t c,
+                                           int i, int j, T (&gs)[6], T (&gd)[4], int& ch) {
   const int ie = g.nxt - g.ng, je = g.nyt - g.ng;
-  if (i > ie || j > je) return;
-  const size_t c = g.at(i, j) + member_base(ms);
   T de = T(0), du = T(0), dv = T(0), db = T(0);
-  int ch = 0;
+  ch = 0;
   auto eta = [&](size_t q) { return V.h[q] + b[q]; };
   for (int dir = 0; dir < 2; ++dir) {
+    const int o = dir == 0 ? 0 : 3;
+    gs[o] = gs[o + 1] = gs[o + 2] = T(0);
     const bool in_range = dir == 0 ? (j >= g.ng && j < je) : (i >= g.ng && i < ie);
     if (!in_range) continue;
     const int lo = dir == 0 ? i : j, hi = dir == 0 ? ie : je;
@@ -579,10 +578,9 @@ __global__ void k_recon_adj(Grid g, size_t ms, Fields<T> V, const T* __restrict_
     du += gr[1] + gl[5];
     dv += gr[2] + gl[6];
     db += gr[3] + gl[7];
-    const int o = dir == 0 ? 0 : 3;
-    R.gs[o][c] = T(0.5) * (gr[0] - gl[4]);
-    R.gs[o + 1][c] = T(0.5) * (gr[1] - gl[5]);
-    R.gs[o + 2][c] = T(0.5) * (gr[2] - gl[6]);
+    gs[o] = T(0.5) * (gr[0] - gl[4]);
+    gs[o + 1] = T(0.5) * (gr[1] - gl[5]);
+    gs[o + 2] = T(0.5) * (gr[2] - gl[6]);
     // minmod branches (cell_slope: zero near dry cells)
     const size_t m = c - step, p = c + step;
     if (!(V.h[c] < T(kThin) || V.h[m] < T(kDry) || V.h[p] < T(kDry))) {
@@ -592,62 +590,85 @@ __global__ void k_recon_adj(Grid g, size_t ms, Fields<T> V, const T* __restrict_
       ch |= (c0 | (c1 << 2) | (c2 << 4)) << (dir * 6);
     }
   }
-  R.gd[0][c] = de;
-  R.gd[1][c] = du;
-  R.gd[2][c] = dv;
-  R.gd[3][c] = db;
-  R.ch[c] = ch;
+  gd[0] = de;
+  gd[1] = du;
+  gd[2] = dv;
+  gd[3] = db;
 }
 
-// Slope gather: every cell collects the slope adjoints of itself and its
-// neighbours (minmod branch a = q_c - q_{c-1}, b = q_{c+1} - q_c), plus the
-// direct reconstruction and cell-update adjoints.  gV receives the adjoint of
-// the stage input (all cells, ghosts included); gb accumulates the bed's.
-// frozen: the limited slopes are held constant (their adjoints are dropped),
-// the derivative of the step with the slopes of the current state frozen.
+// Reconstruction adjoint and slope gather in one launch.  Block (bx, by)
+// gathers the kBX x kBY cells from (ng-2 + bx kBX, ng-2 + by kBY): every cell
+// collects the slope adjoints of itself and its neighbours (minmod branch a =
+// q_c - q_{c-1}, b = q_{c+1} - q_c), plus the direct reconstruction and
+// cell-update adjoints.  The reconstruction adjoints of the block's cells and
+// a one-cell ring around them are computed first into shared memory (the
+// ring's recomputed by both neighbouring blocks, the same bits).  gV receives
+// the adjoint of the stage input (all cells, ghosts included); gb
+// accumulates the bed's.  frozen: the limited slopes are held constant (their
+// adjoints are dropped), the derivative of the step with the slopes of the
+// current state frozen.
+constexpr int kRW = kBX + 2, kRH = kBY + 2, kRN = kRW * kRH;
+
 template <typename T>
-__global__ void k_gather_adj(Grid g, size_t ms, Rev<T> R, Fields<T> gV, T* __restrict__ gb,
-                             int frozen, Fields<T> gadd) {
-  const int i = g.ng - 2 + blockIdx.x * kBX + threadIdx.x % kBX;
-  const int j = g.ng - 2 + blockIdx.y * kBY + threadIdx.x / kBX;
-  if (i > g.nxt - g.ng + 1 || j > g.nyt - g.ng + 1) return;
+__global__ void __launch_bounds__(kBX * kBY)
+    k_recon_gather_adj(Grid g, size_t ms, Fields<T> V, const T* __restrict__ b, Rev<T> R,
+                       Fields<T> gV, T* __restrict__ gb, int frozen, Fields<T> gadd) {
+  __shared__ T s_gs[6][kRN];
+  __shared__ T s_gd[4][kRN];
+  __shared__ int s_ch[kRN];
   const int ie = g.nxt - g.ng, je = g.nyt - g.ng;
   const size_t zb = member_base(ms);
+  const int i0 = g.ng - 2 + (int)blockIdx.x * kBX, j0 = g.ng - 2 + (int)blockIdx.y * kBY;
+  // recon cells: [ng-1, ie] x [ng-1, je]
+  auto rc = [&](int ii, int jj) { return in_box(ii, jj, g.ng - 1, ie, g.ng - 1, je); };
+  for (int k = threadIdx.x; k < kRN; k += kBX * kBY) {
+    const int ii = i0 - 1 + k % kRW, jj = j0 - 1 + k / kRW;
+    T gs[6] = {0, 0, 0, 0, 0, 0}, gd[4] = {0, 0, 0, 0};
+    int ch = 0;
+    if (rc(ii, jj)) recon_cell(g, V, b, R, g.at(ii, jj) + zb, ii, jj, gs, gd, ch);
+    for (int q = 0; q < 6; ++q) s_gs[q][k] = gs[q];
+    for (int q = 0; q < 4; ++q) s_gd[q][k] = gd[q];
+    s_ch[k] = ch;
+  }
+  __syncthreads();
+
+  const int tx = threadIdx.x % kBX, ty = threadIdx.x / kBX;
+  const int i = i0 + tx, j = j0 + ty;
+  if (i > ie + 1 || j > je + 1) return;
   const size_t c = g.at(i, j) + zb;
+  const int t = (ty + 1) * kRW + (tx + 1);  // this cell in the shared arrays
   // slope ranges: x-slopes on [ng-1, ie] x [ng, je-1], y-slopes on [ng, ie-1] x [ng-1, je]
   auto xs = [&](int ii, int jj) { return in_box(ii, jj, g.ng - 1, ie, g.ng, je - 1); };
   auto ys = [&](int ii, int jj) { return in_box(ii, jj, g.ng, ie - 1, g.ng - 1, je); };
-  auto rc = [&](int ii, int jj) { return in_box(ii, jj, g.ng - 1, ie, g.ng - 1, je); };
   T acc[3] = {T(0), T(0), T(0)};
   for (int dir = 0; dir < 2 && !frozen; ++dir) {
     const int di = dir == 0 ? 1 : 0, dj = dir == 0 ? 0 : 1;
+    const int dt = dir == 0 ? 1 : kRW;
     auto has = [&](int ii, int jj) { return dir == 0 ? xs(ii, jj) : ys(ii, jj); };
     for (int v = 0; v < 3; ++v) {
       const int o = dir * 3 + v;
       const int sh = dir * 6 + 2 * v;
       T s = T(0);
       if (has(i, j)) {
-        const int chc = (R.ch[c] >> sh) & 3;
-        if (chc == 1) s += R.gs[o][c];
-        else if (chc == 2) s -= R.gs[o][c];
+        const int chc = (s_ch[t] >> sh) & 3;
+        if (chc == 1) s += s_gs[o][t];
+        else if (chc == 2) s -= s_gs[o][t];
       }
       if (has(i + di, j + dj)) {  // neighbour above chose a = q_{c+1} - q_c
-        const size_t p = g.at(i + di, j + dj) + zb;
-        if (((R.ch[p] >> sh) & 3) == 1) s -= R.gs[o][p];
+        if (((s_ch[t + dt] >> sh) & 3) == 1) s -= s_gs[o][t + dt];
       }
       if (has(i - di, j - dj)) {  // neighbour below chose b = q_c - q_{c-1}
-        const size_t m = g.at(i - di, j - dj) + zb;
-        if (((R.ch[m] >> sh) & 3) == 2) s += R.gs[o][m];
+        if (((s_ch[t - dt] >> sh) & 3) == 2) s += s_gs[o][t - dt];
       }
       acc[v] += s;
     }
   }
   T ge = acc[0], gu = acc[1], gv = acc[2], gbb = T(0);
   if (rc(i, j)) {
-    ge += R.gd[0][c];
-    gu += R.gd[1][c];
-    gv += R.gd[2][c];
-    gbb += R.gd[3][c];
+    ge += s_gd[0][t];
+    gu += s_gd[1][t];
+    gv += s_gd[2][t];
+    gbb += s_gd[3][t];
   }
   T gh = ge;  // eta = h + b
   gbb += ge;
@@ -801,9 +822,8 @@ class Adjoint final : public AdjointBase {
     if (cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking) != cudaSuccess) return -1;
     const size_t f = ms_ * (size_t)nm;  // elements of one batched field
     // fields: b, n; U, Us, lam, lam*, gbase, gV (3 each); gb, gn; tapes
-    // (2 x 21); reverse scratch (3+3+8+8+6+4) + branch bits; checkpoints;
-    // segment states
-    nfields_ = 2 + 6 * 3 + 2 + 2 * 21 + (3 + 3 + 8 + 8 + 6 + 4) + 1 + 3 * (size_t)nck_ +
+    // (2 x 21); reverse scratch (3+3+8+8); checkpoints; segment states
+    nfields_ = 2 + 6 * 3 + 2 + 2 * 21 + (3 + 3 + 8 + 8) + 3 * (size_t)nck_ +
                3 * (size_t)(K_ + 1);
     const size_t fbytes = (f * sizeof(T) + 255) / 256 * 256;
     const size_t nres = (size_t)nsteps * nm * ngauge;
@@ -838,9 +858,6 @@ class Adjoint final : public AdjointBase {
     for (auto& x : R_.ga) x = take();
     for (auto& x : R_.gfx) x = take();
     for (auto& x : R_.gfy) x = take();
-    for (auto& x : R_.gs) x = take();
-    for (auto& x : R_.gd) x = take();
-    R_.ch = (int*)take();  // sizeof(int) <= sizeof(T)
     ck_.resize(nck_);
     for (auto& c : ck_) c = takeset();
     seg_.resize(K_ + 1);
@@ -1212,7 +1229,7 @@ class Adjoint final : public AdjointBase {
   // gV_ (adjoint of the stage input after the wall fold), gbase_ (stage 2).
   int stage_adj(Fields<T> V, Fields<T> base, Tape<T>& Tp, int k, int stage, Fields<T> gout) {
     const int ie = g_.nxt - g_.ng, je = g_.nyt - g_.ng;
-    if (g_.ng > 2) {  // k_gather_adj writes layers ng-2 .. nxt-ng+1: all of them when ng = 2
+    if (g_.ng > 2) {  // the gather writes layers ng-2 .. nxt-ng+1: all of them when ng = 2
       const size_t fb = ms_ * nm_ * sizeof(T);
       ADJ_TRY(cudaMemsetAsync(gV_.h, 0, fb, stream_));
       ADJ_TRY(cudaMemsetAsync(gV_.hu, 0, fb, stream_));
@@ -1230,10 +1247,9 @@ class Adjoint final : public AdjointBase {
     else
       k_faces_adj<T, false><<<blocks(g_.ng, ie, g_.ng, je), kBX * kBY, 0, stream_>>>(g_, ms_, V,
                                                                                      b_, Tp, R_);
-    k_recon_adj<T><<<blocks(g_.ng - 1, ie, g_.ng - 1, je), kBX * kBY, 0, stream_>>>(g_, ms_, V, b_,
-                                                                                   R_);
-    k_gather_adj<T><<<blocks(g_.ng - 2, ie + 1, g_.ng - 2, je + 1), kBX * kBY, 0, stream_>>>(
-        g_, ms_, R_, gV_, gb_, frozen_ ? 1 : 0, stage == 1 ? gbase_ : Fields<T>{});
+    k_recon_gather_adj<T><<<blocks(g_.ng - 2, ie + 1, g_.ng - 2, je + 1), kBX * kBY, 0,
+                            stream_>>>(g_, ms_, V, b_, R_, gV_, gb_, frozen_ ? 1 : 0,
+                                       stage == 1 ? gbase_ : Fields<T>{});
     walls_adj(V, false);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
   }
