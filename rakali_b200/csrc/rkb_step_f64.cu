@@ -349,7 +349,9 @@ __device__ __forceinline__ void stage_body(const Grid& g, StepCtl* ctl, const Ph
       }
     }
   }
-  __syncthreads();
+  // The TMA-staged kernel's threads each waited for the tile copies, so only
+  // the Coriolis terms written by thread 0 (full physics) need this barrier.
+  if (!TMA || !PLAIN) __syncthreads();
 
   auto te = [&](int q) { return th[q] + tb[q]; };  // the surface eta = h + b
   // limited slope (eta, hu, hv) of tile cell q along the direction whose
