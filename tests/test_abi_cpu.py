@@ -121,6 +121,12 @@ def test_bad_handles_rejected(lib):
     nx, ny = ctypes.c_int(7), ctypes.c_int(7)
     assert lib.rki_get_h_ptr(bogus, ctypes.byref(ptr), ctypes.byref(nx), ctypes.byref(ny)) == -100
     assert ptr.value is None and nx.value == 0 and ny.value == 0
+    # simulation and batch handles are looked up in registries, never dereferenced
+    assert lib.rkb_tma_tile_status(h) == -100
+    assert lib.rkb_tma_tile_status(bogus) == -100
+    assert lib.rkb_batch_set_variant(h, 10, 0) == -100
+    assert lib.rkb_batch_set_variant(bogus, 10, 0) == -100
+    assert lib.rkb_adjoint_set_state_budget(h, 0) == -2
 
 
 def _validate(text):
